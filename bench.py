@@ -1,0 +1,423 @@
+#!/usr/bin/env python
+"""Benchmark of the KPM (Chebyshev) LDOS path on B200.
+
+Workload (default): the 2048x2048 periodic square lattice with spin
+(N = 8,388,608, nnz = 41,943,040), t=1, J=0.5, Anderson disorder U[-1, 1],
+scaleFactor 12, 4096 Chebyshev moments, broadening 1e-3, 2000 energies on the
+open grid (-12, 12), LDOS at 64 seeded sites per rank.
+
+One step = the LDOS of the rank's 64 sites: the batched mixed-precision
+recursion (complex64 vectors [N][64], FP64 arithmetic and moments), FP64
+damping and the FP64 energy sum through the lookup table, with the result
+copied to the host.  ``value`` is LDOS solves/s over all ranks (sites per
+step x steps x ranks / max over ranks of the device time).  Beside it the
+line carries the plain FP64 single-vector path (one site per recursion,
+complex128, bit-exact with the reference) on the same sites and matrix,
+the LDOS error of the mixed result against that FP64 result, the roofline
+of the recursion step, and the CPU baseline.
+
+Inputs are larger than L2 (13.8 GB of matrix and vectors per recursion step
+against 126 MB of L2), so no flush is needed between steps.
+
+    python bench.py [--steps K] [--warmup W] [--impl ours|reference]
+    torchrun --nproc-per-node N bench.py --gpus N   (weak scaling: 64 sites per rank)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--sites", type=int, default=64)
+    ap.add_argument("--lattice", type=int, default=2048, help="lattice side L (L x L x 2 states)")
+    ap.add_argument("--moments", type=int, default=4096)
+    ap.add_argument("--plain-sites", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peak_hbm():
+    try:
+        d = json.loads(PEAKS.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_problem(args, rank):
+    from tbtk_b200 import workloads
+    p = workloads.cfg2(n_sites=args.sites, L=args.lattice, seed=2048)
+    # weak scaling: every rank solves its own seeded sites on the same model
+    p.sites = workloads.sample_sites(args.lattice * args.lattice, 2, args.sites, 2049 + 7919 * rank)
+    p.M = args.moments
+    return p
+
+
+def step_bytes(p, B, s_vec):
+    """Algorithmic bytes of one recursion step: the CSR matrix once (values,
+    column indices, row pointers) and three vector passes per source
+    (gather of j_n counted once, read of j_{n-1}, write of j_{n+1})."""
+    return p.nnz * (16 + 4) + 4 * (p.N + 1) + 3 * p.N * B * s_vec
+
+
+# ------------------------------------------------------------------ CPU baselines
+
+def cpu_port_baseline(p, threads, sample_steps=(4, 12)):
+    """The oracle restatement (bit-identical to the reference's CPU
+    recursion), one site per thread, timed at two truncated coefficient
+    counts; per-site time extrapolated linearly to the full M."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle_lib import Oracle
+    o = Oracle()
+    sites = [int(x) for x in p.sites[:threads]]
+
+    def run(M):
+        ts = [0.0] * len(sites)
+
+        def work(i):
+            t0 = time.perf_counter()
+            o.moments(p.rowptr, p.col, p.val, p.scale, M, sites[i], [sites[i]])
+            ts[i] = time.perf_counter() - t0
+
+        th = [threading.Thread(target=work, args=(i,)) for i in range(len(sites))]
+        t0 = time.perf_counter()
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        return time.perf_counter() - t0
+
+    t_lo = run(sample_steps[0])
+    t_hi = run(sample_steps[1])
+    per_step = max(t_hi - t_lo, 1e-9) / (sample_steps[1] - sample_steps[0])
+    fixed = max(t_lo - per_step * sample_steps[0], 0.0)
+    t_site = fixed + per_step * p.M
+    return {"value": len(sites) / t_site, "unit": "LDOS solves/s", "cores": len(sites),
+            "kind": "port",
+            "sample": (f"{len(sites)} sites in parallel (one thread each) at M="
+                       f"{sample_steps[0]} and M={sample_steps[1]} of the same matrix; "
+                       f"per-site time {fixed:.2f} s + {per_step:.3f} s/step extrapolated to "
+                       f"M={p.M} (energy sum excluded)")}
+
+
+def reference_arm(args, world, rank):
+    """The TBTK reference compiled from its sources (oracle/_ref): Model
+    construction once, then per step P threads each running
+    PropertyExtractor::ChebyshevExpander::calculateLDOS for one site with a
+    truncated coefficient count; the per-site time is fitted linearly in M
+    over the warm-up (small M) and timed (larger M) samples and extrapolated
+    to the full M."""
+    if rank != 0:
+        return None
+    sys.path.insert(0, str(ROOT / "oracle"))
+    from oracle_lib import Reference
+    from tbtk_b200 import lattice as L
+    from tbtk_b200 import workloads
+    if not Reference.available():
+        return {"impl": "reference", "unavailable": "oracle/_ref/libtbtkref.so was not built "
+                "(the TBTK reference sources were absent at build time)"}
+    ref = Reference()
+    import psutil
+    avail_gb = psutil.virtual_memory().available / 1e9
+    lat = L.square(args.lattice, args.lattice, t=1.0, J=0.5, W=2.0, periodic=True, seed=2048)
+    t0 = time.perf_counter()
+    model = ref.model(lat)
+    build_s = time.perf_counter() - t0
+    del lat
+    N = args.lattice * args.lattice * 2
+    per_thread_gb = 5e-7 * N  # getSparseMatrix transient, measured at 512^2 and scaled
+    threads = int(max(1, min(os.cpu_count() or 1, 32,
+                             (psutil.virtual_memory().available / 1e9 - 4) // max(per_thread_gb, 0.1))))
+    sites = workloads.sample_sites(args.lattice * args.lattice, 2, threads, 2049)
+    s, E = 12.0, 2000
+    dx = 2 * s / (E + 1)
+    lo, hi = -s + dx, -s + dx + (E - 1) * dx
+
+    def sample(M):
+        def work(i):
+            x, y = divmod(int(sites[i]) // 2, args.lattice)
+            model.ldos(s, M, 1e-3, lo, hi, E, [[x, y, 0]])
+        th = [threading.Thread(target=work, args=(i,)) for i in range(threads)]
+        t0 = time.perf_counter()
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        return time.perf_counter() - t0
+
+    m_lo, m_hi = 4, 16
+    lo_t = [sample(m_lo) for _ in range(max(1, args.warmup))]
+    hi_t = [sample(m_hi) for _ in range(max(1, args.steps))]
+    t_lo, t_hi = statistics.median(lo_t), statistics.median(hi_t)
+    per_step = max(t_hi - t_lo, 1e-9) / (m_hi - m_lo)
+    fixed = max(t_lo - per_step * m_lo, 0.0)
+    t_site = fixed + per_step * args.moments
+    value = threads / t_site
+    return {
+        "impl": "reference", "metric": "LDOS solves/s", "value": value, "unit": "LDOS solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": t_site * 1e3 / threads, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "complex128", "data": "synthetic (seeded lattice)",
+        "config": {"workload": f"square {args.lattice}x{args.lattice} spin periodic, W=2, s=12, "
+                               f"M={args.moments}, E=2000, LDOS per site",
+                   "model_build_s": round(build_s, 1)},
+        "cpu_baseline": {"value": value, "unit": "LDOS solves/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": (f"TBTK PropertyExtractor::calculateLDOS on {threads} threads "
+                                    f"(one site each) at M={m_lo} ({len(lo_t)}x) and M={m_hi} "
+                                    f"({len(hi_t)}x); per-site {fixed:.2f} s + {per_step:.3f} s/step "
+                                    f"extrapolated to M={args.moments}")},
+        "e2e": {"value": value, "unit": "LDOS solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+# ------------------------------------------------------------------ our arm
+
+def ours(args, world, rank, local):
+    import torch
+    from tbtk_b200 import kpm
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    p = make_problem(args, rank)
+    B = p.sites.size
+    stream = torch.cuda.Stream()
+    mat = kpm.Matrix.from_csr(p.rowptr, p.col, p.val, p.scale)
+    tab = kpm.Table.create(p.M, p.energies, p.scale)
+    mat.set_stream(stream.cuda_stream)
+    mat.set_profiling(True)
+
+    def step(prec, sites):
+        return mat.ldos_sites(tab, sites, p.broadening, prec)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step(kpm.MIXED, p.sites)
+        mat.profile()
+        clocks = Clocks(local)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clocks.start()
+        launches0 = kpm.kernel_launches()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        results = None
+        for _ in range(args.steps):
+            results, _ = step(kpm.MIXED, p.sites)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        launches = kpm.kernel_launches() - launches0
+        ck = clocks.stop()
+        total_ms = ev0.elapsed_time(ev1)
+        rec_ms, energy_ms, rec_launches = mat.profile()
+
+        # plain FP64 single-vector path on the first sites: timing + FP64 LDOS
+        plain = []
+        ref_ldos = []
+        step(kpm.FP64, p.sites[:1])  # warm
+        for i in range(args.plain_sites):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            out, _ = step(kpm.FP64, p.sites[i:i + 1])
+            e1.record(stream)
+            torch.cuda.synchronize()
+            plain.append(e0.elapsed_time(e1))
+            ref_ldos.append(out[0])
+        mat.profile()
+    errs = [float(np.abs(results[i] - ref_ldos[i]).max() / np.abs(ref_ldos[i]).max())
+            for i in range(args.plain_sites)]
+
+    # end to end through the C ABI from pinned host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy()
+               for k, v in (("rowptr", p.rowptr), ("col", p.col),
+                            ("val", p.val.view(np.float64)), ("sites", p.sites),
+                            ("energies", p.energies))}
+        val = pin["val"].view(np.complex128)
+
+        def e2e_step():
+            m2 = kpm.Matrix.from_csr(pin["rowptr"], pin["col"], val, p.scale)
+            t2 = kpm.Table.create(p.M, pin["energies"], p.scale)
+            out, _ = m2.ldos_sites(t2, pin["sites"], p.broadening, kpm.MIXED)
+            m2.close()
+            t2.close()
+            return out
+
+        e2e_step()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        h2d = (p.rowptr.nbytes + p.col.nbytes + p.val.nbytes + p.sites.nbytes
+               + p.energies.nbytes)
+        e2e = {"seconds": e2e_s, "h2d": h2d, "d2h": B * p.energies.size * 8}
+
+    # max over ranks
+    times = torch.tensor([total_ms, e2e["seconds"] if e2e else 0.0], dtype=torch.float64,
+                         device="cuda")
+    if dist:
+        dist.all_reduce(times, op=dist.ReduceOp.MAX)
+    total_ms, e2e_max = times.tolist()
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return None
+
+    solves = B * args.steps * world
+    value = solves / (total_ms / 1e3)
+    avg_step_ms = rec_ms / max(rec_launches, 1)
+    bstep = step_bytes(p, B, 8)
+    achieved = bstep / (avg_step_ms / 1e3) / 1e9
+    peak, peak_kind = peak_hbm()
+    plain_ms = statistics.median(plain) if plain else None
+    plain_rate = 1e3 / plain_ms if plain_ms else None
+    out = {
+        "metric": "LDOS solves/s", "value": value, "unit": "LDOS solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64 vectors / f64 arithmetic+moments",
+        "data": "synthetic (seeded lattice, Anderson disorder)",
+        "config": {"workload": (f"square {args.lattice}x{args.lattice} spin periodic (N={p.N}, "
+                                f"nnz={p.nnz}), t=1 J=0.5 W=2, s=12, M={p.M}, broadening 1e-3, "
+                                f"E={p.energies.size} open grid, {B} LDOS sites per rank as one "
+                                f"batched mixed-precision recursion"),
+                   "sites_per_step_per_rank": B, "l2": "inputs larger than L2 (no flush)",
+                   "parallelism": f"replicas x{world} (sites sharded, no collective)"},
+        "gpu_launches": int(launches),
+        "plain_fp64": {"value": plain_rate, "unit": "LDOS solves/s", "ms_per_solve": plain_ms,
+                       "sites": args.plain_sites},
+        "speedup_vs_plain_fp64": (value / world) / plain_rate if plain_rate else None,
+        "ldos_rel_err_vs_fp64": max(errs) if errs else None,
+        "latency_ms": {"p50": statistics.median([total_ms / args.steps]),
+                       "p99": total_ms / args.steps,
+                       "note": "per 64-site batch; request-level latency is in the serving bench"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel": "kpm_step<float2,32,2> (recursion step, B=64)",
+                     "bytes_per_launch": bstep, "avg_launch_ms": avg_step_ms,
+                     "peak_kind": f"{peak_kind} (copy bandwidth)"},
+        "recursion_share": rec_ms / total_ms if total_ms else None,
+        "clocks": ck,
+    }
+    if e2e:
+        out["e2e"] = {"value": solves / e2e_max * args.e2e_steps / args.steps,
+                      "unit": "LDOS solves/s", "h2d_bytes_per_step": e2e["h2d"],
+                      "d2h_bytes_per_step": e2e["d2h"], "steps": args.e2e_steps,
+                      "includes": "CSR upload + device table + recursion + LDOS + download"}
+    if world == 1 and not args.no_cpu:
+        threads = int(min(os.cpu_count() or 1, 16, B))
+        out["cpu_baseline"] = cpu_port_baseline(p, threads)
+    if dist:
+        dist.destroy_process_group()
+    return out
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init()
+    if args.impl == "reference":
+        res = reference_arm(args, world, rank)
+    else:
+        res = ours(args, world, rank, local)
+    if res is not None and rank == 0:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,200 @@
+/* tbtkkpm — the kernel-polynomial (Chebyshev) path of TBTK on NVIDIA B200.
+ *
+ * A C ABI over hand-written sm_100a kernels.  It replaces the device side
+ * of TBTK's Solver::ChebyshevExpander (Lib/src/cuda/ChebyshevSolver.cu) and
+ * the per-site loop of PropertyExtractor::ChebyshevExpander::calculateLDOS.
+ * Plain pointers and sizes only; complex numbers are interleaved
+ * (re, im) doubles; every index is a TBTK basis number (the caller maps
+ * Index -> basis with HoppingAmplitudeSet::getBasisIndex).
+ *
+ * Errors: every entry point returns TBTKKPM_OK (0) or a negative status and
+ * never exits the process; tbtkkpm_last_error() gives the message of the
+ * calling thread's last failure.  (The reference reports errors through
+ * TBTKAssert/TBTKExit, Lib/include/Utilities/TBTK/TBTKMacros.h:55-94, which
+ * print and exit(1); a TBTK-side caller turns a non-zero status back into
+ * TBTKExit.)
+ *
+ * Threads: calls on distinct handles may run concurrently; each handle owns
+ * one CUDA stream on the device that was current when it was created.  Calls
+ * that return host results synchronise that stream before returning.
+ */
+#ifndef TBTKKPM_H
+#define TBTKKPM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define TBTKKPM_API __attribute__((visibility("default")))
+#else
+#define TBTKKPM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status */
+
+#define TBTKKPM_OK 0
+#define TBTKKPM_ERR_ARGUMENT -1   /* an argument is out of range */
+#define TBTKKPM_ERR_CUDA -2       /* a CUDA call failed */
+#define TBTKKPM_ERR_MEMORY -3     /* device memory or HBM budget exhausted */
+#define TBTKKPM_ERR_TIMEOUT -4    /* a bounded device wait ran out */
+#define TBTKKPM_ERR_UNSUPPORTED -5/* combination not available */
+#define TBTKKPM_ERR_STATE -6      /* handle in the wrong state */
+
+/* Message of the calling thread's last failed call ("" if none). */
+TBTKKPM_API const char *tbtkkpm_last_error(void);
+
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+TBTKKPM_API int tbtkkpm_version(void);
+
+/* Number of CUDA devices (the reference's GPUResourceManager device table,
+ * Lib/src/cuda/GPUResourceManager.cu:28-39). */
+TBTKKPM_API int tbtkkpm_device_count(int *count);
+
+/* Selects the device later handle creations on this thread use. */
+TBTKKPM_API int tbtkkpm_set_device(int device);
+
+/* Number of kernels this process has launched through the library.  (No
+ * reference counterpart: instrumentation for benchmarks.) */
+TBTKKPM_API uint64_t tbtkkpm_kernel_launches(void);
+
+/* ------------------------------------------------------------ types */
+
+/* Green's function type, the order of Solver::ChebyshevExpander::Type
+ * (Lib/include/TBTK/Solver/ChebyshevExpander.h:203-208). */
+#define TBTKKPM_ADVANCED 0
+#define TBTKKPM_RETARDED 1
+#define TBTKKPM_PRINCIPAL 2
+#define TBTKKPM_NONPRINCIPAL 3
+
+/* Recursion precision.
+ * FP64: complex128 vectors, the reference's operation order (moments are
+ *   bit-identical to calculateCoefficientsCPU).
+ * MIXED: complex64 vectors in HBM, FP64 arithmetic in registers, FP64
+ *   moments, damping and energy sums. */
+#define TBTKKPM_FP64 0
+#define TBTKKPM_MIXED 1
+
+typedef struct tbtkkpm_matrix tbtkkpm_matrix;
+typedef struct tbtkkpm_table tbtkkpm_table;
+
+/* ------------------------------------------------------------ matrix */
+
+/* Device copy of H/s from a CSR matrix in TBTK's layout: row = basis(to),
+ * col = basis(from), columns ascending within a row, no duplicates
+ * (HoppingAmplitudeSet::getSparseMatrix() after setStorageFormat(CSR),
+ * Lib/include/Core/TBTK/HoppingAmplitudeSet.h:397-424).  rowptr has N+1
+ * entries.  The values are scaled on the device exactly as
+ * calculateCoefficientsCPU scales them (`*= 1/scaleFactor` then `*= 2`,
+ * Lib/src/Solver/ChebyshevExpander.cpp:147,168) and stored in sliced ELL.
+ * scale must be > 0 (ChebyshevExpander.h:394-403). */
+TBTKKPM_API int tbtkkpm_matrix_create_csr(
+	const uint32_t *rowptr, const uint32_t *col, const double *val,
+	uint32_t N, double scale, tbtkkpm_matrix **out);
+
+/* Same from unsorted (row, col, value) triplets in HoppingAmplitudeSet
+ * iteration order; sorting and duplicate summation run on the device with
+ * the semantics of SparseMatrix::constructCSX (SparseMatrix.h:1375-1551;
+ * duplicates d0, d1, d2 of one entry sum as d0 + (d1 + d2)). */
+TBTKKPM_API int tbtkkpm_matrix_create_triplets(
+	const uint32_t *rows, const uint32_t *cols, const double *vals,
+	uint64_t n, uint32_t N, double scale, tbtkkpm_matrix **out);
+
+TBTKKPM_API int tbtkkpm_matrix_destroy(tbtkkpm_matrix *m);
+
+/* Runs this handle's work on the caller's CUDA stream (a cudaStream_t of
+ * the handle's device) instead of its own; NULL restores its own stream.
+ * (No reference counterpart: the reference uses the default stream.) */
+TBTKKPM_API int tbtkkpm_matrix_set_stream(tbtkkpm_matrix *m, void *cuda_stream);
+
+/* Basis size and stored nonzeros of a matrix. */
+TBTKKPM_API int tbtkkpm_matrix_shape(const tbtkkpm_matrix *m, uint32_t *N, uint64_t *nnz);
+
+/* Downloads the scaled CSR (values 2/s * H, i.e. what the recursion
+ * multiplies by after step 1) for checking; rowptr N+1, col/val nnz. */
+TBTKKPM_API int tbtkkpm_matrix_download_csr(
+	const tbtkkpm_matrix *m, uint32_t *rowptr, uint32_t *col, double *val);
+
+/* Phase timing of the calls on this handle, with CUDA events recorded on
+ * the handle's stream around the recursion and around the energy sums.
+ * tbtkkpm_matrix_profile returns the milliseconds and recursion-step
+ * launches accumulated since the previous read and resets them.  (No
+ * reference counterpart: the reference's Timer::tick/tock,
+ * Lib/include/Utilities/TBTK/Timer.h:75-105, is host wall time.) */
+TBTKKPM_API int tbtkkpm_matrix_set_profiling(tbtkkpm_matrix *m, int enable);
+TBTKKPM_API int tbtkkpm_matrix_profile(
+	tbtkkpm_matrix *m, double *recursion_ms, double *energy_ms,
+	uint64_t *recursion_launches);
+
+/* ------------------------------------------------------------ moments */
+
+/* Chebyshev moments mu[k][n] = <to_k| T_n(H/s) |from>, n = 0..M-1, for K
+ * to-indices, then Lorentz damping sinh(lambda(1-n/M))/sinh(lambda),
+ * lambda = broadening*M (none if broadening == 0).  mu_out is [K][M]
+ * complex.  Replaces Solver::ChebyshevExpander::calculateCoefficientsGPU
+ * (Lib/src/cuda/ChebyshevSolver.cu:74-648) and matches
+ * calculateCoefficientsCPU (Lib/src/Solver/ChebyshevExpander.cpp:103-199)
+ * bit for bit at TBTKKPM_FP64. */
+TBTKKPM_API int tbtkkpm_moments(
+	tbtkkpm_matrix *m, uint32_t from, const uint32_t *to, uint32_t K,
+	uint32_t M, double broadening, double *mu_out);
+
+/* Batched moments: B source vectors (from[b]) advance together as one
+ * SpMM-style recursion.  to[k] belongs to source to_owner[k]; mu_out is
+ * [K][M] complex in the order of to[].  precision is TBTKKPM_FP64 or
+ * TBTKKPM_MIXED.  err_out (may be NULL) receives, per to-index, an
+ * estimate of max_n |mu_n - mu_n(FP64)| / max_n |mu_n| (0 at FP64). */
+TBTKKPM_API int tbtkkpm_moments_batched(
+	tbtkkpm_matrix *m, const uint32_t *from, uint32_t B,
+	const uint32_t *to, const uint32_t *to_owner, uint32_t K, uint32_t M,
+	double broadening, int precision, double *mu_out, double *err_out);
+
+/* ------------------------------------------------------------ energy grid */
+
+/* Lookup table T[n][e] = (1/s)(-2i/sqrt(1-x^2)) exp(-i n acos x)/(1+delta_n0),
+ * x = energies[e]/s, generated on the device (generateLookupTable,
+ * Lib/src/Solver/ChebyshevExpander.cpp:201-270).  The energies must lie in
+ * (-s, s) (ChebyshevExpander.cpp:221-236). */
+TBTKKPM_API int tbtkkpm_table_create(
+	uint32_t M, const double *energies, uint32_t E, double scale,
+	tbtkkpm_table **out);
+
+/* Same from a table computed on the host ([M][E] complex), the layout
+ * loadLookupTableGPU uploads (Lib/src/cuda/ChebyshevSolver.cu:672-760). */
+TBTKKPM_API int tbtkkpm_table_upload(
+	uint32_t M, uint32_t E, const double *table, tbtkkpm_table **out);
+
+TBTKKPM_API int tbtkkpm_table_destroy(tbtkkpm_table *t);
+
+/* Green's functions G[k][e] of one type from K damped coefficient vectors
+ * mu[k][n] (n < M of the table), summed in the reference's order
+ * (generateGreensFunctionCPU with a table, ChebyshevExpander.cpp:324-361;
+ * the reference GPU path only had the Retarded type,
+ * ChebyshevSolver.cu:650-670,811-818).  G_out is [K][E] complex. */
+TBTKKPM_API int tbtkkpm_greens(
+	tbtkkpm_table *t, const double *mu, uint32_t K, int type, double *G_out);
+
+/* LDOS[k][e] = Im(G_NonPrincipal[k][e]) / pi (calculateLDOSCallback,
+ * Lib/src/PropertyExtractor/ChebyshevExpander.cpp:661-684).  [K][E]. */
+TBTKKPM_API int tbtkkpm_ldos(
+	tbtkkpm_table *t, const double *mu, uint32_t K, double *ldos_out);
+
+/* LDOS at B sites in one call: the moments <site|T_n|site> of all sites run
+ * as one batched recursion, are damped and summed over the table's energy
+ * grid on the device; only the [B][E] result crosses to the host.
+ * Replaces the per-site loop of PropertyExtractor::ChebyshevExpander::
+ * calculateLDOS (ChebyshevExpander.cpp:475-505 through
+ * PropertyExtractor.h:849-894).  err_out (may be NULL) is per site as in
+ * tbtkkpm_moments_batched. */
+TBTKKPM_API int tbtkkpm_ldos_sites(
+	tbtkkpm_matrix *m, tbtkkpm_table *t, const uint32_t *sites, uint32_t B,
+	double broadening, int precision, double *ldos_out, double *err_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,236 @@
+"""ctypes access to the two CPU checkers of the KPM path (test infrastructure).
+
+* :class:`Oracle` — the C restatement in oracle/kpm_oracle.c
+  (oracle/_build/libkpm_oracle.so, built by ``make -C oracle``).
+* :class:`Reference` — the TBTK reference classes compiled from the reference
+  sources with oracle/ref_driver.cpp (oracle/_ref/libtbtkref.so, built by
+  ``make -C oracle ref``).  Absent when the reference was never compiled.
+
+Complex arrays cross the boundary as interleaved (re, im) doubles.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import pathlib
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent.parent
+# Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+# this module.
+ORACLE_SO = ROOT / "oracle" / "_build" / "libkpm_oracle.so"
+REF_SO = ROOT / "oracle" / "_ref" / "libtbtkref.so"
+
+_p = ctypes.c_void_p
+_d = ctypes.c_double
+_i = ctypes.c_int
+_i64 = ctypes.c_int64
+_u32 = ctypes.c_uint32
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _cx(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.complex128))
+
+
+class Oracle:
+    def __init__(self, path=ORACLE_SO):
+        self.lib = lib = ctypes.CDLL(str(path))
+        lib.kpm_csr_from_triplets.restype = _i64
+        lib.kpm_csr_from_triplets.argtypes = [_i64, _p, _p, _p, _p, _p, _p, _p]
+        lib.kpm_moments.restype = _i
+        lib.kpm_moments.argtypes = [_u32, _p, _p, _p, _d, _i, _u32, _i, _p, _p]
+        lib.kpm_damp.argtypes = [_i, _i, _d, _p]
+        lib.kpm_lookup_table.argtypes = [_i, _i, _p, _d, _p]
+        lib.kpm_greens_table.argtypes = [_i, _i, _p, _i, _p, _p]
+        lib.kpm_greens_closed.argtypes = [_i, _i, _p, _d, _i, _p, _p]
+        lib.kpm_ldos_table.argtypes = [_i, _i, _p, _p, _p]
+        lib.kpm_range.argtypes = [_d, _d, _i, _i, _i, _p]
+
+    def csr_from_triplets(self, rows, cols, vals):
+        rows = np.ascontiguousarray(rows, dtype=np.uint32)
+        cols = np.ascontiguousarray(cols, dtype=np.uint32)
+        vals = _cx(vals)
+        n = rows.size
+        nr = int(rows.max()) + 1 if n else 0
+        rowptr = np.zeros(nr + 1, dtype=np.uint32)
+        col = np.zeros(max(n, 1), dtype=np.uint32)
+        val = np.zeros(max(n, 1), dtype=np.complex128)
+        num_rows = ctypes.c_uint32(0)
+        nnz = self.lib.kpm_csr_from_triplets(
+            n, _ptr(rows), _ptr(cols), _ptr(vals), _ptr(rowptr), _ptr(col),
+            _ptr(val), ctypes.byref(num_rows))
+        return rowptr, col[:nnz].copy(), val[:nnz].copy()
+
+    def moments(self, rowptr, col, val, scale, M, frm, to):
+        rowptr = np.ascontiguousarray(rowptr, dtype=np.uint32)
+        col = np.ascontiguousarray(col, dtype=np.uint32)
+        val = _cx(val)
+        to = np.ascontiguousarray(np.atleast_1d(to), dtype=np.uint32)
+        out = np.zeros((to.size, M), dtype=np.complex128)
+        rc = self.lib.kpm_moments(rowptr.size - 1, _ptr(rowptr), _ptr(col),
+                                  _ptr(val), scale, M, int(frm), to.size,
+                                  _ptr(to), _ptr(out))
+        if rc != 0:
+            raise ValueError("kpm_moments rejected its arguments")
+        return out
+
+    def damp(self, mu, broadening):
+        mu = _cx(mu).copy()
+        K, M = mu.shape
+        self.lib.kpm_damp(K, M, broadening, _ptr(mu))
+        return mu
+
+    def lookup_table(self, M, energies, scale):
+        energies = np.ascontiguousarray(energies, dtype=np.float64)
+        table = np.zeros((M, energies.size), dtype=np.complex128)
+        self.lib.kpm_lookup_table(M, energies.size, _ptr(energies), scale,
+                                  _ptr(table))
+        return table
+
+    def greens_table(self, table, type_, coeff):
+        coeff = _cx(coeff)
+        M, E = table.shape
+        out = np.zeros(E, dtype=np.complex128)
+        self.lib.kpm_greens_table(M, E, _ptr(np.ascontiguousarray(table)),
+                                  type_, _ptr(coeff), _ptr(out))
+        return out
+
+    def greens_closed(self, energies, scale, type_, coeff):
+        coeff = _cx(coeff)
+        energies = np.ascontiguousarray(energies, dtype=np.float64)
+        out = np.zeros(energies.size, dtype=np.complex128)
+        self.lib.kpm_greens_closed(coeff.size, energies.size, _ptr(energies),
+                                   scale, type_, _ptr(coeff), _ptr(out))
+        return out
+
+    def ldos_table(self, table, coeff):
+        coeff = _cx(coeff)
+        M, E = table.shape
+        out = np.zeros(E, dtype=np.float64)
+        self.lib.kpm_ldos_table(M, E, _ptr(np.ascontiguousarray(table)),
+                                _ptr(coeff), _ptr(out))
+        return out
+
+    def range(self, lower, upper, res, incl_lo=True, incl_hi=True):
+        out = np.zeros(res, dtype=np.float64)
+        self.lib.kpm_range(lower, upper, res, int(incl_lo), int(incl_hi),
+                           _ptr(out))
+        return out
+
+
+class Reference:
+    """The compiled TBTK reference, driven through its public classes."""
+
+    def __init__(self, path=REF_SO):
+        self.lib = lib = ctypes.CDLL(str(path))
+        lib.ref_model_create.restype = _p
+        lib.ref_model_create.argtypes = [_i64, _i, _p, _p, _p]
+        lib.ref_model_destroy.argtypes = [_p]
+        lib.ref_model_basis_size.restype = _i
+        lib.ref_model_basis_size.argtypes = [_p]
+        lib.ref_model_basis_index.restype = _i
+        lib.ref_model_basis_index.argtypes = [_p, _p, _i]
+        lib.ref_model_csr.restype = _i64
+        lib.ref_model_csr.argtypes = [_p, _p, _p, _p, _i64, _p]
+        lib.ref_coefficients.restype = _i
+        lib.ref_coefficients.argtypes = [_p, _d, _i, _d, _i, _i, _p, _p, _p]
+        lib.ref_range_value.restype = _d
+        lib.ref_range_value.argtypes = [_d, _d, _i, _i, _i, _i]
+        lib.ref_greens.restype = _i
+        lib.ref_greens.argtypes = [_d, _i, _d, _d, _i, _i, _i, _i, _i, _p, _p]
+        lib.ref_ldos.restype = _i
+        lib.ref_ldos.argtypes = [_p, _d, _i, _d, _d, _d, _i, _i, _i, _i, _p, _p]
+        lib.ref_greens_pe.restype = _i
+        lib.ref_greens_pe.argtypes = [_p, _d, _i, _d, _d, _d, _i, _i, _i, _i,
+                                      _i, _p, _p, _p]
+
+    @staticmethod
+    def available(path=REF_SO) -> bool:
+        return os.path.exists(path)
+
+    def model(self, lat):
+        return RefModel(self, lat)
+
+    def range_value(self, lower, upper, res, incl_lo, incl_hi, k):
+        return self.lib.ref_range_value(lower, upper, res, int(incl_lo),
+                                        int(incl_hi), k)
+
+    def greens(self, scale, coeff, lower, upper, res, type_, use_table,
+               incl_lo=True, incl_hi=True):
+        coeff = _cx(coeff)
+        out = np.zeros(res, dtype=np.complex128)
+        self.lib.ref_greens(scale, coeff.size, lower, upper, res, int(incl_lo),
+                            int(incl_hi), int(use_table), type_, _ptr(coeff),
+                            _ptr(out))
+        return out
+
+
+class RefModel:
+    """A TBTK Model built from a :class:`tbtk_b200.lattice.Lattice`."""
+
+    def __init__(self, ref, lat):
+        self.ref = ref
+        self.lat = lat
+        amp = np.ascontiguousarray(lat.amp.view(np.float64))
+        self.h = ref.lib.ref_model_create(
+            lat.amp.size, lat.idx_len, _ptr(lat.to_index),
+            _ptr(lat.from_index), _ptr(amp))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.ref.lib.ref_model_destroy(self.h)
+            self.h = None
+
+    def _idx(self, idx):
+        return np.ascontiguousarray(np.asarray(idx, dtype=np.int32).reshape(-1, self.lat.idx_len))
+
+    def basis_size(self):
+        return self.ref.lib.ref_model_basis_size(self.h)
+
+    def basis_index(self, idx):
+        a = self._idx(idx)
+        return self.ref.lib.ref_model_basis_index(self.h, _ptr(a), a.shape[1])
+
+    def csr(self):
+        cap = self.lat.amp.size
+        rowptr = np.zeros(self.lat.num_states + 1, dtype=np.uint32)
+        col = np.zeros(cap, dtype=np.uint32)
+        val = np.zeros(cap, dtype=np.complex128)
+        nr = ctypes.c_int(0)
+        nnz = self.ref.lib.ref_model_csr(self.h, _ptr(rowptr), _ptr(col),
+                                         _ptr(val), cap, ctypes.byref(nr))
+        assert nnz >= 0
+        return rowptr[: nr.value + 1].copy(), col[:nnz].copy(), val[:nnz].copy()
+
+    def coefficients(self, scale, M, broadening, to, frm):
+        to = self._idx(to)
+        frm = self._idx(frm)
+        out = np.zeros((to.shape[0], M), dtype=np.complex128)
+        self.ref.lib.ref_coefficients(self.h, scale, M, broadening,
+                                      to.shape[0], to.shape[1], _ptr(to),
+                                      _ptr(frm), _ptr(out))
+        return out
+
+    def ldos(self, scale, M, broadening, lower, upper, res, sites,
+             use_table=True):
+        sites = self._idx(sites)
+        out = np.zeros((sites.shape[0], res), dtype=np.float64)
+        self.ref.lib.ref_ldos(self.h, scale, M, broadening, lower, upper, res,
+                              int(use_table), sites.shape[0], sites.shape[1],
+                              _ptr(sites), _ptr(out))
+        return out
+
+    def greens_pe(self, scale, M, broadening, lower, upper, res, type_, to,
+                  frm, use_table=True):
+        to = self._idx(to)
+        frm = self._idx(frm)
+        out = np.zeros((to.shape[0], res), dtype=np.complex128)
+        self.ref.lib.ref_greens_pe(self.h, scale, M, broadening, lower, upper,
+                                   res, int(use_table), type_, to.shape[0],
+                                   to.shape[1], _ptr(to), _ptr(frm), _ptr(out))
+        return out

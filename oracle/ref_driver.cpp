@@ -1,0 +1,254 @@
+/* Test infrastructure only: a C entry layer over the UNMODIFIED TBTK reference
+ * classes (Model, Solver::ChebyshevExpander, PropertyExtractor::ChebyshevExpander),
+ * compiled against the reference sources by oracle/Makefile into oracle/_ref/.
+ * It is the checker the restatement in kpm_oracle.c is pinned against, and the
+ * CPU baseline the benchmark times.  Nothing in the product links it.
+ *
+ * Reference call sites it drives:
+ *   Model / HoppingAmplitude input      Lib/include/Core/TBTK/Model.h:430-466
+ *   HoppingAmplitudeSet::getSparseMatrix Lib/include/Core/TBTK/HoppingAmplitudeSet.h:397-424
+ *   Solver::ChebyshevExpander           Lib/src/Solver/ChebyshevExpander.cpp:103-435
+ *   PropertyExtractor::calculateLDOS    Lib/src/PropertyExtractor/ChebyshevExpander.cpp:475-505
+ */
+#include "TBTK/Model.h"
+#include "TBTK/PropertyExtractor/ChebyshevExpander.h"
+#include "TBTK/Range.h"
+#include "TBTK/Solver/ChebyshevExpander.h"
+#include "TBTK/Streams.h"
+
+#include <complex>
+#include <cstdint>
+#include <vector>
+
+using namespace TBTK;
+using cplx = std::complex<double>;
+
+namespace {
+
+Index make_index(const int *p, int len){
+	Index idx;
+	for(int k = 0; k < len; k++)
+		idx.pushBack(p[k]);
+	return idx;
+}
+
+Solver::ChebyshevExpander::Type to_type(int type){
+	switch(type){
+	case 0: return Solver::ChebyshevExpander::Type::Advanced;
+	case 1: return Solver::ChebyshevExpander::Type::Retarded;
+	case 2: return Solver::ChebyshevExpander::Type::Principal;
+	default: return Solver::ChebyshevExpander::Type::NonPrincipal;
+	}
+}
+
+struct Quiet{
+	Quiet(){
+		Communicator::setGlobalVerbose(false);
+	}
+} quiet;
+
+} // namespace
+
+extern "C" {
+
+/* Builds and constructs a Model from explicit amplitudes: amplitude k is
+ * amp[2k] + i amp[2k+1], from index from_idx[k*idx_len ...] to index
+ * to_idx[k*idx_len ...].  No Hermitian conjugate is added implicitly. */
+void *ref_model_create(
+	int64_t n_amp, int idx_len, const int *to_idx, const int *from_idx,
+	const double *amp
+){
+	Model *model = new Model();
+	model->setVerbose(false);
+	for(int64_t k = 0; k < n_amp; k++){
+		*model << HoppingAmplitude(
+			cplx(amp[2*k], amp[2*k + 1]),
+			make_index(to_idx + k*idx_len, idx_len),
+			make_index(from_idx + k*idx_len, idx_len)
+		);
+	}
+	model->construct();
+	return model;
+}
+
+void ref_model_destroy(void *model){
+	delete (Model*)model;
+}
+
+int ref_model_basis_size(void *model){
+	return ((Model*)model)->getBasisSize();
+}
+
+int ref_model_basis_index(void *model, const int *idx, int idx_len){
+	return ((Model*)model)->getBasisIndex(make_index(idx, idx_len));
+}
+
+/* CSR of getSparseMatrix() after setStorageFormat(CSR), exactly as
+ * calculateCoefficientsCPU sees it before scaling.  Returns nnz, or -nnz-1
+ * when cap is too small (nothing written then). */
+int64_t ref_model_csr(
+	void *model, uint32_t *rowptr, uint32_t *col, double *val, int64_t cap,
+	int *num_rows
+){
+	const HoppingAmplitudeSet &has
+		= ((Model*)model)->getHoppingAmplitudeSet();
+	SparseMatrix<cplx> sm = has.getSparseMatrix();
+	sm.setStorageFormat(SparseMatrix<cplx>::StorageFormat::CSR);
+	const unsigned int nr = sm.getNumRows();
+	const unsigned int *rp = sm.getCSRRowPointers();
+	const int64_t nnz = rp[nr];
+	*num_rows = (int)nr;
+	if(nnz > cap)
+		return -nnz - 1;
+	const unsigned int *c = sm.getCSRColumns();
+	const cplx *v = sm.getCSRValues();
+	for(unsigned int r = 0; r <= nr; r++)
+		rowptr[r] = rp[r];
+	for(int64_t k = 0; k < nnz; k++){
+		col[k] = c[k];
+		val[2*k] = v[k].real();
+		val[2*k + 1] = v[k].imag();
+	}
+	return nnz;
+}
+
+/* Solver::ChebyshevExpander::calculateCoefficients (CPU) for K to-indices
+ * and one from-index.  out is [K][M][2]. */
+int ref_coefficients(
+	void *model, double scale, int M, double broadening,
+	int K, int idx_len, const int *to, const int *from, double *out
+){
+	Solver::ChebyshevExpander solver;
+	solver.setVerbose(false);
+	solver.setModel(*(Model*)model);
+	solver.setScaleFactor(scale);
+	solver.setNumCoefficients(M);
+	solver.setBroadening(broadening);
+	solver.setCalculateCoefficientsOnGPU(false);
+	std::vector<Index> tos;
+	for(int k = 0; k < K; k++)
+		tos.push_back(make_index(to + k*idx_len, idx_len));
+	std::vector<std::vector<cplx>> c = solver.calculateCoefficients(
+		tos, make_index(from, idx_len)
+	);
+	for(int k = 0; k < K; k++){
+		for(int n = 0; n < M; n++){
+			out[2*((int64_t)k*M + n)] = c[k][n].real();
+			out[2*((int64_t)k*M + n) + 1] = c[k][n].imag();
+		}
+	}
+	return 0;
+}
+
+/* Energy k of Range(lower, upper, res, incl_lo, incl_hi). */
+double ref_range_value(
+	double lower, double upper, int res, int incl_lo, int incl_hi, int k
+){
+	Range r(lower, upper, res, incl_lo != 0, incl_hi != 0);
+	return r[k];
+}
+
+/* Solver::ChebyshevExpander::generateGreensFunction (CPU) for one
+ * coefficient vector of length M.  type: 0 Advanced, 1 Retarded,
+ * 2 Principal, 3 NonPrincipal.  out is [res][2]. */
+int ref_greens(
+	double scale, int M, double lower, double upper, int res, int incl_lo,
+	int incl_hi, int use_table, int type, const double *coeff, double *out
+){
+	Solver::ChebyshevExpander solver;
+	solver.setVerbose(false);
+	solver.setScaleFactor(scale);
+	solver.setNumCoefficients(M);
+	solver.setGenerateGreensFunctionsOnGPU(false);
+	solver.setUseLookupTable(use_table != 0);
+	solver.setEnergyWindow(
+		Range(lower, upper, res, incl_lo != 0, incl_hi != 0)
+	);
+	std::vector<cplx> c(M);
+	for(int n = 0; n < M; n++)
+		c[n] = cplx(coeff[2*n], coeff[2*n + 1]);
+	std::vector<cplx> g = solver.generateGreensFunction(c, to_type(type));
+	for(int e = 0; e < res; e++){
+		out[2*e] = g[e].real();
+		out[2*e + 1] = g[e].imag();
+	}
+	return 0;
+}
+
+/* PropertyExtractor::ChebyshevExpander::calculateLDOS({sites}) with the
+ * PropertyExtractor's inclusive window Range(lower, upper, res).
+ * use_table selects Solver::setUseLookupTable.  out is [n_sites][res]. */
+int ref_ldos(
+	void *model, double scale, int M, double broadening, double lower,
+	double upper, int res, int use_table, int n_sites, int idx_len,
+	const int *sites, double *out
+){
+	Solver::ChebyshevExpander solver;
+	solver.setVerbose(false);
+	solver.setModel(*(Model*)model);
+	solver.setScaleFactor(scale);
+	solver.setNumCoefficients(M);
+	solver.setBroadening(broadening);
+	solver.setUseLookupTable(use_table != 0);
+	PropertyExtractor::ChebyshevExpander pe(solver);
+	pe.setEnergyWindow(lower, upper, res);
+	std::vector<Index> patterns;
+	for(int k = 0; k < n_sites; k++)
+		patterns.push_back(make_index(sites + k*idx_len, idx_len));
+	Property::LDOS ldos = pe.calculateLDOS(patterns);
+	for(int k = 0; k < n_sites; k++){
+		Index site = make_index(sites + k*idx_len, idx_len);
+		for(int e = 0; e < res; e++)
+			out[(int64_t)k*res + e] = ldos(site, e);
+	}
+	return 0;
+}
+
+/* PropertyExtractor::ChebyshevExpander::calculateGreensFunctions(to, from)
+ * with the PropertyExtractor's inclusive window.  out is [K][res][2]. */
+int ref_greens_pe(
+	void *model, double scale, int M, double broadening, double lower,
+	double upper, int res, int use_table, int type, int K, int idx_len,
+	const int *to, const int *from, double *out
+){
+	Solver::ChebyshevExpander solver;
+	solver.setVerbose(false);
+	solver.setModel(*(Model*)model);
+	solver.setScaleFactor(scale);
+	solver.setNumCoefficients(M);
+	solver.setBroadening(broadening);
+	solver.setUseLookupTable(use_table != 0);
+	PropertyExtractor::ChebyshevExpander pe(solver);
+	pe.setEnergyWindow(lower, upper, res);
+	/* calculateGreensFunctions generates G for its to-indices inside an
+	 * OpenMP loop (PropertyExtractor/ChebyshevExpander.cpp:278-292) whose
+	 * first iterations race on the lazy lookup-table build
+	 * (Solver/ChebyshevExpander.h:548-566); one serial call builds the
+	 * table first. */
+	solver.generateGreensFunction(
+		std::vector<cplx>(M, cplx(0, 0)),
+		Solver::ChebyshevExpander::Type::Retarded
+	);
+	std::vector<Index> tos;
+	for(int k = 0; k < K; k++)
+		tos.push_back(make_index(to + k*idx_len, idx_len));
+	Index f = make_index(from, idx_len);
+	Property::GreensFunction::Type t;
+	switch(type){
+	case 0: t = Property::GreensFunction::Type::Advanced; break;
+	case 1: t = Property::GreensFunction::Type::Retarded; break;
+	case 2: t = Property::GreensFunction::Type::Principal; break;
+	default: t = Property::GreensFunction::Type::NonPrincipal; break;
+	}
+	Property::GreensFunction gf = pe.calculateGreensFunctions(tos, f, t);
+	for(int k = 0; k < K; k++){
+		for(int e = 0; e < res; e++){
+			cplx v = gf({tos[k], f}, e);
+			out[2*((int64_t)k*res + e)] = v.real();
+			out[2*((int64_t)k*res + e) + 1] = v.imag();
+		}
+	}
+	return 0;
+}
+
+}

@@ -1,0 +1,93 @@
+// Host-side objects behind the opaque handles of include/tbtkkpm.h.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <mutex>
+
+namespace tbtkkpm {
+
+int fail(int code, const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what);
+int current_device();
+void count_launches(uint64_t n);
+
+// CUDA events around the phases of one call on a handle's stream.
+struct PhaseTimer {
+  bool enabled = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool pending = false;
+  double recursion_ms = 0, energy_ms = 0;
+  uint64_t step_launches = 0, pending_steps = 0;
+  int enable(bool on);
+  void mark(cudaStream_t st, int i) {
+    if (enabled) cudaEventRecord(ev[i], st);
+  }
+  // After the stream reached ev[3]: adds ev0->ev1 to the recursion time and
+  // ev2->ev3 to the energy-sum time.
+  void collect();
+  void destroy();
+};
+
+// A grow-only device allocation.
+struct DevBuf {
+  void *ptr = nullptr;
+  size_t cap = 0;
+  int reserve(size_t n);
+  void release();
+  template <typename T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+// Makes `dev` current for the scope and restores the previous device.
+struct DeviceGuard {
+  int prev = 0, target = 0;
+  explicit DeviceGuard(int dev);
+  ~DeviceGuard();
+};
+
+// Per-call workspace of a matrix handle, reused across calls.
+struct Workspace {
+  DevBuf vec[2];      // two [N][Bp] vector buffers
+  DevBuf bitmap;      // ceil(N/32) words
+  DevBuf tgt;         // target rows, columns, output slots (3*T uint32)
+  DevBuf from;        // source rows
+  DevBuf mu;          // [K][M] complex moments
+  DevBuf damp;        // [M] damping numerators
+  DevBuf out;         // results ([B][E] LDOS)
+  void release() {
+    for (DevBuf *b : {&vec[0], &vec[1], &bitmap, &tgt, &from, &mu, &damp, &out}) b->release();
+  }
+};
+
+}  // namespace tbtkkpm
+
+struct tbtkkpm_matrix {
+  int device = 0;
+  cudaStream_t stream = nullptr;      // the stream work is issued on
+  cudaStream_t own_stream = nullptr;  // created with the handle
+  uint32_t N = 0;
+  uint64_t nnz = 0;
+  double scale = 1;
+  tbtkkpm::DevBuf rowptr, col, val2;  // CSR of 2H/s (complex128)
+  tbtkkpm::Workspace ws;
+  tbtkkpm::PhaseTimer timer;
+  std::mutex lock;
+  void release_all() {
+    rowptr.release();
+    col.release();
+    val2.release();
+    ws.release();
+    timer.destroy();
+  }
+};
+
+struct tbtkkpm_table {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint32_t M = 0, E = 0;
+  tbtkkpm::DevBuf table;   // [M][E] complex128
+  tbtkkpm::DevBuf mu, out; // staging for energy sums
+  std::mutex lock;
+};

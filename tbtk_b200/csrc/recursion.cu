@@ -1,0 +1,556 @@
+// The Chebyshev recursion and the energy-grid sums behind the C ABI.
+#include "tbtkkpm.h"
+#include "kpm_host.h"
+#include "kpm_kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <array>
+#include <cstring>
+#include <vector>
+
+namespace tbtkkpm {
+
+namespace {
+
+inline unsigned blocks_for(uint64_t n, unsigned bs = 256) { return (unsigned)((n + bs - 1) / bs); }
+
+// ------------------------------------------------------------ batch shapes
+// A batch of B vectors is stored [N][Bp]; a row is owned by TPR threads, each
+// holding VPT complex columns (Bp = TPR*VPT >= B).  complex128 batches go up
+// to 128 columns (64 B per thread), complex64 batches to 256 (64 B per
+// thread).
+struct Shape {
+  int tpr, vpt;
+  uint32_t bp() const { return (uint32_t)(tpr * vpt); }
+};
+
+constexpr uint32_t kMaxBatchFP64 = 128;
+constexpr uint32_t kMaxBatchMixed = 256;
+
+Shape shape_for(int precision, uint32_t B) {
+  if (precision == TBTKKPM_FP64) {
+    if (B <= 1) return {1, 1};
+    if (B <= 2) return {2, 1};
+    if (B <= 4) return {4, 1};
+    if (B <= 8) return {8, 1};
+    if (B <= 16) return {16, 1};
+    if (B <= 32) return {32, 1};
+    if (B <= 64) return {32, 2};
+    return {32, 4};
+  }
+  if (B <= 1) return {1, 1};
+  if (B <= 2) return {2, 1};
+  if (B <= 4) return {4, 1};
+  if (B <= 8) return {4, 2};
+  if (B <= 16) return {8, 2};
+  if (B <= 32) return {16, 2};
+  if (B <= 64) return {32, 2};
+  if (B <= 128) return {32, 4};
+  return {32, 8};
+}
+
+using StepFn = void (*)(unsigned, cudaStream_t, uint32_t, uint32_t, const uint32_t *,
+                        const uint32_t *, const double2 *, const void *, void *, Targets,
+                        uint32_t);
+
+template <typename V, int TPR, int VPT, bool EXACT, bool FIRST>
+void launch_step(unsigned grid, cudaStream_t st, uint32_t N, uint32_t Bp, const uint32_t *rowptr,
+                 const uint32_t *col, const double2 *val2, const void *x, void *y, Targets tg,
+                 uint32_t n_out) {
+  kpm_step<V, TPR, VPT, EXACT, FIRST><<<grid, 256, 0, st>>>(
+      N, Bp, rowptr, col, val2, static_cast<const V *>(x), static_cast<V *>(y), tg, n_out);
+}
+
+struct StepPair {
+  StepFn first, rest;
+};
+
+template <typename V, int TPR, int VPT, bool EXACT>
+StepPair pair() {
+  return {&launch_step<V, TPR, VPT, EXACT, true>, &launch_step<V, TPR, VPT, EXACT, false>};
+}
+
+StepPair step_for(int precision, Shape s) {
+#define TBTKKPM_CASE(V, T, P, X) \
+  if (s.tpr == T && s.vpt == P) return pair<V, T, P, X>();
+  if (precision == TBTKKPM_FP64) {
+    TBTKKPM_CASE(double2, 1, 1, true)
+    TBTKKPM_CASE(double2, 2, 1, true)
+    TBTKKPM_CASE(double2, 4, 1, true)
+    TBTKKPM_CASE(double2, 8, 1, true)
+    TBTKKPM_CASE(double2, 16, 1, true)
+    TBTKKPM_CASE(double2, 32, 1, true)
+    TBTKKPM_CASE(double2, 32, 2, true)
+    TBTKKPM_CASE(double2, 32, 4, true)
+  } else {
+    TBTKKPM_CASE(float2, 1, 1, false)
+    TBTKKPM_CASE(float2, 2, 1, false)
+    TBTKKPM_CASE(float2, 4, 1, false)
+    TBTKKPM_CASE(float2, 4, 2, false)
+    TBTKKPM_CASE(float2, 8, 2, false)
+    TBTKKPM_CASE(float2, 16, 2, false)
+    TBTKKPM_CASE(float2, 32, 2, false)
+    TBTKKPM_CASE(float2, 32, 4, false)
+    TBTKKPM_CASE(float2, 32, 8, false)
+  }
+#undef TBTKKPM_CASE
+  return {nullptr, nullptr};
+}
+
+// ------------------------------------------------------------ one batch
+// Runs the M-1 recursion steps of one batch and leaves the undamped moments
+// in ws.mu ([K][M]).  The to-indices (row, batch column, output slot) are
+// given sorted by row.
+struct TargetList {
+  std::vector<uint32_t> row, col, out;
+};
+
+int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &from,
+              const TargetList &tl, uint32_t K, uint32_t M) {
+  Workspace &ws = m->ws;
+  cudaStream_t st = m->stream;
+  const uint32_t B = (uint32_t)from.size();
+  const Shape s = shape_for(precision, B);
+  const uint32_t Bp = s.bp();
+  const StepPair fn = step_for(precision, s);
+  if (!fn.first) return fail(TBTKKPM_ERR_UNSUPPORTED, "no recursion kernel for batch %u", B);
+  const size_t esize = precision == TBTKKPM_FP64 ? sizeof(double2) : sizeof(float2);
+  const size_t vbytes = (size_t)m->N * Bp * esize;
+  const size_t words = ((size_t)m->N + 31) / 32;
+  const uint32_t T = (uint32_t)tl.row.size();
+  int rc;
+  if ((rc = ws.vec[0].reserve(vbytes)) || (rc = ws.vec[1].reserve(vbytes)) ||
+      (rc = ws.bitmap.reserve(4 * words)) || (rc = ws.tgt.reserve(12 * std::max(T, 1u))) ||
+      (rc = ws.from.reserve(4 * std::max(B, 1u))) ||
+      (rc = ws.mu.reserve(sizeof(double2) * (size_t)std::max(K, 1u) * M)))
+    return rc;
+  std::vector<uint32_t> bitmap(words, 0u);
+  for (uint32_t r : tl.row) bitmap[r >> 5] |= 1u << (r & 31);
+  std::vector<uint32_t> tg_host(3 * (size_t)T);
+  std::copy(tl.row.begin(), tl.row.end(), tg_host.begin());
+  std::copy(tl.col.begin(), tl.col.end(), tg_host.begin() + T);
+  std::copy(tl.out.begin(), tl.out.end(), tg_host.begin() + 2 * (size_t)T);
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(ws.bitmap.ptr, bitmap.data(), 4 * words, cudaMemcpyHostToDevice, st)) ||
+      (T && (e = cudaMemcpyAsync(ws.tgt.ptr, tg_host.data(), 12 * (size_t)T,
+                                 cudaMemcpyHostToDevice, st))) ||
+      (e = cudaMemcpyAsync(ws.from.ptr, from.data(), 4 * (size_t)B, cudaMemcpyHostToDevice, st)) ||
+      (e = cudaMemsetAsync(ws.vec[0].ptr, 0, vbytes, st)) ||
+      (e = cudaMemsetAsync(ws.vec[1].ptr, 0, vbytes, st)) ||
+      (e = cudaMemsetAsync(ws.mu.ptr, 0, sizeof(double2) * (size_t)K * M, st)))
+    return cuda_fail(e, "recursion: staging");
+  Targets tg;
+  tg.bitmap = ws.bitmap.as<uint32_t>();
+  tg.row = ws.tgt.as<uint32_t>();
+  tg.col = ws.tgt.as<uint32_t>() + T;
+  tg.out = ws.tgt.as<uint32_t>() + 2 * (size_t)T;
+  tg.count = T;
+  tg.mu = ws.mu.as<double2>();
+  tg.M = M;
+  const unsigned ib = blocks_for(std::max(B, T));
+  if (precision == TBTKKPM_FP64)
+    kpm_init_sources<double2><<<ib, 256, 0, st>>>(B, Bp, ws.from.as<uint32_t>(),
+                                                 ws.vec[0].as<double2>(), tg);
+  else
+    kpm_init_sources<float2><<<ib, 256, 0, st>>>(B, Bp, ws.from.as<uint32_t>(),
+                                                ws.vec[0].as<float2>(), tg);
+  const unsigned grid = blocks_for((uint64_t)m->N * s.tpr);
+  const uint32_t *rp = m->rowptr.as<uint32_t>();
+  const uint32_t *cl = m->col.as<uint32_t>();
+  const double2 *vl = m->val2.as<double2>();
+  void *cur = ws.vec[0].ptr, *prev = ws.vec[1].ptr;
+  m->timer.mark(st, 0);
+  m->timer.pending = m->timer.enabled;
+  m->timer.pending_steps = M >= 2 ? M - 1 : 0;
+  count_launches(1 + (M >= 2 ? M - 1 : 0));
+  if (M >= 2) {
+    fn.first(grid, st, m->N, Bp, rp, cl, vl, cur, prev, tg, 1);
+    std::swap(cur, prev);  // cur = j1, prev = j0
+    for (uint32_t n = 2; n < M; n++) {
+      fn.rest(grid, st, m->N, Bp, rp, cl, vl, cur, prev, tg, n);
+      std::swap(cur, prev);
+    }
+  }
+  m->timer.mark(st, 1);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "recursion: launch");
+  return TBTKKPM_OK;
+}
+
+// Damping numerators a[n] = sinh(lambda(1 - n/M)) and b = sinh(lambda),
+// evaluated with the host's libm exactly as ChebyshevExpander.cpp:192-195.
+void damping_factors(uint32_t M, double broadening, std::vector<double> &a, double &b) {
+  const double lambda = broadening * M;
+  a.resize(M);
+  for (uint32_t n = 0; n < M; n++) a[n] = std::sinh(lambda * (1 - n / (double)M));
+  b = std::sinh(lambda);
+}
+
+int check_precision(int precision) {
+  if (precision != TBTKKPM_FP64 && precision != TBTKKPM_MIXED)
+    return fail(TBTKKPM_ERR_ARGUMENT, "precision %d is neither TBTKKPM_FP64 nor TBTKKPM_MIXED",
+                precision);
+  return TBTKKPM_OK;
+}
+
+}  // namespace
+
+// Moments of several batches: sources split into batches of at most the
+// precision's maximum; to-indices follow their owner.  Results land in host
+// memory mu_out ([K][M]) undamped.
+static int moments_host(tbtkkpm_matrix *m, const uint32_t *from, uint32_t B, const uint32_t *to,
+                        const uint32_t *owner, uint32_t K, uint32_t M, int precision,
+                        double *mu_out) {
+  const uint32_t maxb = precision == TBTKKPM_FP64 ? kMaxBatchFP64 : kMaxBatchMixed;
+  std::vector<std::vector<uint32_t>> by_owner(B);
+  for (uint32_t k = 0; k < K; k++) by_owner[owner[k]].push_back(k);
+  std::vector<double2> mu_host;
+  for (uint32_t b0 = 0; b0 < B; b0 += maxb) {
+    const uint32_t nb = std::min(maxb, B - b0);
+    std::vector<uint32_t> fr(from + b0, from + b0 + nb);
+    std::vector<std::array<uint32_t, 3>> items;  // row, column, output slot (local)
+    std::vector<uint32_t> global_k;
+    for (uint32_t b = 0; b < nb; b++)
+      for (uint32_t k : by_owner[b0 + b]) {
+        items.push_back({to[k], b, (uint32_t)global_k.size()});
+        global_k.push_back(k);
+      }
+    if (items.empty()) continue;
+    std::stable_sort(items.begin(), items.end(),
+                     [](const std::array<uint32_t, 3> &a, const std::array<uint32_t, 3> &b) {
+                       return a[0] < b[0];
+                     });
+    TargetList tl;
+    for (auto &it : items) {
+      tl.row.push_back(it[0]);
+      tl.col.push_back(it[1]);
+      tl.out.push_back(it[2]);
+    }
+    const uint32_t Kb = (uint32_t)global_k.size();
+    int rc = run_batch(m, precision, fr, tl, Kb, M);
+    if (rc) return rc;
+    mu_host.resize((size_t)Kb * M);
+    m->timer.mark(m->stream, 2);
+    m->timer.mark(m->stream, 3);
+    cudaError_t e = cudaMemcpyAsync(mu_host.data(), m->ws.mu.ptr, sizeof(double2) * Kb * M,
+                                    cudaMemcpyDeviceToHost, m->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "moments: download");
+    m->timer.collect();
+    for (uint32_t i = 0; i < Kb; i++)
+      std::memcpy(mu_out + 2 * (size_t)global_k[i] * M, mu_host.data() + (size_t)i * M,
+                  sizeof(double2) * M);
+  }
+  return TBTKKPM_OK;
+}
+
+// Lorentz damping on the host, c*a/b component-wise
+// (ChebyshevExpander.cpp:190-196).
+static void damp_host(uint32_t K, uint32_t M, double broadening, double *mu) {
+  if (broadening == 0) return;
+  std::vector<double> a;
+  double b;
+  damping_factors(M, broadening, a, b);
+  for (uint32_t k = 0; k < K; k++)
+    for (uint32_t n = 0; n < M; n++) {
+      double *c = mu + 2 * ((size_t)k * M + n);
+      c[0] = c[0] * a[n] / b;
+      c[1] = c[1] * a[n] / b;
+    }
+}
+
+static int check_moment_args(tbtkkpm_matrix *m, const uint32_t *from, uint32_t B,
+                             const uint32_t *to, const uint32_t *owner, uint32_t K, uint32_t M,
+                             double broadening, double *mu_out, const char *fn) {
+  if (!m) return fail(TBTKKPM_ERR_ARGUMENT, "%s: NULL matrix", fn);
+  if (M == 0) return fail(TBTKKPM_ERR_ARGUMENT, "%s: numCoefficients has to be larger than 0", fn);
+  if (B == 0 || !from) return fail(TBTKKPM_ERR_ARGUMENT, "%s: no source index", fn);
+  if (K && (!to || !mu_out)) return fail(TBTKKPM_ERR_ARGUMENT, "%s: NULL to/mu_out", fn);
+  if (!std::isfinite(broadening)) return fail(TBTKKPM_ERR_ARGUMENT, "%s: broadening not finite", fn);
+  for (uint32_t b = 0; b < B; b++)
+    if (from[b] >= m->N)
+      return fail(TBTKKPM_ERR_ARGUMENT, "%s: from index %u outside the basis of size %u", fn,
+                  from[b], m->N);
+  for (uint32_t k = 0; k < K; k++) {
+    if (to[k] >= m->N)
+      return fail(TBTKKPM_ERR_ARGUMENT, "%s: to index %u outside the basis of size %u", fn,
+                  to[k], m->N);
+    if (owner && owner[k] >= B)
+      return fail(TBTKKPM_ERR_ARGUMENT, "%s: to_owner[%u]=%u >= B=%u", fn, k, owner[k], B);
+  }
+  return TBTKKPM_OK;
+}
+
+}  // namespace tbtkkpm
+
+using namespace tbtkkpm;
+
+extern "C" int tbtkkpm_moments(tbtkkpm_matrix *m, uint32_t from, const uint32_t *to, uint32_t K,
+                               uint32_t M, double broadening, double *mu_out) {
+  int rc = check_moment_args(m, &from, 1, to, nullptr, K, M, broadening, mu_out, "moments");
+  if (rc) return rc;
+  if (K == 0) return TBTKKPM_OK;
+  std::lock_guard<std::mutex> lk(m->lock);
+  DeviceGuard g(m->device);
+  std::vector<uint32_t> owner(K, 0u);
+  rc = moments_host(m, &from, 1, to, owner.data(), K, M, TBTKKPM_FP64, mu_out);
+  if (rc) return rc;
+  damp_host(K, M, broadening, mu_out);
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_moments_batched(tbtkkpm_matrix *m, const uint32_t *from, uint32_t B,
+                                       const uint32_t *to, const uint32_t *to_owner, uint32_t K,
+                                       uint32_t M, double broadening, int precision,
+                                       double *mu_out, double *err_out) {
+  int rc = check_precision(precision);
+  if (rc) return rc;
+  if (K && !to_owner) return fail(TBTKKPM_ERR_ARGUMENT, "moments_batched: NULL to_owner");
+  rc = check_moment_args(m, from, B, to, to_owner, K, M, broadening, mu_out, "moments_batched");
+  if (rc) return rc;
+  if (K == 0) return TBTKKPM_OK;
+  std::lock_guard<std::mutex> lk(m->lock);
+  DeviceGuard g(m->device);
+  rc = moments_host(m, from, B, to, to_owner, K, M, precision, mu_out);
+  if (rc) return rc;
+  damp_host(K, M, broadening, mu_out);
+  if (err_out)
+    for (uint32_t k = 0; k < K; k++) err_out[k] = precision == TBTKKPM_FP64 ? 0.0 : -1.0;
+  return TBTKKPM_OK;
+}
+
+// ---------------------------------------------------------------- tables
+
+static int table_alloc(uint32_t M, uint32_t E, tbtkkpm_table **out) {
+  int ndev = 0;
+  tbtkkpm_device_count(&ndev);
+  if (ndev == 0) return fail(TBTKKPM_ERR_CUDA, "no CUDA device available");
+  auto *t = new tbtkkpm_table();
+  t->device = current_device();
+  t->M = M;
+  t->E = E;
+  DeviceGuard g(t->device);
+  cudaError_t e = cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete t;
+    return cuda_fail(e, "cudaStreamCreate");
+  }
+  int rc = t->table.reserve(sizeof(double2) * (size_t)M * E);
+  if (rc) {
+    tbtkkpm_table_destroy(t);
+    return rc;
+  }
+  *out = t;
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_table_create(uint32_t M, const double *energies, uint32_t E, double scale,
+                                    tbtkkpm_table **out) {
+  if (!out) return fail(TBTKKPM_ERR_ARGUMENT, "table_create: out is NULL");
+  *out = nullptr;
+  if (M == 0) return fail(TBTKKPM_ERR_ARGUMENT, "table_create: numCoefficients has to be larger than 0");
+  if (E == 0 || !energies)
+    return fail(TBTKKPM_ERR_ARGUMENT, "table_create: The energy windows resolution has to be larger than 0.");
+  if (!(scale > 0)) return fail(TBTKKPM_ERR_ARGUMENT, "table_create: scaleFactor must be > 0");
+  for (uint32_t e = 0; e < E; e++)
+    if (!(energies[e] > -scale && energies[e] < scale))
+      return fail(TBTKKPM_ERR_ARGUMENT,
+                  "table_create: energy %g is not contained in the interval (-scaleFactor, "
+                  "scaleFactor)=(%g, %g)",
+                  energies[e], -scale, scale);
+  tbtkkpm_table *t = nullptr;
+  int rc = table_alloc(M, E, &t);
+  if (rc) return rc;
+  DeviceGuard g(t->device);
+  DevBuf en;
+  if ((rc = en.reserve(8 * (size_t)E))) {
+    tbtkkpm_table_destroy(t);
+    return rc;
+  }
+  cudaMemcpyAsync(en.ptr, energies, 8 * (size_t)E, cudaMemcpyHostToDevice, t->stream);
+  kpm_table_gen<<<blocks_for((uint64_t)M * E), 256, 0, t->stream>>>(M, E, en.as<double>(), scale,
+                                                                     t->table.as<double2>());
+  count_launches(1);
+  cudaError_t e = cudaStreamSynchronize(t->stream);
+  en.release();
+  if (e != cudaSuccess) {
+    tbtkkpm_table_destroy(t);
+    return cuda_fail(e, "table_create");
+  }
+  *out = t;
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_table_upload(uint32_t M, uint32_t E, const double *table,
+                                    tbtkkpm_table **out) {
+  if (!out) return fail(TBTKKPM_ERR_ARGUMENT, "table_upload: out is NULL");
+  *out = nullptr;
+  if (M == 0 || E == 0 || !table) return fail(TBTKKPM_ERR_ARGUMENT, "table_upload: empty table");
+  tbtkkpm_table *t = nullptr;
+  int rc = table_alloc(M, E, &t);
+  if (rc) return rc;
+  DeviceGuard g(t->device);
+  cudaError_t e = cudaMemcpyAsync(t->table.ptr, table, sizeof(double2) * (size_t)M * E,
+                                  cudaMemcpyHostToDevice, t->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
+  if (e != cudaSuccess) {
+    tbtkkpm_table_destroy(t);
+    return cuda_fail(e, "table_upload");
+  }
+  *out = t;
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_table_destroy(tbtkkpm_table *t) {
+  if (!t) return TBTKKPM_OK;
+  {
+    DeviceGuard g(t->device);
+    if (t->stream) cudaStreamSynchronize(t->stream);
+    t->table.release();
+    t->mu.release();
+    t->out.release();
+    if (t->stream) cudaStreamDestroy(t->stream);
+  }
+  delete t;
+  return TBTKKPM_OK;
+}
+
+namespace tbtkkpm {
+
+// Launches the energy sum of `type` (0-3 Green's functions, 4 = LDOS) for K
+// coefficient vectors resident on the device.
+int launch_energy_sum(cudaStream_t st, const tbtkkpm_table *t, const double2 *mu, uint32_t K,
+                      int type, void *out) {
+  const uint32_t M = t->M, E = t->E;
+  const int KT = K == 1 ? 1 : (K <= 4 ? 4 : 8);
+  dim3 grid((E + kEnergyBlock - 1) / kEnergyBlock, (K + KT - 1) / KT);
+  const double2 *tb = t->table.as<double2>();
+#define TBTKKPM_G(TY, KK) \
+  kpm_greens<TY, KK><<<grid, kEnergyBlock, 0, st>>>(M, E, K, tb, mu, static_cast<double2 *>(out))
+#define TBTKKPM_TYPES(KK)                       \
+  switch (type) {                               \
+    case 0: TBTKKPM_G(0, KK); break;            \
+    case 1: TBTKKPM_G(1, KK); break;            \
+    case 2: TBTKKPM_G(2, KK); break;            \
+    case 3: TBTKKPM_G(3, KK); break;            \
+    default:                                    \
+      kpm_ldos<KK><<<grid, kEnergyBlock, 0, st>>>(M, E, K, tb, mu, static_cast<double *>(out)); \
+  }
+  if (KT == 1) {
+    TBTKKPM_TYPES(1)
+  } else if (KT == 4) {
+    TBTKKPM_TYPES(4)
+  } else {
+    TBTKKPM_TYPES(8)
+  }
+#undef TBTKKPM_TYPES
+#undef TBTKKPM_G
+  count_launches(1);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "energy sum: launch");
+  return TBTKKPM_OK;
+}
+
+static int energy_sum_host(tbtkkpm_table *t, const double *mu, uint32_t K, int type, void *out,
+                           size_t out_elem) {
+  std::lock_guard<std::mutex> lk(t->lock);
+  DeviceGuard g(t->device);
+  const size_t mbytes = sizeof(double2) * (size_t)K * t->M;
+  const size_t obytes = out_elem * (size_t)K * t->E;
+  int rc;
+  if ((rc = t->mu.reserve(mbytes)) || (rc = t->out.reserve(obytes))) return rc;
+  cudaError_t e = cudaMemcpyAsync(t->mu.ptr, mu, mbytes, cudaMemcpyHostToDevice, t->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "energy sum: upload");
+  if ((rc = launch_energy_sum(t->stream, t, t->mu.as<double2>(), K, type, t->out.ptr))) return rc;
+  e = cudaMemcpyAsync(out, t->out.ptr, obytes, cudaMemcpyDeviceToHost, t->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "energy sum: download");
+  return TBTKKPM_OK;
+}
+
+}  // namespace tbtkkpm
+
+extern "C" int tbtkkpm_greens(tbtkkpm_table *t, const double *mu, uint32_t K, int type,
+                              double *G_out) {
+  if (!t) return fail(TBTKKPM_ERR_ARGUMENT, "greens: NULL table");
+  if (type < 0 || type > 3) return fail(TBTKKPM_ERR_ARGUMENT, "greens: Unkown Green's function type %d", type);
+  if (K == 0) return TBTKKPM_OK;
+  if (!mu || !G_out) return fail(TBTKKPM_ERR_ARGUMENT, "greens: NULL buffers");
+  return energy_sum_host(t, mu, K, type, G_out, sizeof(double2));
+}
+
+extern "C" int tbtkkpm_ldos(tbtkkpm_table *t, const double *mu, uint32_t K, double *ldos_out) {
+  if (!t) return fail(TBTKKPM_ERR_ARGUMENT, "ldos: NULL table");
+  if (K == 0) return TBTKKPM_OK;
+  if (!mu || !ldos_out) return fail(TBTKKPM_ERR_ARGUMENT, "ldos: NULL buffers");
+  return energy_sum_host(t, mu, K, 4, ldos_out, sizeof(double));
+}
+
+extern "C" int tbtkkpm_ldos_sites(tbtkkpm_matrix *m, tbtkkpm_table *t, const uint32_t *sites,
+                                  uint32_t B, double broadening, int precision, double *ldos_out,
+                                  double *err_out) {
+  int rc = check_precision(precision);
+  if (rc) return rc;
+  if (!t) return fail(TBTKKPM_ERR_ARGUMENT, "ldos_sites: NULL table");
+  if (B && !ldos_out) return fail(TBTKKPM_ERR_ARGUMENT, "ldos_sites: NULL ldos_out");
+  const uint32_t M = t->M, E = t->E;
+  if (B == 0) return TBTKKPM_OK;
+  rc = check_moment_args(m, sites, B, sites, nullptr, B, M, broadening, ldos_out, "ldos_sites");
+  if (rc) return rc;
+  if (m->device != t->device)
+    return fail(TBTKKPM_ERR_ARGUMENT, "ldos_sites: matrix and table live on different devices");
+  std::lock_guard<std::mutex> lk(m->lock);
+  DeviceGuard g(m->device);
+  const uint32_t maxb = precision == TBTKKPM_FP64 ? kMaxBatchFP64 : kMaxBatchMixed;
+  std::vector<double> a;
+  double b = 1;
+  const bool damp = broadening != 0;
+  if (damp) damping_factors(M, broadening, a, b);
+  Workspace &ws = m->ws;
+  if ((rc = ws.damp.reserve(8 * (size_t)M)) ||
+      (rc = ws.out.reserve(sizeof(double) * (size_t)std::min(B, maxb) * E)))
+    return rc;
+  cudaError_t e;
+  if (damp && (e = cudaMemcpyAsync(ws.damp.ptr, a.data(), 8 * (size_t)M, cudaMemcpyHostToDevice,
+                                   m->stream)) != cudaSuccess)
+    return cuda_fail(e, "ldos_sites: damping upload");
+  // Table reads happen on the matrix stream; order them after the table's own work.
+  cudaStreamSynchronize(t->stream);
+  for (uint32_t b0 = 0; b0 < B; b0 += maxb) {
+    const uint32_t nb = std::min(maxb, B - b0);
+    std::vector<uint32_t> fr(sites + b0, sites + b0 + nb);
+    std::vector<std::array<uint32_t, 2>> items;
+    for (uint32_t i = 0; i < nb; i++) items.push_back({fr[i], i});
+    std::stable_sort(items.begin(), items.end(),
+                     [](const std::array<uint32_t, 2> &x, const std::array<uint32_t, 2> &y) {
+                       return x[0] < y[0];
+                     });
+    TargetList tl;
+    for (auto &it : items) {
+      tl.row.push_back(it[0]);
+      tl.col.push_back(it[1]);
+      tl.out.push_back(it[1]);
+    }
+    if ((rc = run_batch(m, precision, fr, tl, nb, M))) return rc;
+    m->timer.mark(m->stream, 2);
+    if (damp) {
+      kpm_damp<<<blocks_for((uint64_t)nb * M), 256, 0, m->stream>>>(nb, M, ws.damp.as<double>(), b,
+                                                                   ws.mu.as<double2>());
+      count_launches(1);
+    }
+    if ((rc = launch_energy_sum(m->stream, t, ws.mu.as<double2>(), nb, 4, ws.out.ptr))) return rc;
+    m->timer.mark(m->stream, 3);
+    e = cudaMemcpyAsync(ldos_out + (size_t)b0 * E, ws.out.ptr, sizeof(double) * (size_t)nb * E,
+                        cudaMemcpyDeviceToHost, m->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "ldos_sites: download");
+    if (m->timer.enabled) {
+      if ((e = cudaStreamSynchronize(m->stream)) != cudaSuccess) return cuda_fail(e, "ldos_sites");
+      m->timer.collect();
+    }
+  }
+  if ((e = cudaStreamSynchronize(m->stream)) != cudaSuccess) return cuda_fail(e, "ldos_sites");
+  if (err_out)
+    for (uint32_t i = 0; i < B; i++) err_out[i] = precision == TBTKKPM_FP64 ? 0.0 : -1.0;
+  return TBTKKPM_OK;
+}

@@ -1,0 +1,443 @@
+"""Python host layer over the C ABI of include/tbtkkpm.h (libtbtkkpm.so).
+
+The classes mirror the TBTK interface of the KPM path so that calling code
+reads like TBTK's own:
+
+* :class:`ChebyshevExpander` — ``Solver::ChebyshevExpander``
+  (Lib/include/TBTK/Solver/ChebyshevExpander.h:72-223): the same setters,
+  defaults (scale 1.1, 1000 coefficients, broadening 1e-6, window
+  Range(-1, 1, 1000)) and argument checks, ``calculateCoefficients`` and
+  ``generateGreensFunction``.  The model is a CSR matrix in TBTK basis
+  order (what ``HoppingAmplitudeSet::getSparseMatrix`` returns).
+* :class:`PropertyExtractor` — ``PropertyExtractor::ChebyshevExpander``
+  (Lib/include/TBTK/PropertyExtractor/ChebyshevExpander.h:51-178):
+  ``setEnergyWindow``, ``calculateLDOS`` and ``calculateGreensFunctions``
+  over basis indices.
+
+Where the reference exits through TBTKAssert/TBTKExit
+(Lib/include/Utilities/TBTK/TBTKMacros.h:55-94) these classes raise
+:class:`TBTKError`.  There is no CPU fallback: importing this module on a
+machine without the built library raises, and every compute call needs a
+CUDA device.
+"""
+from __future__ import annotations
+
+import ctypes
+import pathlib
+
+import numpy as np
+
+LIB_PATH = pathlib.Path(__file__).resolve().parent / "lib" / "libtbtkkpm.so"
+
+OK = 0
+ERR_ARGUMENT = -1
+ERR_CUDA = -2
+ERR_MEMORY = -3
+ERR_TIMEOUT = -4
+ERR_UNSUPPORTED = -5
+ERR_STATE = -6
+
+ADVANCED, RETARDED, PRINCIPAL, NONPRINCIPAL = 0, 1, 2, 3
+FP64, MIXED = 0, 1
+
+_TYPES = {"Advanced": ADVANCED, "Retarded": RETARDED, "Principal": PRINCIPAL,
+          "NonPrincipal": NONPRINCIPAL}
+
+
+class TBTKError(RuntimeError):
+    """A failed call of the C ABI (status, message)."""
+
+    def __init__(self, status, message):
+        super().__init__(f"[{status}] {message}")
+        self.status = status
+
+
+_p = ctypes.c_void_p
+_d = ctypes.c_double
+_i = ctypes.c_int
+_u32 = ctypes.c_uint32
+_u64 = ctypes.c_uint64
+
+# (name, restype, argtypes) for every entry point of include/tbtkkpm.h
+SIGNATURES = [
+    ("tbtkkpm_last_error", ctypes.c_char_p, []),
+    ("tbtkkpm_version", _i, []),
+    ("tbtkkpm_device_count", _i, [_p]),
+    ("tbtkkpm_set_device", _i, [_i]),
+    ("tbtkkpm_kernel_launches", _u64, []),
+    ("tbtkkpm_matrix_set_profiling", _i, [_p, _i]),
+    ("tbtkkpm_matrix_profile", _i, [_p, _p, _p, _p]),
+    ("tbtkkpm_matrix_create_csr", _i, [_p, _p, _p, _u32, _d, _p]),
+    ("tbtkkpm_matrix_create_triplets", _i, [_p, _p, _p, _u64, _u32, _d, _p]),
+    ("tbtkkpm_matrix_destroy", _i, [_p]),
+    ("tbtkkpm_matrix_set_stream", _i, [_p, _p]),
+    ("tbtkkpm_matrix_shape", _i, [_p, _p, _p]),
+    ("tbtkkpm_matrix_download_csr", _i, [_p, _p, _p, _p]),
+    ("tbtkkpm_moments", _i, [_p, _u32, _p, _u32, _u32, _d, _p]),
+    ("tbtkkpm_moments_batched", _i, [_p, _p, _u32, _p, _p, _u32, _u32, _d, _i, _p, _p]),
+    ("tbtkkpm_table_create", _i, [_u32, _p, _u32, _d, _p]),
+    ("tbtkkpm_table_upload", _i, [_u32, _u32, _p, _p]),
+    ("tbtkkpm_table_destroy", _i, [_p]),
+    ("tbtkkpm_greens", _i, [_p, _p, _u32, _i, _p]),
+    ("tbtkkpm_ldos", _i, [_p, _p, _u32, _p]),
+    ("tbtkkpm_ldos_sites", _i, [_p, _p, _p, _u32, _d, _i, _p, _p]),
+]
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Loads libtbtkkpm.so; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not pathlib.Path(path).exists():
+            raise ImportError(
+                f"{path} is missing: build it with __graft_entry__.build() "
+                "(make -C tbtk_b200/csrc); there is no CPU fallback")
+        lib = ctypes.CDLL(str(path))
+        for name, res, args in SIGNATURES:
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def _check(rc):
+    if rc != OK:
+        msg = load_library().tbtkkpm_last_error().decode(errors="replace")
+        raise TBTKError(rc, msg)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _u32a(a):
+    return np.ascontiguousarray(np.atleast_1d(np.asarray(a)), dtype=np.uint32)
+
+
+def _cxa(a):
+    return np.ascontiguousarray(np.asarray(a), dtype=np.complex128)
+
+
+def kernel_launches() -> int:
+    """Kernels launched by this process through the library."""
+    return int(load_library().tbtkkpm_kernel_launches())
+
+
+def device_count() -> int:
+    n = ctypes.c_int(0)
+    _check(load_library().tbtkkpm_device_count(ctypes.byref(n)))
+    return n.value
+
+
+def tbtk_range(lower, upper, resolution, include_lower=True,
+               include_upper=True):
+    """Energies of TBTK's ``Range`` (Lib/src/Utilities/Range.cpp:30-57):
+    ``start + k*dx`` with the reference's dx/start rules."""
+    if resolution <= 1:
+        raise TBTKError(ERR_ARGUMENT, "'resolution' must be larger than 1.")
+    if include_lower and include_upper:
+        dx = (upper - lower) / (resolution - 1)
+    elif include_lower or include_upper:
+        dx = (upper - lower) / resolution
+    else:
+        dx = (upper - lower) / (resolution + 1)
+    start = lower if include_lower else lower + dx
+    return np.array([start + k * dx for k in range(resolution)])
+
+
+class Matrix:
+    """Device copy of H/s (the C ABI's ``tbtkkpm_matrix``)."""
+
+    def __init__(self, handle, N):
+        self._h = handle
+        self.N = N
+
+    @classmethod
+    def from_csr(cls, rowptr, col, val, scale):
+        lib = load_library()
+        rowptr = _u32a(rowptr)
+        col = _u32a(col)
+        val = _cxa(val)
+        h = ctypes.c_void_p()
+        _check(lib.tbtkkpm_matrix_create_csr(_ptr(rowptr), _ptr(col), _ptr(val),
+                                             rowptr.size - 1, float(scale),
+                                             ctypes.byref(h)))
+        return cls(h, rowptr.size - 1)
+
+    @classmethod
+    def from_triplets(cls, rows, cols, vals, N, scale):
+        lib = load_library()
+        rows = _u32a(rows)
+        cols = _u32a(cols)
+        vals = _cxa(vals)
+        h = ctypes.c_void_p()
+        _check(lib.tbtkkpm_matrix_create_triplets(_ptr(rows), _ptr(cols), _ptr(vals),
+                                                  rows.size, N, float(scale),
+                                                  ctypes.byref(h)))
+        return cls(h, N)
+
+    def shape(self):
+        n = ctypes.c_uint32()
+        nnz = ctypes.c_uint64()
+        _check(load_library().tbtkkpm_matrix_shape(self._h, ctypes.byref(n),
+                                                   ctypes.byref(nnz)))
+        return n.value, nnz.value
+
+    def set_stream(self, cuda_stream):
+        """Issue this handle's work on ``cuda_stream`` (an int cudaStream_t,
+        e.g. ``torch.cuda.current_stream().cuda_stream``; 0/None restores
+        the handle's own stream)."""
+        _check(load_library().tbtkkpm_matrix_set_stream(self._h, cuda_stream or None))
+
+    def set_profiling(self, enable=True):
+        _check(load_library().tbtkkpm_matrix_set_profiling(self._h, int(enable)))
+
+    def profile(self):
+        """(recursion ms, energy-sum ms, recursion-step launches) accumulated
+        since the last read, from CUDA events on the handle's stream."""
+        r = ctypes.c_double()
+        e = ctypes.c_double()
+        n = ctypes.c_uint64()
+        _check(load_library().tbtkkpm_matrix_profile(self._h, ctypes.byref(r),
+                                                     ctypes.byref(e), ctypes.byref(n)))
+        return r.value, e.value, n.value
+
+    def download_csr(self):
+        N, nnz = self.shape()
+        rowptr = np.zeros(N + 1, dtype=np.uint32)
+        col = np.zeros(max(nnz, 1), dtype=np.uint32)
+        val = np.zeros(max(nnz, 1), dtype=np.complex128)
+        _check(load_library().tbtkkpm_matrix_download_csr(self._h, _ptr(rowptr),
+                                                          _ptr(col), _ptr(val)))
+        return rowptr, col[:nnz], val[:nnz]
+
+    def moments(self, frm, to, M, broadening):
+        to = _u32a(to)
+        out = np.zeros((to.size, M), dtype=np.complex128)
+        _check(load_library().tbtkkpm_moments(self._h, int(frm), _ptr(to), to.size,
+                                              M, float(broadening), _ptr(out)))
+        return out
+
+    def moments_batched(self, frm, to, owner, M, broadening, precision=FP64):
+        frm = _u32a(frm)
+        to = _u32a(to)
+        owner = _u32a(owner)
+        out = np.zeros((to.size, M), dtype=np.complex128)
+        err = np.zeros(to.size, dtype=np.float64)
+        _check(load_library().tbtkkpm_moments_batched(
+            self._h, _ptr(frm), frm.size, _ptr(to), _ptr(owner), to.size, M,
+            float(broadening), int(precision), _ptr(out), _ptr(err)))
+        return out, err
+
+    def ldos_sites(self, table, sites, broadening, precision=FP64):
+        sites = _u32a(sites)
+        out = np.zeros((sites.size, table.E), dtype=np.float64)
+        err = np.zeros(sites.size, dtype=np.float64)
+        _check(load_library().tbtkkpm_ldos_sites(self._h, table._h, _ptr(sites),
+                                                 sites.size, float(broadening),
+                                                 int(precision), _ptr(out), _ptr(err)))
+        return out, err
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().tbtkkpm_matrix_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+
+class Table:
+    """Device lookup table T[n][e] (the C ABI's ``tbtkkpm_table``)."""
+
+    def __init__(self, handle, M, E):
+        self._h = handle
+        self.M = M
+        self.E = E
+
+    @classmethod
+    def create(cls, M, energies, scale):
+        energies = np.ascontiguousarray(energies, dtype=np.float64)
+        h = ctypes.c_void_p()
+        _check(load_library().tbtkkpm_table_create(M, _ptr(energies), energies.size,
+                                                   float(scale), ctypes.byref(h)))
+        return cls(h, M, energies.size)
+
+    @classmethod
+    def upload(cls, table):
+        table = _cxa(table)
+        M, E = table.shape
+        h = ctypes.c_void_p()
+        _check(load_library().tbtkkpm_table_upload(M, E, _ptr(table), ctypes.byref(h)))
+        return cls(h, M, E)
+
+    def greens(self, mu, type_):
+        mu = _cxa(np.atleast_2d(mu))
+        out = np.zeros((mu.shape[0], self.E), dtype=np.complex128)
+        _check(load_library().tbtkkpm_greens(self._h, _ptr(mu), mu.shape[0],
+                                             int(type_), _ptr(out)))
+        return out
+
+    def ldos(self, mu):
+        mu = _cxa(np.atleast_2d(mu))
+        out = np.zeros((mu.shape[0], self.E), dtype=np.float64)
+        _check(load_library().tbtkkpm_ldos(self._h, _ptr(mu), mu.shape[0], _ptr(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().tbtkkpm_table_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+
+class ChebyshevExpander:
+    """``Solver::ChebyshevExpander`` over the B200 kernels.
+
+    Coefficients and Green's functions always run on the GPU here; the
+    ``set...OnGPU`` flags are kept for interface compatibility and
+    ``setUseLookupTable(False)`` with GPU Green's functions is rejected as in
+    ``ensureLookupTableIsReady`` (ChebyshevExpander.h:548-566).
+    """
+
+    Type = _TYPES
+
+    def __init__(self):
+        self.scaleFactor = 1.1
+        self.numCoefficients = 1000
+        self.broadening = 1e-6
+        self.energyWindow = tbtk_range(-1, 1, 1000)
+        self.calculateCoefficientsOnGPU = True
+        self.generateGreensFunctionsOnGPU = True
+        self.useLookupTable = True
+        self.precision = FP64
+        self._csr = None
+        self._matrix = None
+        self._table = None
+
+    # -- model -------------------------------------------------------------
+    def setModel(self, csr):
+        """csr = (rowptr, col, val) of H in TBTK basis order."""
+        self._csr = csr
+        self._matrix = None
+
+    def _get_matrix(self):
+        if self._csr is None:
+            raise TBTKError(ERR_STATE, "Solver::ChebyshevExpander: no model set")
+        if self._matrix is None:
+            self._matrix = Matrix.from_csr(*self._csr, self.scaleFactor)
+        return self._matrix
+
+    # -- setters (ChebyshevExpander.h:394-489) ------------------------------
+    def setScaleFactor(self, scaleFactor):
+        if not scaleFactor > 0:
+            raise TBTKError(ERR_ARGUMENT, f"The 'scaleFactor={scaleFactor}' has to be larger than '0'.")
+        self.scaleFactor = float(scaleFactor)
+        self._matrix = None
+        self._table = None
+
+    def getScaleFactor(self):
+        return self.scaleFactor
+
+    def setNumCoefficients(self, numCoefficients):
+        self.numCoefficients = int(numCoefficients)
+        self._table = None
+
+    def getNumCoefficients(self):
+        return self.numCoefficients
+
+    def setBroadening(self, broadening):
+        self.broadening = float(broadening)
+
+    def getBroadening(self):
+        return self.broadening
+
+    def setEnergyWindow(self, energies):
+        energies = np.asarray(energies, dtype=np.float64)
+        eps = np.finfo(np.float64).eps
+        s = self.scaleFactor
+        if not (energies[0] > -s * (1 - 16 * eps) and energies[-1] < s * (1 - 16 * eps)):
+            raise TBTKError(
+                ERR_ARGUMENT,
+                f"Invalid energy window. The 'energyWindow=[{energies[0]}, {energies[-1]}]' is"
+                f" not contained in the interval (-scaleFactor, scaleFactor)=({-s}, {s}).")
+        self.energyWindow = energies
+        self._table = None
+
+    def getEnergyWindow(self):
+        return self.energyWindow
+
+    def setCalculateCoefficientsOnGPU(self, flag):
+        self.calculateCoefficientsOnGPU = bool(flag)
+
+    def setGenerateGreensFunctionsOnGPU(self, flag):
+        self.generateGreensFunctionsOnGPU = bool(flag)
+
+    def setUseLookupTable(self, flag):
+        self.useLookupTable = bool(flag)
+        if not flag:
+            self._table = None
+
+    def setPrecision(self, precision):
+        if precision not in (FP64, MIXED):
+            raise TBTKError(ERR_ARGUMENT, f"unknown precision {precision}")
+        self.precision = precision
+
+    # -- compute -----------------------------------------------------------
+    def calculateCoefficients(self, to, frm):
+        """``calculateCoefficients(to, from)``: [K][M] damped moments for a
+        list of to basis indices (or one index -> [M])."""
+        if self.numCoefficients <= 0:
+            raise TBTKError(ERR_ARGUMENT, "numCoefficients has to be larger than 0.")
+        single = np.ndim(to) == 0
+        mu = self._get_matrix().moments(frm, to, self.numCoefficients, self.broadening)
+        return mu[0] if single else mu
+
+    def _get_table(self):
+        if not self.useLookupTable:
+            raise TBTKError(ERR_STATE, "Green's functions can only be generated on GPU using lookup tables.")
+        if self._table is None:
+            e = self.energyWindow
+            s = self.scaleFactor
+            if not (e[0] > -s and e[-1] < s):
+                raise TBTKError(ERR_ARGUMENT, "The energy windows bounds have to lie in (-scaleFactor, scaleFactor).")
+            self._table = Table.create(self.numCoefficients, e, s)
+        return self._table
+
+    def generateGreensFunction(self, coefficients, type_="Retarded"):
+        t = _TYPES[type_] if isinstance(type_, str) else int(type_)
+        g = self._get_table().greens(coefficients, t)
+        return g[0] if np.ndim(coefficients) == 1 else g
+
+
+class PropertyExtractor:
+    """``PropertyExtractor::ChebyshevExpander`` over basis indices."""
+
+    def __init__(self, solver: ChebyshevExpander):
+        self.solver = solver
+        e = solver.getEnergyWindow()
+        self.setEnergyWindow(e[0], e[-1], e.size)
+
+    def setEnergyWindow(self, lowerBound, upperBound, energyResolution):
+        """Inclusive ``Range(lower, upper, res)`` pushed to the solver
+        (PropertyExtractor ChebyshevExpander.cpp:79-94)."""
+        self.solver.setEnergyWindow(tbtk_range(lowerBound, upperBound, energyResolution))
+
+    def getEnergyWindow(self):
+        return self.solver.getEnergyWindow()
+
+    def calculateLDOS(self, sites):
+        """LDOS [len(sites)][E] at basis indices, all sites in one batched
+        recursion (the reference loops over sites one recursion each)."""
+        s = self.solver
+        out, _ = s._get_matrix().ldos_sites(s._get_table(), sites, s.broadening,
+                                            s.precision)
+        return out
+
+    def calculateGreensFunctions(self, to, frm, type_="Retarded"):
+        s = self.solver
+        mu = s.calculateCoefficients(np.atleast_1d(to), frm)
+        return s.generateGreensFunction(mu, type_)

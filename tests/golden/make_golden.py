@@ -1,0 +1,128 @@
+"""Generates the golden vectors of the KPM path from the TBTK reference.
+
+Runs the reference classes compiled from the reference sources
+(oracle/_ref/libtbtkref.so, ``make -C oracle ref``) through
+tests/oracle_lib.py and writes tests/golden/*.npz.  Every array comes from a
+reference call: Model -> HoppingAmplitudeSet::getSparseMatrix (CSR),
+Solver::ChebyshevExpander::calculateCoefficients (moments),
+generateGreensFunction (G, table and closed form), and
+PropertyExtractor::ChebyshevExpander::calculateLDOS /
+calculateGreensFunctions.
+
+    python tests/golden/make_golden.py
+"""
+import pathlib
+import sys
+
+import numpy as np
+
+HERE = pathlib.Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+from oracle_lib import Reference  # noqa: E402
+from tbtk_b200 import lattice as L  # noqa: E402
+
+
+def pe_window(s, res):
+    """Open grid (-s, s) with res points, as the PropertyExtractor's inclusive
+    Range(lo, hi, res) with lo = -s + 2s/(res+1), hi = lo + (res-1)*dx."""
+    dx = 2 * s / (res + 1)
+    lo = -s + dx
+    hi = lo + (res - 1) * dx
+    return lo, hi
+
+
+def model_case(ref, lat, s, M, bro, to, frm, ldos_sites, E, types=(0, 1, 2, 3)):
+    m = ref.model(lat)
+    rowptr, col, val = m.csr()
+    out = dict(rowptr=rowptr, col=col, val=val, shape=np.array(lat.shape),
+               scale=s, M=M, broadening=bro,
+               to=np.array([lat.basis(t) for t in to], dtype=np.uint32),
+               frm=np.uint32(lat.basis(frm)),
+               to_index=np.array(to, dtype=np.int32),
+               from_index=np.array(frm, dtype=np.int32))
+    out["moments"] = m.coefficients(s, M, bro, to, frm)
+    lo, hi = pe_window(s, E)
+    out["window"] = np.array([lo, hi, E])
+    out["ldos_sites"] = np.array([lat.basis(t) for t in ldos_sites], dtype=np.uint32)
+    out["ldos"] = m.ldos(s, M, bro, lo, hi, E, ldos_sites)
+    for ty in types:
+        out[f"greens_{ty}"] = m.greens_pe(s, M, bro, lo, hi, E, ty, to, frm)
+    return out
+
+
+def main():
+    ref = Reference()
+    cases = {}
+
+    # Reference coefficient test: 5x5 periodic spinless, mu=-2, t=1, s=10,
+    # M=100, broadening 0 (Test/include/TBTK/Test/Solver/ChebyshevExpander.h:184-278).
+    lat = L.test_square()
+    m = ref.model(lat)
+    rowptr, col, val = m.csr()
+    cases["kat5x5"] = dict(
+        rowptr=rowptr, col=col, val=val, scale=10.0, M=100, broadening=0.0,
+        to=np.array([lat.basis((0, 0)), lat.basis((1, 0))], dtype=np.uint32),
+        frm=np.uint32(lat.basis((0, 0))),
+        moments=m.coefficients(10.0, 100, 0.0, [[0, 0], [1, 0]], [0, 0]))
+
+    # The CPU-runnable configuration: 30x30 with spin, open, t=1, J=0.5,
+    # s=10, M=1000, broadening 1e-3, site (15,15,0), 1000 open-grid energies.
+    lat = L.square(30, 30, t=1.0, J=0.5, periodic=False)
+    cases["cfg1"] = model_case(ref, lat, 10.0, 1000, 1e-3,
+                               [(15, 15, 0), (16, 15, 0), (15, 15, 1)],
+                               (15, 15, 0), [(15, 15, 0), (0, 0, 1)], 1000)
+
+    # Rashba + disorder, periodic (complex off-diagonal amplitudes).
+    lat = L.square(8, 6, t=1.0, J=0.5, W=2.0, alpha=0.3, periodic=True, seed=11)
+    cases["rashba"] = model_case(ref, lat, 12.0, 256, 1e-3,
+                                 [(3, 2, 0), (3, 2, 1), (4, 2, 1), (0, 5, 0)],
+                                 (3, 2, 0), [(3, 2, 0), (7, 5, 1), (1, 1, 0)], 300)
+
+    # Honeycomb + disorder, periodic.
+    lat = L.honeycomb(6, 5, t=1.0, J=0.3, W=1.5, periodic=True, seed=5)
+    cases["honeycomb"] = model_case(ref, lat, 12.0, 200, 1e-3,
+                                    [(2, 2, 0, 0), (2, 2, 1, 0), (1, 2, 1, 0)],
+                                    (2, 2, 0, 0), [(2, 2, 0, 0), (5, 4, 1, 1)], 128)
+
+    # Duplicate amplitudes: a 2x2 periodic lattice repeats each hopping, and
+    # mu, Zeeman and disorder stack three on-site terms.
+    lat = L.square(2, 2, t=1.0, J=0.5, mu=0.7, W=1.0, periodic=True, seed=2)
+    cases["duplicates"] = model_case(ref, lat, 10.0, 64, 1e-3,
+                                     [(0, 0, 0), (1, 1, 1)], (0, 0, 0),
+                                     [(0, 0, 0)], 50)
+
+    # Reference LDOS test ring: 10 sites, s=10, default M=1000 and
+    # broadening 1e-6, windows +-9 and +-7 of 1000 points
+    # (Test/include/TBTK/Test/PropertyExtractor/ChebyshevExpander.h:19-45).
+    lat = L.ring(10)
+    m = ref.model(lat)
+    rowptr, col, val = m.csr()
+    ring = dict(rowptr=rowptr, col=col, val=val, scale=10.0, M=1000, broadening=1e-6)
+    for f in (0.9, 0.7):
+        ring[f"ldos_{int(f * 10)}"] = m.ldos(10.0, 1000, 1e-6, -10 * f, 10 * f, 1000, [[0]])
+    cases["ring"] = ring
+
+    # Closed-form Green's functions, c = {1, 2, 3}, s = 10, Range(-5, 5, 10)
+    # (ChebyshevExpander.h:371-564), and complex coefficients on a half-open
+    # window.
+    g = {}
+    for ty in range(4):
+        for tab in (0, 1):
+            g[f"real_{ty}_{tab}"] = ref.greens(10.0, [1, 2, 3], -5, 5, 10, ty, tab)
+    cc = np.array([1 + 0.5j, 2 - 1j, 3 + 2j, -0.3 + 0.1j])
+    g["cc"] = cc
+    for ty in range(4):
+        for tab in (0, 1):
+            g[f"cplx_{ty}_{tab}"] = ref.greens(10.0, cc, -9.5, 9.5, 37, ty, tab, False, True)
+    cases["greens"] = g
+
+    for name, arrays in cases.items():
+        np.savez_compressed(HERE / f"{name}.npz", **arrays)
+        print(name, sum(np.asarray(v).nbytes for v in arrays.values()), "bytes")
+
+
+if __name__ == "__main__":
+    main()
