@@ -272,6 +272,9 @@ def ours(args, world, rank, local):
     mat = kpm.Matrix.from_csr(p.rowptr, p.col, p.val, p.scale)
     tab = kpm.Table.create(p.M, p.energies, p.scale)
     mat.set_stream(stream.cuda_stream)
+    # project autotuner: pick the step configuration of both batch shapes
+    tuned_mixed = mat.autotune(B, kpm.MIXED, ldos=True, probe_steps=6)
+    tuned_plain = mat.autotune(1, kpm.FP64, ldos=True, probe_steps=6)
     mat.set_profiling(True)
 
     def step(prec, sites):
@@ -378,6 +381,10 @@ def ours(args, world, rank, local):
                                 f"E={p.energies.size} open grid, {B} LDOS sites per rank as one "
                                 f"batched mixed-precision recursion"),
                    "sites_per_step_per_rank": B, "l2": "inputs larger than L2 (no flush)",
+                   "autotuned": {"mixed_ldos": dict(zip(("tpr", "vpt", "minb", "ms_per_step"),
+                                                        tuned_mixed)),
+                                 "plain_fp64": dict(zip(("tpr", "vpt", "minb", "ms_per_step"),
+                                                        tuned_plain))},
                    "parallelism": f"replicas x{world} (sites sharded, no collective)"},
         "gpu_launches": int(launches),
         "plain_fp64": {"value": plain_rate, "unit": "LDOS solves/s", "ms_per_solve": plain_ms,
@@ -389,7 +396,8 @@ def ours(args, world, rank, local):
                        "note": "per 64-site batch; request-level latency is in the serving bench"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None,
-                     "kernel": "kpm_step<float2,32,2> (recursion step, B=64)",
+                     "kernel": (f"kpm_step<float2, tpr={tuned_mixed[0]}, vpt={tuned_mixed[1]}, "
+                                f"dots, minb={tuned_mixed[2]}> (recursion step, B={B})"),
                      "bytes_per_launch": bstep, "avg_launch_ms": avg_step_ms,
                      "peak_kind": f"{peak_kind} (copy bandwidth)"},
         "recursion_share": rec_ms / total_ms if total_ms else None,

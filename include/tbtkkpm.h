@@ -74,9 +74,15 @@ TBTKKPM_API uint64_t tbtkkpm_kernel_launches(void);
  * FP64: complex128 vectors, the reference's operation order (moments are
  *   bit-identical to calculateCoefficientsCPU).
  * MIXED: complex64 vectors in HBM, FP64 arithmetic in registers, FP64
- *   moments, damping and energy sums. */
+ *   moments, damping and energy sums.  For LDOS (a source's only to-index is
+ *   itself) the recursion runs to j_{M/2} only and takes two moments per
+ *   step from FP64 dot products: mu_{2n} = 2<j_n|j_n> - mu_0,
+ *   mu_{2n+1} = 2<j_{n+1}|j_n> - mu_1 (H Hermitian).
+ * MIXED_DIRECT: MIXED with every moment gathered directly (no dot-product
+ *   identities), M-1 steps. */
 #define TBTKKPM_FP64 0
 #define TBTKKPM_MIXED 1
+#define TBTKKPM_MIXED_DIRECT 2
 
 typedef struct tbtkkpm_matrix tbtkkpm_matrix;
 typedef struct tbtkkpm_table tbtkkpm_table;
@@ -181,6 +187,22 @@ TBTKKPM_API int tbtkkpm_greens(
  * Lib/src/PropertyExtractor/ChebyshevExpander.cpp:661-684).  [K][E]. */
 TBTKKPM_API int tbtkkpm_ldos(
 	tbtkkpm_table *t, const double *mu, uint32_t K, double *ldos_out);
+
+/* Autotuner.  Times every compiled recursion-step configuration (threads
+ * per row, complex values per thread, register cap) that serves batches of
+ * B sources at this precision on this matrix, probe_steps steps each with
+ * CUDA events on the handle's stream, and keeps the fastest for later calls
+ * on this handle.  ldos != 0 tunes the kernels tbtkkpm_ldos_sites uses (the
+ * dot-product variant at TBTKKPM_MIXED), 0 those of the moment calls.
+ * Outputs (may be NULL): the chosen configuration and its ms per step.
+ * tbtkkpm_matrix_set_config installs a known choice without timing.
+ * (No reference counterpart.) */
+TBTKKPM_API int tbtkkpm_matrix_autotune(
+	tbtkkpm_matrix *m, uint32_t B, int precision, int ldos,
+	uint32_t probe_steps, int *tpr, int *vpt, int *minb, double *ms_per_step);
+TBTKKPM_API int tbtkkpm_matrix_set_config(
+	tbtkkpm_matrix *m, uint32_t B, int precision, int ldos, int tpr, int vpt,
+	int minb);
 
 /* LDOS at B sites in one call: the moments <site|T_n|site> of all sites run
  * as one batched recursion, are damped and summed over the table's energy

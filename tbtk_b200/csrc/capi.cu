@@ -46,6 +46,20 @@ int current_device() {
   return d;
 }
 
+int sm_count(int device) {
+  static std::atomic<int> cache[64];
+  if (device < 0 || device >= 64) return 148;
+  int v = cache[device].load();
+  if (v == 0) {
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || v <= 0) {
+      cudaGetLastError();
+      v = 148;
+    }
+    cache[device].store(v);
+  }
+  return v;
+}
+
 static std::atomic<uint64_t> g_launches{0};
 
 void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
@@ -173,6 +187,44 @@ static inline unsigned blocks_for(uint64_t n, unsigned bs = 256) {
   return (unsigned)((n + bs - 1) / bs);
 }
 
+// SELL-32 copy of the scaled CSR (the layout the recursion reads).
+static int build_sell(tbtkkpm_matrix *m, cudaStream_t st) {
+  const uint32_t N = m->N;
+  const uint32_t ns = (N + 31) / 32;
+  m->nslices = ns;
+  DevBuf width, tmp;
+  int rc;
+  if ((rc = width.reserve(4 * ((size_t)ns + 1))) ||
+      (rc = m->slice_ptr.reserve(4 * ((size_t)ns + 1))))
+    return rc;
+  cudaError_t e = cudaMemsetAsync(width.ptr, 0, 4 * ((size_t)ns + 1), st);
+  if (e != cudaSuccess) return cuda_fail(e, "SELL build");
+  k_sell_width<<<blocks_for(ns), 256, 0, st>>>(N, ns, m->rowptr.as<uint32_t>(),
+                                               width.as<uint32_t>());
+  size_t tb = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, tb, width.as<uint32_t>(), m->slice_ptr.as<uint32_t>(),
+                                (int64_t)ns + 1, st);
+  if ((rc = tmp.reserve(std::max<size_t>(tb, 16)))) return rc;
+  cub::DeviceScan::ExclusiveSum(tmp.ptr, tb, width.as<uint32_t>(), m->slice_ptr.as<uint32_t>(),
+                                (int64_t)ns + 1, st);
+  uint32_t chunks = 0;
+  e = cudaMemcpyAsync(&chunks, m->slice_ptr.as<uint32_t>() + ns, 4, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  width.release();
+  tmp.release();
+  if (e != cudaSuccess) return cuda_fail(e, "SELL build");
+  m->chunks = chunks;
+  const size_t slots = std::max<size_t>((size_t)chunks * 32, 1);
+  if ((rc = m->scol.reserve(4 * slots)) || (rc = m->sval.reserve(16 * slots))) return rc;
+  k_sell_fill<<<blocks_for((uint64_t)ns * 32), 256, 0, st>>>(
+      N, ns, m->rowptr.as<uint32_t>(), m->col.as<uint32_t>(), m->val2.as<double2>(),
+      m->slice_ptr.as<uint32_t>(), m->scol.as<uint32_t>(), m->sval.as<double2>());
+  count_launches(2);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "SELL build");
+  return TBTKKPM_OK;
+}
+
 }  // namespace tbtkkpm
 
 using namespace tbtkkpm;
@@ -298,6 +350,10 @@ extern "C" int tbtkkpm_matrix_create_csr(const uint32_t *rowptr, const uint32_t 
                                                           (double2 *)m->val2.ptr);
     count_launches(1);
   }
+  if ((rc = build_sell(m, m->stream))) {
+    tbtkkpm_matrix_destroy(m);
+    return rc;
+  }
   if ((e = cudaStreamSynchronize(m->stream)) != cudaSuccess) {
     tbtkkpm_matrix_destroy(m);
     return cuda_fail(e, "matrix_create_csr: scale");
@@ -405,6 +461,10 @@ extern "C" int tbtkkpm_matrix_create_triplets(const uint32_t *rows, const uint32
   if (e != cudaSuccess) {
     tbtkkpm_matrix_destroy(m);
     return cuda_fail(e, "matrix_create_triplets: build");
+  }
+  if ((rc = build_sell(m, m->stream))) {
+    tbtkkpm_matrix_destroy(m);
+    return rc;
   }
   *out = m;
   return TBTKKPM_OK;

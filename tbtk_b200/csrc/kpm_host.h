@@ -3,8 +3,10 @@
 
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cstddef>
 #include <cstdint>
+#include <map>
 #include <mutex>
 
 namespace tbtkkpm {
@@ -13,6 +15,7 @@ int fail(int code, const char *fmt, ...);
 int cuda_fail(cudaError_t e, const char *what);
 int current_device();
 void count_launches(uint64_t n);
+int sm_count(int device);
 
 // CUDA events around the phases of one call on a handle's stream.
 struct PhaseTimer {
@@ -56,8 +59,13 @@ struct Workspace {
   DevBuf mu;          // [K][M] complex moments
   DevBuf damp;        // [M] damping numerators
   DevBuf out;         // results ([B][E] LDOS)
+  DevBuf mu_direct;   // [K][steps+1] directly gathered moments (doubling runs)
+  DevBuf dots;        // [grid][2][Bp] per-block dot products (doubling runs)
+  DevBuf col_out;     // [Bp] output slot of each batch column (doubling runs)
   void release() {
-    for (DevBuf *b : {&vec[0], &vec[1], &bitmap, &tgt, &from, &mu, &damp, &out}) b->release();
+    for (DevBuf *b : {&vec[0], &vec[1], &bitmap, &tgt, &from, &mu, &damp, &out, &mu_direct,
+                      &dots, &col_out})
+      b->release();
   }
 };
 
@@ -71,13 +79,24 @@ struct tbtkkpm_matrix {
   uint64_t nnz = 0;
   double scale = 1;
   tbtkkpm::DevBuf rowptr, col, val2;  // CSR of 2H/s (complex128)
+  // SELL-32 copy the recursion reads: slice_ptr[nslices+1] (chunk offsets),
+  // scol/sval[chunks*32]
+  tbtkkpm::DevBuf slice_ptr, scol, sval;
+  uint32_t nslices = 0;
+  uint64_t chunks = 0;
   tbtkkpm::Workspace ws;
   tbtkkpm::PhaseTimer timer;
+  // autotuned step configuration per (kernel class, padded batch width):
+  // {threads per row, values per thread, min blocks per SM}
+  std::map<uint64_t, std::array<int, 3>> tuned;
   std::mutex lock;
   void release_all() {
     rowptr.release();
     col.release();
     val2.release();
+    slice_ptr.release();
+    scol.release();
+    sval.release();
     ws.release();
     timer.destroy();
   }

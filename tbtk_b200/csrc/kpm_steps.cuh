@@ -1,0 +1,73 @@
+// Launch wrappers and the dispatch table of the recursion-step kernels.
+// Each table entry is one compiled configuration (vector type, threads per
+// row TPR, values per thread VPT, register cap MINB); the driver or the
+// autotuner picks an entry per batch shape.
+#pragma once
+
+#include "kpm_host.h"
+#include "kpm_kernels.cuh"
+
+#include <algorithm>
+
+namespace tbtkkpm {
+
+// Vector classes of the step kernels.
+enum StepClass : int { kClassFP64 = 0, kClassMixed = 1, kClassMixedDots = 2 };
+
+struct StepArgs {
+  Sell A;
+  uint32_t Bp;
+  const void *x;
+  void *y;
+  Targets tg;
+  uint32_t n_out;
+  double2 *dots;
+};
+
+// Launches one step with a grid of min(tiles, resident blocks, max_grid)
+// blocks and returns the grid used (the caller sizes per-block buffers).
+using StepFn = void (*)(cudaStream_t, int device, unsigned max_grid, const StepArgs &,
+                        unsigned *grid);
+
+struct StepEntry {
+  int cls, tpr, vpt, minb;
+  StepFn first, rest;
+};
+
+template <typename V, int TPR, int VPT, bool EXACT, bool FIRST, bool DOTS, int MINB>
+void launch_step(cudaStream_t st, int device, unsigned max_grid, const StepArgs &a,
+                 unsigned *grid) {
+  auto kern = kpm_step<V, TPR, VPT, EXACT, FIRST, DOTS, MINB>;
+  static int per_sm[64] = {0};
+  const int d = device & 63;
+  if (per_sm[d] == 0) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kBlock, 0) != cudaSuccess ||
+        nb < 1) {
+      cudaGetLastError();
+      nb = 1;
+    }
+    per_sm[d] = nb;
+  }
+  constexpr int RPB = kBlock / TPR;
+  const uint64_t tiles = ((uint64_t)a.A.nslices * 32 + RPB - 1) / RPB;
+  uint64_t g = std::min<uint64_t>(tiles, (uint64_t)per_sm[d] * sm_count(device));
+  if (max_grid) g = std::min<uint64_t>(g, max_grid);
+  g = std::max<uint64_t>(g, 1);
+  *grid = (unsigned)g;
+  kern<<<(unsigned)g, kBlock, 0, st>>>(a.A, a.Bp, static_cast<const V *>(a.x),
+                                       static_cast<V *>(a.y), a.tg, a.n_out, a.dots);
+}
+
+#define TBTKKPM_STEP_ENTRY(CLS, V, T, P, X, D, MB)                                  \
+  {CLS, T, P, MB, &launch_step<V, T, P, X, true, D, MB>,                            \
+   &launch_step<V, T, P, X, false, D, MB>}
+
+extern const StepEntry kStepsFP64[];
+extern const int kNumStepsFP64;
+extern const StepEntry kStepsMixed[];
+extern const int kNumStepsMixed;
+extern const StepEntry kStepsMixedDots[];
+extern const int kNumStepsMixedDots;
+
+}  // namespace tbtkkpm

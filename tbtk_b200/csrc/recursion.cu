@@ -2,12 +2,13 @@
 #include "tbtkkpm.h"
 #include "kpm_host.h"
 #include "kpm_kernels.cuh"
+#include "kpm_steps.cuh"
 
 #include <algorithm>
-#include <cmath>
-#include <numeric>
 #include <array>
+#include <cmath>
 #include <cstring>
+#include <numeric>
 #include <vector>
 
 namespace tbtkkpm {
@@ -29,8 +30,10 @@ struct Shape {
 constexpr uint32_t kMaxBatchFP64 = 128;
 constexpr uint32_t kMaxBatchMixed = 256;
 
+bool is_mixed(int precision) { return precision != TBTKKPM_FP64; }
+
 Shape shape_for(int precision, uint32_t B) {
-  if (precision == TBTKKPM_FP64) {
+  if (!is_mixed(precision)) {
     if (B <= 1) return {1, 1};
     if (B <= 2) return {2, 1};
     if (B <= 4) return {4, 1};
@@ -51,80 +54,88 @@ Shape shape_for(int precision, uint32_t B) {
   return {32, 8};
 }
 
-using StepFn = void (*)(unsigned, cudaStream_t, uint32_t, uint32_t, const uint32_t *,
-                        const uint32_t *, const double2 *, const void *, void *, Targets,
-                        uint32_t);
-
-template <typename V, int TPR, int VPT, bool EXACT, bool FIRST>
-void launch_step(unsigned grid, cudaStream_t st, uint32_t N, uint32_t Bp, const uint32_t *rowptr,
-                 const uint32_t *col, const double2 *val2, const void *x, void *y, Targets tg,
-                 uint32_t n_out) {
-  kpm_step<V, TPR, VPT, EXACT, FIRST><<<grid, 256, 0, st>>>(
-      N, Bp, rowptr, col, val2, static_cast<const V *>(x), static_cast<V *>(y), tg, n_out);
+int step_class(int precision, bool dots) {
+  if (!is_mixed(precision)) return kClassFP64;
+  return dots ? kClassMixedDots : kClassMixed;
 }
 
-struct StepPair {
-  StepFn first, rest;
-};
-
-template <typename V, int TPR, int VPT, bool EXACT>
-StepPair pair() {
-  return {&launch_step<V, TPR, VPT, EXACT, true>, &launch_step<V, TPR, VPT, EXACT, false>};
-}
-
-StepPair step_for(int precision, Shape s) {
-#define TBTKKPM_CASE(V, T, P, X) \
-  if (s.tpr == T && s.vpt == P) return pair<V, T, P, X>();
-  if (precision == TBTKKPM_FP64) {
-    TBTKKPM_CASE(double2, 1, 1, true)
-    TBTKKPM_CASE(double2, 2, 1, true)
-    TBTKKPM_CASE(double2, 4, 1, true)
-    TBTKKPM_CASE(double2, 8, 1, true)
-    TBTKKPM_CASE(double2, 16, 1, true)
-    TBTKKPM_CASE(double2, 32, 1, true)
-    TBTKKPM_CASE(double2, 32, 2, true)
-    TBTKKPM_CASE(double2, 32, 4, true)
+void step_table(int cls, const StepEntry **t, int *n) {
+  if (cls == kClassFP64) {
+    *t = kStepsFP64;
+    *n = kNumStepsFP64;
+  } else if (cls == kClassMixed) {
+    *t = kStepsMixed;
+    *n = kNumStepsMixed;
   } else {
-    TBTKKPM_CASE(float2, 1, 1, false)
-    TBTKKPM_CASE(float2, 2, 1, false)
-    TBTKKPM_CASE(float2, 4, 1, false)
-    TBTKKPM_CASE(float2, 4, 2, false)
-    TBTKKPM_CASE(float2, 8, 2, false)
-    TBTKKPM_CASE(float2, 16, 2, false)
-    TBTKKPM_CASE(float2, 32, 2, false)
-    TBTKKPM_CASE(float2, 32, 4, false)
-    TBTKKPM_CASE(float2, 32, 8, false)
+    *t = kStepsMixedDots;
+    *n = kNumStepsMixedDots;
   }
-#undef TBTKKPM_CASE
-  return {nullptr, nullptr};
+}
+
+const StepEntry *find_step(int cls, int tpr, int vpt, int minb) {
+  const StepEntry *t;
+  int n;
+  step_table(cls, &t, &n);
+  for (int i = 0; i < n; i++)
+    if (t[i].tpr == tpr && t[i].vpt == vpt && t[i].minb == minb) return &t[i];
+  return nullptr;
+}
+
+uint64_t tune_key(int cls, uint32_t Bp) { return ((uint64_t)cls << 32) | Bp; }
+
+// The configuration of a batch: a forced entry, the handle's tuned choice
+// for this (class, padded width), or the default shape with MINB 2.
+const StepEntry *pick_step(const tbtkkpm_matrix *m, int precision, bool dots, uint32_t B,
+                           const StepEntry *force) {
+  if (force) return force;
+  const int cls = step_class(precision, dots);
+  const Shape s = shape_for(precision, B);
+  auto it = m->tuned.find(tune_key(cls, s.bp()));
+  if (it != m->tuned.end()) {
+    const StepEntry *e = find_step(cls, it->second[0], it->second[1], it->second[2]);
+    if (e) return e;
+  }
+  return find_step(cls, s.tpr, s.vpt, 2);
 }
 
 // ------------------------------------------------------------ one batch
-// Runs the M-1 recursion steps of one batch and leaves the undamped moments
-// in ws.mu ([K][M]).  The to-indices (row, batch column, output slot) are
-// given sorted by row.
+// The to-indices of a batch (row, batch column, output slot), sorted by row.
 struct TargetList {
   std::vector<uint32_t> row, col, out;
 };
 
+// Runs the recursion of one batch and leaves the undamped moments in ws.mu
+// ([K][M]).  doubling: every source's only target is itself (an LDOS batch);
+// the recursion stops at j_{M/2} and the moments come from the doubling
+// identities, while the directly gathered moments of steps 0..M/2 land in
+// ws.mu_direct ([K][M/2+1]) for the error estimate.
 int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &from,
-              const TargetList &tl, uint32_t K, uint32_t M) {
+              const TargetList &tl, uint32_t K, uint32_t M, bool doubling,
+              const StepEntry *force = nullptr) {
   Workspace &ws = m->ws;
   cudaStream_t st = m->stream;
   const uint32_t B = (uint32_t)from.size();
-  const Shape s = shape_for(precision, B);
-  const uint32_t Bp = s.bp();
-  const StepPair fn = step_for(precision, s);
-  if (!fn.first) return fail(TBTKKPM_ERR_UNSUPPORTED, "no recursion kernel for batch %u", B);
-  const size_t esize = precision == TBTKKPM_FP64 ? sizeof(double2) : sizeof(float2);
+  const StepEntry *fn = pick_step(m, precision, doubling, B, force);
+  if (!fn) return fail(TBTKKPM_ERR_UNSUPPORTED, "no recursion kernel for batch %u", B);
+  const uint32_t Bp = (uint32_t)(fn->tpr * fn->vpt);
+  if (Bp < B) return fail(TBTKKPM_ERR_ARGUMENT, "configuration of %u columns for %u sources", Bp, B);
+  const size_t esize = is_mixed(precision) ? sizeof(float2) : sizeof(double2);
   const size_t vbytes = (size_t)m->N * Bp * esize;
   const size_t words = ((size_t)m->N + 31) / 32;
   const uint32_t T = (uint32_t)tl.row.size();
+  const uint32_t steps = doubling ? M / 2 : (M >= 2 ? M - 1 : 0);  // last j index computed
+  const uint32_t ld_direct = doubling ? steps + 1 : M;
+  const unsigned max_grid = (unsigned)sm_count(m->device) * 8;
   int rc;
   if ((rc = ws.vec[0].reserve(vbytes)) || (rc = ws.vec[1].reserve(vbytes)) ||
       (rc = ws.bitmap.reserve(4 * words)) || (rc = ws.tgt.reserve(12 * std::max(T, 1u))) ||
       (rc = ws.from.reserve(4 * std::max(B, 1u))) ||
       (rc = ws.mu.reserve(sizeof(double2) * (size_t)std::max(K, 1u) * M)))
+    return rc;
+  if (doubling &&
+      ((rc = ws.mu_direct.reserve(sizeof(double2) * (size_t)std::max(K, 1u) * ld_direct)) ||
+       (rc = ws.dots.reserve(sizeof(double2) * 2 * (size_t)Bp * max_grid)) ||
+       (rc = ws.col_out.reserve(4 * (size_t)Bp))))
     return rc;
   std::vector<uint32_t> bitmap(words, 0u);
   for (uint32_t r : tl.row) bitmap[r >> 5] |= 1u << (r & 31);
@@ -141,37 +152,68 @@ int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &fro
       (e = cudaMemsetAsync(ws.vec[1].ptr, 0, vbytes, st)) ||
       (e = cudaMemsetAsync(ws.mu.ptr, 0, sizeof(double2) * (size_t)K * M, st)))
     return cuda_fail(e, "recursion: staging");
+  if (doubling) {
+    std::vector<uint32_t> col_out(Bp, kPad);
+    for (uint32_t i = 0; i < T; i++) col_out[tl.col[i]] = tl.out[i];
+    if ((e = cudaMemcpyAsync(ws.col_out.ptr, col_out.data(), 4 * (size_t)Bp,
+                             cudaMemcpyHostToDevice, st)) ||
+        (e = cudaMemsetAsync(ws.mu_direct.ptr, 0, sizeof(double2) * (size_t)K * ld_direct, st)))
+      return cuda_fail(e, "recursion: staging");
+  }
   Targets tg;
   tg.bitmap = ws.bitmap.as<uint32_t>();
   tg.row = ws.tgt.as<uint32_t>();
   tg.col = ws.tgt.as<uint32_t>() + T;
   tg.out = ws.tgt.as<uint32_t>() + 2 * (size_t)T;
   tg.count = T;
-  tg.mu = ws.mu.as<double2>();
-  tg.M = M;
+  tg.mu = doubling ? ws.mu_direct.as<double2>() : ws.mu.as<double2>();
+  tg.ld = ld_direct;
   const unsigned ib = blocks_for(std::max(B, T));
-  if (precision == TBTKKPM_FP64)
-    kpm_init_sources<double2><<<ib, 256, 0, st>>>(B, Bp, ws.from.as<uint32_t>(),
-                                                 ws.vec[0].as<double2>(), tg);
-  else
+  if (is_mixed(precision))
     kpm_init_sources<float2><<<ib, 256, 0, st>>>(B, Bp, ws.from.as<uint32_t>(),
                                                 ws.vec[0].as<float2>(), tg);
-  const unsigned grid = blocks_for((uint64_t)m->N * s.tpr);
-  const uint32_t *rp = m->rowptr.as<uint32_t>();
-  const uint32_t *cl = m->col.as<uint32_t>();
-  const double2 *vl = m->val2.as<double2>();
+  else
+    kpm_init_sources<double2><<<ib, 256, 0, st>>>(B, Bp, ws.from.as<uint32_t>(),
+                                                 ws.vec[0].as<double2>(), tg);
+  StepArgs a;
+  a.A.slice_ptr = m->slice_ptr.as<uint32_t>();
+  a.A.col = m->scol.as<uint32_t>();
+  a.A.val = m->sval.as<double2>();
+  a.A.N = m->N;
+  a.A.nslices = m->nslices;
+  a.Bp = Bp;
+  a.tg = tg;
+  a.dots = doubling ? ws.dots.as<double2>() : nullptr;
   void *cur = ws.vec[0].ptr, *prev = ws.vec[1].ptr;
   m->timer.mark(st, 0);
   m->timer.pending = m->timer.enabled;
-  m->timer.pending_steps = M >= 2 ? M - 1 : 0;
-  count_launches(1 + (M >= 2 ? M - 1 : 0));
-  if (M >= 2) {
-    fn.first(grid, st, m->N, Bp, rp, cl, vl, cur, prev, tg, 1);
-    std::swap(cur, prev);  // cur = j1, prev = j0
-    for (uint32_t n = 2; n < M; n++) {
-      fn.rest(grid, st, m->N, Bp, rp, cl, vl, cur, prev, tg, n);
-      std::swap(cur, prev);
+  m->timer.pending_steps = steps;
+  count_launches(1 + (uint64_t)steps * (doubling ? 2 : 1));
+  for (uint32_t n = 1; n <= steps; n++) {
+    a.x = cur;
+    a.y = prev;
+    a.n_out = n;
+    unsigned grid = 0;
+    (n == 1 ? fn->first : fn->rest)(st, m->device, max_grid, a, &grid);
+    std::swap(cur, prev);
+    if (doubling) {
+      if (n == 1) {
+        // mu_0 and mu_1 of the direct gather seed the doubling identities
+        e = cudaMemcpy2DAsync(ws.mu.ptr, sizeof(double2) * M, ws.mu_direct.ptr,
+                              sizeof(double2) * ld_direct, sizeof(double2) * std::min(M, 2u),
+                              K, cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return cuda_fail(e, "recursion: seed moments");
+      }
+      kpm_dots_finalize<<<Bp, kFinalizeBlock, 0, st>>>(Bp, grid, ws.dots.as<double2>(),
+                                                              ws.col_out.as<uint32_t>(),
+                                                              ws.mu.as<double2>(), M, M, n);
     }
+  }
+  if (doubling && steps == 0) {
+    e = cudaMemcpy2DAsync(ws.mu.ptr, sizeof(double2) * M, ws.mu_direct.ptr,
+                          sizeof(double2) * ld_direct, sizeof(double2), K,
+                          cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return cuda_fail(e, "recursion: seed moments");
   }
   m->timer.mark(st, 1);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "recursion: launch");
@@ -188,10 +230,31 @@ void damping_factors(uint32_t M, double broadening, std::vector<double> &a, doub
 }
 
 int check_precision(int precision) {
-  if (precision != TBTKKPM_FP64 && precision != TBTKKPM_MIXED)
-    return fail(TBTKKPM_ERR_ARGUMENT, "precision %d is neither TBTKKPM_FP64 nor TBTKKPM_MIXED",
+  if (precision != TBTKKPM_FP64 && precision != TBTKKPM_MIXED && precision != TBTKKPM_MIXED_DIRECT)
+    return fail(TBTKKPM_ERR_ARGUMENT,
+                "precision %d is none of TBTKKPM_FP64, TBTKKPM_MIXED, TBTKKPM_MIXED_DIRECT",
                 precision);
   return TBTKKPM_OK;
+}
+
+// Error estimate of a doubling run for each output slot: the largest
+// difference between the directly gathered moments (n <= M/2) and the
+// doubling moments of the same n, relative to max |mu|, scaled by sqrt(2)
+// for the moments past M/2 and by a safety factor of 4.
+void doubling_error(const std::vector<double2> &mu, const std::vector<double2> &direct,
+                    uint32_t K, uint32_t M, uint32_t ld, double *err) {
+  for (uint32_t k = 0; k < K; k++) {
+    double dmax = 0, scale = 0;
+    for (uint32_t n = 0; n < M; n++) {
+      const double2 v = mu[(size_t)k * M + n];
+      scale = std::max(scale, std::hypot(v.x, v.y));
+    }
+    for (uint32_t n = 2; n < std::min(ld, M); n++) {
+      const double2 a = mu[(size_t)k * M + n], b = direct[(size_t)k * ld + n];
+      dmax = std::max(dmax, std::hypot(a.x - b.x, a.y - b.y));
+    }
+    err[k] = scale > 0 ? 4.0 * std::sqrt(2.0) * dmax / scale : 0.0;
+  }
 }
 
 }  // namespace
@@ -202,7 +265,7 @@ int check_precision(int precision) {
 static int moments_host(tbtkkpm_matrix *m, const uint32_t *from, uint32_t B, const uint32_t *to,
                         const uint32_t *owner, uint32_t K, uint32_t M, int precision,
                         double *mu_out) {
-  const uint32_t maxb = precision == TBTKKPM_FP64 ? kMaxBatchFP64 : kMaxBatchMixed;
+  const uint32_t maxb = is_mixed(precision) ? kMaxBatchMixed : kMaxBatchFP64;
   std::vector<std::vector<uint32_t>> by_owner(B);
   for (uint32_t k = 0; k < K; k++) by_owner[owner[k]].push_back(k);
   std::vector<double2> mu_host;
@@ -228,7 +291,7 @@ static int moments_host(tbtkkpm_matrix *m, const uint32_t *from, uint32_t B, con
       tl.out.push_back(it[2]);
     }
     const uint32_t Kb = (uint32_t)global_k.size();
-    int rc = run_batch(m, precision, fr, tl, Kb, M);
+    int rc = run_batch(m, precision, fr, tl, Kb, M, false);
     if (rc) return rc;
     mu_host.resize((size_t)Kb * M);
     m->timer.mark(m->stream, 2);
@@ -316,7 +379,7 @@ extern "C" int tbtkkpm_moments_batched(tbtkkpm_matrix *m, const uint32_t *from, 
   if (rc) return rc;
   damp_host(K, M, broadening, mu_out);
   if (err_out)
-    for (uint32_t k = 0; k < K; k++) err_out[k] = precision == TBTKKPM_FP64 ? 0.0 : -1.0;
+    for (uint32_t k = 0; k < K; k++) err_out[k] = is_mixed(precision) ? -1.0 : 0.0;
   return TBTKKPM_OK;
 }
 
@@ -502,7 +565,8 @@ extern "C" int tbtkkpm_ldos_sites(tbtkkpm_matrix *m, tbtkkpm_table *t, const uin
     return fail(TBTKKPM_ERR_ARGUMENT, "ldos_sites: matrix and table live on different devices");
   std::lock_guard<std::mutex> lk(m->lock);
   DeviceGuard g(m->device);
-  const uint32_t maxb = precision == TBTKKPM_FP64 ? kMaxBatchFP64 : kMaxBatchMixed;
+  const uint32_t maxb = is_mixed(precision) ? kMaxBatchMixed : kMaxBatchFP64;
+  const bool doubling = precision == TBTKKPM_MIXED;
   std::vector<double> a;
   double b = 1;
   const bool damp = broadening != 0;
@@ -517,6 +581,7 @@ extern "C" int tbtkkpm_ldos_sites(tbtkkpm_matrix *m, tbtkkpm_table *t, const uin
     return cuda_fail(e, "ldos_sites: damping upload");
   // Table reads happen on the matrix stream; order them after the table's own work.
   cudaStreamSynchronize(t->stream);
+  std::vector<double2> mu_h, direct_h;
   for (uint32_t b0 = 0; b0 < B; b0 += maxb) {
     const uint32_t nb = std::min(maxb, B - b0);
     std::vector<uint32_t> fr(sites + b0, sites + b0 + nb);
@@ -532,7 +597,27 @@ extern "C" int tbtkkpm_ldos_sites(tbtkkpm_matrix *m, tbtkkpm_table *t, const uin
       tl.col.push_back(it[1]);
       tl.out.push_back(it[1]);
     }
-    if ((rc = run_batch(m, precision, fr, tl, nb, M))) return rc;
+    if ((rc = run_batch(m, precision, fr, tl, nb, M, doubling))) return rc;
+    const uint32_t ld = M / 2 + 1;
+    if (doubling && err_out) {
+      // undamped moments for the estimate
+      mu_h.resize((size_t)nb * M);
+      direct_h.resize((size_t)nb * ld);
+      cudaMemcpyAsync(mu_h.data(), ws.mu.ptr, sizeof(double2) * nb * M, cudaMemcpyDeviceToHost,
+                      m->stream);
+      cudaMemcpyAsync(direct_h.data(), ws.mu_direct.ptr, sizeof(double2) * nb * ld,
+                      cudaMemcpyDeviceToHost, m->stream);
+    }
+    if (doubling) {
+      // Moments n <= M/2 were gathered directly as well; those carry less
+      // rounding than the dot-product identities, so they replace the
+      // doubled values, which remain only past M/2 where the damping
+      // sinh(lambda(1-n/M))/sinh(lambda) shrinks their weight.
+      e = cudaMemcpy2DAsync(ws.mu.ptr, sizeof(double2) * M, ws.mu_direct.ptr,
+                            sizeof(double2) * ld, sizeof(double2) * std::min(ld, M), nb,
+                            cudaMemcpyDeviceToDevice, m->stream);
+      if (e != cudaSuccess) return cuda_fail(e, "ldos_sites: direct moments");
+    }
     m->timer.mark(m->stream, 2);
     if (damp) {
       kpm_damp<<<blocks_for((uint64_t)nb * M), 256, 0, m->stream>>>(nb, M, ws.damp.as<double>(), b,
@@ -544,13 +629,112 @@ extern "C" int tbtkkpm_ldos_sites(tbtkkpm_matrix *m, tbtkkpm_table *t, const uin
     e = cudaMemcpyAsync(ldos_out + (size_t)b0 * E, ws.out.ptr, sizeof(double) * (size_t)nb * E,
                         cudaMemcpyDeviceToHost, m->stream);
     if (e != cudaSuccess) return cuda_fail(e, "ldos_sites: download");
-    if (m->timer.enabled) {
+    if (m->timer.enabled || (doubling && err_out)) {
       if ((e = cudaStreamSynchronize(m->stream)) != cudaSuccess) return cuda_fail(e, "ldos_sites");
       m->timer.collect();
     }
+    if (err_out) {
+      if (doubling)
+        doubling_error(mu_h, direct_h, nb, M, ld, err_out + b0);
+      else
+        for (uint32_t i = 0; i < nb; i++) err_out[b0 + i] = is_mixed(precision) ? -1.0 : 0.0;
+    }
   }
   if ((e = cudaStreamSynchronize(m->stream)) != cudaSuccess) return cuda_fail(e, "ldos_sites");
-  if (err_out)
-    for (uint32_t i = 0; i < B; i++) err_out[i] = precision == TBTKKPM_FP64 ? 0.0 : -1.0;
+  return TBTKKPM_OK;
+}
+
+// ---------------------------------------------------------------- autotuner
+// Times every compiled step configuration whose padded width serves B
+// sources on this matrix (probe_steps steps each, best of two runs, CUDA
+// events on the handle's stream around the steps) and keeps the fastest for
+// later batches of that width on this handle.
+extern "C" int tbtkkpm_matrix_autotune(tbtkkpm_matrix *m, uint32_t B, int precision, int ldos,
+                                       uint32_t probe_steps, int *tpr, int *vpt, int *minb,
+                                       double *ms_per_step) {
+  int rc = check_precision(precision);
+  if (rc) return rc;
+  if (!m) return fail(TBTKKPM_ERR_ARGUMENT, "matrix_autotune: NULL matrix");
+  const uint32_t maxb = is_mixed(precision) ? kMaxBatchMixed : kMaxBatchFP64;
+  if (B == 0 || B > maxb || B > m->N)
+    return fail(TBTKKPM_ERR_ARGUMENT, "matrix_autotune: batch %u outside [1, %u]", B,
+                std::min(maxb, m->N));
+  if (probe_steps == 0) return fail(TBTKKPM_ERR_ARGUMENT, "matrix_autotune: probe_steps is 0");
+  std::lock_guard<std::mutex> lk(m->lock);
+  DeviceGuard g(m->device);
+  const bool doubling = ldos && precision == TBTKKPM_MIXED;
+  const int cls = step_class(precision, doubling);
+  const uint32_t Bp = shape_for(precision, B).bp();
+  const uint32_t M = doubling ? 2 * probe_steps : probe_steps + 1;
+  std::vector<uint32_t> fr(B);
+  for (uint32_t b = 0; b < B; b++) fr[b] = (uint32_t)((uint64_t)b * m->N / B);
+  TargetList tl;
+  for (uint32_t b = 0; b < B; b++) {
+    tl.row.push_back(fr[b]);
+    tl.col.push_back(b);
+    tl.out.push_back(b);
+  }
+  PhaseTimer saved = m->timer;
+  if ((rc = m->timer.enable(true))) return rc;
+  const StepEntry *t;
+  int n;
+  step_table(cls, &t, &n);
+  const StepEntry *best = nullptr;
+  double best_ms = 0;
+  for (int i = 0; i < n; i++) {
+    if ((uint32_t)(t[i].tpr * t[i].vpt) != Bp) continue;
+    double ms = 0;
+    for (int rep = 0; rep < 2; rep++) {
+      m->timer.recursion_ms = 0;
+      if ((rc = run_batch(m, precision, fr, tl, B, M, doubling, &t[i]))) break;
+      cudaError_t e = cudaStreamSynchronize(m->stream);
+      if (e != cudaSuccess) {
+        rc = cuda_fail(e, "matrix_autotune");
+        break;
+      }
+      m->timer.collect();
+      const double v = m->timer.recursion_ms / probe_steps;
+      ms = rep == 0 ? v : std::min(ms, v);
+    }
+    if (rc) break;
+    if (!best || ms < best_ms) {
+      best = &t[i];
+      best_ms = ms;
+    }
+  }
+  const bool created = saved.ev[0] == nullptr;
+  if (created) m->timer.destroy();
+  else {
+    m->timer.enabled = saved.enabled;
+    m->timer.recursion_ms = saved.recursion_ms;
+    m->timer.energy_ms = saved.energy_ms;
+    m->timer.step_launches = saved.step_launches;
+    m->timer.pending = false;
+  }
+  if (rc) return rc;
+  if (!best) return fail(TBTKKPM_ERR_UNSUPPORTED, "matrix_autotune: no configuration for %u", B);
+  m->tuned[tune_key(cls, Bp)] = {best->tpr, best->vpt, best->minb};
+  if (tpr) *tpr = best->tpr;
+  if (vpt) *vpt = best->vpt;
+  if (minb) *minb = best->minb;
+  if (ms_per_step) *ms_per_step = best_ms;
+  return TBTKKPM_OK;
+}
+
+// Records a configuration for batches of B sources without timing (a
+// cached autotuner result).
+extern "C" int tbtkkpm_matrix_set_config(tbtkkpm_matrix *m, uint32_t B, int precision, int ldos,
+                                         int tpr, int vpt, int minb) {
+  int rc = check_precision(precision);
+  if (rc) return rc;
+  if (!m) return fail(TBTKKPM_ERR_ARGUMENT, "matrix_set_config: NULL matrix");
+  const bool doubling = ldos && precision == TBTKKPM_MIXED;
+  const int cls = step_class(precision, doubling);
+  const uint32_t Bp = shape_for(precision, std::max(B, 1u)).bp();
+  if ((uint32_t)(tpr * vpt) != Bp || !find_step(cls, tpr, vpt, minb))
+    return fail(TBTKKPM_ERR_ARGUMENT, "matrix_set_config: no compiled configuration %d x %d / %d "
+                "for %u columns", tpr, vpt, minb, Bp);
+  std::lock_guard<std::mutex> lk(m->lock);
+  m->tuned[tune_key(cls, Bp)] = {tpr, vpt, minb};
   return TBTKKPM_OK;
 }

@@ -38,7 +38,7 @@ ERR_UNSUPPORTED = -5
 ERR_STATE = -6
 
 ADVANCED, RETARDED, PRINCIPAL, NONPRINCIPAL = 0, 1, 2, 3
-FP64, MIXED = 0, 1
+FP64, MIXED, MIXED_DIRECT = 0, 1, 2
 
 _TYPES = {"Advanced": ADVANCED, "Retarded": RETARDED, "Principal": PRINCIPAL,
           "NonPrincipal": NONPRINCIPAL}
@@ -81,7 +81,34 @@ SIGNATURES = [
     ("tbtkkpm_greens", _i, [_p, _p, _u32, _i, _p]),
     ("tbtkkpm_ldos", _i, [_p, _p, _u32, _p]),
     ("tbtkkpm_ldos_sites", _i, [_p, _p, _p, _u32, _d, _i, _p, _p]),
+    ("tbtkkpm_matrix_autotune", _i, [_p, _u32, _i, _i, _u32, _p, _p, _p, _p]),
+    ("tbtkkpm_matrix_set_config", _i, [_p, _u32, _i, _i, _i, _i, _i]),
 ]
+
+# Step-kernel configurations compiled into the library, per kernel class:
+# (threads per row, complex values per thread); each with register caps
+# (min blocks per SM) 2, 3 and 4.
+CONFIGS_FP64 = [(1, 1), (2, 1), (4, 1), (8, 1), (16, 1), (32, 1), (16, 2), (32, 2), (16, 4),
+                (32, 4)]
+CONFIGS_MIXED = [(1, 1), (2, 1), (4, 1), (4, 2), (8, 2), (16, 2), (8, 4), (32, 2), (16, 4),
+                 (8, 8), (32, 4), (16, 8), (32, 8)]
+MINBS = (2, 3, 4)
+
+
+def padded_width(B, precision):
+    """Batch columns the library allocates for B sources."""
+    widths = [1, 2, 4, 8, 16, 32, 64, 128] + ([256] if precision != FP64 else [])
+    for w in widths:
+        if B <= w:
+            return w
+    raise TBTKError(ERR_ARGUMENT, f"batch of {B} exceeds one launch")
+
+
+def configs_for(B, precision):
+    """All compiled (tpr, vpt, minb) serving batches of B sources."""
+    w = padded_width(B, precision)
+    shapes = CONFIGS_FP64 if precision == FP64 else CONFIGS_MIXED
+    return [(t, v, mb) for (t, v) in shapes if t * v == w for mb in MINBS]
 
 _lib = None
 
@@ -191,6 +218,23 @@ class Matrix:
         e.g. ``torch.cuda.current_stream().cuda_stream``; 0/None restores
         the handle's own stream)."""
         _check(load_library().tbtkkpm_matrix_set_stream(self._h, cuda_stream or None))
+
+    def autotune(self, B, precision, ldos=True, probe_steps=8):
+        """Times the compiled step configurations for batches of B sources
+        and keeps the fastest on this handle; returns (tpr, vpt, minb,
+        ms per step)."""
+        t = ctypes.c_int()
+        v = ctypes.c_int()
+        mb = ctypes.c_int()
+        ms = ctypes.c_double()
+        _check(load_library().tbtkkpm_matrix_autotune(
+            self._h, int(B), int(precision), int(bool(ldos)), int(probe_steps),
+            ctypes.byref(t), ctypes.byref(v), ctypes.byref(mb), ctypes.byref(ms)))
+        return t.value, v.value, mb.value, ms.value
+
+    def set_config(self, B, precision, tpr, vpt, minb, ldos=True):
+        _check(load_library().tbtkkpm_matrix_set_config(
+            self._h, int(B), int(precision), int(bool(ldos)), int(tpr), int(vpt), int(minb)))
 
     def set_profiling(self, enable=True):
         _check(load_library().tbtkkpm_matrix_set_profiling(self._h, int(enable)))
@@ -382,7 +426,7 @@ class ChebyshevExpander:
             self._table = None
 
     def setPrecision(self, precision):
-        if precision not in (FP64, MIXED):
+        if precision not in (FP64, MIXED, MIXED_DIRECT):
             raise TBTKError(ERR_ARGUMENT, f"unknown precision {precision}")
         self.precision = precision
 

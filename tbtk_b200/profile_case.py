@@ -1,0 +1,81 @@
+"""One small LDOS batch of the KPM path, for profiler captures and sweeps.
+
+    python -m tbtk_b200.profile_case --lattice 2048 --sites 1 --precision fp64 --moments 8
+    python -m tbtk_b200.profile_case --lattice 2048 --sites 64 --sweep --moments 32
+
+Builds the periodic square lattice with spin (L x L x 2 states, t=1, J=0.5,
+disorder U[-1, 1]; Rashba spin-orbit with --rashba), a device lookup table
+of --moments coefficients over --energies points, and runs
+tbtkkpm_ldos_sites for --sites seeded sites.  Prints the device time of the
+recursion (CUDA events on the handle's stream) and its bandwidth in
+algorithmic bytes (matrix once per step plus three vector passes per
+source).  --sweep times every compiled step configuration for the batch;
+--autotune lets the library's autotuner choose first; --config T,V,MB forces
+one.
+"""
+from __future__ import annotations
+
+import argparse
+import time
+
+from tbtk_b200 import kpm, workloads
+
+
+def step_bytes(N, nnz, B, s_vec):
+    return nnz * 20 + 4 * (N + 1) + 3 * N * B * s_vec
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--lattice", type=int, default=1024)
+    ap.add_argument("--sites", type=int, default=64)
+    ap.add_argument("--precision", choices=["fp64", "mixed", "mixed_direct"], default="mixed")
+    ap.add_argument("--moments", type=int, default=8)
+    ap.add_argument("--energies", type=int, default=256)
+    ap.add_argument("--rashba", type=float, default=0.0)
+    ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--sweep", action="store_true")
+    ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--config", default=None)
+    a = ap.parse_args()
+    prec = {"fp64": kpm.FP64, "mixed": kpm.MIXED, "mixed_direct": kpm.MIXED_DIRECT}[a.precision]
+    rowptr, col, val = workloads.square_csr(a.lattice, a.lattice, t=1.0, J=0.5, W=2.0,
+                                            alpha=a.rashba, seed=a.lattice)
+    N, nnz = rowptr.size - 1, int(rowptr[-1])
+    sites = workloads.sample_sites(a.lattice * a.lattice, 2, a.sites, 1 + a.lattice)
+    mat = kpm.Matrix.from_csr(rowptr, col, val, 12.0)
+    tab = kpm.Table.create(a.moments, workloads.open_grid(12.0, a.energies), 12.0)
+    mat.set_profiling(True)
+    s_vec = 16 if prec == kpm.FP64 else 8
+    bstep = step_bytes(N, nnz, a.sites, s_vec)
+
+    def run(label):
+        for _ in range(a.repeat):
+            t0 = time.perf_counter()
+            mat.ldos_sites(tab, sites, 1e-3, prec)
+            wall = time.perf_counter() - t0
+            rec, en, steps = mat.profile()
+            ms = rec / max(steps, 1)
+            print(f"{label} N={N} nnz={nnz} B={a.sites} {a.precision} M={a.moments}: "
+                  f"recursion {rec:.3f} ms / {steps} steps = {ms:.4f} ms/step "
+                  f"({bstep / ms / 1e6:.0f} GB/s algorithmic), energy {en:.3f} ms, "
+                  f"wall {wall * 1e3:.1f} ms", flush=True)
+
+    if a.config:
+        t, v, mb = (int(x) for x in a.config.split(","))
+        mat.set_config(a.sites, prec, t, v, mb)
+    if a.autotune:
+        t, v, mb, ms = mat.autotune(a.sites, prec, ldos=True, probe_steps=8)
+        print(f"autotune: tpr={t} vpt={v} minb={mb} {ms:.4f} ms/step", flush=True)
+    if a.sweep:
+        for (t, v, mb) in kpm.configs_for(a.sites, prec):
+            mat.set_config(a.sites, prec, t, v, mb)
+            mat.ldos_sites(tab, sites, 1e-3, prec)  # warm
+            mat.profile()
+            run(f"[tpr={t} vpt={v} minb={mb}]")
+    else:
+        run("")
+
+
+if __name__ == "__main__":
+    main()

@@ -145,8 +145,11 @@ def test_device_table_close_to_host_table(gpu, oracle):
     for j, n in enumerate((0, 1, M - 1)):
         eye[j, n] = 1
     got = dev.greens(eye, gpu.RETARDED)
+    # CUDA's acos and glibc's may differ by an ulp; exp(-i n acos x) carries
+    # that difference times n, so the bound grows with the coefficient index.
+    eps = np.finfo(np.float64).eps
     for j, n in enumerate((0, 1, M - 1)):
-        assert rel_err(got[j], host[n]) <= 1e-13
+        assert rel_err(got[j], host[n]) <= 4 * max(n, 1) * eps + 4 * eps
 
 
 @pytest.mark.parametrize("name", MODEL_CASES)
@@ -175,6 +178,80 @@ def test_ldos_sites_mixed(gpu, name):
     ldos, _ = m.ldos_sites(dev, g["ldos_sites"], float(g["broadening"]), gpu.MIXED)
     for k in range(ldos.shape[0]):
         assert rel_err(ldos[k], g["ldos"][k]) <= 1e-6, rel_err(ldos[k], g["ldos"][k])
+
+
+@pytest.mark.parametrize("name", MODEL_CASES)
+def test_ldos_sites_mixed_direct(gpu, name):
+    """complex64 vectors with every moment gathered directly (no doubling)."""
+    g = golden(name)
+    lo, hi, E = g["window"]
+    energies = gpu.tbtk_range(lo, hi, int(E))
+    s, M = float(g["scale"]), int(g["M"])
+    m = gpu.Matrix.from_csr(g["rowptr"], g["col"], g["val"], s)
+    dev = gpu.Table.create(M, energies, s)
+    ldos, err = m.ldos_sites(dev, g["ldos_sites"], float(g["broadening"]), gpu.MIXED_DIRECT)
+    assert np.all(err == -1.0)
+    for k in range(ldos.shape[0]):
+        assert rel_err(ldos[k], g["ldos"][k]) <= 1e-6, rel_err(ldos[k], g["ldos"][k])
+
+
+@pytest.mark.parametrize("M", [1, 2, 3, 4, 5, 64, 257])
+def test_doubling_moment_counts(gpu, M):
+    """The doubling schedule covers every moment for odd and even M."""
+    lat = L.square(7, 6, t=1.0, J=0.5, W=1.5, alpha=0.2, periodic=True, seed=12)
+    rowptr, col, val = lat.csr()
+    s = 12.0
+    sites = L.random_sites(lat, 5, seed=M)
+    energies = gpu.tbtk_range(-11.0, 11.0, 64)
+    m = gpu.Matrix.from_csr(rowptr, col, val, s)
+    t = gpu.Table.create(M, energies, s)
+    ref, _ = m.ldos_sites(t, sites, 1e-3, gpu.FP64)
+    got, err = m.ldos_sites(t, sites, 1e-3, gpu.MIXED)
+    for k in range(sites.size):
+        assert rel_err(got[k], ref[k]) <= 1e-6, (M, k, rel_err(got[k], ref[k]))
+    assert np.all(err >= 0)
+
+
+def test_doubling_error_estimate(gpu):
+    """On a disordered Rashba lattice at M=2048 the doubling LDOS stays within
+    1e-6 of the FP64 recursion and the per-site estimate is small and
+    non-negative."""
+    lat = L.square(40, 40, t=1.0, J=0.5, W=2.0, alpha=0.3, periodic=True, seed=21)
+    rowptr, col, val = lat.csr()
+    s, M = 12.0, 2048
+    sites = L.random_sites(lat, 24, seed=5)
+    energies = gpu.tbtk_range(-12.0, 12.0, 500, False, False)
+    m = gpu.Matrix.from_csr(rowptr, col, val, s)
+    t = gpu.Table.create(M, energies, s)
+    ref, _ = m.ldos_sites(t, sites, 1e-3, gpu.FP64)
+    got, err = m.ldos_sites(t, sites, 1e-3, gpu.MIXED)
+    errs = [rel_err(got[k], ref[k]) for k in range(sites.size)]
+    assert max(errs) <= 1e-6, max(errs)
+    assert np.all(err >= 0) and np.all(err < 1e-4), err
+
+
+def test_every_config_same_result(gpu, oracle):
+    """Every compiled step configuration of a batch width gives the same
+    FP64 moments (bit for bit) and the autotuner picks one of them."""
+    lat = L.square(11, 9, t=1.0, J=0.5, W=2.0, alpha=0.25, periodic=True, seed=31)
+    rowptr, col, val = lat.csr()
+    s, M = 12.0, 40
+    frm = L.random_sites(lat, 40, seed=2)
+    ref = None
+    for (t, v, mb) in gpu.configs_for(40, gpu.FP64):
+        m = gpu.Matrix.from_csr(rowptr, col, val, s)
+        m.set_config(40, gpu.FP64, t, v, mb, ldos=False)
+        mu, _ = m.moments_batched(frm, frm, np.arange(40), M, 0.0, gpu.FP64)
+        if ref is None:
+            ref = mu
+            o = oracle.moments(rowptr, col, val, s, M, int(frm[7]), [int(frm[7])])
+            assert np.array_equal(mu[7], o[0])
+        assert np.array_equal(mu, ref), (t, v, mb)
+    m = gpu.Matrix.from_csr(rowptr, col, val, s)
+    t, v, mb, ms = m.autotune(40, gpu.MIXED, ldos=True, probe_steps=4)
+    assert (t, v, mb) in gpu.configs_for(40, gpu.MIXED) and ms > 0
+    with pytest.raises(gpu.TBTKError):
+        m.set_config(40, gpu.MIXED, 32, 1, 2)
 
 
 def test_ring_ldos_integral(gpu):
