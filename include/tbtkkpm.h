@@ -204,6 +204,14 @@ TBTKKPM_API int tbtkkpm_matrix_set_config(
 	tbtkkpm_matrix *m, uint32_t B, int precision, int ldos, int tpr, int vpt,
 	int minb);
 
+/* Lists the compiled step configurations of the kernels a call at this
+ * precision uses as (tpr, vpt, variant) triples into out[3*cap]; returns
+ * their number (-1 for an unknown precision).  variant 2..4 is the register
+ * cap (min blocks per SM) of a register-staged kernel; 100 + 10*S + W is a
+ * bulk-copy kernel with a ring of S stages per warp and W warps per block.
+ * (No reference counterpart.) */
+TBTKKPM_API int tbtkkpm_step_configs(int precision, int ldos, int *out, int cap);
+
 /* LDOS at B sites in one call: the moments <site|T_n|site> of all sites run
  * as one batched recursion, are damped and summed over the table's energy
  * grid on the device; only the [B][E] result crosses to the host.

@@ -1,0 +1,64 @@
+"""Writes the instantiation lists of the recursion-step kernels.
+
+    python tbtk_b200/csrc/gen_steps.py
+
+Each listed configuration (threads per row, complex values per thread,
+register cap as min blocks per SM) is compiled into libtbtkkpm.so; the
+driver's defaults and the autotuner choose among them.  Keep the shape lists
+in step with CONFIGS_FP64 / CONFIGS_MIXED in tbtk_b200/kpm.py.
+"""
+import pathlib
+
+HERE = pathlib.Path(__file__).resolve().parent
+
+SHAPES_FP64 = [(1, 1), (2, 1), (4, 1), (8, 1), (16, 1), (32, 1), (16, 2), (32, 2), (16, 4), (32, 4)]
+SHAPES_MIXED = [(1, 1), (2, 1), (4, 1), (4, 2), (8, 2), (16, 2), (8, 4), (32, 2), (16, 4), (8, 8),
+                (32, 4), (16, 8), (32, 8)]
+MINBS = [1, 2, 3, 4]
+
+UNITS = [
+    ("steps_fp64.cu", "kStepsFP64", "kClassFP64", "double2", "Exact64", "false", SHAPES_FP64,
+     "Recursion steps on complex128 vectors in the reference operation order."),
+    ("steps_mixed.cu", "kStepsMixed", "kClassMixed", "float2", "Wide64", "false", SHAPES_MIXED,
+     "Recursion steps on complex64 vectors with FP64 arithmetic."),
+    ("steps_mixed_dots.cu", "kStepsMixedDots", "kClassMixedDots", "float2", "Wide64", "true",
+     SHAPES_MIXED,
+     "Recursion steps on complex64 vectors with the FP64 doubling dot products."),
+]
+
+
+# Bulk-copy kernels (one warp per row, a ring of S stages per warp, WPB
+# warps per block): complex values per lane and (S, WPB) variants that fit
+# the 227 KB of shared memory a block may use.
+BULK_VPT = {"double2": [1, 2, 4], "float2": [1, 2, 4, 8]}
+BULK_VARIANTS = [(2, 2), (3, 2), (2, 4), (3, 4), (4, 4), (2, 8), (3, 8)]
+SMEM_LIMIT = 227 * 1024
+STAGE_META = 384  # StageMeta rounded up to 128 B (kpm_bulk.cuh)
+WMAX = 12
+
+
+def bulk_smem(V, vpt, s, wpb, dots):
+    size = {"double2": 16, "float2": 8}[V]
+    stage = STAGE_META + (WMAX + 1) * 32 * vpt * size
+    return s * wpb * stage + (wpb * 32 * 2 * 16 if dots == "true" else 0)
+
+
+def main():
+    for fname, table, cls, V, AR, dots, shapes, doc in UNITS:
+        lines = [f"// {doc}", "// Written by gen_steps.py: every configuration the driver and the",
+                 "// autotuner can pick.", '#include "kpm_steps.cuh"', "", "namespace tbtkkpm {", "",
+                 f"const StepEntry {table}[] = {{"]
+        for (t, p) in shapes:
+            for mb in MINBS:
+                lines.append(f"    TBTKKPM_STEP_ENTRY({cls}, {V}, {AR}, {t}, {p}, {dots}, {mb}),")
+        for p in BULK_VPT[V]:
+            for (s, wpb) in BULK_VARIANTS:
+                if bulk_smem(V, p, s, wpb, dots) <= SMEM_LIMIT:
+                    lines.append(f"    TBTKKPM_BULK_ENTRY({cls}, {V}, {AR}, {p}, {dots}, {s}, {wpb}),")
+        lines += ["};", f"const int kNum{table[1:]} = sizeof({table}) / sizeof({table}[0]);", "",
+                  "}  // namespace tbtkkpm", ""]
+        (HERE / fname).write_text("\n".join(lines))
+
+
+if __name__ == "__main__":
+    main()

@@ -62,9 +62,10 @@ struct Workspace {
   DevBuf mu_direct;   // [K][steps+1] directly gathered moments (doubling runs)
   DevBuf dots;        // [grid][2][Bp] per-block dot products (doubling runs)
   DevBuf col_out;     // [Bp] output slot of each batch column (doubling runs)
+  DevBuf err;         // device flag of a bounded wait that ran out
   void release() {
     for (DevBuf *b : {&vec[0], &vec[1], &bitmap, &tgt, &from, &mu, &damp, &out, &mu_direct,
-                      &dots, &col_out})
+                      &dots, &col_out, &err})
       b->release();
   }
 };

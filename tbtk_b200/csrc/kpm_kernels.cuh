@@ -57,42 +57,62 @@ __device__ __forceinline__ double2 cmac(double2 acc, double2 v, double2 x) {
 }
 
 // ---------------------------------------------------------------- vector packs
-// VPT consecutive complex values of one row as raw loads: complex128 as
-// double2 each; complex64 as float2 (VPT = 1) or float4 pairs.
-template <typename V, int VPT> struct Pack;
+// The VPT complex values a thread owns in one row of a batch, as raw loads:
+// complex128 as double2 each; complex64 as float2 (VPT = 1) or float4 pairs.
+// Ownership is interleaved: chunk q of thread `sub` of a TPR-thread group is
+// chunk q*TPR + sub of the row, so every load instruction of the group reads
+// one contiguous span (full 32-byte sectors) rather than strided pieces.
+template <typename V, int TPR, int VPT> struct Pack;
 
-template <int VPT> struct Pack<double2, VPT> {
+template <int TPR, int VPT> struct Pack<double2, TPR, VPT> {
   using L = double2;
   static constexpr int NL = VPT;
-  __device__ __forceinline__ static void load(const double2 *p, L (&o)[NL]) {
-#pragma unroll
-    for (int j = 0; j < NL; j++) o[j] = __ldg(p + j);
+  __device__ __forceinline__ static uint32_t col_of(int sub, int j) { return j * TPR + sub; }
+  // value j of `sub` holding batch column c, or -1
+  __device__ __forceinline__ static int slot_of(int sub, uint32_t c) {
+    return (int)(c % TPR) == sub ? (int)(c / TPR) : -1;
   }
-  __device__ __forceinline__ static void load_rw(const double2 *p, L (&o)[NL]) {
+  __device__ __forceinline__ static void load(const double2 *row, int sub, L (&o)[NL]) {
 #pragma unroll
-    for (int j = 0; j < NL; j++) o[j] = p[j];
+    for (int j = 0; j < NL; j++) o[j] = __ldg(row + j * TPR + sub);
+  }
+  __device__ __forceinline__ static void load_rw(const double2 *row, int sub, L (&o)[NL]) {
+#pragma unroll
+    for (int j = 0; j < NL; j++) o[j] = row[j * TPR + sub];
   }
   __device__ __forceinline__ static double2 get(const L (&o)[NL], int j) { return o[j]; }
   // Stores v and returns the values as stored.
-  __device__ __forceinline__ static void store(double2 *p, double2 (&v)[VPT]) {
+  __device__ __forceinline__ static void store(double2 *row, int sub, double2 (&v)[VPT]) {
 #pragma unroll
-    for (int j = 0; j < VPT; j++) p[j] = v[j];
+    for (int j = 0; j < VPT; j++) row[j * TPR + sub] = v[j];
   }
 };
 
-template <int VPT> struct Pack<float2, VPT> {
+template <int TPR, int VPT> struct Pack<float2, TPR, VPT> {
   static_assert(VPT == 1 || VPT % 2 == 0, "complex64 packs are 8 B or multiples of 16 B");
   using L = typename std::conditional<VPT == 1, float2, float4>::type;
   static constexpr int NL = VPT == 1 ? 1 : VPT / 2;
-  __device__ __forceinline__ static void load(const float2 *p, L (&o)[NL]) {
-    const L *q = reinterpret_cast<const L *>(p);
-#pragma unroll
-    for (int j = 0; j < NL; j++) o[j] = __ldg(q + j);
+  __device__ __forceinline__ static uint32_t col_of(int sub, int j) {
+    if constexpr (VPT == 1) return sub;
+    else return (uint32_t)(((j >> 1) * TPR + sub) * 2 + (j & 1));
   }
-  __device__ __forceinline__ static void load_rw(const float2 *p, L (&o)[NL]) {
-    const L *q = reinterpret_cast<const L *>(p);
+  __device__ __forceinline__ static int slot_of(int sub, uint32_t c) {
+    if constexpr (VPT == 1) {
+      return (int)c == sub ? 0 : -1;
+    } else {
+      const uint32_t p = c >> 1;
+      return (int)(p % TPR) == sub ? (int)(p / TPR) * 2 + (int)(c & 1) : -1;
+    }
+  }
+  __device__ __forceinline__ static void load(const float2 *row, int sub, L (&o)[NL]) {
+    const L *q = reinterpret_cast<const L *>(row);
 #pragma unroll
-    for (int j = 0; j < NL; j++) o[j] = q[j];
+    for (int j = 0; j < NL; j++) o[j] = __ldg(q + j * TPR + sub);
+  }
+  __device__ __forceinline__ static void load_rw(const float2 *row, int sub, L (&o)[NL]) {
+    const L *q = reinterpret_cast<const L *>(row);
+#pragma unroll
+    for (int j = 0; j < NL; j++) o[j] = q[j * TPR + sub];
   }
   __device__ __forceinline__ static double2 get(const L (&o)[NL], int j) {
     if constexpr (VPT == 1) {
@@ -102,25 +122,46 @@ template <int VPT> struct Pack<float2, VPT> {
       return (j & 1) ? make_double2(f.z, f.w) : make_double2(f.x, f.y);
     }
   }
-  __device__ __forceinline__ static void store(float2 *p, double2 (&v)[VPT]) {
+  __device__ __forceinline__ static float2 getf(const L (&o)[NL], int j) {
+    if constexpr (VPT == 1) {
+      return o[0];
+    } else {
+      const float4 f = o[j >> 1];
+      return (j & 1) ? make_float2(f.z, f.w) : make_float2(f.x, f.y);
+    }
+  }
+  __device__ __forceinline__ static void storef(float2 *row, int sub, const float2 (&v)[VPT]) {
+    if constexpr (VPT == 1) {
+      row[sub] = v[0];
+    } else {
+      float4 *q = reinterpret_cast<float4 *>(row);
+#pragma unroll
+      for (int j = 0; j < VPT / 2; j++)
+        q[j * TPR + sub] = make_float4(v[2 * j].x, v[2 * j].y, v[2 * j + 1].x, v[2 * j + 1].y);
+    }
+  }
+  __device__ __forceinline__ static void store(float2 *row, int sub, double2 (&v)[VPT]) {
 #pragma unroll
     for (int j = 0; j < VPT; j++)
       v[j] = make_double2((double)__double2float_rn(v[j].x), (double)__double2float_rn(v[j].y));
     if constexpr (VPT == 1) {
-      p[0] = make_float2((float)v[0].x, (float)v[0].y);
+      row[sub] = make_float2((float)v[0].x, (float)v[0].y);
     } else {
-      float4 *q = reinterpret_cast<float4 *>(p);
+      float4 *q = reinterpret_cast<float4 *>(row);
 #pragma unroll
       for (int j = 0; j < VPT / 2; j++)
-        q[j] = make_float4((float)v[2 * j].x, (float)v[2 * j].y, (float)v[2 * j + 1].x,
-                           (float)v[2 * j + 1].y);
+        q[j * TPR + sub] = make_float4((float)v[2 * j].x, (float)v[2 * j].y, (float)v[2 * j + 1].x,
+                                       (float)v[2 * j + 1].y);
     }
   }
 };
 
-// Entries in flight per thread: about 16-32 B of vector data per entry.
-template <typename V, int VPT> __host__ __device__ constexpr int entries_in_flight() {
-  return sizeof(V) * VPT <= 16 ? 8 : (sizeof(V) * VPT <= 32 ? 4 : 2);
+// Row entries a thread gathers at once.  With the register cap of one block
+// per SM (MINB = 1) a whole tight-binding row (up to 8 entries) is in flight
+// in one round trip; otherwise the count shrinks with the bytes per entry so
+// the gathers fit the cap.
+template <typename V, int VPT, int MINB> __host__ __device__ constexpr int entries_in_flight() {
+  return MINB == 1 ? 8 : (sizeof(V) * VPT <= 16 ? 8 : (sizeof(V) * VPT <= 32 ? 4 : 2));
 }
 
 // ---------------------------------------------------------------- matrix / targets
@@ -130,6 +171,35 @@ struct Sell {
   const uint32_t *col;        // [chunks * 32], kPad in padding slots
   const double2 *val;         // [chunks * 32], 2H/s
   uint32_t N, nslices;
+};
+
+// ---------------------------------------------------------------- arithmetic
+// How a step multiplies and accumulates.  Exact64: complex128 vectors, each
+// operation rounded once in the reference's order.  Wide64: complex64
+// vectors widened to FP64 in registers, FMA arithmetic, one rounding when
+// the result is stored back to complex64.
+struct Exact64 {
+  using Acc = double2;
+  using Val = double2;
+  __device__ __forceinline__ static Val value(const Sell &A, uint64_t slot) {
+    return __ldcs(A.val + slot);
+  }
+  __device__ __forceinline__ static Val half(Val v) { return make_double2(v.x * 0.5, v.y * 0.5); }
+  __device__ __forceinline__ static Acc mac(Acc acc, Val v, Acc x) {
+    return cadd_exact(acc, cmul_exact(v, x));
+  }
+  __device__ __forceinline__ static double2 wide(Acc a) { return a; }
+};
+
+struct Wide64 {
+  using Acc = double2;
+  using Val = double2;
+  __device__ __forceinline__ static Val value(const Sell &A, uint64_t slot) {
+    return __ldcs(A.val + slot);
+  }
+  __device__ __forceinline__ static Val half(Val v) { return make_double2(v.x * 0.5, v.y * 0.5); }
+  __device__ __forceinline__ static Acc mac(Acc acc, Val v, Acc x) { return cmac<false>(acc, v, x); }
+  __device__ __forceinline__ static double2 wide(Acc a) { return a; }
 };
 
 // Rows whose moments are wanted: bit r of `bitmap` is set when row r is the
@@ -163,11 +233,11 @@ __device__ __forceinline__ uint32_t target_first(const Targets &t, uint32_t r) {
 // stored [N][Bp]:
 //   FIRST: y = (H/s) x          (|j1> = H~|j0>, ChebyshevExpander.cpp:160)
 //   else:  y = (2H/s) x - y     (:172-174; y holds j_{n-1} on entry)
-// val holds 2H/s (the reference's stored values after `*= 2`); FIRST uses
-// val * 0.5, which is exact.
-// EXACT: per element the reference's operations in the reference's order
-// (acc = -y; acc += v*x for ascending columns), each rounded once, so the
-// FP64 result is bit-identical to calculateCoefficientsCPU.  Otherwise FMA.
+// The matrix holds 2H/s (the reference's stored values after `*= 2`); FIRST
+// uses half of it, which is exact.  With Exact64 each element sees the
+// reference's operations in the reference's order (acc = -y; acc += v*x
+// for ascending columns), each rounded once, so the FP64 result is
+// bit-identical to calculateCoefficientsCPU.
 //
 // A group of TPR consecutive threads owns one row; thread `sub` of the group
 // owns batch columns [sub*VPT, sub*VPT + VPT).  Blocks stride over tiles of
@@ -178,22 +248,36 @@ __device__ __forceinline__ uint32_t target_first(const Targets &t, uint32_t r) {
 // MINB is the minimum number of resident blocks the compiler must allow
 // (register cap), a tuning parameter.
 // DOTS: each block writes its partial sums of conj(j_{n+1}) j_{n+1} and
-// conj(j_{n+1}) j_n per column to dots[blockIdx.x][2][Bp] (values as stored).
+// conj(j_{n+1}) j_n per column, accumulated in FP64, to
+// dots[blockIdx.x][2][Bp] (values as stored).
+
+template <typename P, typename Acc, typename L, int NL>
+__device__ __forceinline__ Acc pack_get(const L (&o)[NL], int j) {
+  if constexpr (std::is_same<Acc, float2>::value) return P::getf(o, j);
+  else return P::get(o, j);
+}
+
+// Stores the accumulators; afterwards acc holds the values as stored.
+template <typename P, typename V, typename Acc, int VPT>
+__device__ __forceinline__ void pack_store(V *row, int sub, Acc (&acc)[VPT]) {
+  if constexpr (std::is_same<Acc, float2>::value) P::storef(row, sub, acc);
+  else P::store(row, sub, acc);
+}
 
 // The prefetched part of a row: slice bounds, first entries, j_{n-1}.
-template <typename V, int TPR, int VPT, int PF>
+template <typename V, typename AR, int TPR, int VPT, int PF>
 struct RowFetch {
-  using L = typename Pack<V, VPT>::L;
+  using L = typename Pack<V, TPR, VPT>::L;
   uint32_t row, l, cb, ce;
   bool ok, live;
-  uint32_t cc[PF];      // column indices of entries sub + q*TPR (TPR > 1) or q (TPR == 1)
-  double2 vv[TPR > 1 ? PF : 1];
-  L yr[Pack<V, VPT>::NL];
+  uint32_t cc[PF];  // column indices of entries sub + q*TPR (TPR > 1) or q (TPR == 1)
+  typename AR::Val vv[TPR > 1 ? PF : 1];
+  L yr[Pack<V, TPR, VPT>::NL];
 };
 
-template <typename V, int TPR, int VPT, int PF, bool FIRST>
+template <typename V, typename AR, int TPR, int VPT, int PF, bool FIRST>
 __device__ __forceinline__ void fetch_row(const Sell &A, uint32_t Bp, const V *y, uint64_t tile,
-                                          int grp, int sub, RowFetch<V, TPR, VPT, PF> &f) {
+                                          int grp, int sub, RowFetch<V, AR, TPR, VPT, PF> &f) {
   constexpr int RPB = kBlock / TPR;
   f.row = (uint32_t)(tile * RPB + grp);
   const uint32_t s = f.row >> 5;
@@ -209,61 +293,62 @@ __device__ __forceinline__ void fetch_row(const Sell &A, uint32_t Bp, const V *y
     const uint32_t k = TPR > 1 ? (uint32_t)(q * TPR + sub) : (uint32_t)q;
     f.cc[q] = (f.cb + k < f.ce) ? __ldcs(A.col + (uint64_t)(f.cb + k) * 32 + f.l) : kPad;
     if constexpr (TPR > 1)
-      f.vv[q] = f.cc[q] != kPad ? __ldcs(A.val + (uint64_t)(f.cb + k) * 32 + f.l)
-                                : make_double2(0.0, 0.0);
+      f.vv[q] = f.cc[q] != kPad ? AR::value(A, (uint64_t)(f.cb + k) * 32 + f.l)
+                                : typename AR::Val{0, 0};
   }
   if constexpr (!FIRST)
-    if (f.live) Pack<V, VPT>::load_rw(y + (uint64_t)f.row * Bp + sub * VPT, f.yr);
+    if (f.live) Pack<V, TPR, VPT>::load_rw(y + (uint64_t)f.row * Bp, sub, f.yr);
 }
 
-template <typename V, int TPR, int VPT, bool EXACT, bool FIRST, bool DOTS, int MINB>
+template <typename V, typename AR, int TPR, int VPT, bool FIRST, bool DOTS, int MINB>
 __global__ void __launch_bounds__(kBlock, MINB)
 kpm_step(Sell A, uint32_t Bp, const V *__restrict__ x, V *__restrict__ y, Targets tg,
          uint32_t n_out, double2 *__restrict__ dots) {
-  using P = Pack<V, VPT>;
+  using P = Pack<V, TPR, VPT>;
   using L = typename P::L;
+  using Acc = typename AR::Acc;
+  using Val = typename AR::Val;
   constexpr int NL = P::NL;
-  constexpr int G = entries_in_flight<V, VPT>();
+  constexpr int G = entries_in_flight<V, VPT, MINB>();
   constexpr int RPB = kBlock / TPR;
   // entries per row prefetched: G for a thread-per-row, one per thread of
   // the group otherwise
   constexpr int PF = TPR == 1 ? G : 1;
   const int sub = threadIdx.x % TPR;
   const int grp = threadIdx.x / TPR;
-  const uint32_t c0 = sub * VPT;
   const unsigned mask = 0xffffffffu;
-  double2 d_nn[DOTS ? VPT : 1], d_np[DOTS ? VPT : 1];
+  // <j_{n+1}|j_{n+1}> and Re<j_{n+1}|j_n> per owned column (real for a
+  // Hermitian H and a diagonal moment)
+  double d_nn[DOTS ? VPT : 1], d_np[DOTS ? VPT : 1];
   if constexpr (DOTS) {
 #pragma unroll
-    for (int j = 0; j < VPT; j++) d_nn[j] = d_np[j] = make_double2(0.0, 0.0);
+    for (int j = 0; j < VPT; j++) d_nn[j] = d_np[j] = 0.0;
   }
   const uint64_t ntiles = ((uint64_t)A.nslices * 32 + RPB - 1) / RPB;
-  RowFetch<V, TPR, VPT, PF> cur, nxt;
-  if (blockIdx.x < ntiles) fetch_row<V, TPR, VPT, PF, FIRST>(A, Bp, y, blockIdx.x, grp, sub, cur);
+  RowFetch<V, AR, TPR, VPT, PF> cur, nxt;
+  if (blockIdx.x < ntiles) fetch_row<V, AR, TPR, VPT, PF, FIRST>(A, Bp, y, blockIdx.x, grp, sub, cur);
   for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     // issue the next row's loads before this row's gathers
     const uint64_t tnext = tile + gridDim.x;
-    if (tnext < ntiles) fetch_row<V, TPR, VPT, PF, FIRST>(A, Bp, y, tnext, grp, sub, nxt);
+    if (tnext < ntiles) fetch_row<V, AR, TPR, VPT, PF, FIRST>(A, Bp, y, tnext, grp, sub, nxt);
     // Whole warps past the last slice skip (the rows of a warp share a slice).
     if (cur.ok) {
       const uint32_t row = cur.row, l = cur.l, cb = cur.cb, ce = cur.ce, w = ce - cb;
-      double2 acc[VPT];
+      Acc acc[VPT];
 #pragma unroll
       for (int j = 0; j < VPT; j++) {
         if constexpr (FIRST) {
-          acc[j] = make_double2(0.0, 0.0);
+          acc[j] = Acc{0, 0};
         } else {
-          const double2 v = cur.live ? P::get(cur.yr, j) : make_double2(0.0, 0.0);
-          acc[j] = make_double2(-v.x, -v.y);
+          const Acc v = cur.live ? pack_get<P, Acc>(cur.yr, j) : Acc{0, 0};
+          acc[j] = Acc{-v.x, -v.y};
         }
       }
-      L self[NL];
-      bool have_self = false;
       if constexpr (TPR == 1) {
         // entries [0, G) are prefetched; wider rows continue on demand
         for (uint32_t kb = 0; kb < w; kb += G) {
           uint32_t cc[G];
-          double2 vv[G];
+          Val vv[G];
           L raw[G][NL];
 #pragma unroll
           for (int g = 0; g < G; g++)
@@ -272,39 +357,32 @@ kpm_step(Sell A, uint32_t Bp, const V *__restrict__ x, V *__restrict__ y, Target
 #pragma unroll
           for (int g = 0; g < G; g++)
             if (cc[g] != kPad) {
-              vv[g] = __ldcs(A.val + (uint64_t)(cb + kb + g) * 32 + l);
-              P::load(x + (uint64_t)cc[g] * Bp + c0, raw[g]);
+              vv[g] = AR::value(A, (uint64_t)(cb + kb + g) * 32 + l);
+              P::load(x + (uint64_t)cc[g] * Bp, sub, raw[g]);
             }
 #pragma unroll
           for (int g = 0; g < G; g++) {
             if (cc[g] == kPad) continue;
-            double2 v = vv[g];
-            if constexpr (FIRST) v = make_double2(v.x * 0.5, v.y * 0.5);
+            Val v = vv[g];
+            if constexpr (FIRST) v = AR::half(v);
 #pragma unroll
-            for (int j = 0; j < VPT; j++) acc[j] = cmac<EXACT>(acc[j], v, P::get(raw[g], j));
-            if constexpr (DOTS) {
-              if (cc[g] == row) {
-#pragma unroll
-                for (int q = 0; q < NL; q++) self[q] = raw[g][q];
-                have_self = true;
-              }
-            }
+            for (int j = 0; j < VPT; j++) acc[j] = AR::mac(acc[j], v, pack_get<P, Acc>(raw[g], j));
           }
         }
       } else {
         // entries [kb, kb + TPR): thread sub holds entry kb + sub
         for (uint32_t kb = 0; kb < w; kb += TPR) {
           uint32_t myc;
-          double2 myv;
+          Val myv;
           if (kb == 0) {
             myc = cur.cc[0];
             myv = cur.vv[0];
           } else {
             myc = kPad;
-            myv = make_double2(0.0, 0.0);
+            myv = Val{0, 0};
             if (kb + sub < w) {
               myc = __ldcs(A.col + (uint64_t)(cb + kb + sub) * 32 + l);
-              if (myc != kPad) myv = __ldcs(A.val + (uint64_t)(cb + kb + sub) * 32 + l);
+              if (myc != kPad) myv = AR::value(A, (uint64_t)(cb + kb + sub) * 32 + l);
             }
           }
           const uint32_t nk = min((uint32_t)TPR, w - kb);
@@ -318,49 +396,64 @@ kpm_step(Sell A, uint32_t Bp, const V *__restrict__ x, V *__restrict__ y, Target
             }
 #pragma unroll
             for (int g = 0; g < G; g++)
-              if (cc[g] != kPad) P::load(x + (uint64_t)cc[g] * Bp + c0, raw[g]);
+              if (cc[g] != kPad) P::load(x + (uint64_t)cc[g] * Bp, sub, raw[g]);
 #pragma unroll
             for (int g = 0; g < G; g++) {
               const int src = (int)min(j0 + g, nk - 1);
-              double2 v;
+              Val v;
               v.x = __shfl_sync(mask, myv.x, src, TPR);
               v.y = __shfl_sync(mask, myv.y, src, TPR);
               if (cc[g] == kPad) continue;
-              if constexpr (FIRST) v = make_double2(v.x * 0.5, v.y * 0.5);
+              if constexpr (FIRST) v = AR::half(v);
 #pragma unroll
-              for (int j = 0; j < VPT; j++) acc[j] = cmac<EXACT>(acc[j], v, P::get(raw[g], j));
-              if constexpr (DOTS) {
-                if (cc[g] == row) {
-#pragma unroll
-                  for (int q = 0; q < NL; q++) self[q] = raw[g][q];
-                  have_self = true;
-                }
-              }
+              for (int j = 0; j < VPT; j++) acc[j] = AR::mac(acc[j], v, pack_get<P, Acc>(raw[g], j));
             }
           }
         }
       }
       if (cur.live) {
-        // moments of flagged rows from the FP64 register values
+        // moments of flagged rows from the register values
         if (target_hit(tg, row)) {
           for (uint32_t i = target_first(tg, row); i < tg.count && __ldg(tg.row + i) == row; i++) {
-            const uint32_t bc = __ldg(tg.col + i);
-            if (bc >= c0 && bc < c0 + VPT) {
+            const int jt = P::slot_of(sub, __ldg(tg.col + i));
+            if (jt >= 0) {
 #pragma unroll
               for (int j = 0; j < VPT; j++)
-                if (bc == c0 + j) tg.mu[(uint64_t)__ldg(tg.out + i) * tg.ld + n_out] = acc[j];
+                if (j == jt) tg.mu[(uint64_t)__ldg(tg.out + i) * tg.ld + n_out] = AR::wide(acc[j]);
             }
           }
         }
-        P::store(y + (uint64_t)row * Bp + c0, acc);  // acc now holds the stored values
-        if constexpr (DOTS) {
-          if (!have_self) P::load(x + (uint64_t)row * Bp + c0, self);
+        if constexpr (DOTS && std::is_same<V, float2>::value) {
+          // Round j_{n+1} to complex64 once, store it, and form both dot
+          // products from the stored values: each term a complex64 product
+          // summed in FP32 (one rounding of a 48-bit product per term, far
+          // below the storage rounding the identities already carry) and
+          // accumulated in FP64.  j_n of this row was just gathered by the
+          // diagonal entry, so its reload hits L1.
+          float2 af[VPT];
+#pragma unroll
+          for (int j = 0; j < VPT; j++)
+            af[j] = make_float2(__double2float_rn(acc[j].x), __double2float_rn(acc[j].y));
+          P::storef(y + (uint64_t)row * Bp, sub, af);
+          L self[NL];
+          P::load(x + (uint64_t)row * Bp, sub, self);
 #pragma unroll
           for (int j = 0; j < VPT; j++) {
-            const double2 a = acc[j], b = P::get(self, j);
-            d_nn[j].x = fma(a.x, a.x, fma(a.y, a.y, d_nn[j].x));
-            d_np[j].x = fma(a.x, b.x, fma(a.y, b.y, d_np[j].x));
-            d_np[j].y = fma(a.x, b.y, fma(-a.y, b.x, d_np[j].y));
+            const float2 b = P::getf(self, j);
+            d_nn[j] += (double)fmaf(af[j].x, af[j].x, af[j].y * af[j].y);
+            d_np[j] += (double)fmaf(af[j].x, b.x, af[j].y * b.y);
+          }
+        } else {
+          pack_store<P, V, Acc, VPT>(y + (uint64_t)row * Bp, sub, acc);
+          if constexpr (DOTS) {
+            L self[NL];
+            P::load(x + (uint64_t)row * Bp, sub, self);
+#pragma unroll
+            for (int j = 0; j < VPT; j++) {
+              const double2 a = AR::wide(acc[j]), b = P::get(self, j);
+              d_nn[j] = fma(a.x, a.x, fma(a.y, a.y, d_nn[j]));
+              d_np[j] = fma(a.x, b.x, fma(a.y, b.y, d_np[j]));
+            }
           }
         }
       }
@@ -370,23 +463,22 @@ kpm_step(Sell A, uint32_t Bp, const V *__restrict__ x, V *__restrict__ y, Target
   if constexpr (DOTS) {
     // Sum over the RPB groups of the block, one column at a time, in a fixed
     // order.
-    __shared__ double2 red[kBlock][2];
+    __shared__ double red[kBlock][2];
 #pragma unroll 1
     for (int j = 0; j < VPT; j++) {
       red[threadIdx.x][0] = d_nn[j];
       red[threadIdx.x][1] = d_np[j];
       __syncthreads();
       if (grp == 0) {
-        double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
+        double a = 0.0, b = 0.0;
         for (int r = 0; r < RPB; r++) {
-          const double2 u = red[r * TPR + sub][0], v = red[r * TPR + sub][1];
-          a.x += u.x;
-          b.x += v.x;
-          b.y += v.y;
+          a += red[r * TPR + sub][0];
+          b += red[r * TPR + sub][1];
         }
         double2 *o = dots + (uint64_t)blockIdx.x * 2 * Bp;
-        o[c0 + j] = a;
-        o[Bp + c0 + j] = b;
+        const uint32_t c = P::col_of(sub, j);
+        o[c] = make_double2(a, 0.0);
+        o[Bp + c] = make_double2(b, 0.0);
       }
       __syncthreads();
     }

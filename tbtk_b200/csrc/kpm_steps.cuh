@@ -4,6 +4,7 @@
 // autotuner picks an entry per batch shape.
 #pragma once
 
+#include "kpm_bulk.cuh"
 #include "kpm_host.h"
 #include "kpm_kernels.cuh"
 
@@ -22,6 +23,7 @@ struct StepArgs {
   Targets tg;
   uint32_t n_out;
   double2 *dots;
+  int *err;  // device flag set by a bounded wait that ran out (bulk kernels)
 };
 
 // Launches one step with a grid of min(tiles, resident blocks, max_grid)
@@ -29,15 +31,47 @@ struct StepArgs {
 using StepFn = void (*)(cudaStream_t, int device, unsigned max_grid, const StepArgs &,
                         unsigned *grid);
 
+// variant: the register cap (min blocks per SM, 2-4) of a register-staged
+// kernel, or 100 + 10*stages + warps per block of a bulk-copy kernel.
 struct StepEntry {
   int cls, tpr, vpt, minb;
   StepFn first, rest;
 };
 
-template <typename V, int TPR, int VPT, bool EXACT, bool FIRST, bool DOTS, int MINB>
+template <typename V, typename AR, int VPT, bool FIRST, bool DOTS, int S, int WPB>
+void launch_bulk(cudaStream_t st, int device, unsigned max_grid, const StepArgs &a,
+                 unsigned *grid) {
+  auto kern = kpm_step_bulk<V, AR, VPT, FIRST, DOTS, S, WPB>;
+  constexpr uint32_t smem = bulk_smem_bytes<V, VPT, S, WPB>();
+  static int per_sm[64] = {0};
+  const int d = device & 63;
+  if (per_sm[d] == 0) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 32 * WPB, smem) != cudaSuccess ||
+        nb < 1) {
+      cudaGetLastError();
+      nb = 1;
+    }
+    per_sm[d] = nb;
+  }
+  const uint64_t rows = (uint64_t)a.A.nslices * 32;
+  uint64_t g = std::min<uint64_t>((rows + WPB - 1) / WPB, (uint64_t)per_sm[d] * sm_count(device));
+  if (max_grid) g = std::min<uint64_t>(g, max_grid);
+  g = std::max<uint64_t>(g, 1);
+  *grid = (unsigned)g;
+  kern<<<(unsigned)g, 32 * WPB, smem, st>>>(a.A, a.Bp, static_cast<const V *>(a.x),
+                                             static_cast<V *>(a.y), a.tg, a.n_out, a.dots, a.err);
+}
+
+#define TBTKKPM_BULK_ENTRY(CLS, V, AR, P, D, S, WPB)                                 \
+  {CLS, 32, P, 100 + 10 * S + WPB, &launch_bulk<V, AR, P, true, D, S, WPB>,          \
+   &launch_bulk<V, AR, P, false, D, S, WPB>}
+
+template <typename V, typename AR, int TPR, int VPT, bool FIRST, bool DOTS, int MINB>
 void launch_step(cudaStream_t st, int device, unsigned max_grid, const StepArgs &a,
                  unsigned *grid) {
-  auto kern = kpm_step<V, TPR, VPT, EXACT, FIRST, DOTS, MINB>;
+  auto kern = kpm_step<V, AR, TPR, VPT, FIRST, DOTS, MINB>;
   static int per_sm[64] = {0};
   const int d = device & 63;
   if (per_sm[d] == 0) {
@@ -59,9 +93,9 @@ void launch_step(cudaStream_t st, int device, unsigned max_grid, const StepArgs 
                                        static_cast<V *>(a.y), a.tg, a.n_out, a.dots);
 }
 
-#define TBTKKPM_STEP_ENTRY(CLS, V, T, P, X, D, MB)                                  \
-  {CLS, T, P, MB, &launch_step<V, T, P, X, true, D, MB>,                            \
-   &launch_step<V, T, P, X, false, D, MB>}
+#define TBTKKPM_STEP_ENTRY(CLS, V, AR, T, P, D, MB)                                 \
+  {CLS, T, P, MB, &launch_step<V, AR, T, P, true, D, MB>,                           \
+   &launch_step<V, AR, T, P, false, D, MB>}
 
 extern const StepEntry kStepsFP64[];
 extern const int kNumStepsFP64;

@@ -129,7 +129,7 @@ int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &fro
   int rc;
   if ((rc = ws.vec[0].reserve(vbytes)) || (rc = ws.vec[1].reserve(vbytes)) ||
       (rc = ws.bitmap.reserve(4 * words)) || (rc = ws.tgt.reserve(12 * std::max(T, 1u))) ||
-      (rc = ws.from.reserve(4 * std::max(B, 1u))) ||
+      (rc = ws.from.reserve(4 * std::max(B, 1u))) || (rc = ws.err.reserve(16)) ||
       (rc = ws.mu.reserve(sizeof(double2) * (size_t)std::max(K, 1u) * M)))
     return rc;
   if (doubling &&
@@ -150,6 +150,7 @@ int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &fro
       (e = cudaMemcpyAsync(ws.from.ptr, from.data(), 4 * (size_t)B, cudaMemcpyHostToDevice, st)) ||
       (e = cudaMemsetAsync(ws.vec[0].ptr, 0, vbytes, st)) ||
       (e = cudaMemsetAsync(ws.vec[1].ptr, 0, vbytes, st)) ||
+      (e = cudaMemsetAsync(ws.err.ptr, 0, 16, st)) ||
       (e = cudaMemsetAsync(ws.mu.ptr, 0, sizeof(double2) * (size_t)K * M, st)))
     return cuda_fail(e, "recursion: staging");
   if (doubling) {
@@ -184,6 +185,7 @@ int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &fro
   a.Bp = Bp;
   a.tg = tg;
   a.dots = doubling ? ws.dots.as<double2>() : nullptr;
+  a.err = ws.err.as<int>();
   void *cur = ws.vec[0].ptr, *prev = ws.vec[1].ptr;
   m->timer.mark(st, 0);
   m->timer.pending = m->timer.enabled;
@@ -217,6 +219,18 @@ int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &fro
   }
   m->timer.mark(st, 1);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "recursion: launch");
+  return TBTKKPM_OK;
+}
+
+// After the stream has passed a batch: a bounded device wait that ran out
+// turns into TBTKKPM_ERR_TIMEOUT.
+int check_device_flag(tbtkkpm_matrix *m) {
+  int flag = 0;
+  cudaError_t e = cudaMemcpy(&flag, m->ws.err.ptr, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "recursion: status");
+  if (flag)
+    return fail(TBTKKPM_ERR_TIMEOUT,
+                "recursion: a bounded wait for staged rows ran out (status %d)", flag);
   return TBTKKPM_OK;
 }
 
@@ -301,6 +315,7 @@ static int moments_host(tbtkkpm_matrix *m, const uint32_t *from, uint32_t B, con
     if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
     if (e != cudaSuccess) return cuda_fail(e, "moments: download");
     m->timer.collect();
+    if ((rc = check_device_flag(m))) return rc;
     for (uint32_t i = 0; i < Kb; i++)
       std::memcpy(mu_out + 2 * (size_t)global_k[i] * M, mu_host.data() + (size_t)i * M,
                   sizeof(double2) * M);
@@ -629,10 +644,11 @@ extern "C" int tbtkkpm_ldos_sites(tbtkkpm_matrix *m, tbtkkpm_table *t, const uin
     e = cudaMemcpyAsync(ldos_out + (size_t)b0 * E, ws.out.ptr, sizeof(double) * (size_t)nb * E,
                         cudaMemcpyDeviceToHost, m->stream);
     if (e != cudaSuccess) return cuda_fail(e, "ldos_sites: download");
-    if (m->timer.enabled || (doubling && err_out)) {
-      if ((e = cudaStreamSynchronize(m->stream)) != cudaSuccess) return cuda_fail(e, "ldos_sites");
-      m->timer.collect();
-    }
+    // one synchronisation per batch of up to 256 sites (seconds of work at
+    // full size): timers, the error estimate and the device status
+    if ((e = cudaStreamSynchronize(m->stream)) != cudaSuccess) return cuda_fail(e, "ldos_sites");
+    m->timer.collect();
+    if ((rc = check_device_flag(m))) return rc;
     if (err_out) {
       if (doubling)
         doubling_error(mu_h, direct_h, nb, M, ld, err_out + b0);
@@ -693,6 +709,7 @@ extern "C" int tbtkkpm_matrix_autotune(tbtkkpm_matrix *m, uint32_t B, int precis
         break;
       }
       m->timer.collect();
+      if ((rc = check_device_flag(m))) break;
       const double v = m->timer.recursion_ms / probe_steps;
       ms = rep == 0 ? v : std::min(ms, v);
     }
@@ -737,4 +754,20 @@ extern "C" int tbtkkpm_matrix_set_config(tbtkkpm_matrix *m, uint32_t B, int prec
   std::lock_guard<std::mutex> lk(m->lock);
   m->tuned[tune_key(cls, Bp)] = {tpr, vpt, minb};
   return TBTKKPM_OK;
+}
+
+// The compiled step configurations of the kernel class a call at this
+// precision uses (ldos != 0: tbtkkpm_ldos_sites), as (tpr, vpt, variant)
+// triples; returns how many there are (writes at most cap triples).
+extern "C" int tbtkkpm_step_configs(int precision, int ldos, int *out, int cap) {
+  if (check_precision(precision)) return -1;
+  const StepEntry *t;
+  int n;
+  step_table(step_class(precision, ldos && precision == TBTKKPM_MIXED), &t, &n);
+  for (int i = 0; i < n && i < cap && out; i++) {
+    out[3 * i] = t[i].tpr;
+    out[3 * i + 1] = t[i].vpt;
+    out[3 * i + 2] = t[i].minb;
+  }
+  return n;
 }

@@ -83,16 +83,21 @@ SIGNATURES = [
     ("tbtkkpm_ldos_sites", _i, [_p, _p, _p, _u32, _d, _i, _p, _p]),
     ("tbtkkpm_matrix_autotune", _i, [_p, _u32, _i, _i, _u32, _p, _p, _p, _p]),
     ("tbtkkpm_matrix_set_config", _i, [_p, _u32, _i, _i, _i, _i, _i]),
+    ("tbtkkpm_step_configs", _i, [_i, _i, _p, _i]),
 ]
 
-# Step-kernel configurations compiled into the library, per kernel class:
-# (threads per row, complex values per thread); each with register caps
-# (min blocks per SM) 2, 3 and 4.
-CONFIGS_FP64 = [(1, 1), (2, 1), (4, 1), (8, 1), (16, 1), (32, 1), (16, 2), (32, 2), (16, 4),
-                (32, 4)]
-CONFIGS_MIXED = [(1, 1), (2, 1), (4, 1), (4, 2), (8, 2), (16, 2), (8, 4), (32, 2), (16, 4),
-                 (8, 8), (32, 4), (16, 8), (32, 8)]
-MINBS = (2, 3, 4)
+
+def step_configs(precision, ldos=True):
+    """Compiled step configurations (tpr, vpt, variant) of the kernels a call
+    at this precision uses; variant 2-4 is a register cap, 100 + 10*S + W a
+    bulk-copy kernel with S stages per warp and W warps per block."""
+    lib = load_library()
+    n = lib.tbtkkpm_step_configs(int(precision), int(bool(ldos)), None, 0)
+    if n < 0:
+        raise TBTKError(ERR_ARGUMENT, f"unknown precision {precision}")
+    out = np.zeros(3 * n, dtype=np.int32)
+    lib.tbtkkpm_step_configs(int(precision), int(bool(ldos)), _ptr(out), n)
+    return [tuple(int(v) for v in out[3 * i:3 * i + 3]) for i in range(n)]
 
 
 def padded_width(B, precision):
@@ -104,11 +109,10 @@ def padded_width(B, precision):
     raise TBTKError(ERR_ARGUMENT, f"batch of {B} exceeds one launch")
 
 
-def configs_for(B, precision):
-    """All compiled (tpr, vpt, minb) serving batches of B sources."""
+def configs_for(B, precision, ldos=True):
+    """All compiled (tpr, vpt, variant) serving batches of B sources."""
     w = padded_width(B, precision)
-    shapes = CONFIGS_FP64 if precision == FP64 else CONFIGS_MIXED
-    return [(t, v, mb) for (t, v) in shapes if t * v == w for mb in MINBS]
+    return [c for c in step_configs(precision, ldos) if c[0] * c[1] == w]
 
 _lib = None
 
