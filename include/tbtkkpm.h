@@ -148,6 +148,26 @@ TBTKKPM_API int tbtkkpm_moments(
 	tbtkkpm_matrix *m, uint32_t from, const uint32_t *to, uint32_t K,
 	uint32_t M, double broadening, double *mu_out);
 
+/* tbtkkpm_moments for callers that cannot allocate device memory (code
+ * inside another framework's memory pool, or under a fixed device-memory
+ * budget).  It allocates nothing: the matrix (CSR as for
+ * tbtkkpm_matrix_create_csr, unscaled) and the output are the caller's
+ * device buffers (d_to: K basis indices; d_mu_out: [K][M] complex, damped
+ * as tbtkkpm_moments), and its scratch is a fixed 32 MiB array compiled into
+ * the library, which every GPU that loads the library keeps until exit.
+ * Sizes with 32*N + 8*M + 256 > 32 MiB are rejected (use tbtkkpm_moments).
+ * The first call on a device looks the array up on the current device;
+ * make it before any stream capture.  Calls share the array: each call
+ * clears what it uses, and calls that overlap on the GPU race.  Work runs on
+ * `stream` (NULL: the default stream) and the call returns when it is done.
+ * Bad column or to indices found on the device return TBTKKPM_ERR_ARGUMENT.
+ * (No counterpart in the reference.) */
+TBTKKPM_API int tbtkkpm_moments_noalloc(
+	const uint32_t *d_rowptr, const uint32_t *d_col, const double *d_val,
+	uint32_t N, double scale, uint32_t from, const uint32_t *d_to,
+	uint32_t K, uint32_t M, double broadening, double *d_mu_out,
+	void *stream);
+
 /* Batched moments: B source vectors (from[b]) advance together as one
  * SpMM-style recursion.  to[k] belongs to source to_owner[k]; mu_out is
  * [K][M] complex in the order of to[].  precision is TBTKKPM_FP64 or

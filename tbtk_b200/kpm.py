@@ -74,6 +74,7 @@ SIGNATURES = [
     ("tbtkkpm_matrix_shape", _i, [_p, _p, _p]),
     ("tbtkkpm_matrix_download_csr", _i, [_p, _p, _p, _p]),
     ("tbtkkpm_moments", _i, [_p, _u32, _p, _u32, _u32, _d, _p]),
+    ("tbtkkpm_moments_noalloc", _i, [_p, _p, _p, _u32, _d, _u32, _p, _u32, _u32, _d, _p, _p]),
     ("tbtkkpm_moments_batched", _i, [_p, _p, _u32, _p, _p, _u32, _u32, _d, _i, _p, _p]),
     ("tbtkkpm_table_create", _i, [_u32, _p, _u32, _d, _p]),
     ("tbtkkpm_table_upload", _i, [_u32, _u32, _p, _p]),
