@@ -264,14 +264,17 @@ __device__ __forceinline__ void pack_store(V *row, int sub, Acc (&acc)[VPT]) {
   else P::store(row, sub, acc);
 }
 
-// The prefetched part of a row: slice bounds and first entries.  (j_{n-1}
-// of the row is loaded with the row's gathers, in the same round trip.)
+// The prefetched part of a row: slice bounds, first entries and j_{n-1}
+// (prefetching j_{n-1} a row ahead measured faster than loading it with the
+// row's gathers, despite the registers it holds).
 template <typename V, typename AR, int TPR, int VPT, int PF>
 struct RowFetch {
+  using L = typename Pack<V, TPR, VPT>::L;
   uint32_t row, l, cb, ce;
   bool ok, live;
   uint32_t cc[PF];  // column indices of entries sub + q*TPR (TPR > 1) or q (TPR == 1)
   typename AR::Val vv[TPR > 1 ? PF : 1];
+  L yr[Pack<V, TPR, VPT>::NL];
 };
 
 template <typename V, typename AR, int TPR, int VPT, int PF, bool FIRST>
@@ -295,6 +298,8 @@ __device__ __forceinline__ void fetch_row(const Sell &A, uint32_t Bp, const V *y
       f.vv[q] = f.cc[q] != kPad ? AR::value(A, (uint64_t)(f.cb + k) * 32 + f.l)
                                 : typename AR::Val{0, 0};
   }
+  if constexpr (!FIRST)
+    if (f.live) Pack<V, TPR, VPT>::load_rw(y + (uint64_t)f.row * Bp, sub, f.yr);
 }
 
 template <typename V, typename AR, int TPR, int VPT, bool FIRST, bool DOTS, int MINB>
@@ -331,17 +336,13 @@ kpm_step(Sell A, uint32_t Bp, const V *__restrict__ x, V *__restrict__ y, Target
     // Whole warps past the last slice skip (the rows of a warp share a slice).
     if (cur.ok) {
       const uint32_t row = cur.row, l = cur.l, cb = cur.cb, ce = cur.ce, w = ce - cb;
-      // j_{n-1} of the row, issued ahead of the gathers (same round trip)
-      L yr[NL];
-      if constexpr (!FIRST)
-        if (cur.live) P::load_rw(y + (uint64_t)row * Bp, sub, yr);
       Acc acc[VPT];
 #pragma unroll
       for (int j = 0; j < VPT; j++) {
         if constexpr (FIRST) {
           acc[j] = Acc{0, 0};
         } else {
-          const Acc v = cur.live ? pack_get<P, Acc>(yr, j) : Acc{0, 0};
+          const Acc v = cur.live ? pack_get<P, Acc>(cur.yr, j) : Acc{0, 0};
           acc[j] = Acc{-v.x, -v.y};
         }
       }
