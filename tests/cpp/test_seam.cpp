@@ -1,0 +1,223 @@
+/* TBTK's own Solver/PropertyExtractor::ChebyshevExpander, linked against the
+ * B200 seam (tbtk_b200/seam) instead of Lib/src/cuda or Lib/src/nocuda, run
+ * with the reference's GPU flags and compared with the same objects on their
+ * CPU path.
+ *
+ *   test_seam            all parity checks; exit 0 when all pass
+ *   test_seam exit-short generateGreensFunction on the GPU path with fewer
+ *                        coefficients than the lookup table; must end in
+ *                        TBTKExit (message on Streams::err, exit status 1)
+ *
+ * Expected agreement: coefficients bit-identical (the library's FP64 step
+ * follows calculateCoefficientsCPU's operation order,
+ * Lib/src/Solver/ChebyshevExpander.cpp:150-238); Green's functions from the
+ * uploaded host lookup table bit-identical to generateGreensFunctionCPU's
+ * table branch (ChebyshevExpander.cpp:371-398); LDOS therefore identical.
+ */
+#include "TBTK/GPUResourceManager.h"
+#include "TBTK/Model.h"
+#include "TBTK/PropertyExtractor/ChebyshevExpander.h"
+#include "TBTK/Range.h"
+#include "TBTK/Solver/ChebyshevExpander.h"
+#include "TBTK/Streams.h"
+
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace TBTK;
+using cplx = std::complex<double>;
+using Type = Solver::ChebyshevExpander::Type;
+
+namespace{
+
+int failures = 0;
+
+void report(const std::string &name, bool ok, const std::string &detail){
+	std::printf("[%s] %s %s\n", ok ? "PASS" : "FAIL", name.c_str(),
+		detail.c_str());
+	if(!ok)
+		failures++;
+}
+
+/* 6x6 open square lattice with spin: nearest-neighbour hopping -1, a
+ * complex spin-flip hopping 0.3i on +x bonds, on-site energies from a fixed
+ * integer sequence in [-0.5, 0.5]. */
+void buildModel(Model &model){
+	const int L = 6;
+	unsigned int state = 12345u;
+	auto next = [&state](){
+		state = state*1103515245u + 12345u;
+		return ((state >> 8) & 0xffff)/65535.0 - 0.5;
+	};
+	for(int x = 0; x < L; x++){
+		for(int y = 0; y < L; y++){
+			for(int s = 0; s < 2; s++){
+				model << HoppingAmplitude(
+					next(), {x, y, s}, {x, y, s}
+				);
+				if(x + 1 < L){
+					model << HoppingAmplitude(
+						-1.0, {x + 1, y, s}, {x, y, s}
+					) + HC;
+					model << HoppingAmplitude(
+						cplx(0, 0.3), {x + 1, y, 1 - s},
+						{x, y, s}
+					) + HC;
+				}
+				if(y + 1 < L){
+					model << HoppingAmplitude(
+						-1.0, {x, y + 1, s}, {x, y, s}
+					) + HC;
+				}
+			}
+		}
+	}
+	model.construct();
+}
+
+void configure(
+	Solver::ChebyshevExpander &solver, Model &model, int M, bool gpu
+){
+	solver.setVerbose(false);
+	solver.setModel(model);
+	solver.setScaleFactor(8);
+	solver.setNumCoefficients(M);
+	solver.setBroadening(1e-3);
+	solver.setEnergyWindow(Range(-4, 4, 401, false, false));
+	solver.setUseLookupTable(true);
+	solver.setCalculateCoefficientsOnGPU(gpu);
+	solver.setGenerateGreensFunctionsOnGPU(gpu);
+}
+
+bool sameBits(const std::vector<cplx> &a, const std::vector<cplx> &b){
+	return a.size() == b.size()
+		&& std::memcmp(a.data(), b.data(), a.size()*sizeof(cplx)) == 0;
+}
+
+double maxDiff(const std::vector<cplx> &a, const std::vector<cplx> &b){
+	double d = a.size() == b.size() ? 0 : INFINITY;
+	for(size_t n = 0; n < a.size() && n < b.size(); n++)
+		d = std::fmax(d, std::abs(a[n] - b[n]));
+	return d;
+}
+
+void testDevices(){
+	const int n = GPUResourceManager::getInstance().getNumDevices();
+	report("device_table", n >= 1, "devices=" + std::to_string(n));
+}
+
+void testCoefficients(Model &model){
+	Solver::ChebyshevExpander cpu, gpu;
+	configure(cpu, model, 512, false);
+	configure(gpu, model, 512, true);
+
+	std::vector<Index> to = {
+		{0, 0, 0}, {0, 0, 1}, {3, 2, 0}, {5, 5, 1}, {2, 4, 1}
+	};
+	const Index from = {3, 2, 0};
+	std::vector<std::vector<cplx>> a = cpu.calculateCoefficients(to, from);
+	std::vector<std::vector<cplx>> b = gpu.calculateCoefficients(to, from);
+	bool ok = a.size() == b.size();
+	double d = 0;
+	for(size_t k = 0; ok && k < a.size(); k++){
+		ok = ok && sameBits(a[k], b[k]);
+		d = std::fmax(d, maxDiff(a[k], b[k]));
+	}
+	report("coefficients_many_to", ok, "max|diff|=" + std::to_string(d));
+
+	std::vector<cplx> c = cpu.calculateCoefficients({2, 4, 1}, {2, 4, 1});
+	std::vector<cplx> g = gpu.calculateCoefficients({2, 4, 1}, {2, 4, 1});
+	report("coefficients_single", sameBits(c, g),
+		"max|diff|=" + std::to_string(maxDiff(c, g)));
+}
+
+void testGreens(Model &model){
+	Solver::ChebyshevExpander cpu, gpu;
+	configure(cpu, model, 256, false);
+	configure(gpu, model, 256, true);
+	std::vector<cplx> c = cpu.calculateCoefficients({1, 1, 0}, {1, 1, 0});
+
+	const Type types[] = {
+		Type::Advanced, Type::Retarded, Type::Principal,
+		Type::NonPrincipal
+	};
+	const char *names[] = {
+		"advanced", "retarded", "principal", "nonprincipal"
+	};
+	for(int t = 0; t < 4; t++){
+		std::vector<cplx> a = cpu.generateGreensFunction(c, types[t]);
+		std::vector<cplx> b = gpu.generateGreensFunction(c, types[t]);
+		report(std::string("greens_") + names[t], sameBits(a, b),
+			"max|diff|=" + std::to_string(maxDiff(a, b)));
+	}
+
+	//Changing the number of coefficients drops the device table
+	//(ChebyshevExpander.h:414-420); the next call uploads a new one.
+	cpu.setNumCoefficients(128);
+	gpu.setNumCoefficients(128);
+	std::vector<cplx> c2 = cpu.calculateCoefficients({4, 1, 1}, {4, 1, 1});
+	std::vector<cplx> a = cpu.generateGreensFunction(c2, Type::Retarded);
+	std::vector<cplx> b = gpu.generateGreensFunction(c2, Type::Retarded);
+	report("greens_after_table_reload", sameBits(a, b),
+		"max|diff|=" + std::to_string(maxDiff(a, b)));
+}
+
+void testLDOS(Model &model){
+	Solver::ChebyshevExpander cpu, gpu;
+	configure(cpu, model, 256, false);
+	configure(gpu, model, 256, true);
+	PropertyExtractor::ChebyshevExpander peCPU(cpu), peGPU(gpu);
+	peCPU.setEnergyWindow(-4, 4, 301);
+	peGPU.setEnergyWindow(-4, 4, 301);
+
+	std::vector<Index> patterns = {{0, 0, 0}, {2, 3, 1}, {5, 1, IDX_ALL}};
+	Property::LDOS a = peCPU.calculateLDOS(patterns);
+	Property::LDOS b = peGPU.calculateLDOS(patterns);
+	const std::vector<double> &da = a.getData();
+	const std::vector<double> &db = b.getData();
+	double d = da.size() == db.size() ? 0 : INFINITY;
+	for(size_t n = 0; n < da.size() && n < db.size(); n++)
+		d = std::fmax(d, std::fabs(da[n] - db[n]));
+	const bool ok = da.size() == db.size() && da.size() == 4*301
+		&& std::memcmp(da.data(), db.data(), da.size()*sizeof(double))
+			== 0;
+	report("ldos_property_extractor", ok,
+		"values=" + std::to_string(db.size()) + " max|diff|="
+		+ std::to_string(d));
+}
+
+int exitShort(){
+	Model model;
+	model.setVerbose(false);
+	buildModel(model);
+	Solver::ChebyshevExpander gpu;
+	configure(gpu, model, 64, true);
+	std::vector<cplx> shortCoefficients(10, cplx(1, 0));
+	gpu.generateGreensFunction(shortCoefficients, Type::Retarded);
+	std::printf("no exit\n");
+	return 0;
+}
+
+}	//End of anonymous namespace
+
+int main(int argc, char **argv){
+	Communicator::setGlobalVerbose(false);
+	if(argc > 1 && std::strcmp(argv[1], "exit-short") == 0)
+		return exitShort();
+
+	Model model;
+	model.setVerbose(false);
+	buildModel(model);
+
+	testDevices();
+	testCoefficients(model);
+	testGreens(model);
+	testLDOS(model);
+
+	std::printf("%d failure(s)\n", failures);
+	return failures == 0 ? 0 : 1;
+}
