@@ -243,6 +243,89 @@ TBTKKPM_API int tbtkkpm_ldos_sites(
 	tbtkkpm_matrix *m, tbtkkpm_table *t, const uint32_t *sites, uint32_t B,
 	double broadening, int precision, double *ldos_out, double *err_out);
 
+/* ------------------------------------------------------------ LDOS server
+ *
+ * A device-resident LDOS service over many models (no reference
+ * counterpart: the reference answers one calculateLDOS call at a time,
+ * Lib/src/PropertyExtractor/ChebyshevExpander.cpp:475-505).  Each model
+ * owns `width` lanes; a request (model, up to `width` sites, M moments,
+ * broadening) takes free lanes at the next step boundary, and one kernel
+ * launch per step advances every lane of every resident model (continuous
+ * batching).  Lanes run complex64 vectors with FP64 arithmetic, FP64
+ * moments and the doubling identities; a request whose error estimate
+ * exceeds `tolerance` is recomputed in FP64 (tbtkkpm_ldos_sites at
+ * TBTKKPM_FP64).  Each result depends only on its own request: the same
+ * bits alone or among any other requests.  Lane memory (vectors, moments)
+ * of a model is allocated when it first gets a request and counts against
+ * `hbm_budget` (bytes); idle models are evicted least recently used first;
+ * a request whose model does not fit waits.  Any thread may submit and
+ * wait; one worker thread per server drives the device. */
+
+typedef struct tbtkkpm_server tbtkkpm_server;
+
+#define TBTKKPM_PENDING 1  /* tbtkkpm_server_wait: not finished yet */
+
+/* energies[E]: the energy grid of every result (inside (-s, s) of every
+ * model).  max_moments: the largest M a request may ask for.  tick_steps:
+ * recursion steps between admission points (0: 64).  tolerance <= 0 never
+ * recomputes. */
+TBTKKPM_API int tbtkkpm_server_create(
+	uint32_t max_moments, const double *energies, uint32_t E,
+	uint64_t hbm_budget, uint32_t tick_steps, double tolerance,
+	tbtkkpm_server **out);
+
+/* Registers a model from its CSR (as tbtkkpm_matrix_create_csr) with
+ * `width` lanes (1, 2, 4, ..., 64).  The model id is returned in *model. */
+TBTKKPM_API int tbtkkpm_server_add_model(
+	tbtkkpm_server *s, const uint32_t *rowptr, const uint32_t *col,
+	const double *val, uint32_t N, double scale, uint32_t width,
+	uint32_t *model);
+
+/* Queues the LDOS of n_sites sites of a model (1 <= n_sites <= width,
+ * 2 <= M <= max_moments); *request identifies it. */
+TBTKKPM_API int tbtkkpm_server_submit(
+	tbtkkpm_server *s, uint32_t model, const uint32_t *sites,
+	uint32_t n_sites, uint32_t M, double broadening, uint64_t *request);
+
+/* Waits up to timeout_s seconds (0: poll) for a request.  Returns
+ * TBTKKPM_OK with ldos_out [n_sites][E], err_out [n_sites] (error estimate
+ * of the mixed-precision run) and rerun_out [n_sites] (1 where the FP64
+ * recomputation replaced it) filled and the request released, or
+ * TBTKKPM_PENDING.  Output pointers may be NULL. */
+TBTKKPM_API int tbtkkpm_server_wait(
+	tbtkkpm_server *s, uint64_t request, double timeout_s, double *ldos_out,
+	double *err_out, int32_t *rerun_out);
+
+/* Statistics into out[n] (n <= TBTKKPM_STAT_COUNT): */
+#define TBTKKPM_STAT_COMPLETED 0  /* requests finished */
+#define TBTKKPM_STAT_P50_MS 1     /* median submit-to-finish latency */
+#define TBTKKPM_STAT_P99_MS 2     /* 99th percentile latency */
+#define TBTKKPM_STAT_MEAN_MS 3
+#define TBTKKPM_STAT_RERUNS 4     /* sites recomputed in FP64 */
+#define TBTKKPM_STAT_TICKS 5
+#define TBTKKPM_STAT_STEPS 6      /* recursion steps launched */
+#define TBTKKPM_STAT_LANE_STEPS 7 /* sum over requests of sites * steps */
+#define TBTKKPM_STAT_RESIDENT 8   /* lane bytes resident now */
+#define TBTKKPM_STAT_EVICTIONS 9
+#define TBTKKPM_STAT_WAITED 10    /* admissions deferred by the budget */
+#define TBTKKPM_STAT_BUSY_S 11    /* worker time with lanes in flight */
+#define TBTKKPM_STAT_COUNT 12
+TBTKKPM_API int tbtkkpm_server_stats(tbtkkpm_server *s, double *out, uint32_t n);
+
+/* Times every compiled step configuration of lane width `width` for
+ * probe_steps steps on the largest registered model of that width (the
+ * server must be idle) and keeps the fastest; set_config installs a known
+ * one.  Results do not depend on the configuration. */
+TBTKKPM_API int tbtkkpm_server_autotune(
+	tbtkkpm_server *s, uint32_t width, uint32_t probe_steps, int *tpr,
+	int *vpt, int *minb, double *ms_per_step);
+TBTKKPM_API int tbtkkpm_server_set_config(
+	tbtkkpm_server *s, uint32_t width, int tpr, int vpt, int minb);
+
+/* Stops the worker (requests still queued or in flight are dropped) and
+ * frees the server. */
+TBTKKPM_API int tbtkkpm_server_destroy(tbtkkpm_server *s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -46,6 +46,12 @@ int current_device() {
   return d;
 }
 
+int swap_selected_device(int device) {
+  const int prev = g_device;
+  g_device = device;
+  return prev;
+}
+
 int sm_count(int device) {
   static std::atomic<int> cache[64];
   if (device < 0 || device >= 64) return 148;

@@ -43,7 +43,29 @@ def bulk_smem(V, vpt, s, wpb, dots):
     return s * wpb * stage + (wpb * 32 * 2 * 16 if dots == "true" else 0)
 
 
+# Multi-model (server) steps: lane width -> (threads per row, values per
+# thread) shapes, each with the register caps MULTI_MINBS.
+MULTI_SHAPES = {1: [(1, 1)], 2: [(2, 1)], 4: [(4, 1), (2, 2)], 8: [(4, 2), (2, 4), (8, 1)],
+                16: [(8, 2), (4, 4), (2, 8)], 32: [(16, 2), (8, 4), (4, 8)],
+                64: [(32, 2), (16, 4), (8, 8)]}
+MULTI_MINBS = [1, 2]
+
+
+def write_multi():
+    lines = ["// Multi-model recursion steps for every lane width the server offers.",
+             "// Written by gen_steps.py.", '#include "kpm_multi.cuh"', "", "namespace tbtkkpm {", "",
+             "const MultiEntry kMultiSteps[] = {"]
+    for w, shapes in MULTI_SHAPES.items():
+        for (t, p) in shapes:
+            for mb in MULTI_MINBS:
+                lines.append(f"    TBTKKPM_MULTI_ENTRY({t}, {p}, {mb}),")
+    lines += ["};", "const int kNumMultiSteps = sizeof(kMultiSteps) / sizeof(kMultiSteps[0]);", "",
+              "}  // namespace tbtkkpm", ""]
+    (HERE / "steps_multi.cu").write_text("\n".join(lines))
+
+
 def main():
+    write_multi()
     for fname, table, cls, V, AR, dots, shapes, doc in UNITS:
         lines = [f"// {doc}", "// Written by gen_steps.py: every configuration the driver and the",
                  "// autotuner can pick.", '#include "kpm_steps.cuh"', "", "namespace tbtkkpm {", "",

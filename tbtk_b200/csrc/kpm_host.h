@@ -14,6 +14,9 @@ namespace tbtkkpm {
 int fail(int code, const char *fmt, ...);
 int cuda_fail(cudaError_t e, const char *what);
 int current_device();
+// Sets the device handle creations on this thread use (-1: the CUDA current
+// device) and returns the previous selection.
+int swap_selected_device(int device);
 void count_launches(uint64_t n);
 int sm_count(int device);
 
@@ -111,3 +114,19 @@ struct tbtkkpm_table {
   tbtkkpm::DevBuf mu, out; // staging for energy sums
   std::mutex lock;
 };
+
+#include <vector>
+
+namespace tbtkkpm {
+
+// Energy sum of `type` (0-3 Green's functions, 4 = LDOS) over K moment
+// vectors [K][terms] on the device (terms 0: the table's M).
+int launch_energy_sum(cudaStream_t st, const tbtkkpm_table *t, const double2 *mu, uint32_t K,
+                      int type, void *out, uint32_t terms = 0);
+// Lorentz damping numerators a[n] and denominator b (host libm).
+void damping_factors(uint32_t M, double broadening, std::vector<double> &a, double &b);
+// Error estimate of doubled moments against the directly gathered ones.
+void doubling_error(const std::vector<double2> &mu, const std::vector<double2> &direct,
+                    uint32_t K, uint32_t M, uint32_t ld, double *err);
+
+}  // namespace tbtkkpm

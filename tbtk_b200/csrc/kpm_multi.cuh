@@ -1,0 +1,417 @@
+// Multi-model recursion: one launch advances every active model of a server
+// (or an uneven batch of models) by one Chebyshev step.
+//
+// Each model keeps its own SELL matrix and its own pair of complex64 vector
+// buffers [rows][W] (W = the model's lane width).  A lane is one LDOS
+// request site: it joins at a step boundary with j_0 = e_site in its column
+// and runs its own local step count, so requests enter and leave while the
+// others keep going (continuous batching).  A lane whose local step is 1
+// takes j_1 = H~ j_0 (the reference's first step,
+// Lib/src/Solver/ChebyshevExpander.cpp:159-169); every later step takes
+// j_{n+1} = 2H~ j_n - j_{n-1} (:171-186).  The per-element arithmetic is
+// the single-model kernel's (entry order, FMA, one rounding to complex64),
+// so a lane's direct moments do not depend on the other lanes or models.
+//
+// The doubling dot products <j_n|j_n> and Re<j_n|j_{n-1}> are accumulated
+// in 64-bit fixed point (2^-61 units): every term is one complex64 product
+// rounded once to FP32 and then to the fixed-point grid, and integer sums
+// are associative, so the moments of a lane are bit-identical whatever the
+// grid, the launch configuration, the tile schedule or the other models in
+// the launch.  |terms| and all partial sums stay below 1 (||j_n|| <= 1 for
+// a spectrum inside [-1, 1]), so 2^61 leaves headroom of 4.
+#pragma once
+
+#include "kpm_kernels.cuh"
+
+namespace tbtkkpm {
+
+constexpr int32_t kLaneIdle = INT32_MIN / 2;  // base step of a lane without a request
+constexpr float kFixScale = 2305843009213693952.0f;  // 2^61
+constexpr double kFixUnit = 1.0 / 2305843009213693952.0;  // 2^-61
+
+// One model of a launch (device resident, rebuilt by the host per tick).
+struct MultiModel {
+  Sell A;                    // model-local SELL, 2H/s
+  float2 *vec[2];            // [nslices*32][W]; step n reads vec[(n+1)&1], writes vec[n&1]
+  const uint32_t *bitmap;    // rows that are some lane's site
+  const uint32_t *trow;      // sorted target rows
+  const uint32_t *tcol;      // lane of each target
+  uint32_t tcount;
+  const int32_t *base;       // [W] global step of the lane's local step 0, or kLaneIdle
+  const uint32_t *lane_M;    // [W] moments the lane's request asks for
+  long long *dots;           // [2][W] fixed-point sums of the current step
+  double2 *mu;               // [W][Mmax] doubled moments (0 and 1 seeded)
+  double2 *mu_direct;        // [W][ld] directly gathered moments
+  uint32_t tile0;            // first tile of this model in the launch
+  uint32_t ntiles;
+};
+
+// Per-tick launch header (device resident): the models, their tile total
+// and the global step of step offset 0.
+struct MultiHeader {
+  uint32_t nmodels;
+  uint32_t total_tiles;
+  int32_t n_base;
+};
+
+__device__ __forceinline__ uint32_t multi_find(const MultiModel *models, uint32_t nmodels,
+                                               uint32_t w) {
+  uint32_t lo = 0, hi = nmodels;  // last model with tile0 <= w
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(&models[mid].tile0) <= w) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+template <typename P, int VPT, int TPR>
+__device__ __forceinline__ void multi_flush(long long (&s_nn)[VPT], long long (&s_np)[VPT],
+                                            long long *dots, uint32_t W, int sub) {
+#pragma unroll
+  for (int j = 0; j < VPT; j++) {
+    long long a = s_nn[j], b = s_np[j];
+#pragma unroll
+    for (int off = TPR; off < 32; off <<= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, off);
+      b += __shfl_xor_sync(0xffffffffu, b, off);
+    }
+    if ((threadIdx.x & 31) < TPR) {
+      const uint32_t c = P::col_of(sub, j);
+      if (a) atomicAdd(reinterpret_cast<unsigned long long *>(dots + c), (unsigned long long)a);
+      if (b) atomicAdd(reinterpret_cast<unsigned long long *>(dots + W + c), (unsigned long long)b);
+    }
+    s_nn[j] = s_np[j] = 0;
+  }
+}
+
+// One recursion step for every model of the launch.  Blocks stride over the
+// concatenated tiles (kBlock/TPR rows each) of all models; a tile's row
+// fetch is issued one tile ahead as in kpm_step.
+template <int TPR, int VPT, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB)
+kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restrict__ hdr,
+               uint32_t step_offset, uint32_t W, uint32_t ld) {
+  using V = float2;
+  using AR = Wide64;
+  using P = Pack<V, TPR, VPT>;
+  using L = typename P::L;
+  using Acc = double2;
+  using Val = double2;
+  constexpr int NL = P::NL;
+  constexpr int G = entries_in_flight<V, VPT, MINB>();
+  constexpr int PF = TPR == 1 ? G : 1;
+  const int sub = threadIdx.x % TPR;
+  const int grp = threadIdx.x / TPR;
+  const unsigned mask = 0xffffffffu;
+  const uint32_t nmodels = hdr->nmodels, total = hdr->total_tiles;
+  const int32_t n = hdr->n_base + (int32_t)step_offset;
+  if (nmodels == 0) return;
+
+  long long s_nn[VPT], s_np[VPT];
+#pragma unroll
+  for (int j = 0; j < VPT; j++) s_nn[j] = s_np[j] = 0;
+
+  // the model of the tile being computed and of the one being fetched
+  uint32_t mi = kPad, fi = kPad;
+  Sell A{}, FA{};
+  const float2 *x = nullptr;
+  float2 *y = nullptr;
+  const float2 *fy = nullptr;
+  uint32_t first = 0;  // bit j: lane of value j is at its local step 1
+  // fields of the current model kept in registers
+  const uint32_t *t_bitmap = nullptr, *t_row = nullptr, *t_col = nullptr;
+  const int32_t *t_base = nullptr;
+  double2 *t_mud = nullptr;
+  long long *t_dots = nullptr;
+  uint32_t t_count = 0;
+
+  auto fetch = [&](uint32_t w, RowFetch<V, AR, TPR, VPT, PF> &f, uint32_t &fmodel) {
+    const uint32_t i = multi_find(models, nmodels, w);
+    if (i != fi) {
+      fi = i;
+      const MultiModel *q = models + i;
+      FA.slice_ptr = q->A.slice_ptr;
+      FA.col = q->A.col;
+      FA.val = q->A.val;
+      FA.N = q->A.N;
+      FA.nslices = q->A.nslices;
+      fy = q->vec[n & 1];
+    }
+    fmodel = i;
+    fetch_row<V, AR, TPR, VPT, PF, false>(FA, W, fy, w - __ldg(&models[i].tile0), grp, sub, f);
+  };
+
+  RowFetch<V, AR, TPR, VPT, PF> cur, nxt;
+  uint32_t cur_model = 0, nxt_model = 0;
+  if (blockIdx.x < total) fetch(blockIdx.x, cur, cur_model);
+  for (uint32_t w = blockIdx.x; w < total; w += gridDim.x) {
+    if (cur_model != mi) {
+      // block-uniform: every thread of the block is on the same tile
+      if (mi != kPad) multi_flush<P, VPT, TPR>(s_nn, s_np, t_dots, W, sub);
+      mi = cur_model;
+      const MultiModel *md = models + mi;
+      A.slice_ptr = md->A.slice_ptr;
+      A.col = md->A.col;
+      A.val = md->A.val;
+      A.N = md->A.N;
+      A.nslices = md->A.nslices;
+      x = md->vec[(n + 1) & 1];
+      y = md->vec[n & 1];
+      t_bitmap = md->bitmap;
+      t_row = md->trow;
+      t_col = md->tcol;
+      t_count = md->tcount;
+      t_base = md->base;
+      t_mud = md->mu_direct;
+      t_dots = md->dots;
+      first = 0;
+#pragma unroll
+      for (int j = 0; j < VPT; j++)
+        if (n - __ldg(t_base + P::col_of(sub, j)) == 1) first |= 1u << j;
+    }
+    const uint32_t wn = w + gridDim.x;
+    if (wn < total) fetch(wn, nxt, nxt_model);
+    if (cur.ok) {
+      const uint32_t row = cur.row, l = cur.l, cb = cur.cb, ce = cur.ce, wd = ce - cb;
+      Acc acc[VPT];
+#pragma unroll
+      for (int j = 0; j < VPT; j++) {
+        if ((first >> j) & 1u) {
+          acc[j] = Acc{0, 0};
+        } else {
+          const Acc v = cur.live ? pack_get<P, Acc>(cur.yr, j) : Acc{0, 0};
+          acc[j] = Acc{-v.x, -v.y};
+        }
+      }
+      if constexpr (TPR == 1) {
+        for (uint32_t kb = 0; kb < wd; kb += G) {
+          uint32_t cc[G];
+          Val vv[G];
+          L raw[G][NL];
+#pragma unroll
+          for (int g = 0; g < G; g++)
+            cc[g] = kb == 0 ? cur.cc[g]
+                            : ((kb + g < wd) ? __ldcs(A.col + (uint64_t)(cb + kb + g) * 32 + l) : kPad);
+#pragma unroll
+          for (int g = 0; g < G; g++)
+            if (cc[g] != kPad) {
+              vv[g] = AR::value(A, (uint64_t)(cb + kb + g) * 32 + l);
+              P::load(x + (uint64_t)cc[g] * W, sub, raw[g]);
+            }
+#pragma unroll
+          for (int g = 0; g < G; g++) {
+            if (cc[g] == kPad) continue;
+#pragma unroll
+            for (int j = 0; j < VPT; j++) acc[j] = AR::mac(acc[j], vv[g], pack_get<P, Acc>(raw[g], j));
+          }
+        }
+      } else {
+        for (uint32_t kb = 0; kb < wd; kb += TPR) {
+          uint32_t myc;
+          Val myv;
+          if (kb == 0) {
+            myc = cur.cc[0];
+            myv = cur.vv[0];
+          } else {
+            myc = kPad;
+            myv = Val{0, 0};
+            if (kb + sub < wd) {
+              myc = __ldcs(A.col + (uint64_t)(cb + kb + sub) * 32 + l);
+              if (myc != kPad) myv = AR::value(A, (uint64_t)(cb + kb + sub) * 32 + l);
+            }
+          }
+          const uint32_t nk = min((uint32_t)TPR, wd - kb);
+          for (uint32_t j0 = 0; j0 < nk; j0 += G) {
+            uint32_t cc[G];
+            L raw[G][NL];
+#pragma unroll
+            for (int g = 0; g < G; g++) {
+              cc[g] = __shfl_sync(mask, myc, (int)min(j0 + g, nk - 1), TPR);
+              if (j0 + g >= nk) cc[g] = kPad;
+            }
+#pragma unroll
+            for (int g = 0; g < G; g++)
+              if (cc[g] != kPad) P::load(x + (uint64_t)cc[g] * W, sub, raw[g]);
+#pragma unroll
+            for (int g = 0; g < G; g++) {
+              const int src = (int)min(j0 + g, nk - 1);
+              Val v;
+              v.x = __shfl_sync(mask, myv.x, src, TPR);
+              v.y = __shfl_sync(mask, myv.y, src, TPR);
+              if (cc[g] == kPad) continue;
+#pragma unroll
+              for (int j = 0; j < VPT; j++) acc[j] = AR::mac(acc[j], v, pack_get<P, Acc>(raw[g], j));
+            }
+          }
+        }
+      }
+      if (cur.live) {
+        // first-step lanes: j_1 = (1/2)(2H~) j_0, an exact halving of the
+        // same accumulation
+#pragma unroll
+        for (int j = 0; j < VPT; j++)
+          if ((first >> j) & 1u) acc[j] = AR::half(acc[j]);
+        if ((__ldg(t_bitmap + (row >> 5)) >> (row & 31)) & 1u) {
+          uint32_t lo = 0, hi = t_count;
+          while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(t_row + mid) < row) lo = mid + 1; else hi = mid;
+          }
+          for (uint32_t i = lo; i < t_count && __ldg(t_row + i) == row; i++) {
+            const uint32_t c = __ldg(t_col + i);
+            const int jt = P::slot_of(sub, c);
+            if (jt < 0) continue;
+            const int32_t nl = n - __ldg(t_base + c);
+            if (nl >= 1 && (uint32_t)nl < ld) {
+#pragma unroll
+              for (int j = 0; j < VPT; j++)
+                if (j == jt) t_mud[(uint64_t)c * ld + nl] = acc[j];
+            }
+          }
+        }
+        float2 af[VPT];
+#pragma unroll
+        for (int j = 0; j < VPT; j++)
+          af[j] = make_float2(__double2float_rn(acc[j].x), __double2float_rn(acc[j].y));
+        P::storef(y + (uint64_t)row * W, sub, af);
+        L self[NL];
+        P::load(x + (uint64_t)row * W, sub, self);
+#pragma unroll
+        for (int j = 0; j < VPT; j++) {
+          const float2 b = P::getf(self, j);
+          s_nn[j] += __float2ll_rn(fmaf(af[j].x, af[j].x, af[j].y * af[j].y) * kFixScale);
+          s_np[j] += __float2ll_rn(fmaf(af[j].x, b.x, af[j].y * b.y) * kFixScale);
+        }
+      }
+    }
+    cur = nxt;
+    cur_model = nxt_model;
+  }
+  if (mi != kPad) multi_flush<P, VPT, TPR>(s_nn, s_np, t_dots, W, sub);
+}
+
+// After a step: the doubled moments of every active lane,
+// mu_{2m} = 2<j_m|j_m> - mu_0 and mu_{2m-1} = 2<j_m|j_{m-1}> - mu_1 for the
+// lane's local step m, and the fixed-point sums cleared for the next step.
+// One block per model, one thread per lane.
+static __global__ void kpm_multi_finalize(const MultiModel *__restrict__ models,
+                                   const MultiHeader *__restrict__ hdr, uint32_t step_offset,
+                                   uint32_t W, uint32_t Mmax, uint32_t ld) {
+  if (blockIdx.x >= hdr->nmodels) return;
+  const MultiModel *md = models + blockIdx.x;
+  const int32_t n = hdr->n_base + (int32_t)step_offset;
+  for (uint32_t c = threadIdx.x; c < W; c += blockDim.x) {
+    const long long a = md->dots[c], b = md->dots[W + c];
+    md->dots[c] = 0;
+    md->dots[W + c] = 0;
+    const int32_t base = md->base[c];
+    if (base == kLaneIdle) continue;
+    const int32_t m = n - base;
+    const uint32_t M = md->lane_M[c];
+    if (m < 1 || (uint32_t)m > M / 2) continue;
+    double2 *row = md->mu + (uint64_t)c * Mmax;
+    if (m == 1) row[1] = md->mu_direct[(uint64_t)c * ld + 1];
+    const double2 mu0 = row[0], mu1 = row[1];
+    const double sa = (double)a * kFixUnit, sb = (double)b * kFixUnit;
+    if (2 * (uint32_t)m < M) row[2 * m] = make_double2(2.0 * sa - mu0.x, -mu0.y);
+    if (m >= 2 && 2 * (uint32_t)m - 1 < M) row[2 * m - 1] = make_double2(2.0 * sb - mu1.x, -mu1.y);
+  }
+}
+
+// A lane joining at global step g (its local step 1 is computed at g):
+// column c of the buffer step g reads as j_0 becomes e_site, its moment rows
+// are cleared and mu_0 = <site|site> = 1 is set.
+struct MultiJoin {
+  float2 *x;          // the model's vec[(g+1)&1]
+  double2 *mu;        // the lane's row of mu [Mmax]
+  double2 *mu_direct; // the lane's row of mu_direct [ld]
+  uint32_t rows;      // model rows (N)
+  uint32_t col, site;
+  uint32_t W;         // the model's lane width
+};
+
+static __global__ void kpm_multi_join(const MultiJoin *__restrict__ joins, uint32_t Mmax, uint32_t ld) {
+  const MultiJoin jn = joins[blockIdx.y];
+  const uint32_t W = jn.W;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < jn.rows; r += stride)
+    jn.x[r * W + jn.col] = r == jn.site ? make_float2(1.0f, 0.0f) : make_float2(0.0f, 0.0f);
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < Mmax; k += stride) {
+    jn.mu[k] = make_double2(k == 0 ? 1.0 : 0.0, 0.0);
+    if (k < ld) jn.mu_direct[k] = make_double2(k == 0 ? 1.0 : 0.0, 0.0);
+  }
+}
+
+// The moments of a finished request, [K][M] contiguous: the direct moments
+// for n <= M/2 and the doubled ones above, damped by a[n]/b as kpm_damp
+// (raw copies of both kinds go to the error estimate).
+struct MultiDone {
+  const double2 *mu;        // lane row [Mmax]
+  const double2 *mu_direct; // lane row [ld]
+};
+
+static __global__ void kpm_multi_prepare(const MultiDone *__restrict__ lanes, uint32_t K, uint32_t M,
+                                  const double *__restrict__ a, double b, int damp,
+                                  double2 *__restrict__ out, double2 *__restrict__ raw,
+                                  double2 *__restrict__ raw_direct) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (uint64_t)K * M) return;
+  const uint32_t k = (uint32_t)(i / M), nn = (uint32_t)(i % M);
+  const uint32_t half = M / 2;
+  const MultiDone d = lanes[k];
+  const double2 dbl = d.mu[nn];
+  raw[i] = dbl;
+  double2 c = dbl;
+  if (nn <= half) {
+    c = d.mu_direct[nn];
+    raw_direct[(uint64_t)k * (half + 1) + nn] = c;
+  }
+  if (damp) {
+    const double an = a[nn];
+    c = make_double2(__ddiv_rn(__dmul_rn(c.x, an), b), __ddiv_rn(__dmul_rn(c.y, an), b));
+  }
+  out[i] = c;
+}
+
+}  // namespace tbtkkpm
+
+// ---------------------------------------------------------------- dispatch
+#include "kpm_host.h"
+
+namespace tbtkkpm {
+
+using MultiFn = void (*)(cudaStream_t, int device, const MultiModel *, const MultiHeader *,
+                         uint32_t step_offset, uint32_t W, uint32_t ld);
+
+// One compiled configuration of kpm_multi_step for lane width tpr*vpt.
+struct MultiEntry {
+  int tpr, vpt, minb;
+  MultiFn launch;
+};
+
+// Grid: every resident block of the device (the kernel strides over tiles).
+template <int TPR, int VPT, int MINB>
+void launch_multi(cudaStream_t st, int device, const MultiModel *models, const MultiHeader *hdr,
+                  uint32_t step_offset, uint32_t W, uint32_t ld) {
+  auto kern = kpm_multi_step<TPR, VPT, MINB>;
+  static int per_sm[64] = {0};
+  const int d = device & 63;
+  if (per_sm[d] == 0) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kBlock, 0) != cudaSuccess ||
+        nb < 1) {
+      cudaGetLastError();
+      nb = 1;
+    }
+    per_sm[d] = nb;
+  }
+  kern<<<(unsigned)(per_sm[d] * sm_count(device)), kBlock, 0, st>>>(models, hdr, step_offset, W,
+                                                                    ld);
+}
+
+#define TBTKKPM_MULTI_ENTRY(T, P, MB) {T, P, MB, &launch_multi<T, P, MB>}
+
+extern const MultiEntry kMultiSteps[];
+extern const int kNumMultiSteps;
+
+}  // namespace tbtkkpm

@@ -234,6 +234,8 @@ int check_device_flag(tbtkkpm_matrix *m) {
   return TBTKKPM_OK;
 }
 
+}  // namespace
+
 // Damping numerators a[n] = sinh(lambda(1 - n/M)) and b = sinh(lambda),
 // evaluated with the host's libm exactly as ChebyshevExpander.cpp:192-195.
 void damping_factors(uint32_t M, double broadening, std::vector<double> &a, double &b) {
@@ -270,8 +272,6 @@ void doubling_error(const std::vector<double2> &mu, const std::vector<double2> &
     err[k] = scale > 0 ? 4.0 * std::sqrt(2.0) * dmax / scale : 0.0;
   }
 }
-
-}  // namespace
 
 // Moments of several batches: sources split into batches of at most the
 // precision's maximum; to-indices follow their owner.  Results land in host
@@ -497,10 +497,11 @@ extern "C" int tbtkkpm_table_destroy(tbtkkpm_table *t) {
 namespace tbtkkpm {
 
 // Launches the energy sum of `type` (0-3 Green's functions, 4 = LDOS) for K
-// coefficient vectors resident on the device.
+// coefficient vectors resident on the device ([K][M] with M = terms, or the
+// table's M when terms is 0; a table of more rows serves fewer terms).
 int launch_energy_sum(cudaStream_t st, const tbtkkpm_table *t, const double2 *mu, uint32_t K,
-                      int type, void *out) {
-  const uint32_t M = t->M, E = t->E;
+                      int type, void *out, uint32_t terms) {
+  const uint32_t M = terms ? terms : t->M, E = t->E;
   const int KT = K == 1 ? 1 : (K <= 4 ? 4 : 8);
   dim3 grid((E + kEnergyBlock - 1) / kEnergyBlock, (K + KT - 1) / KT);
   const double2 *tb = t->table.as<double2>();

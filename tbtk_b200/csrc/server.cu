@@ -1,0 +1,1012 @@
+// The LDOS server behind tbtkkpm_server_* (include/tbtkkpm.h): continuous
+// batching of LDOS requests over many device-resident models.
+//
+// One worker thread per server repeats
+//   admit  - queued requests take free lanes of their model at the next
+//            step boundary; a model's lane memory is allocated on its first
+//            request within the HBM budget, evicting idle models (LRU);
+//   tick   - joins (column = e_site), then S steps of kpm_multi_step +
+//            kpm_multi_finalize per lane width over all models with busy
+//            lanes, S ending no later than the first lane that finishes;
+//   finish - for every finished request: moments (direct n <= M/2, doubled
+//            above) damped and summed over the energy grid on the device,
+//            the error estimate on the host, an FP64 recomputation
+//            (tbtkkpm_ldos_sites) of the sites past the tolerance, release
+//            of the lanes.
+// Submitters only queue and wait; all device work runs on the worker.
+#include "tbtkkpm.h"
+#include "kpm_host.h"
+#include "kpm_multi.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace tbtkkpm {
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+inline unsigned blocks_for(uint64_t n, unsigned bs = 256) { return (unsigned)((n + bs - 1) / bs); }
+
+constexpr uint32_t kMaxWidth = 64;
+
+bool valid_width(uint32_t w) { return w >= 1 && w <= kMaxWidth && (w & (w - 1)) == 0; }
+
+struct Request {
+  uint64_t id = 0;
+  uint32_t model = 0;
+  std::vector<uint32_t> sites;
+  uint32_t M = 0;
+  double broadening = 0;
+  Clock::time_point t_submit;
+  std::vector<uint32_t> lanes;
+  int32_t base = 0;
+  bool done = false;
+  int status = TBTKKPM_OK;
+  std::string message;
+  std::vector<double> ldos, err;
+  std::vector<int32_t> rerun;
+  // staging of the finish phase
+  std::vector<double2> raw, raw_direct;
+  size_t stage_off = 0;
+};
+
+struct Model {
+  uint32_t id = 0;
+  tbtkkpm_matrix *mat = nullptr;
+  tbtkkpm_table *table = nullptr;  // the server's table of this scale
+  uint32_t N = 0, W = 0;
+  double scale = 1;
+  bool resident = false;
+  uint64_t bytes = 0;
+  uint64_t last_tick = 0;
+  DevBuf vec[2], dots, mu, mu_direct, base, laneM, bitmap, tlist;
+  std::vector<int32_t> base_h;
+  std::vector<uint32_t> M_h;
+  std::vector<uint64_t> lane_req;  // request per lane, 0 when free
+  std::vector<uint32_t> lane_site;
+  std::vector<uint32_t> bitmap_h;
+  uint32_t busy = 0;
+  uint32_t tcount = 0;
+  bool dirty = true;
+  void release_lanes() {
+    for (DevBuf *b : {&vec[0], &vec[1], &dots, &mu, &mu_direct, &base, &laneM, &bitmap, &tlist})
+      b->release();
+    resident = false;
+  }
+};
+
+// Lane memory of a model: vectors, fixed-point sums, moments, lane tables,
+// target bitmap and list.
+uint64_t lane_bytes(uint32_t N, uint32_t W, uint32_t Mmax, uint32_t ld) {
+  return 2ull * N * W * sizeof(float2) + 2ull * W * sizeof(long long) +
+         (uint64_t)W * Mmax * sizeof(double2) + (uint64_t)W * ld * sizeof(double2) +
+         8ull * W + 4ull * ((N + 31) / 32) + 8ull * W;
+}
+
+const MultiEntry *find_multi(int tpr, int vpt, int minb) {
+  for (int i = 0; i < kNumMultiSteps; i++)
+    if (kMultiSteps[i].tpr == tpr && kMultiSteps[i].vpt == vpt && kMultiSteps[i].minb == minb)
+      return &kMultiSteps[i];
+  return nullptr;
+}
+
+// Default shape per width (measured choice of the single-model kernels:
+// few threads per row, several values each).
+std::array<int, 3> default_config(uint32_t W) {
+  switch (W) {
+    case 1: return {1, 1, 2};
+    case 2: return {2, 1, 2};
+    case 4: return {2, 2, 2};
+    case 8: return {4, 2, 2};
+    case 16: return {8, 2, 2};
+    case 32: return {8, 4, 2};
+    default: return {8, 8, 2};
+  }
+}
+
+}  // namespace
+}  // namespace tbtkkpm
+
+using namespace tbtkkpm;
+
+struct tbtkkpm_server {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint32_t Mmax = 0, E = 0, ld = 0;
+  std::vector<double> energies;
+  uint64_t budget = 0;
+  uint32_t tick_steps = 64;
+  double tol = 0;
+
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<std::unique_ptr<Model>> models;
+  std::map<double, tbtkkpm_table *> tables;                         // Mmax rows per scale
+  std::map<std::pair<uint32_t, double>, tbtkkpm_table *> exact;     // FP64 reruns
+  std::map<uint32_t, std::array<int, 3>> config;                    // width -> tpr, vpt, minb
+  std::deque<uint64_t> pending;
+  std::map<uint64_t, std::unique_ptr<Request>> requests;
+  uint64_t next_id = 1;
+  bool stop = false;
+  bool working = false;  // a tick or finish phase is running
+  int failed = 0;
+  std::string fail_msg;
+  std::thread worker;
+
+  int32_t n_global = 1;  // next global step
+  uint64_t tick_no = 0;
+  uint64_t resident = 0;
+  DevBuf d_models, d_hdr, d_joins, d_done, d_stage, d_damp;
+  // statistics
+  std::vector<double> latencies_ms;
+  double reruns = 0, ticks = 0, steps = 0, lane_steps = 0, evictions = 0, waited = 0, busy_s = 0;
+
+  const std::array<int, 3> &config_for(uint32_t W) {
+    auto it = config.find(W);
+    if (it == config.end()) it = config.emplace(W, default_config(W)).first;
+    return it->second;
+  }
+};
+
+namespace tbtkkpm {
+namespace {
+
+// ------------------------------------------------------------ admission
+
+int make_resident(tbtkkpm_server *s, Model *m) {
+  const uint32_t W = m->W, N = m->N;
+  const size_t words = (N + 31) / 32;
+  int rc;
+  if ((rc = m->vec[0].reserve(sizeof(float2) * (size_t)N * W)) ||
+      (rc = m->vec[1].reserve(sizeof(float2) * (size_t)N * W)) ||
+      (rc = m->dots.reserve(2 * sizeof(long long) * W)) ||
+      (rc = m->mu.reserve(sizeof(double2) * (size_t)W * s->Mmax)) ||
+      (rc = m->mu_direct.reserve(sizeof(double2) * (size_t)W * s->ld)) ||
+      (rc = m->base.reserve(4 * (size_t)W)) || (rc = m->laneM.reserve(4 * (size_t)W)) ||
+      (rc = m->bitmap.reserve(4 * words)) || (rc = m->tlist.reserve(8 * (size_t)W))) {
+    m->release_lanes();
+    return rc;
+  }
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(m->vec[0].ptr, 0, sizeof(float2) * (size_t)N * W, s->stream)) ||
+      (e = cudaMemsetAsync(m->vec[1].ptr, 0, sizeof(float2) * (size_t)N * W, s->stream)) ||
+      (e = cudaMemsetAsync(m->dots.ptr, 0, 2 * sizeof(long long) * W, s->stream))) {
+    m->release_lanes();
+    return cuda_fail(e, "server: lane memory");
+  }
+  m->base_h.assign(W, kLaneIdle);
+  m->M_h.assign(W, 0);
+  m->lane_req.assign(W, 0);
+  m->lane_site.assign(W, 0);
+  m->bitmap_h.assign(words, 0);
+  m->busy = 0;
+  m->dirty = true;
+  m->resident = true;
+  s->resident += m->bytes;
+  return TBTKKPM_OK;
+}
+
+void evict(tbtkkpm_server *s, Model *m) {
+  cudaStreamSynchronize(s->stream);
+  m->release_lanes();
+  s->resident -= m->bytes;
+  s->evictions += 1;
+}
+
+// Room for `need` more bytes: idle resident models leave, least recently
+// used first.  False if the busy ones alone leave no room.
+bool make_room(tbtkkpm_server *s, uint64_t need, const Model *keep) {
+  while (s->resident + need > s->budget) {
+    Model *victim = nullptr;
+    for (auto &p : s->models) {
+      Model *m = p.get();
+      if (m == keep || !m->resident || m->busy) continue;
+      if (!victim || m->last_tick < victim->last_tick) victim = m;
+    }
+    if (!victim) return false;
+    evict(s, victim);
+  }
+  return true;
+}
+
+// Under s->mu.  Queued requests take free lanes in arrival order; the joins
+// of this step boundary are appended.
+int admit(tbtkkpm_server *s, std::vector<MultiJoin> &joins) {
+  for (auto it = s->pending.begin(); it != s->pending.end();) {
+    Request *r = s->requests.at(*it).get();
+    Model *m = s->models[r->model].get();
+    const uint32_t K = (uint32_t)r->sites.size();
+    if (m->resident && m->W - m->busy < K) {
+      ++it;
+      continue;
+    }
+    if (!m->resident) {
+      if (!make_room(s, m->bytes, m)) {
+        s->waited += 1;
+        ++it;
+        continue;
+      }
+      int rc = make_resident(s, m);
+      if (rc == TBTKKPM_ERR_MEMORY) {
+        s->waited += 1;
+        ++it;
+        continue;
+      }
+      if (rc) return rc;
+    }
+    r->base = s->n_global - 1;
+    for (uint32_t c = 0, k = 0; c < m->W && k < K; c++) {
+      if (m->lane_req[c]) continue;
+      const uint32_t site = r->sites[k++];
+      m->lane_req[c] = r->id;
+      m->lane_site[c] = site;
+      m->base_h[c] = r->base;
+      m->M_h[c] = r->M;
+      m->bitmap_h[site >> 5] |= 1u << (site & 31);
+      r->lanes.push_back(c);
+      MultiJoin j;
+      j.x = m->vec[(s->n_global + 1) & 1].as<float2>();
+      j.mu = m->mu.as<double2>() + (size_t)c * s->Mmax;
+      j.mu_direct = m->mu_direct.as<double2>() + (size_t)c * s->ld;
+      j.rows = m->N;
+      j.col = c;
+      j.site = site;
+      j.W = m->W;
+      joins.push_back(j);
+    }
+    m->busy += K;
+    m->dirty = true;
+    it = s->pending.erase(it);
+  }
+  return TBTKKPM_OK;
+}
+
+// ------------------------------------------------------------ one tick
+
+struct ClassPlan {
+  uint32_t W;
+  const MultiEntry *entry;
+  std::vector<MultiModel> models;
+  uint32_t total_tiles = 0;
+};
+
+// Uploads the lane tables and targets of changed models (under s->mu; the
+// copies come from pageable memory, so the host arrays are free on return).
+int upload_lanes(tbtkkpm_server *s, Model *m) {
+  if (!m->dirty) return TBTKKPM_OK;
+  // target list: busy lanes sorted by site row
+  std::vector<std::pair<uint32_t, uint32_t>> t;
+  std::fill(m->bitmap_h.begin(), m->bitmap_h.end(), 0u);
+  for (uint32_t c = 0; c < m->W; c++)
+    if (m->lane_req[c]) {
+      t.push_back({m->lane_site[c], c});
+      m->bitmap_h[m->lane_site[c] >> 5] |= 1u << (m->lane_site[c] & 31);
+    }
+  std::sort(t.begin(), t.end());
+  std::vector<uint32_t> tl(2 * (size_t)m->W, 0);
+  for (size_t i = 0; i < t.size(); i++) {
+    tl[i] = t[i].first;
+    tl[m->W + i] = t[i].second;
+  }
+  m->tcount = (uint32_t)t.size();
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(m->base.ptr, m->base_h.data(), 4 * (size_t)m->W, cudaMemcpyHostToDevice,
+                           s->stream)) ||
+      (e = cudaMemcpyAsync(m->laneM.ptr, m->M_h.data(), 4 * (size_t)m->W, cudaMemcpyHostToDevice,
+                           s->stream)) ||
+      (e = cudaMemcpyAsync(m->bitmap.ptr, m->bitmap_h.data(), 4 * m->bitmap_h.size(),
+                           cudaMemcpyHostToDevice, s->stream)) ||
+      (e = cudaMemcpyAsync(m->tlist.ptr, tl.data(), 4 * tl.size(), cudaMemcpyHostToDevice,
+                           s->stream)))
+    return cuda_fail(e, "server: lane tables");
+  m->dirty = false;
+  return TBTKKPM_OK;
+}
+
+MultiModel describe(const tbtkkpm_server *s, const Model *m) {
+  MultiModel d{};
+  d.A.slice_ptr = m->mat->slice_ptr.as<uint32_t>();
+  d.A.col = m->mat->scol.as<uint32_t>();
+  d.A.val = m->mat->sval.as<double2>();
+  d.A.N = m->N;
+  d.A.nslices = m->mat->nslices;
+  d.vec[0] = m->vec[0].as<float2>();
+  d.vec[1] = m->vec[1].as<float2>();
+  d.bitmap = m->bitmap.as<uint32_t>();
+  d.trow = m->tlist.as<uint32_t>();
+  d.tcol = m->tlist.as<uint32_t>() + m->W;
+  d.tcount = m->tcount;
+  d.base = m->base.as<int32_t>();
+  d.lane_M = m->laneM.as<uint32_t>();
+  d.dots = m->dots.as<long long>();
+  d.mu = m->mu.as<double2>();
+  d.mu_direct = m->mu_direct.as<double2>();
+  (void)s;
+  return d;
+}
+
+// Builds the per-width launch plans of all models with busy lanes (under
+// s->mu).
+int plan_tick(tbtkkpm_server *s, std::vector<ClassPlan> &plans) {
+  std::map<uint32_t, size_t> index;
+  for (auto &p : s->models) {
+    Model *m = p.get();
+    if (!m->resident || !m->busy) continue;
+    int rc = upload_lanes(s, m);
+    if (rc) return rc;
+    m->last_tick = s->tick_no;
+    auto it = index.find(m->W);
+    if (it == index.end()) {
+      const auto &cfg = s->config_for(m->W);
+      ClassPlan cp;
+      cp.W = m->W;
+      cp.entry = find_multi(cfg[0], cfg[1], cfg[2]);
+      if (!cp.entry)
+        return fail(TBTKKPM_ERR_UNSUPPORTED, "server: no step kernel for width %u", m->W);
+      it = index.emplace(m->W, plans.size()).first;
+      plans.push_back(std::move(cp));
+    }
+    ClassPlan &cp = plans[it->second];
+    MultiModel d = describe(s, m);
+    const uint32_t rpb = kBlock / cp.entry->tpr;
+    d.tile0 = cp.total_tiles;
+    d.ntiles = (uint32_t)(((uint64_t)m->mat->nslices * 32 + rpb - 1) / rpb);
+    cp.total_tiles += d.ntiles;
+    cp.models.push_back(d);
+  }
+  return TBTKKPM_OK;
+}
+
+// Launches joins and `nsteps` steps of every plan starting at global step
+// s->n_global (worker thread, no lock held).
+int run_tick(tbtkkpm_server *s, const std::vector<MultiJoin> &joins,
+             const std::vector<ClassPlan> &plans, uint32_t nsteps) {
+  cudaStream_t st = s->stream;
+  int rc;
+  cudaError_t e;
+  if (!joins.empty()) {
+    if ((rc = s->d_joins.reserve(sizeof(MultiJoin) * joins.size()))) return rc;
+    if ((e = cudaMemcpyAsync(s->d_joins.ptr, joins.data(), sizeof(MultiJoin) * joins.size(),
+                             cudaMemcpyHostToDevice, st)))
+      return cuda_fail(e, "server: joins");
+    uint32_t rows = 0;
+    for (const MultiJoin &j : joins) rows = std::max(rows, j.rows);
+    const unsigned bx = std::max(1u, std::min(blocks_for(std::max(rows, s->Mmax)), 512u));
+    for (size_t j0 = 0; j0 < joins.size(); j0 += 65535) {
+      const unsigned nj = (unsigned)std::min<size_t>(65535, joins.size() - j0);
+      kpm_multi_join<<<dim3(bx, nj), 256, 0, st>>>(s->d_joins.as<MultiJoin>() + j0, s->Mmax, s->ld);
+    }
+    count_launches((joins.size() + 65534) / 65535);
+  }
+  // descriptors and headers of all plans in one upload
+  size_t nm = 0;
+  for (const ClassPlan &cp : plans) nm += cp.models.size();
+  std::vector<MultiModel> all;
+  all.reserve(nm);
+  std::vector<MultiHeader> hdr;
+  for (const ClassPlan &cp : plans) {
+    all.insert(all.end(), cp.models.begin(), cp.models.end());
+    hdr.push_back({(uint32_t)cp.models.size(), cp.total_tiles, s->n_global});
+  }
+  if ((rc = s->d_models.reserve(sizeof(MultiModel) * std::max<size_t>(nm, 1))) ||
+      (rc = s->d_hdr.reserve(sizeof(MultiHeader) * std::max<size_t>(hdr.size(), 1))))
+    return rc;
+  if ((e = cudaMemcpyAsync(s->d_models.ptr, all.data(), sizeof(MultiModel) * nm,
+                           cudaMemcpyHostToDevice, st)) ||
+      (e = cudaMemcpyAsync(s->d_hdr.ptr, hdr.data(), sizeof(MultiHeader) * hdr.size(),
+                           cudaMemcpyHostToDevice, st)))
+    return cuda_fail(e, "server: descriptors");
+  for (uint32_t k = 0; k < nsteps; k++) {
+    size_t off = 0;
+    for (size_t p = 0; p < plans.size(); p++) {
+      const ClassPlan &cp = plans[p];
+      const MultiModel *dm = s->d_models.as<MultiModel>() + off;
+      const MultiHeader *dh = s->d_hdr.as<MultiHeader>() + p;
+      cp.entry->launch(st, s->device, dm, dh, k, cp.W, s->ld);
+      kpm_multi_finalize<<<(unsigned)cp.models.size(), std::min<uint32_t>(std::max(cp.W, 32u), 64u), 0,
+                           st>>>(dm, dh, k, cp.W, s->Mmax, s->ld);
+      off += cp.models.size();
+    }
+  }
+  count_launches(2ull * nsteps * plans.size());
+  if ((e = cudaGetLastError())) return cuda_fail(e, "server: step launch");
+  return TBTKKPM_OK;
+}
+
+// ------------------------------------------------------------ finish
+
+tbtkkpm_table *exact_table(tbtkkpm_server *s, uint32_t M, double scale, int *rc) {
+  auto key = std::make_pair(M, scale);
+  auto it = s->exact.find(key);
+  if (it != s->exact.end()) return it->second;
+  tbtkkpm_table *t = nullptr;
+  const int prev = swap_selected_device(s->device);
+  *rc = tbtkkpm_table_create(M, s->energies.data(), s->E, scale, &t);
+  swap_selected_device(prev);
+  if (*rc) return nullptr;
+  s->exact[key] = t;
+  return t;
+}
+
+// Energy sums, error estimates and FP64 recomputations of the finished
+// requests (worker thread, no lock held; the requests are no longer
+// reachable by admission).
+int finish(tbtkkpm_server *s, const std::vector<Request *> &done,
+           const std::vector<Model *> &owner) {
+  if (done.empty()) return TBTKKPM_OK;
+  cudaStream_t st = s->stream;
+  const uint32_t E = s->E;
+  // stage layout per request: out [K][M] | raw [K][M] | raw_direct [K][M/2+1] | ldos [K][E]
+  size_t total = 0, lanes = 0, damp_len = 0;
+  for (Request *r : done) {
+    const size_t K = r->sites.size(), M = r->M;
+    r->stage_off = total;
+    total += sizeof(double2) * (2 * K * M + K * (M / 2 + 1)) + sizeof(double) * K * E;
+    total = (total + 255) & ~(size_t)255;
+    lanes += K;
+    damp_len += M;
+  }
+  int rc;
+  if ((rc = s->d_stage.reserve(total)) || (rc = s->d_done.reserve(sizeof(MultiDone) * lanes)) ||
+      (rc = s->d_damp.reserve(sizeof(double) * damp_len)))
+    return rc;
+  std::vector<MultiDone> lane_ptr;
+  std::vector<double> damp_all;
+  std::vector<double> bvals;
+  for (size_t i = 0; i < done.size(); i++) {
+    Request *r = done[i];
+    Model *m = owner[i];
+    for (uint32_t c : r->lanes)
+      lane_ptr.push_back({m->mu.as<double2>() + (size_t)c * s->Mmax,
+                          m->mu_direct.as<double2>() + (size_t)c * s->ld});
+    std::vector<double> a;
+    double b = 1;
+    if (r->broadening != 0) damping_factors(r->M, r->broadening, a, b);
+    else a.assign(r->M, 1.0);
+    damp_all.insert(damp_all.end(), a.begin(), a.end());
+    bvals.push_back(b);
+  }
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(s->d_done.ptr, lane_ptr.data(), sizeof(MultiDone) * lanes,
+                           cudaMemcpyHostToDevice, st)) ||
+      (e = cudaMemcpyAsync(s->d_damp.ptr, damp_all.data(), sizeof(double) * damp_len,
+                           cudaMemcpyHostToDevice, st)))
+    return cuda_fail(e, "server: finish staging");
+  size_t lane0 = 0, d0 = 0;
+  for (size_t i = 0; i < done.size(); i++) {
+    Request *r = done[i];
+    Model *m = owner[i];
+    const uint32_t K = (uint32_t)r->sites.size(), M = r->M;
+    char *base = s->d_stage.as<char>() + r->stage_off;
+    double2 *out = reinterpret_cast<double2 *>(base);
+    double2 *raw = out + (size_t)K * M;
+    double2 *rawd = raw + (size_t)K * M;
+    double *ldos = reinterpret_cast<double *>(rawd + (size_t)K * (M / 2 + 1));
+    kpm_multi_prepare<<<blocks_for((uint64_t)K * M), 256, 0, st>>>(
+        s->d_done.as<MultiDone>() + lane0, K, M, s->d_damp.as<double>() + d0, bvals[i],
+        r->broadening != 0, out, raw, rawd);
+    count_launches(1);
+    if ((rc = launch_energy_sum(st, m->table, out, K, 4, ldos, M))) return rc;
+    r->ldos.resize((size_t)K * E);
+    r->raw.resize((size_t)K * M);
+    r->raw_direct.resize((size_t)K * (M / 2 + 1));
+    if ((e = cudaMemcpyAsync(r->ldos.data(), ldos, sizeof(double) * K * E, cudaMemcpyDeviceToHost,
+                             st)) ||
+        (e = cudaMemcpyAsync(r->raw.data(), raw, sizeof(double2) * K * M, cudaMemcpyDeviceToHost,
+                             st)) ||
+        (e = cudaMemcpyAsync(r->raw_direct.data(), rawd, sizeof(double2) * K * (M / 2 + 1),
+                             cudaMemcpyDeviceToHost, st)))
+      return cuda_fail(e, "server: results");
+    lane0 += K;
+    d0 += M;
+  }
+  if ((e = cudaStreamSynchronize(st))) return cuda_fail(e, "server: finish");
+  for (size_t i = 0; i < done.size(); i++) {
+    Request *r = done[i];
+    Model *m = owner[i];
+    const uint32_t K = (uint32_t)r->sites.size(), M = r->M;
+    r->err.assign(K, 0.0);
+    r->rerun.assign(K, 0);
+    doubling_error(r->raw, r->raw_direct, K, M, M / 2 + 1, r->err.data());
+    r->raw.clear();
+    r->raw.shrink_to_fit();
+    r->raw_direct.clear();
+    r->raw_direct.shrink_to_fit();
+    std::vector<uint32_t> miss;
+    std::vector<uint32_t> idx;
+    for (uint32_t k = 0; k < K; k++)
+      if (s->tol > 0 && !(r->err[k] <= s->tol)) {
+        miss.push_back(r->sites[k]);
+        idx.push_back(k);
+      }
+    if (!miss.empty()) {
+      tbtkkpm_table *t = exact_table(s, M, m->scale, &rc);
+      if (!t) return rc;
+      std::vector<double> out((size_t)miss.size() * E);
+      if ((rc = tbtkkpm_ldos_sites(m->mat, t, miss.data(), (uint32_t)miss.size(), r->broadening,
+                                   TBTKKPM_FP64, out.data(), nullptr)))
+        return rc;
+      for (size_t q = 0; q < idx.size(); q++) {
+        std::memcpy(r->ldos.data() + (size_t)idx[q] * E, out.data() + q * E, sizeof(double) * E);
+        r->rerun[idx[q]] = 1;
+      }
+      s->reruns += (double)miss.size();
+    }
+  }
+  return TBTKKPM_OK;
+}
+
+// ------------------------------------------------------------ worker
+
+void fail_all(tbtkkpm_server *s, int rc, const std::string &msg) {
+  s->failed = rc;
+  s->fail_msg = msg;
+  for (auto &p : s->requests) {
+    Request *r = p.second.get();
+    if (!r->done) {
+      r->done = true;
+      r->status = rc;
+      r->message = msg;
+    }
+  }
+  s->pending.clear();
+  s->cv_done.notify_all();
+}
+
+void worker(tbtkkpm_server *s) {
+  cudaSetDevice(s->device);
+  swap_selected_device(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (!s->stop) {
+    bool busy = false;
+    for (auto &p : s->models) busy = busy || (p->resident && p->busy);
+    if (!busy && s->pending.empty()) {
+      s->cv_work.wait(lk);
+      continue;
+    }
+    const auto t0 = Clock::now();
+    s->working = true;
+    std::vector<MultiJoin> joins;
+    int rc = admit(s, joins);
+    std::vector<ClassPlan> plans;
+    if (!rc) rc = plan_tick(s, plans);
+    if (rc) {
+      fail_all(s, rc, tbtkkpm_last_error());
+      break;
+    }
+    if (plans.empty()) {
+      // queued work that cannot start yet (it waits for memory)
+      s->working = false;
+      s->cv_work.wait_for(lk, std::chrono::milliseconds(5));
+      continue;
+    }
+    // steps until the first busy lane finishes, at most tick_steps
+    uint32_t nsteps = s->tick_steps;
+    for (auto &p : s->models) {
+      Model *m = p.get();
+      if (!m->resident || !m->busy) continue;
+      for (uint32_t c = 0; c < m->W; c++)
+        if (m->lane_req[c]) {
+          const int64_t last = (int64_t)m->base_h[c] + m->M_h[c] / 2;  // global step of the last local step
+          const int64_t left = last - (int64_t)s->n_global + 1;
+          nsteps = (uint32_t)std::min<int64_t>(nsteps, std::max<int64_t>(left, 1));
+        }
+    }
+    s->tick_no += 1;
+    lk.unlock();
+    rc = run_tick(s, joins, plans, nsteps);
+    cudaError_t e = cudaSuccess;
+    if (!rc && (e = cudaStreamSynchronize(s->stream)) != cudaSuccess)
+      rc = cuda_fail(e, "server: tick");
+    lk.lock();
+    if (rc) {
+      fail_all(s, rc, tbtkkpm_last_error());
+      break;
+    }
+    s->n_global += (int32_t)nsteps;
+    s->ticks += 1;
+    s->steps += nsteps;
+    // finished requests: every lane past its last local step
+    std::vector<Request *> done;
+    std::vector<Model *> owner;
+    for (auto &p : s->models) {
+      Model *m = p.get();
+      if (!m->resident || !m->busy) continue;
+      for (uint32_t c = 0; c < m->W; c++) {
+        const uint64_t id = m->lane_req[c];
+        if (!id) continue;
+        Request *r = s->requests.at(id).get();
+        if (r->lanes.empty() || r->lanes[0] != c) continue;  // one entry per request
+        if ((int64_t)r->base + r->M / 2 <= (int64_t)s->n_global - 1) {
+          done.push_back(r);
+          owner.push_back(m);
+        }
+      }
+    }
+    lk.unlock();
+    rc = finish(s, done, owner);
+    lk.lock();
+    if (rc) {
+      fail_all(s, rc, tbtkkpm_last_error());
+      break;
+    }
+    const auto t1 = Clock::now();
+    s->busy_s += std::chrono::duration<double>(t1 - t0).count();
+    for (size_t i = 0; i < done.size(); i++) {
+      Request *r = done[i];
+      Model *m = owner[i];
+      for (uint32_t c : r->lanes) {
+        m->lane_req[c] = 0;
+        m->base_h[c] = kLaneIdle;
+        m->M_h[c] = 0;
+      }
+      m->busy -= (uint32_t)r->lanes.size();
+      m->dirty = true;
+      s->lane_steps += (double)r->lanes.size() * (r->M / 2);
+      s->latencies_ms.push_back(std::chrono::duration<double, std::milli>(t1 - r->t_submit).count());
+      r->done = true;
+    }
+    s->working = false;
+    if (!done.empty()) s->cv_done.notify_all();
+  }
+  s->working = false;
+}
+
+}  // namespace
+}  // namespace tbtkkpm
+
+// ---------------------------------------------------------------- C ABI
+
+extern "C" int tbtkkpm_server_create(uint32_t max_moments, const double *energies, uint32_t E,
+                                     uint64_t hbm_budget, uint32_t tick_steps, double tolerance,
+                                     tbtkkpm_server **out) {
+  if (!out) return fail(TBTKKPM_ERR_ARGUMENT, "server_create: out is NULL");
+  *out = nullptr;
+  if (max_moments < 2) return fail(TBTKKPM_ERR_ARGUMENT, "server_create: max_moments < 2");
+  if (!energies || E == 0) return fail(TBTKKPM_ERR_ARGUMENT, "server_create: empty energy grid");
+  if (hbm_budget == 0) return fail(TBTKKPM_ERR_ARGUMENT, "server_create: hbm_budget is 0");
+  int ndev = 0;
+  tbtkkpm_device_count(&ndev);
+  if (ndev == 0) return fail(TBTKKPM_ERR_CUDA, "no CUDA device available");
+  auto *s = new tbtkkpm_server();
+  s->device = current_device();
+  s->Mmax = max_moments;
+  s->ld = max_moments / 2 + 1;
+  s->E = E;
+  s->energies.assign(energies, energies + E);
+  s->budget = hbm_budget;
+  s->tick_steps = tick_steps ? tick_steps : 64;
+  s->tol = tolerance;
+  {
+    DeviceGuard g(s->device);
+    cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      delete s;
+      return cuda_fail(e, "server_create: stream");
+    }
+  }
+  s->worker = std::thread(worker, s);
+  *out = s;
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_server_add_model(tbtkkpm_server *s, const uint32_t *rowptr,
+                                        const uint32_t *col, const double *val, uint32_t N,
+                                        double scale, uint32_t width, uint32_t *model) {
+  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_add_model: NULL server");
+  if (!model) return fail(TBTKKPM_ERR_ARGUMENT, "server_add_model: model is NULL");
+  if (!valid_width(width))
+    return fail(TBTKKPM_ERR_ARGUMENT, "server_add_model: width %u is not a power of two in [1, %u]",
+                width, kMaxWidth);
+  for (uint32_t e = 0; e < s->E; e++)
+    if (!(std::fabs(s->energies[e]) < scale))
+      return fail(TBTKKPM_ERR_ARGUMENT,
+                  "server_add_model: energy %g outside (-s, s) for s=%g", s->energies[e], scale);
+  auto m = std::make_unique<Model>();
+  const int prev = swap_selected_device(s->device);
+  int rc = tbtkkpm_matrix_create_csr(rowptr, col, val, N, scale, &m->mat);
+  tbtkkpm_table *t = nullptr;
+  bool new_table = false;
+  if (!rc) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->tables.find(scale);
+    if (it != s->tables.end()) t = it->second;
+  }
+  if (!rc && !t) {
+    rc = tbtkkpm_table_create(s->Mmax, s->energies.data(), s->E, scale, &t);
+    new_table = rc == 0;
+  }
+  swap_selected_device(prev);
+  if (rc) {
+    tbtkkpm_matrix_destroy(m->mat);
+    return rc;
+  }
+  m->N = N;
+  m->W = width;
+  m->scale = scale;
+  m->bytes = lane_bytes(N, width, s->Mmax, s->ld);
+  if (m->bytes > s->budget) {
+    tbtkkpm_matrix_destroy(m->mat);
+    if (new_table) tbtkkpm_table_destroy(t);
+    return fail(TBTKKPM_ERR_MEMORY,
+                "server_add_model: lane memory of %llu bytes exceeds the budget of %llu",
+                (unsigned long long)m->bytes, (unsigned long long)s->budget);
+  }
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (new_table) {
+    auto ins = s->tables.emplace(scale, t);
+    if (!ins.second) tbtkkpm_table_destroy(t);  // another thread made one meanwhile
+  }
+  m->table = s->tables.at(scale);
+  m->id = (uint32_t)s->models.size();
+  *model = m->id;
+  s->models.push_back(std::move(m));
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_server_submit(tbtkkpm_server *s, uint32_t model, const uint32_t *sites,
+                                     uint32_t n_sites, uint32_t M, double broadening,
+                                     uint64_t *request) {
+  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: NULL server");
+  if (!request || (!sites && n_sites)) return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: NULL pointer");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->failed) return fail(s->failed, "server: %s", s->fail_msg.c_str());
+  if (model >= s->models.size())
+    return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: no model %u", model);
+  Model *m = s->models[model].get();
+  if (n_sites == 0 || n_sites > m->W)
+    return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: %u sites for a model of %u lanes", n_sites,
+                m->W);
+  if (M < 2 || M > s->Mmax)
+    return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: M=%u outside [2, %u]", M, s->Mmax);
+  if (!(broadening >= 0)) return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: broadening < 0");
+  for (uint32_t k = 0; k < n_sites; k++)
+    if (sites[k] >= m->N)
+      return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: site %u >= N=%u", sites[k], m->N);
+  auto r = std::make_unique<Request>();
+  r->id = s->next_id++;
+  r->model = model;
+  r->sites.assign(sites, sites + n_sites);
+  r->M = M;
+  r->broadening = broadening;
+  r->t_submit = Clock::now();
+  *request = r->id;
+  s->pending.push_back(r->id);
+  s->requests.emplace(r->id, std::move(r));
+  s->cv_work.notify_one();
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_server_wait(tbtkkpm_server *s, uint64_t request, double timeout_s,
+                                   double *ldos_out, double *err_out, int32_t *rerun_out) {
+  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_wait: NULL server");
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->requests.find(request);
+  if (it == s->requests.end())
+    return fail(TBTKKPM_ERR_ARGUMENT, "server_wait: no request %llu", (unsigned long long)request);
+  Request *r = it->second.get();
+  if (!r->done && timeout_s > 0) {
+    const auto until = Clock::now() + std::chrono::duration_cast<Clock::duration>(
+                                          std::chrono::duration<double>(timeout_s));
+    s->cv_done.wait_until(lk, until, [&] { return r->done; });
+  }
+  if (!r->done) return TBTKKPM_PENDING;
+  if (r->status) {
+    const int rc = fail(r->status, "server: %s", r->message.c_str());
+    s->requests.erase(it);
+    return rc;
+  }
+  const size_t K = r->sites.size();
+  if (ldos_out) std::memcpy(ldos_out, r->ldos.data(), sizeof(double) * K * s->E);
+  if (err_out) std::memcpy(err_out, r->err.data(), sizeof(double) * K);
+  if (rerun_out) std::memcpy(rerun_out, r->rerun.data(), sizeof(int32_t) * K);
+  s->requests.erase(it);
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_server_stats(tbtkkpm_server *s, double *out, uint32_t n) {
+  if (!s || (!out && n)) return fail(TBTKKPM_ERR_ARGUMENT, "server_stats: NULL pointer");
+  std::lock_guard<std::mutex> lk(s->mu);
+  double v[TBTKKPM_STAT_COUNT] = {0};
+  std::vector<double> l = s->latencies_ms;
+  v[TBTKKPM_STAT_COMPLETED] = (double)l.size();
+  if (!l.empty()) {
+    std::sort(l.begin(), l.end());
+    auto pct = [&](double p) {
+      const size_t i = (size_t)std::min<double>(l.size() - 1, std::ceil(p * l.size()) - 1);
+      return l[i];
+    };
+    v[TBTKKPM_STAT_P50_MS] = pct(0.50);
+    v[TBTKKPM_STAT_P99_MS] = pct(0.99);
+    double sum = 0;
+    for (double x : l) sum += x;
+    v[TBTKKPM_STAT_MEAN_MS] = sum / l.size();
+  }
+  v[TBTKKPM_STAT_RERUNS] = s->reruns;
+  v[TBTKKPM_STAT_TICKS] = s->ticks;
+  v[TBTKKPM_STAT_STEPS] = s->steps;
+  v[TBTKKPM_STAT_LANE_STEPS] = s->lane_steps;
+  v[TBTKKPM_STAT_RESIDENT] = (double)s->resident;
+  v[TBTKKPM_STAT_EVICTIONS] = s->evictions;
+  v[TBTKKPM_STAT_WAITED] = s->waited;
+  v[TBTKKPM_STAT_BUSY_S] = s->busy_s;
+  for (uint32_t i = 0; i < n && i < TBTKKPM_STAT_COUNT; i++) out[i] = v[i];
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_server_set_config(tbtkkpm_server *s, uint32_t width, int tpr, int vpt,
+                                         int minb) {
+  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_set_config: NULL server");
+  if (!valid_width(width) || tpr * vpt != (int)width || !find_multi(tpr, vpt, minb))
+    return fail(TBTKKPM_ERR_UNSUPPORTED,
+                "server_set_config: no compiled step (tpr=%d, vpt=%d, minb=%d) for width %u", tpr,
+                vpt, minb, width);
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->config[width] = {tpr, vpt, minb};
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32_t probe_steps,
+                                       int *tpr, int *vpt, int *minb, double *ms_per_step) {
+  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_autotune: NULL server");
+  if (!valid_width(width)) return fail(TBTKKPM_ERR_ARGUMENT, "server_autotune: bad width %u", width);
+  if (probe_steps < 2) return fail(TBTKKPM_ERR_ARGUMENT, "server_autotune: probe_steps < 2");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->failed) return fail(s->failed, "server: %s", s->fail_msg.c_str());
+  if (s->working || !s->pending.empty())
+    return fail(TBTKKPM_ERR_STATE, "server_autotune: the server is busy");
+  for (auto &p : s->models)
+    if (p->busy) return fail(TBTKKPM_ERR_STATE, "server_autotune: the server is busy");
+  const Model *probe = nullptr;
+  for (auto &p : s->models)
+    if (p->W == width && (!probe || p->N > probe->N)) probe = p.get();
+  if (!probe) return fail(TBTKKPM_ERR_STATE, "server_autotune: no model of width %u", width);
+  DeviceGuard g(s->device);
+  cudaStream_t st = s->stream;
+  // a private copy of the lane state: every lane busy from global step 1
+  const uint32_t W = width, N = probe->N, Mp = 2 * probe_steps + 2, ldp = Mp / 2 + 1;
+  DevBuf vec[2], dots, mu, mud, base, laneM, bitmap, tlist, dm, dh;
+  int rc;
+  if ((rc = vec[0].reserve(sizeof(float2) * (size_t)N * W)) ||
+      (rc = vec[1].reserve(sizeof(float2) * (size_t)N * W)) ||
+      (rc = dots.reserve(2 * sizeof(long long) * W)) || (rc = mu.reserve(sizeof(double2) * W * Mp)) ||
+      (rc = mud.reserve(sizeof(double2) * W * ldp)) || (rc = base.reserve(4 * W)) ||
+      (rc = laneM.reserve(4 * W)) || (rc = bitmap.reserve(4 * (size_t)((N + 31) / 32))) ||
+      (rc = tlist.reserve(8 * W)) || (rc = dm.reserve(sizeof(MultiModel))) ||
+      (rc = dh.reserve(sizeof(MultiHeader))))
+    return rc;
+  std::vector<int32_t> base_h(W, 0);
+  std::vector<uint32_t> M_h(W, Mp), bm((N + 31) / 32, 0), tl(2 * (size_t)W);
+  std::vector<std::pair<uint32_t, uint32_t>> t;
+  std::vector<MultiJoin> joins;
+  for (uint32_t c = 0; c < W; c++) {
+    const uint32_t site = (uint32_t)((uint64_t)c * N / W);
+    t.push_back({site, c});
+    bm[site >> 5] |= 1u << (site & 31);
+    joins.push_back({vec[0].as<float2>(), mu.as<double2>() + (size_t)c * Mp,
+                     mud.as<double2>() + (size_t)c * ldp, N, c, site, W});
+  }
+  std::sort(t.begin(), t.end());
+  for (uint32_t i = 0; i < W; i++) {
+    tl[i] = t[i].first;
+    tl[W + i] = t[i].second;
+  }
+  cudaError_t e;
+  DevBuf dj;
+  if ((rc = dj.reserve(sizeof(MultiJoin) * W))) return rc;
+  if ((e = cudaMemsetAsync(vec[1].ptr, 0, sizeof(float2) * (size_t)N * W, st)) ||
+      (e = cudaMemsetAsync(dots.ptr, 0, 2 * sizeof(long long) * W, st)) ||
+      (e = cudaMemcpyAsync(base.ptr, base_h.data(), 4 * W, cudaMemcpyHostToDevice, st)) ||
+      (e = cudaMemcpyAsync(laneM.ptr, M_h.data(), 4 * W, cudaMemcpyHostToDevice, st)) ||
+      (e = cudaMemcpyAsync(bitmap.ptr, bm.data(), 4 * bm.size(), cudaMemcpyHostToDevice, st)) ||
+      (e = cudaMemcpyAsync(tlist.ptr, tl.data(), 4 * tl.size(), cudaMemcpyHostToDevice, st)) ||
+      (e = cudaMemcpyAsync(dj.ptr, joins.data(), sizeof(MultiJoin) * W, cudaMemcpyHostToDevice, st)))
+    return cuda_fail(e, "server_autotune: staging");
+  kpm_multi_join<<<dim3(std::max(1u, std::min(blocks_for(std::max(N, Mp)), 512u)), W), 256, 0, st>>>(
+      dj.as<MultiJoin>(), Mp, ldp);
+  count_launches(1);
+  cudaEvent_t ev[2];
+  cudaEventCreate(&ev[0]);
+  cudaEventCreate(&ev[1]);
+  const MultiEntry *best = nullptr;
+  double best_ms = 0;
+  int32_t n = 1;
+  for (int i = 0; i < kNumMultiSteps && !rc; i++) {
+    const MultiEntry &en = kMultiSteps[i];
+    if ((uint32_t)(en.tpr * en.vpt) != W) continue;
+    MultiModel d{};
+    d.A.slice_ptr = probe->mat->slice_ptr.as<uint32_t>();
+    d.A.col = probe->mat->scol.as<uint32_t>();
+    d.A.val = probe->mat->sval.as<double2>();
+    d.A.N = N;
+    d.A.nslices = probe->mat->nslices;
+    d.vec[0] = vec[0].as<float2>();
+    d.vec[1] = vec[1].as<float2>();
+    d.bitmap = bitmap.as<uint32_t>();
+    d.trow = tlist.as<uint32_t>();
+    d.tcol = tlist.as<uint32_t>() + W;
+    d.tcount = W;
+    d.base = base.as<int32_t>();
+    d.lane_M = laneM.as<uint32_t>();
+    d.dots = dots.as<long long>();
+    d.mu = mu.as<double2>();
+    d.mu_direct = mud.as<double2>();
+    d.tile0 = 0;
+    d.ntiles = (uint32_t)(((uint64_t)d.A.nslices * 32 + kBlock / en.tpr - 1) / (kBlock / en.tpr));
+    MultiHeader h{1, d.ntiles, n};
+    // parity of the buffers follows the global step, so the probe keeps
+    // counting across configurations
+    if ((e = cudaMemcpyAsync(dm.ptr, &d, sizeof(d), cudaMemcpyHostToDevice, st)) ||
+        (e = cudaMemcpyAsync(dh.ptr, &h, sizeof(h), cudaMemcpyHostToDevice, st))) {
+      rc = cuda_fail(e, "server_autotune: descriptors");
+      break;
+    }
+    for (uint32_t k = 0; k < probe_steps; k++) {
+      if (k == 1) cudaEventRecord(ev[0], st);
+      en.launch(st, s->device, dm.as<MultiModel>(), dh.as<MultiHeader>(), k, W, ldp);
+      kpm_multi_finalize<<<1, std::min<uint32_t>(std::max(W, 32u), 64u), 0, st>>>(
+          dm.as<MultiModel>(), dh.as<MultiHeader>(), k, W, Mp, ldp);
+    }
+    count_launches(2ull * probe_steps);
+    cudaEventRecord(ev[1], st);
+    if ((e = cudaEventSynchronize(ev[1])) != cudaSuccess) {
+      rc = cuda_fail(e, "server_autotune: probe");
+      break;
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev[0], ev[1]);
+    const double per = ms / (probe_steps - 1);
+    if (!best || per < best_ms) {
+      best = &en;
+      best_ms = per;
+    }
+    n += (int32_t)probe_steps;
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  cudaStreamSynchronize(st);
+  if (rc) return rc;
+  if (!best) return fail(TBTKKPM_ERR_UNSUPPORTED, "server_autotune: no kernel for width %u", W);
+  s->config[W] = {best->tpr, best->vpt, best->minb};
+  if (tpr) *tpr = best->tpr;
+  if (vpt) *vpt = best->vpt;
+  if (minb) *minb = best->minb;
+  if (ms_per_step) *ms_per_step = best_ms;
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_server_destroy(tbtkkpm_server *s) {
+  if (!s) return TBTKKPM_OK;
+  {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+  }
+  s->cv_work.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  {
+    DeviceGuard g(s->device);
+    cudaStreamSynchronize(s->stream);
+    for (auto &p : s->models) {
+      p->release_lanes();
+      tbtkkpm_matrix_destroy(p->mat);
+    }
+    for (auto &t : s->tables) tbtkkpm_table_destroy(t.second);
+    for (auto &t : s->exact) tbtkkpm_table_destroy(t.second);
+    for (DevBuf *b : {&s->d_models, &s->d_hdr, &s->d_joins, &s->d_done, &s->d_stage, &s->d_damp})
+      b->release();
+    cudaStreamDestroy(s->stream);
+  }
+  delete s;
+  return TBTKKPM_OK;
+}

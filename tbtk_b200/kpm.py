@@ -85,7 +85,19 @@ SIGNATURES = [
     ("tbtkkpm_matrix_autotune", _i, [_p, _u32, _i, _i, _u32, _p, _p, _p, _p]),
     ("tbtkkpm_matrix_set_config", _i, [_p, _u32, _i, _i, _i, _i, _i]),
     ("tbtkkpm_step_configs", _i, [_i, _i, _p, _i]),
+    ("tbtkkpm_server_create", _i, [_u32, _p, _u32, _u64, _u32, _d, _p]),
+    ("tbtkkpm_server_add_model", _i, [_p, _p, _p, _p, _u32, _d, _u32, _p]),
+    ("tbtkkpm_server_submit", _i, [_p, _u32, _p, _u32, _u32, _d, _p]),
+    ("tbtkkpm_server_wait", _i, [_p, _u64, _d, _p, _p, _p]),
+    ("tbtkkpm_server_stats", _i, [_p, _p, _u32]),
+    ("tbtkkpm_server_autotune", _i, [_p, _u32, _u32, _p, _p, _p, _p]),
+    ("tbtkkpm_server_set_config", _i, [_p, _u32, _i, _i, _i]),
+    ("tbtkkpm_server_destroy", _i, [_p]),
 ]
+
+PENDING = 1
+STAT_NAMES = ["completed", "p50_ms", "p99_ms", "mean_ms", "reruns", "ticks", "steps",
+              "lane_steps", "resident_bytes", "evictions", "waited", "busy_s"]
 
 
 def step_configs(precision, ldos=True):
@@ -338,6 +350,76 @@ class Table:
     def close(self):
         if getattr(self, "_h", None):
             load_library().tbtkkpm_table_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+
+class Server:
+    """Continuous-batching LDOS service over many device-resident models
+    (the C ABI's ``tbtkkpm_server``).  ``submit`` queues the LDOS of up to
+    ``width`` sites of a registered model and returns a request id;
+    ``wait`` returns ``(ldos [K][E], err [K], rerun [K])`` once it is done
+    (``None`` on timeout).  Any thread may submit and wait."""
+
+    def __init__(self, max_moments, energies, hbm_budget, tick_steps=64, tolerance=1e-6):
+        self.energies = np.ascontiguousarray(energies, dtype=np.float64)
+        self.E = self.energies.size
+        h = ctypes.c_void_p()
+        _check(load_library().tbtkkpm_server_create(
+            int(max_moments), _ptr(self.energies), self.E, int(hbm_budget), int(tick_steps),
+            float(tolerance), ctypes.byref(h)))
+        self._h = h
+        self._sites = {}
+
+    def add_model(self, rowptr, col, val, scale, width):
+        rowptr, col, val = _u32a(rowptr), _u32a(col), _cxa(val)
+        mid = ctypes.c_uint32()
+        _check(load_library().tbtkkpm_server_add_model(
+            self._h, _ptr(rowptr), _ptr(col), _ptr(val), rowptr.size - 1, float(scale),
+            int(width), ctypes.byref(mid)))
+        return mid.value
+
+    def submit(self, model, sites, M, broadening):
+        sites = _u32a(sites)
+        rid = ctypes.c_uint64()
+        _check(load_library().tbtkkpm_server_submit(self._h, int(model), _ptr(sites), sites.size,
+                                                    int(M), float(broadening), ctypes.byref(rid)))
+        self._sites[rid.value] = sites.size
+        return rid.value
+
+    def wait(self, request, timeout=600.0):
+        K = self._sites[request]
+        ldos = np.zeros((K, self.E), dtype=np.float64)
+        err = np.zeros(K, dtype=np.float64)
+        rerun = np.zeros(K, dtype=np.int32)
+        rc = load_library().tbtkkpm_server_wait(self._h, ctypes.c_uint64(request), float(timeout),
+                                                _ptr(ldos), _ptr(err), _ptr(rerun))
+        if rc == PENDING:
+            return None
+        del self._sites[request]
+        _check(rc)
+        return ldos, err, rerun
+
+    def stats(self):
+        out = np.zeros(len(STAT_NAMES), dtype=np.float64)
+        _check(load_library().tbtkkpm_server_stats(self._h, _ptr(out), out.size))
+        return dict(zip(STAT_NAMES, out.tolist()))
+
+    def autotune(self, width, probe_steps=8):
+        t, v, m, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        _check(load_library().tbtkkpm_server_autotune(
+            self._h, int(width), int(probe_steps), ctypes.byref(t), ctypes.byref(v),
+            ctypes.byref(m), ctypes.byref(ms)))
+        return {"tpr": t.value, "vpt": v.value, "minb": m.value, "ms_per_step": ms.value}
+
+    def set_config(self, width, tpr, vpt, minb):
+        _check(load_library().tbtkkpm_server_set_config(self._h, int(width), int(tpr), int(vpt),
+                                                        int(minb)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().tbtkkpm_server_destroy(self._h)
             self._h = None
 
     __del__ = close

@@ -1,0 +1,255 @@
+"""The LDOS server (tbtkkpm_server_*): continuous batching over many models.
+
+Parity: every result against tbtkkpm_ldos_sites on the same model (FP64:
+the reference-exact path, pinned against TBTK elsewhere) within the mixed
+precision bar, and bit-identical whether a request runs alone or among
+others, joins at step 1 or in the middle of other requests, and whatever
+the step configuration.
+"""
+import threading
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from tbtk_b200 import workloads
+
+S = 12.0
+E = 200
+TOL_MIXED = 1e-6
+
+
+def grid():
+    return workloads.open_grid(S, E)
+
+
+def models():
+    """Square, Rashba and honeycomb models of different sizes."""
+    return [
+        ("square", workloads.square_csr(24, 24, J=0.5, W=2.0, seed=1)),
+        ("rashba", workloads.square_csr(20, 20, J=0.5, W=2.0, alpha=0.3, seed=2)),
+        ("honeycomb", workloads.honeycomb_csr(16, 16, J=0.3, W=1.0, seed=3)),
+        ("small", workloads.square_csr(8, 8, J=0.2, W=1.0, seed=4)),
+    ]
+
+
+def fp64_ldos(kpm, csr, sites, M, broadening):
+    m = kpm.Matrix.from_csr(*csr, S)
+    t = kpm.Table.create(M, grid(), S)
+    out, _ = m.ldos_sites(t, sites, broadening, kpm.FP64)
+    return out
+
+
+@pytest.mark.gpu
+def test_server_matches_fp64_ldos(gpu):
+    kpm = gpu
+    srv = kpm.Server(512, grid(), hbm_budget=1 << 30, tick_steps=16, tolerance=0)
+    ms = models()
+    ids = [srv.add_model(*csr, S, 8) for _, csr in ms]
+    rng = np.random.default_rng(0)
+    jobs = []
+    for i, (_, csr) in enumerate(ms):
+        N = csr[0].size - 1
+        for M in (64, 257, 512):
+            sites = rng.choice(N, size=int(rng.integers(1, 9)), replace=False).astype(np.uint32)
+            jobs.append((i, csr, sites, M, srv.submit(ids[i], sites, M, 1e-3)))
+    for i, csr, sites, M, rid in jobs:
+        ldos, err, rerun = srv.wait(rid)
+        ref = fp64_ldos(kpm, csr, sites, M, 1e-3)
+        assert not rerun.any()
+        for k in range(sites.size):
+            assert rel_err(ldos[k], ref[k]) <= TOL_MIXED, (ms[i][0], M, k)
+            assert 0 <= err[k] < 1e-4
+    st = srv.stats()
+    assert st["completed"] == len(jobs)
+    assert st["p99_ms"] >= st["p50_ms"] > 0
+    srv.close()
+
+
+def _solo(kpm, csr, sites, M, broadening, width, config=None):
+    srv = kpm.Server(512, grid(), hbm_budget=1 << 30, tick_steps=16, tolerance=0)
+    mid = srv.add_model(*csr, S, width)
+    if config:
+        srv.set_config(width, *config)
+    out = srv.wait(srv.submit(mid, sites, M, broadening))
+    srv.close()
+    return out
+
+
+@pytest.mark.gpu
+def test_server_result_alone_equals_in_mix(gpu):
+    kpm = gpu
+    name, csr = models()[1]
+    probe_sites = np.array([5, 77, 300], dtype=np.uint32)
+    alone = _solo(kpm, csr, probe_sites, 384, 1e-3, 8)
+
+    srv = kpm.Server(512, grid(), hbm_budget=1 << 30, tick_steps=7, tolerance=0)
+    ms = models()
+    ids = [srv.add_model(*c, S, 8) for _, c in ms]
+    rng = np.random.default_rng(1)
+    # background traffic on every model, the probe request in the middle
+    bg = []
+    for r in range(12):
+        i = r % len(ms)
+        N = ms[i][1][0].size - 1
+        sites = rng.choice(N, size=int(rng.integers(1, 6)), replace=False).astype(np.uint32)
+        bg.append(srv.submit(ids[i], sites, int(rng.integers(16, 512)), 1e-3))
+    import time
+    time.sleep(0.05)
+    rid = srv.submit(ids[1], probe_sites, 384, 1e-3)
+    more = [srv.submit(ids[1], np.array([1, 2], dtype=np.uint32), 100, 1e-3)]
+    mixed = srv.wait(rid)
+    for b in bg + more:
+        srv.wait(b)
+    for a, b in zip(alone, mixed):
+        assert np.array_equal(a, b)
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_server_result_independent_of_configuration(gpu):
+    kpm = gpu
+    _, csr = models()[0]
+    sites = np.array([0, 33, 101, 400], dtype=np.uint32)
+    ref = _solo(kpm, csr, sites, 200, 1e-3, 16)
+    for cfg in [(8, 2, 1), (4, 4, 2), (2, 8, 1)]:
+        got = _solo(kpm, csr, sites, 200, 1e-3, 16, cfg)
+        for a, b in zip(ref, got):
+            assert np.array_equal(a, b), cfg
+
+
+@pytest.mark.gpu
+def test_server_widths(gpu):
+    kpm = gpu
+    _, csr = models()[3]
+    sites = np.array([3], dtype=np.uint32)
+    ref = _solo(kpm, csr, sites, 128, 1e-3, 1)
+    for w in (2, 4, 8, 16, 32, 64):
+        got = _solo(kpm, csr, sites, 128, 1e-3, w)
+        for a, b in zip(ref, got):
+            assert np.array_equal(a, b), w
+
+
+@pytest.mark.gpu
+def test_server_fp64_rerun_on_miss(gpu):
+    kpm = gpu
+    _, csr = models()[0]
+    srv = kpm.Server(512, grid(), hbm_budget=1 << 30, tick_steps=16, tolerance=1e-300)
+    mid = srv.add_model(*csr, S, 4)
+    sites = np.array([7, 8, 200], dtype=np.uint32)
+    ldos, err, rerun = srv.wait(srv.submit(mid, sites, 256, 1e-3))
+    assert rerun.all()
+    assert np.array_equal(ldos, fp64_ldos(kpm, csr, sites, 256, 1e-3))
+    assert srv.stats()["reruns"] == 3
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_server_hbm_budget_admission(gpu):
+    """A budget for one model's lanes: requests to two models alternate
+    through eviction and still give the right answers."""
+    kpm = gpu
+    ms = models()[:2]
+    probe = kpm.Server(256, grid(), hbm_budget=1 << 30, tick_steps=8, tolerance=0)
+    probe.add_model(*ms[0][1], S, 8)
+    probe.close()
+    N0 = ms[0][1][0].size - 1
+    N1 = ms[1][1][0].size - 1
+    need = max(2 * N * 8 * 8 + 8 * (256 + 129) * 16 + 1024 + N // 8 for N in (N0, N1))
+    srv = kpm.Server(256, grid(), hbm_budget=need, tick_steps=8, tolerance=0)
+    ids = [srv.add_model(*c, S, 8) for _, c in ms]
+    jobs = []
+    for r in range(6):
+        i = r % 2
+        sites = np.array([r, r + 10], dtype=np.uint32)
+        jobs.append((i, sites, srv.submit(ids[i], sites, 128, 1e-3)))
+    for i, sites, rid in jobs:
+        ldos, _, _ = srv.wait(rid)
+        ref = fp64_ldos(kpm, ms[i][1], sites, 128, 1e-3)
+        assert rel_err(ldos, ref) <= TOL_MIXED
+    st = srv.stats()
+    assert st["evictions"] >= 1
+    assert st["resident_bytes"] <= need
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_server_concurrent_submitters(gpu):
+    kpm = gpu
+    ms = models()
+    srv = kpm.Server(256, grid(), hbm_budget=1 << 30, tick_steps=8, tolerance=0)
+    ids = [srv.add_model(*c, S, 16) for _, c in ms]
+    results = {}
+    lock = threading.Lock()
+
+    def client(t):
+        rng = np.random.default_rng(100 + t)
+        for _ in range(5):
+            i = int(rng.integers(len(ms)))
+            N = ms[i][1][0].size - 1
+            sites = rng.choice(N, size=int(rng.integers(1, 5)), replace=False).astype(np.uint32)
+            M = int(rng.integers(8, 256))
+            out = srv.wait(srv.submit(ids[i], sites, M, 1e-3))
+            with lock:
+                results[(t, len(results))] = (i, sites, M, out)
+
+    th = [threading.Thread(target=client, args=(t,)) for t in range(4)]
+    for x in th:
+        x.start()
+    for x in th:
+        x.join()
+    assert len(results) == 20
+    for i, sites, M, (ldos, _, _) in results.values():
+        assert rel_err(ldos, fp64_ldos(kpm, ms[i][1], sites, M, 1e-3)) <= TOL_MIXED
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_server_argument_errors(gpu):
+    kpm = gpu
+    _, csr = models()[3]
+    srv = kpm.Server(128, grid(), hbm_budget=1 << 30, tick_steps=8, tolerance=0)
+    with pytest.raises(kpm.TBTKError):
+        srv.add_model(*csr, S, 3)               # width not a power of two
+    with pytest.raises(kpm.TBTKError):
+        srv.add_model(*csr, 5.0, 4)             # energies outside (-s, s)
+    mid = srv.add_model(*csr, S, 4)
+    with pytest.raises(kpm.TBTKError):
+        srv.submit(mid, np.arange(5), 64, 1e-3)  # more sites than lanes
+    with pytest.raises(kpm.TBTKError):
+        srv.submit(mid, [0], 129, 1e-3)          # M above max_moments
+    with pytest.raises(kpm.TBTKError):
+        srv.submit(mid, [0], 1, 1e-3)            # M < 2
+    with pytest.raises(kpm.TBTKError):
+        srv.submit(mid, [10 ** 6], 64, 1e-3)     # site outside the model
+    with pytest.raises(kpm.TBTKError):
+        srv.submit(mid + 1, [0], 64, 1e-3)       # no such model
+    with pytest.raises(kpm.TBTKError):
+        srv.set_config(4, 8, 8, 2)               # shape of another width
+    srv.close()
+    small = kpm.Server(128, grid(), hbm_budget=1000, tick_steps=8, tolerance=0)
+    with pytest.raises(kpm.TBTKError):
+        small.add_model(*csr, S, 4)              # lanes exceed the budget
+    small.close()
+
+
+@pytest.mark.gpu
+def test_server_autotune(gpu):
+    kpm = gpu
+    _, csr = models()[0]
+    srv = kpm.Server(256, grid(), hbm_budget=1 << 30, tick_steps=8, tolerance=0)
+    mid = srv.add_model(*csr, S, 16)
+    cfg = srv.autotune(16, probe_steps=4)
+    assert cfg["tpr"] * cfg["vpt"] == 16 and cfg["ms_per_step"] > 0
+    sites = np.array([1, 2, 3], dtype=np.uint32)
+    ldos, _, _ = srv.wait(srv.submit(mid, sites, 128, 1e-3))
+    assert rel_err(ldos, fp64_ldos(kpm, csr, sites, 128, 1e-3)) <= TOL_MIXED
+    srv.close()
+
+
+def test_server_needs_a_device(kpm):
+    if kpm.device_count() > 0:
+        pytest.skip("a GPU is visible")
+    with pytest.raises(kpm.TBTKError) as e:
+        kpm.Server(128, grid(), hbm_budget=1 << 20)
+    assert e.value.status == kpm.ERR_CUDA
