@@ -309,7 +309,11 @@ TBTKKPM_API int tbtkkpm_server_wait(
 #define TBTKKPM_STAT_EVICTIONS 9
 #define TBTKKPM_STAT_WAITED 10    /* admissions deferred by the budget */
 #define TBTKKPM_STAT_BUSY_S 11    /* worker time with lanes in flight */
-#define TBTKKPM_STAT_COUNT 12
+#define TBTKKPM_STAT_STEP_S 12    /* device time of the recursion steps */
+#define TBTKKPM_STAT_STEP_BYTES 13 /* algorithmic bytes of those steps */
+#define TBTKKPM_STAT_FINISH_S 14  /* worker time in energy sums and results */
+#define TBTKKPM_STAT_RERUN_S 15   /* of which FP64 recomputations */
+#define TBTKKPM_STAT_COUNT 16
 TBTKKPM_API int tbtkkpm_server_stats(tbtkkpm_server *s, double *out, uint32_t n);
 
 /* Times every compiled step configuration of lane width `width` for

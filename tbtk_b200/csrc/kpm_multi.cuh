@@ -46,22 +46,25 @@ struct MultiModel {
   uint32_t ntiles;
 };
 
-// Per-tick launch header (device resident): the models, their tile total
-// and the global step of step offset 0.
+// Per-tick launch header (device resident): the models, their tile total,
+// the global step of step offset 0 and the model of every tile.
 struct MultiHeader {
   uint32_t nmodels;
   uint32_t total_tiles;
   int32_t n_base;
+  const uint32_t *tile_model;  // [total_tiles]
 };
 
-__device__ __forceinline__ uint32_t multi_find(const MultiModel *models, uint32_t nmodels,
-                                               uint32_t w) {
-  uint32_t lo = 0, hi = nmodels;  // last model with tile0 <= w
-  while (hi - lo > 1) {
-    const uint32_t mid = (lo + hi) >> 1;
-    if (__ldg(&models[mid].tile0) <= w) lo = mid; else hi = mid;
-  }
-  return lo;
+// A block takes runs of kRun consecutive tiles (run r, r + gridDim.x, ...),
+// so it changes model (and flushes its sums) at most once per run.
+constexpr uint32_t kRun = 8;
+
+// Fills the tile -> model map of a launch: one block per model.
+static __global__ void kpm_multi_tilemap(const MultiModel *__restrict__ models,
+                                         const MultiHeader *__restrict__ hdr, uint32_t *tile_model) {
+  if (blockIdx.x >= hdr->nmodels) return;
+  const uint32_t t0 = models[blockIdx.x].tile0, nt = models[blockIdx.x].ntiles;
+  for (uint32_t t = threadIdx.x; t < nt; t += blockDim.x) tile_model[t0 + t] = blockIdx.x;
 }
 
 template <typename P, int VPT, int TPR>
@@ -84,8 +87,8 @@ __device__ __forceinline__ void multi_flush(long long (&s_nn)[VPT], long long (&
   }
 }
 
-// One recursion step for every model of the launch.  Blocks stride over the
-// concatenated tiles (kBlock/TPR rows each) of all models; a tile's row
+// One recursion step for every model of the launch.  Blocks take runs of
+// the concatenated tiles (kBlock/TPR rows each) of all models; a tile's row
 // fetch is issued one tile ahead as in kpm_step.
 template <int TPR, int VPT, int MINB>
 __global__ void __launch_bounds__(kBlock, MINB)
@@ -104,6 +107,7 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
   const int grp = threadIdx.x / TPR;
   const unsigned mask = 0xffffffffu;
   const uint32_t nmodels = hdr->nmodels, total = hdr->total_tiles;
+  const uint32_t *__restrict__ tile_model = hdr->tile_model;
   const int32_t n = hdr->n_base + (int32_t)step_offset;
   if (nmodels == 0) return;
 
@@ -117,6 +121,7 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
   const float2 *x = nullptr;
   float2 *y = nullptr;
   const float2 *fy = nullptr;
+  uint32_t ft0 = 0;    // first tile of the fetched tile's model
   uint32_t first = 0;  // bit j: lane of value j is at its local step 1
   // fields of the current model kept in registers
   const uint32_t *t_bitmap = nullptr, *t_row = nullptr, *t_col = nullptr;
@@ -126,7 +131,7 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
   uint32_t t_count = 0;
 
   auto fetch = [&](uint32_t w, RowFetch<V, AR, TPR, VPT, PF> &f, uint32_t &fmodel) {
-    const uint32_t i = multi_find(models, nmodels, w);
+    const uint32_t i = __ldg(tile_model + w);
     if (i != fi) {
       fi = i;
       const MultiModel *q = models + i;
@@ -136,15 +141,23 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
       FA.N = q->A.N;
       FA.nslices = q->A.nslices;
       fy = q->vec[n & 1];
+      ft0 = q->tile0;
     }
     fmodel = i;
-    fetch_row<V, AR, TPR, VPT, PF, false>(FA, W, fy, w - __ldg(&models[i].tile0), grp, sub, f);
+    fetch_row<V, AR, TPR, VPT, PF, false>(FA, W, fy, w - ft0, grp, sub, f);
+  };
+  // the tile after w in this block's order
+  auto next_tile = [&](uint32_t w) -> uint32_t {
+    const uint32_t nw = w + 1;
+    if (nw % kRun != 0) return nw;
+    return (w / kRun + gridDim.x) * kRun;
   };
 
   RowFetch<V, AR, TPR, VPT, PF> cur, nxt;
   uint32_t cur_model = 0, nxt_model = 0;
-  if (blockIdx.x < total) fetch(blockIdx.x, cur, cur_model);
-  for (uint32_t w = blockIdx.x; w < total; w += gridDim.x) {
+  uint32_t w = blockIdx.x * kRun;
+  if (w < total) fetch(w, cur, cur_model);
+  for (; w < total; w = next_tile(w)) {
     if (cur_model != mi) {
       // block-uniform: every thread of the block is on the same tile
       if (mi != kPad) multi_flush<P, VPT, TPR>(s_nn, s_np, t_dots, W, sub);
@@ -169,7 +182,7 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
       for (int j = 0; j < VPT; j++)
         if (n - __ldg(t_base + P::col_of(sub, j)) == 1) first |= 1u << j;
     }
-    const uint32_t wn = w + gridDim.x;
+    const uint32_t wn = next_tile(w);
     if (wn < total) fetch(wn, nxt, nxt_model);
     if (cur.ok) {
       const uint32_t row = cur.row, l = cur.l, cb = cur.cb, ce = cur.ce, wd = ce - cb;

@@ -147,10 +147,12 @@ struct tbtkkpm_server {
   int32_t n_global = 1;  // next global step
   uint64_t tick_no = 0;
   uint64_t resident = 0;
-  DevBuf d_models, d_hdr, d_joins, d_done, d_stage, d_damp;
+  DevBuf d_models, d_hdr, d_joins, d_done, d_stage, d_damp, d_tiles;
   // statistics
   std::vector<double> latencies_ms;
   double reruns = 0, ticks = 0, steps = 0, lane_steps = 0, evictions = 0, waited = 0, busy_s = 0;
+  double step_s = 0, step_bytes = 0, finish_s = 0, rerun_s = 0;
+  cudaEvent_t ev[2] = {nullptr, nullptr};  // around the steps of a tick
 
   const std::array<int, 3> &config_for(uint32_t W) {
     auto it = config.find(W);
@@ -279,6 +281,7 @@ struct ClassPlan {
   const MultiEntry *entry;
   std::vector<MultiModel> models;
   uint32_t total_tiles = 0;
+  double bytes = 0;  // algorithmic bytes of one step
 };
 
 // Uploads the lane tables and targets of changed models (under s->mu; the
@@ -363,6 +366,9 @@ int plan_tick(tbtkkpm_server *s, std::vector<ClassPlan> &plans) {
     d.tile0 = cp.total_tiles;
     d.ntiles = (uint32_t)(((uint64_t)m->mat->nslices * 32 + rpb - 1) / rpb);
     cp.total_tiles += d.ntiles;
+    // matrix once (value + column index, row pointers) and three vector
+    // passes of the lanes
+    cp.bytes += 20.0 * m->mat->nnz + 4.0 * (m->N + 1) + 3.0 * m->N * m->W * sizeof(float2);
     cp.models.push_back(d);
   }
   return TBTKKPM_OK;
@@ -395,9 +401,15 @@ int run_tick(tbtkkpm_server *s, const std::vector<MultiJoin> &joins,
   std::vector<MultiModel> all;
   all.reserve(nm);
   std::vector<MultiHeader> hdr;
+  size_t tiles = 0;
+  for (const ClassPlan &cp : plans) tiles += cp.total_tiles;
+  if ((rc = s->d_tiles.reserve(sizeof(uint32_t) * std::max<size_t>(tiles, 1)))) return rc;
+  tiles = 0;
   for (const ClassPlan &cp : plans) {
     all.insert(all.end(), cp.models.begin(), cp.models.end());
-    hdr.push_back({(uint32_t)cp.models.size(), cp.total_tiles, s->n_global});
+    hdr.push_back({(uint32_t)cp.models.size(), cp.total_tiles, s->n_global,
+                   s->d_tiles.as<uint32_t>() + tiles});
+    tiles += cp.total_tiles;
   }
   if ((rc = s->d_models.reserve(sizeof(MultiModel) * std::max<size_t>(nm, 1))) ||
       (rc = s->d_hdr.reserve(sizeof(MultiHeader) * std::max<size_t>(hdr.size(), 1))))
@@ -407,6 +419,18 @@ int run_tick(tbtkkpm_server *s, const std::vector<MultiJoin> &joins,
       (e = cudaMemcpyAsync(s->d_hdr.ptr, hdr.data(), sizeof(MultiHeader) * hdr.size(),
                            cudaMemcpyHostToDevice, st)))
     return cuda_fail(e, "server: descriptors");
+  {
+    size_t off = 0, toff = 0;
+    for (size_t p = 0; p < plans.size(); p++) {
+      kpm_multi_tilemap<<<(unsigned)plans[p].models.size(), 256, 0, st>>>(
+          s->d_models.as<MultiModel>() + off, s->d_hdr.as<MultiHeader>() + p,
+          s->d_tiles.as<uint32_t>() + toff);
+      off += plans[p].models.size();
+      toff += plans[p].total_tiles;
+    }
+    count_launches(plans.size());
+  }
+  cudaEventRecord(s->ev[0], st);
   for (uint32_t k = 0; k < nsteps; k++) {
     size_t off = 0;
     for (size_t p = 0; p < plans.size(); p++) {
@@ -419,6 +443,7 @@ int run_tick(tbtkkpm_server *s, const std::vector<MultiJoin> &joins,
       off += cp.models.size();
     }
   }
+  cudaEventRecord(s->ev[1], st);
   count_launches(2ull * nsteps * plans.size());
   if ((e = cudaGetLastError())) return cuda_fail(e, "server: step launch");
   return TBTKKPM_OK;
@@ -531,6 +556,7 @@ int finish(tbtkkpm_server *s, const std::vector<Request *> &done,
         idx.push_back(k);
       }
     if (!miss.empty()) {
+      const auto r0 = Clock::now();
       tbtkkpm_table *t = exact_table(s, M, m->scale, &rc);
       if (!t) return rc;
       std::vector<double> out((size_t)miss.size() * E);
@@ -542,6 +568,7 @@ int finish(tbtkkpm_server *s, const std::vector<Request *> &done,
         r->rerun[idx[q]] = 1;
       }
       s->reruns += (double)miss.size();
+      s->rerun_s += std::chrono::duration<double>(Clock::now() - r0).count();
     }
   }
   return TBTKKPM_OK;
@@ -617,6 +644,10 @@ void worker(tbtkkpm_server *s) {
     s->n_global += (int32_t)nsteps;
     s->ticks += 1;
     s->steps += nsteps;
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]) == cudaSuccess) s->step_s += ms * 1e-3;
+    cudaGetLastError();
+    for (const ClassPlan &cp : plans) s->step_bytes += cp.bytes * nsteps;
     // finished requests: every lane past its last local step
     std::vector<Request *> done;
     std::vector<Model *> owner;
@@ -635,8 +666,11 @@ void worker(tbtkkpm_server *s) {
       }
     }
     lk.unlock();
+    const auto f0 = Clock::now();
     rc = finish(s, done, owner);
+    const double fs = std::chrono::duration<double>(Clock::now() - f0).count();
     lk.lock();
+    s->finish_s += fs;
     if (rc) {
       fail_all(s, rc, tbtkkpm_last_error());
       break;
@@ -691,6 +725,8 @@ extern "C" int tbtkkpm_server_create(uint32_t max_moments, const double *energie
   {
     DeviceGuard g(s->device);
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev[0]);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->ev[1]);
     if (e != cudaSuccess) {
       delete s;
       return cuda_fail(e, "server_create: stream");
@@ -841,6 +877,10 @@ extern "C" int tbtkkpm_server_stats(tbtkkpm_server *s, double *out, uint32_t n) 
   v[TBTKKPM_STAT_EVICTIONS] = s->evictions;
   v[TBTKKPM_STAT_WAITED] = s->waited;
   v[TBTKKPM_STAT_BUSY_S] = s->busy_s;
+  v[TBTKKPM_STAT_STEP_S] = s->step_s;
+  v[TBTKKPM_STAT_STEP_BYTES] = s->step_bytes;
+  v[TBTKKPM_STAT_FINISH_S] = s->finish_s;
+  v[TBTKKPM_STAT_RERUN_S] = s->rerun_s;
   for (uint32_t i = 0; i < n && i < TBTKKPM_STAT_COUNT; i++) out[i] = v[i];
   return TBTKKPM_OK;
 }
@@ -876,7 +916,7 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
   cudaStream_t st = s->stream;
   // a private copy of the lane state: every lane busy from global step 1
   const uint32_t W = width, N = probe->N, Mp = 2 * probe_steps + 2, ldp = Mp / 2 + 1;
-  DevBuf vec[2], dots, mu, mud, base, laneM, bitmap, tlist, dm, dh;
+  DevBuf vec[2], dots, mu, mud, base, laneM, bitmap, tlist, dm, dh, tmap;
   int rc;
   if ((rc = vec[0].reserve(sizeof(float2) * (size_t)N * W)) ||
       (rc = vec[1].reserve(sizeof(float2) * (size_t)N * W)) ||
@@ -944,7 +984,13 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
     d.mu_direct = mud.as<double2>();
     d.tile0 = 0;
     d.ntiles = (uint32_t)(((uint64_t)d.A.nslices * 32 + kBlock / en.tpr - 1) / (kBlock / en.tpr));
-    MultiHeader h{1, d.ntiles, n};
+    // one model: every tile maps to model 0
+    if ((rc = tmap.reserve(4 * (size_t)d.ntiles))) break;
+    if ((e = cudaMemsetAsync(tmap.ptr, 0, 4 * (size_t)d.ntiles, st))) {
+      rc = cuda_fail(e, "server_autotune: tile map");
+      break;
+    }
+    MultiHeader h{1, d.ntiles, n, tmap.as<uint32_t>()};
     // parity of the buffers follows the global step, so the probe keeps
     // counting across configurations
     if ((e = cudaMemcpyAsync(dm.ptr, &d, sizeof(d), cudaMemcpyHostToDevice, st)) ||
@@ -1003,8 +1049,11 @@ extern "C" int tbtkkpm_server_destroy(tbtkkpm_server *s) {
     }
     for (auto &t : s->tables) tbtkkpm_table_destroy(t.second);
     for (auto &t : s->exact) tbtkkpm_table_destroy(t.second);
-    for (DevBuf *b : {&s->d_models, &s->d_hdr, &s->d_joins, &s->d_done, &s->d_stage, &s->d_damp})
+    for (DevBuf *b : {&s->d_models, &s->d_hdr, &s->d_joins, &s->d_done, &s->d_stage, &s->d_damp,
+                      &s->d_tiles})
       b->release();
+    for (cudaEvent_t &ev : s->ev)
+      if (ev) cudaEventDestroy(ev);
     cudaStreamDestroy(s->stream);
   }
   delete s;

@@ -166,6 +166,40 @@ def cfg4_specs(n_models=1000, seed=4):
     return specs
 
 
+def cfg5_pool(n_models=64, seed=5):
+    """Serving pool: (kind, L, J, W, alpha, model seed) with the basis size
+    log-uniform in [1e3, 4e6] over square, honeycomb and Rashba lattices."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pool = []
+    for i in range(n_models):
+        kind = ("square", "honeycomb", "rashba")[i % 3]
+        N = float(np.exp(rng.uniform(np.log(1e3), np.log(4e6))))
+        per_cell = 4 if kind == "honeycomb" else 2
+        L = max(8, int(round((N / per_cell) ** 0.5)))
+        J = float(rng.uniform(0, 1))
+        W = float(rng.uniform(0, 3))
+        pool.append((kind, L, J, W, 0.3 if kind == "rashba" else 0.0, seed * 100000 + i))
+    return pool
+
+
+def cfg5_requests(pool_sizes, rate, duration, seed=55, max_sites=16, m_range=(512, 4096)):
+    """Poisson arrivals at `rate` per second for `duration` seconds: (time,
+    model, sites, M) with 1..max_sites distinct sites and M uniform in
+    m_range."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    t = 0.0
+    while True:
+        t += float(rng.exponential(1.0 / rate))
+        if t >= duration:
+            return out
+        m = int(rng.integers(len(pool_sizes)))
+        k = int(rng.integers(1, max_sites + 1))
+        sites = rng.choice(pool_sizes[m], size=k, replace=False).astype(np.uint32)
+        M = int(rng.integers(m_range[0], m_range[1] + 1))
+        out.append((t, m, sites, M))
+
+
 def build_model(kind, L, J, W, seed, alpha=0.0):
     if kind == "square":
         return square_csr(L, L, t=1.0, J=J, W=W, seed=seed)
