@@ -135,6 +135,15 @@ def make_problem(args, rank):
     return p
 
 
+def max_over_ranks(values, dist, device):
+    """Element-wise maximum of per-rank timings; every rank gets it."""
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def step_bytes(p, B, s_vec):
     """Algorithmic bytes of one recursion step: the CSR matrix once (values,
     column indices, row pointers) and three vector passes per source
@@ -350,12 +359,7 @@ def ours(args, world, rank, local):
                + p.energies.nbytes)
         e2e = {"seconds": e2e_s, "h2d": h2d, "d2h": B * p.energies.size * 8}
 
-    # max over ranks
-    times = torch.tensor([total_ms, e2e["seconds"] if e2e else 0.0], dtype=torch.float64,
-                         device="cuda")
-    if dist:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    total_ms, e2e_max = times.tolist()
+    total_ms, e2e_max = max_over_ranks([total_ms, e2e["seconds"] if e2e else 0.0], dist, "cuda")
 
     if rank != 0:
         if dist:

@@ -83,8 +83,20 @@ const StepEntry *find_step(int cls, int tpr, int vpt, int minb) {
 
 uint64_t tune_key(int cls, uint32_t Bp) { return ((uint64_t)cls << 32) | Bp; }
 
+// Autotuning results of this process by (device, class, padded width, N,
+// nnz): a new handle for a matrix of a tuned shape starts with the tuned
+// configuration.
+using ShapeKey = std::array<uint64_t, 5>;
+std::mutex g_tuned_mu;
+std::map<ShapeKey, std::array<int, 3>> g_tuned;
+
+ShapeKey shape_key(const tbtkkpm_matrix *m, int cls, uint32_t Bp) {
+  return {(uint64_t)m->device, (uint64_t)cls, Bp, m->N, m->nnz};
+}
+
 // The configuration of a batch: a forced entry, the handle's tuned choice
-// for this (class, padded width), or the default shape with MINB 2.
+// for this (class, padded width), this process's choice for a matrix of the
+// same shape, or the default shape with MINB 2.
 const StepEntry *pick_step(const tbtkkpm_matrix *m, int precision, bool dots, uint32_t B,
                            const StepEntry *force) {
   if (force) return force;
@@ -94,6 +106,14 @@ const StepEntry *pick_step(const tbtkkpm_matrix *m, int precision, bool dots, ui
   if (it != m->tuned.end()) {
     const StepEntry *e = find_step(cls, it->second[0], it->second[1], it->second[2]);
     if (e) return e;
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_tuned_mu);
+    auto git = g_tuned.find(shape_key(m, cls, s.bp()));
+    if (git != g_tuned.end()) {
+      const StepEntry *e = find_step(cls, git->second[0], git->second[1], git->second[2]);
+      if (e) return e;
+    }
   }
   return find_step(cls, s.tpr, s.vpt, 2);
 }
@@ -732,6 +752,10 @@ extern "C" int tbtkkpm_matrix_autotune(tbtkkpm_matrix *m, uint32_t B, int precis
   if (rc) return rc;
   if (!best) return fail(TBTKKPM_ERR_UNSUPPORTED, "matrix_autotune: no configuration for %u", B);
   m->tuned[tune_key(cls, Bp)] = {best->tpr, best->vpt, best->minb};
+  {
+    std::lock_guard<std::mutex> lk(g_tuned_mu);
+    g_tuned[shape_key(m, cls, Bp)] = {best->tpr, best->vpt, best->minb};
+  }
   if (tpr) *tpr = best->tpr;
   if (vpt) *vpt = best->vpt;
   if (minb) *minb = best->minb;
