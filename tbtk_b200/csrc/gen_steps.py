@@ -37,6 +37,18 @@ STAGE_META = 384  # StageMeta rounded up to 128 B (kpm_bulk.cuh)
 WMAX = 12
 
 
+# cp.async-staged kernels (complex64 only): values per lane, stages, staged
+# entries per row, warps per block.
+ASYNC_VPT = [1, 2, 4]
+ASYNC_STAGES = [2, 3, 4]
+ASYNC_WMAX = [6, 10]
+ASYNC_WPB = [4]
+
+
+def async_smem(vpt, s, wmax, wpb):
+    return s * wpb * (wmax + 1) * 32 * vpt * 8 + wpb * 32 * 2 * 8
+
+
 def bulk_smem(V, vpt, s, wpb, dots):
     size = {"double2": 16, "float2": 8}[V]
     stage = STAGE_META + (WMAX + 1) * 32 * vpt * size
@@ -77,6 +89,14 @@ def main():
             for (s, wpb) in BULK_VARIANTS:
                 if bulk_smem(V, p, s, wpb, dots) <= SMEM_LIMIT:
                     lines.append(f"    TBTKKPM_BULK_ENTRY({cls}, {V}, {AR}, {p}, {dots}, {s}, {wpb}),")
+        if V == "float2":
+            for p in ASYNC_VPT:
+                for s in ASYNC_STAGES:
+                    for wmax in ASYNC_WMAX:
+                        for wpb in ASYNC_WPB:
+                            if async_smem(p, s, wmax, wpb) <= SMEM_LIMIT:
+                                lines.append(f"    TBTKKPM_ASYNC_ENTRY({cls}, {p}, {dots}, {s}, "
+                                             f"{wmax}, {wpb}),")
         lines += ["};", f"const int kNum{table[1:]} = sizeof({table}) / sizeof({table}[0]);", "",
                   "}  // namespace tbtkkpm", ""]
         (HERE / fname).write_text("\n".join(lines))

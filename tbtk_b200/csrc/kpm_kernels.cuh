@@ -264,9 +264,16 @@ __device__ __forceinline__ void pack_store(V *row, int sub, Acc (&acc)[VPT]) {
   else P::store(row, sub, acc);
 }
 
-// The prefetched part of a row: slice bounds, first entries and j_{n-1}
-// (prefetching j_{n-1} a row ahead measured faster than loading it with the
-// row's gathers, despite the registers it holds).
+// j_{n-1} is prefetched a row ahead when a thread's share of it is at most
+// 64 bytes: measured faster than loading it at the start of its own row for
+// every compiled shape, including (8, 8) complex64 where the second copy
+// costs spills.
+template <typename V, int VPT> __host__ __device__ constexpr bool prefetch_y() {
+  return sizeof(V) * VPT <= 64;
+}
+
+// The prefetched part of a row: slice bounds, first entries and (see
+// prefetch_y) j_{n-1}.
 template <typename V, typename AR, int TPR, int VPT, int PF>
 struct RowFetch {
   using L = typename Pack<V, TPR, VPT>::L;
@@ -274,7 +281,7 @@ struct RowFetch {
   bool ok, live;
   uint32_t cc[PF];  // column indices of entries sub + q*TPR (TPR > 1) or q (TPR == 1)
   typename AR::Val vv[TPR > 1 ? PF : 1];
-  L yr[Pack<V, TPR, VPT>::NL];
+  L yr[prefetch_y<V, VPT>() ? Pack<V, TPR, VPT>::NL : 1];
 };
 
 template <typename V, typename AR, int TPR, int VPT, int PF, bool FIRST>
@@ -298,8 +305,22 @@ __device__ __forceinline__ void fetch_row(const Sell &A, uint32_t Bp, const V *y
       f.vv[q] = f.cc[q] != kPad ? AR::value(A, (uint64_t)(f.cb + k) * 32 + f.l)
                                 : typename AR::Val{0, 0};
   }
-  if constexpr (!FIRST)
+  if constexpr (!FIRST && prefetch_y<V, VPT>())
     if (f.live) Pack<V, TPR, VPT>::load_rw(y + (uint64_t)f.row * Bp, sub, f.yr);
+}
+
+// j_{n-1} of the current row: the prefetched copy, or a load issued now.
+template <typename V, typename AR, int TPR, int VPT, int PF>
+__device__ __forceinline__ void row_y(const RowFetch<V, AR, TPR, VPT, PF> &f, const V *y,
+                                      uint32_t Bp, int sub,
+                                      typename Pack<V, TPR, VPT>::L (&out)[Pack<V, TPR, VPT>::NL]) {
+  constexpr int NL = Pack<V, TPR, VPT>::NL;
+  if constexpr (prefetch_y<V, VPT>()) {
+#pragma unroll
+    for (int q = 0; q < NL; q++) out[q] = f.yr[q];
+  } else {
+    if (f.live) Pack<V, TPR, VPT>::load_rw(y + (uint64_t)f.row * Bp, sub, out);
+  }
 }
 
 template <typename V, typename AR, int TPR, int VPT, bool FIRST, bool DOTS, int MINB>
@@ -320,7 +341,9 @@ kpm_step(Sell A, uint32_t Bp, const V *__restrict__ x, V *__restrict__ y, Target
   const int grp = threadIdx.x / TPR;
   const unsigned mask = 0xffffffffu;
   // <j_{n+1}|j_{n+1}> and Re<j_{n+1}|j_n> per owned column (real for a
-  // Hermitian H and a diagonal moment)
+  // Hermitian H and a diagonal moment).  Kept in registers: measured 4-7%
+  // faster for the (8, 8) complex64 shape than per-thread sums in shared
+  // memory, although the registers cost about 200 spilled bytes there.
   double d_nn[DOTS ? VPT : 1], d_np[DOTS ? VPT : 1];
   if constexpr (DOTS) {
 #pragma unroll
@@ -337,12 +360,15 @@ kpm_step(Sell A, uint32_t Bp, const V *__restrict__ x, V *__restrict__ y, Target
     if (cur.ok) {
       const uint32_t row = cur.row, l = cur.l, cb = cur.cb, ce = cur.ce, w = ce - cb;
       Acc acc[VPT];
+      if constexpr (FIRST) {
 #pragma unroll
-      for (int j = 0; j < VPT; j++) {
-        if constexpr (FIRST) {
-          acc[j] = Acc{0, 0};
-        } else {
-          const Acc v = cur.live ? pack_get<P, Acc>(cur.yr, j) : Acc{0, 0};
+        for (int j = 0; j < VPT; j++) acc[j] = Acc{0, 0};
+      } else {
+        L yv[NL];
+        row_y(cur, y, Bp, sub, yv);
+#pragma unroll
+        for (int j = 0; j < VPT; j++) {
+          const Acc v = cur.live ? pack_get<P, Acc>(yv, j) : Acc{0, 0};
           acc[j] = Acc{-v.x, -v.y};
         }
       }

@@ -67,12 +67,15 @@ static __global__ void kpm_multi_tilemap(const MultiModel *__restrict__ models,
   for (uint32_t t = threadIdx.x; t < nt; t += blockDim.x) tile_model[t0 + t] = blockIdx.x;
 }
 
+// Adds a thread's fixed-point sums (msum[j][tid] for <j|j>, msum[VPT + j]
+// for <j|j_prev>) into the model's dots: a sum over the warp's threads of
+// the same columns, then one atomic per column and warp; clears the sums.
 template <typename P, int VPT, int TPR>
-__device__ __forceinline__ void multi_flush(long long (&s_nn)[VPT], long long (&s_np)[VPT],
-                                            long long *dots, uint32_t W, int sub) {
+__device__ __forceinline__ void multi_flush(long long (*msum)[kBlock], long long *dots,
+                                            uint32_t W, int sub) {
 #pragma unroll
   for (int j = 0; j < VPT; j++) {
-    long long a = s_nn[j], b = s_np[j];
+    long long a = msum[j][threadIdx.x], b = msum[VPT + j][threadIdx.x];
 #pragma unroll
     for (int off = TPR; off < 32; off <<= 1) {
       a += __shfl_xor_sync(0xffffffffu, a, off);
@@ -83,7 +86,7 @@ __device__ __forceinline__ void multi_flush(long long (&s_nn)[VPT], long long (&
       if (a) atomicAdd(reinterpret_cast<unsigned long long *>(dots + c), (unsigned long long)a);
       if (b) atomicAdd(reinterpret_cast<unsigned long long *>(dots + W + c), (unsigned long long)b);
     }
-    s_nn[j] = s_np[j] = 0;
+    msum[j][threadIdx.x] = msum[VPT + j][threadIdx.x] = 0;
   }
 }
 
@@ -111,9 +114,10 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
   const int32_t n = hdr->n_base + (int32_t)step_offset;
   if (nmodels == 0) return;
 
-  long long s_nn[VPT], s_np[VPT];
+  // per-thread fixed-point sums in shared memory (see multi_flush)
+  __shared__ long long msum[2 * VPT][kBlock];
 #pragma unroll
-  for (int j = 0; j < VPT; j++) s_nn[j] = s_np[j] = 0;
+  for (int j = 0; j < 2 * VPT; j++) msum[j][threadIdx.x] = 0;
 
   // the model of the tile being computed and of the one being fetched
   uint32_t mi = kPad, fi = kPad;
@@ -160,7 +164,7 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
   for (; w < total; w = next_tile(w)) {
     if (cur_model != mi) {
       // block-uniform: every thread of the block is on the same tile
-      if (mi != kPad) multi_flush<P, VPT, TPR>(s_nn, s_np, t_dots, W, sub);
+      if (mi != kPad) multi_flush<P, VPT, TPR>(msum, t_dots, W, sub);
       mi = cur_model;
       const MultiModel *md = models + mi;
       A.slice_ptr = md->A.slice_ptr;
@@ -187,12 +191,14 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
     if (cur.ok) {
       const uint32_t row = cur.row, l = cur.l, cb = cur.cb, ce = cur.ce, wd = ce - cb;
       Acc acc[VPT];
+      L yv[NL];
+      row_y(cur, y, W, sub, yv);
 #pragma unroll
       for (int j = 0; j < VPT; j++) {
         if ((first >> j) & 1u) {
           acc[j] = Acc{0, 0};
         } else {
-          const Acc v = cur.live ? pack_get<P, Acc>(cur.yr, j) : Acc{0, 0};
+          const Acc v = cur.live ? pack_get<P, Acc>(yv, j) : Acc{0, 0};
           acc[j] = Acc{-v.x, -v.y};
         }
       }
@@ -292,15 +298,15 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
 #pragma unroll
         for (int j = 0; j < VPT; j++) {
           const float2 b = P::getf(self, j);
-          s_nn[j] += __float2ll_rn(fmaf(af[j].x, af[j].x, af[j].y * af[j].y) * kFixScale);
-          s_np[j] += __float2ll_rn(fmaf(af[j].x, b.x, af[j].y * b.y) * kFixScale);
+          msum[j][threadIdx.x] += __float2ll_rn(fmaf(af[j].x, af[j].x, af[j].y * af[j].y) * kFixScale);
+          msum[VPT + j][threadIdx.x] += __float2ll_rn(fmaf(af[j].x, b.x, af[j].y * b.y) * kFixScale);
         }
       }
     }
     cur = nxt;
     cur_model = nxt_model;
   }
-  if (mi != kPad) multi_flush<P, VPT, TPR>(s_nn, s_np, t_dots, W, sub);
+  if (mi != kPad) multi_flush<P, VPT, TPR>(msum, t_dots, W, sub);
 }
 
 // After a step: the doubled moments of every active lane,

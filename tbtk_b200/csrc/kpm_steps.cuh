@@ -4,6 +4,7 @@
 // autotuner picks an entry per batch shape.
 #pragma once
 
+#include "kpm_async.cuh"
 #include "kpm_bulk.cuh"
 #include "kpm_host.h"
 #include "kpm_kernels.cuh"
@@ -96,6 +97,38 @@ void launch_step(cudaStream_t st, int device, unsigned max_grid, const StepArgs 
 #define TBTKKPM_STEP_ENTRY(CLS, V, AR, T, P, D, MB)                                 \
   {CLS, T, P, MB, &launch_step<V, AR, T, P, true, D, MB>,                           \
    &launch_step<V, AR, T, P, false, D, MB>}
+
+template <int VPT, bool FIRST, bool DOTS, int S, int WMAX, int WPB>
+void launch_async(cudaStream_t st, int device, unsigned max_grid, const StepArgs &a,
+                  unsigned *grid) {
+  auto kern = kpm_step_async<VPT, FIRST, DOTS, S, WMAX, WPB>;
+  constexpr uint32_t smem = async_smem_bytes<VPT, S, WMAX, WPB>();
+  static int per_sm[64] = {0};
+  const int d = device & 63;
+  if (per_sm[d] == 0) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 32 * WPB, smem) != cudaSuccess ||
+        nb < 1) {
+      cudaGetLastError();
+      nb = 1;
+    }
+    per_sm[d] = nb;
+  }
+  const uint64_t tiles = ((uint64_t)a.A.nslices * 32 + WPB - 1) / WPB;
+  uint64_t g = std::min<uint64_t>(tiles, (uint64_t)per_sm[d] * sm_count(device));
+  if (max_grid) g = std::min<uint64_t>(g, max_grid);
+  g = std::max<uint64_t>(g, 1);
+  *grid = (unsigned)g;
+  kern<<<(unsigned)g, 32 * WPB, smem, st>>>(a.A, a.Bp, static_cast<const float2 *>(a.x),
+                                             static_cast<float2 *>(a.y), a.tg, a.n_out, a.dots);
+}
+
+// variant 10000 + 1000*S + 10*WMAX + WPB: the cp.async-staged kernel with S
+// stages of WMAX gathered rows per warp, WPB warps per block
+#define TBTKKPM_ASYNC_ENTRY(CLS, P, D, S, WMAX, WPB)                                \
+  {CLS, 32, P, 10000 + 1000 * S + 10 * WMAX + WPB,                                 \
+   &launch_async<P, true, D, S, WMAX, WPB>, &launch_async<P, false, D, S, WMAX, WPB>}
 
 extern const StepEntry kStepsFP64[];
 extern const int kNumStepsFP64;
