@@ -134,8 +134,17 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
   long long *t_dots = nullptr;
   uint32_t t_count = 0;
 
-  auto fetch = [&](uint32_t w, RowFetch<V, AR, TPR, VPT, PF> &f, uint32_t &fmodel) {
-    const uint32_t i = __ldg(tile_model + w);
+  // model and slice bounds of the row a thread takes in tile w (issued a tile
+  // before the row's entries, which depend on them)
+  auto bounds_of = [&](uint32_t w, uint32_t &model) -> RowBounds {
+    model = __ldg(tile_model + w);
+    const MultiModel *q = models + model;
+    Sell s{};
+    s.slice_ptr = q->A.slice_ptr;
+    s.nslices = q->A.nslices;
+    return load_bounds<TPR>(s, w - q->tile0, grp);
+  };
+  auto fetch = [&](uint32_t w, uint32_t i, RowBounds b, RowFetch<V, AR, TPR, VPT, PF> &f) {
     if (i != fi) {
       fi = i;
       const MultiModel *q = models + i;
@@ -147,8 +156,7 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
       fy = q->vec[n & 1];
       ft0 = q->tile0;
     }
-    fmodel = i;
-    fetch_row<V, AR, TPR, VPT, PF, false>(FA, W, fy, w - ft0, grp, sub, f);
+    fetch_row<V, AR, TPR, VPT, PF, false>(FA, W, fy, w - ft0, grp, sub, b, f);
   };
   // the tile after w in this block's order
   auto next_tile = [&](uint32_t w) -> uint32_t {
@@ -160,8 +168,14 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
   RowFetch<V, AR, TPR, VPT, PF> cur, nxt;
   uint32_t cur_model = 0, nxt_model = 0;
   uint32_t w = blockIdx.x * kRun;
-  if (w < total) fetch(w, cur, cur_model);
-  for (; w < total; w = next_tile(w)) {
+  if (w < total) {
+    const RowBounds b0 = bounds_of(w, cur_model);
+    fetch(w, cur_model, b0, cur);
+  }
+  uint32_t wn = next_tile(w), bm = 0;  // next tile, its model and bounds
+  RowBounds bb{0, 0};
+  if (wn < total) bb = bounds_of(wn, bm);
+  for (; w < total; w = wn, wn = next_tile(wn)) {
     if (cur_model != mi) {
       // block-uniform: every thread of the block is on the same tile
       if (mi != kPad) multi_flush<P, VPT, TPR>(msum, t_dots, W, sub);
@@ -186,8 +200,12 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
       for (int j = 0; j < VPT; j++)
         if (n - __ldg(t_base + P::col_of(sub, j)) == 1) first |= 1u << j;
     }
-    const uint32_t wn = next_tile(w);
-    if (wn < total) fetch(wn, nxt, nxt_model);
+    if (wn < total) {
+      fetch(wn, bm, bb, nxt);
+      nxt_model = bm;
+    }
+    const uint32_t wn2 = next_tile(wn);
+    if (wn2 < total) bb = bounds_of(wn2, bm);
     if (cur.ok) {
       const uint32_t row = cur.row, l = cur.l, cb = cur.cb, ce = cur.ce, wd = ce - cb;
       Acc acc[VPT];
