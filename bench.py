@@ -111,6 +111,14 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# DRAM bytes (read + write) of one launch of the batched step,
+# kpm_step<float2, Wide64, 8, 8, dots, minb 2>, from one ncu capture on the
+# 1024x1024 lattice (N = 2,097,152 rows, B = 64): 3.427 GB.  The traffic
+# grows with the rows (the algorithmic bytes there are 3.439 GB), so a
+# launch on N rows moves TRAFFIC_PER_ROW_B64 * N bytes.
+TRAFFIC_PER_ROW_B64 = 3.427e9 / 2097152
+
+
 def peak_hbm():
     try:
         d = json.loads(PEAKS.read_text())
@@ -399,7 +407,11 @@ def ours(args, world, rank, local):
                        "p99": total_ms / args.steps,
                        "note": "per 64-site batch; request-level latency is in the serving bench"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak,
+                     "traffic": (TRAFFIC_PER_ROW_B64 * p.N
+                                 if B == 64 and tuple(tuned_mixed[:3]) == (8, 8, 2) else None),
+                     "traffic_source": ("ncu dram__bytes_read+write of this kernel on the "
+                                        "1024x1024 lattice (N=2097152), scaled by rows to N"),
                      "kernel": (f"kpm_step<float2, tpr={tuned_mixed[0]}, vpt={tuned_mixed[1]}, "
                                 f"dots, minb={tuned_mixed[2]}> (recursion step, B={B})"),
                      "bytes_per_launch": bstep, "avg_launch_ms": avg_step_ms,
