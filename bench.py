@@ -111,12 +111,14 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-# DRAM bytes (read + write) of one launch of the batched step,
-# kpm_step<float2, Wide64, 8, 8, dots, minb 2>, from one ncu capture on the
-# 1024x1024 lattice (N = 2,097,152 rows, B = 64): 3.427 GB.  The traffic
-# grows with the rows (the algorithmic bytes there are 3.439 GB), so a
-# launch on N rows moves TRAFFIC_PER_ROW_B64 * N bytes.
-TRAFFIC_PER_ROW_B64 = 3.427e9 / 2097152
+# DRAM bytes (read + write) per row of one launch of the batched step, by
+# (vectors, B, tpr, vpt, variant), from ncu captures on the 1024x1024
+# lattice (N = 2,097,152 rows); the traffic grows with the rows, so a launch
+# on N rows moves that figure times N.  complex64 (8, 8, 2): 3.427 GB there
+# (algorithmic bytes 3.439 GB); real float vectors (8, 8, 2): 1.721 GB
+# (algorithmic bytes 1.744 GB).
+TRAFFIC_PER_ROW = {("complex64", 64, 8, 8, 2): 3.427e9 / 2097152,
+                   ("real float", 64, 8, 8, 2): 1.721e9 / 2097152}
 
 
 def peak_hbm():
@@ -152,11 +154,13 @@ def max_over_ranks(values, dist, device):
     return t.tolist()
 
 
-def step_bytes(p, B, s_vec):
+def step_bytes(p, B, s_vec, s_val=16):
     """Algorithmic bytes of one recursion step: the CSR matrix once (values,
     column indices, row pointers) and three vector passes per source
-    (gather of j_n counted once, read of j_{n-1}, write of j_{n+1})."""
-    return p.nnz * (16 + 4) + 4 * (p.N + 1) + 3 * p.N * B * s_vec
+    (gather of j_n counted once, read of j_{n-1}, write of j_{n+1}).
+    s_vec/s_val: bytes per vector element / stored value (complex128 16/16,
+    complex64 8/16, real vectors of a real matrix 4/8)."""
+    return p.nnz * (s_val + 4) + 4 * (p.N + 1) + 3 * p.N * B * s_vec
 
 
 # ------------------------------------------------------------------ CPU baselines
@@ -292,6 +296,7 @@ def ours(args, world, rank, local):
     # project autotuner: pick the step configuration of both batch shapes
     tuned_mixed = mat.autotune(B, kpm.MIXED, ldos=True, probe_steps=6)
     tuned_plain = mat.autotune(1, kpm.FP64, ldos=True, probe_steps=6)
+    real_vectors = mat.real()[1]  # the model is real: the mixed path runs real vectors
     mat.set_profiling(True)
 
     def step(prec, sites):
@@ -377,8 +382,10 @@ def ours(args, world, rank, local):
     solves = B * args.steps * world
     value = solves / (total_ms / 1e3)
     avg_step_ms = rec_ms / max(rec_launches, 1)
-    bstep = step_bytes(p, B, 8)
+    bstep = step_bytes(p, B, 4, 8) if real_vectors else step_bytes(p, B, 8)
     achieved = bstep / (avg_step_ms / 1e3) / 1e9
+    vec_kind = "real float" if real_vectors else "complex64"
+    traffic_row = TRAFFIC_PER_ROW.get((vec_kind, B) + tuple(tuned_mixed[:3]))
     peak, peak_kind = peak_hbm()
     plain_ms = statistics.median(plain) if plain else None
     plain_rate = 1e3 / plain_ms if plain_ms else None
@@ -386,7 +393,9 @@ def ours(args, world, rank, local):
         "metric": "LDOS solves/s", "value": value, "unit": "LDOS solves/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c64 vectors / f64 arithmetic+moments",
+        "vs_baseline": None,
+        "dtype": (("f32 vectors (real model)" if real_vectors else "c64 vectors")
+                  + " / f64 arithmetic+moments"),
         "data": "synthetic (seeded lattice, Anderson disorder)",
         "config": {"workload": (f"square {args.lattice}x{args.lattice} spin periodic (N={p.N}, "
                                 f"nnz={p.nnz}), t=1 J=0.5 W=2, s=12, M={p.M}, broadening 1e-3, "
@@ -408,12 +417,13 @@ def ours(args, world, rank, local):
                        "note": "per 64-site batch; request-level latency is in the serving bench"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak,
-                     "traffic": (TRAFFIC_PER_ROW_B64 * p.N
-                                 if B == 64 and tuple(tuned_mixed[:3]) == (8, 8, 2) else None),
+                     "traffic": traffic_row * p.N if traffic_row else None,
                      "traffic_source": ("ncu dram__bytes_read+write of this kernel on the "
                                         "1024x1024 lattice (N=2097152), scaled by rows to N"),
-                     "kernel": (f"kpm_step<float2, tpr={tuned_mixed[0]}, vpt={tuned_mixed[1]}, "
-                                f"dots, minb={tuned_mixed[2]}> (recursion step, B={B})"),
+                     "kernel": (f"{'kpm_step_real' if real_vectors else 'kpm_step<float2'}, "
+                                f"tpr={tuned_mixed[0]}, vpt={tuned_mixed[1]}, dots, "
+                                f"minb={tuned_mixed[2]} (recursion step, B={B}, {vec_kind} "
+                                f"vectors)"),
                      "bytes_per_launch": bstep, "avg_launch_ms": avg_step_ms,
                      "peak_kind": f"{peak_kind} (copy bandwidth)"},
         "recursion_share": rec_ms / total_ms if total_ms else None,

@@ -232,6 +232,22 @@ TBTKKPM_API int tbtkkpm_matrix_set_config(
  * (No reference counterpart.) */
 TBTKKPM_API int tbtkkpm_step_configs(int precision, int ldos, int *out, int cap);
 
+/* Real Hamiltonians.  When every scaled value 2H/s of a matrix has a zero
+ * imaginary part, the mixed precisions (TBTKKPM_MIXED, TBTKKPM_MIXED_DIRECT)
+ * run on real float vectors instead of complex64 ones: every Chebyshev
+ * vector of a real matrix started from basis vectors is real, and the real
+ * kernels give the same moments (value, 0) with half the vector bytes.
+ * The FP64 precision keeps complex128 vectors (the reference's data).
+ * set_real(m, 0) turns the real vectors off (1, the default, allows them);
+ * tbtkkpm_matrix_real reports whether the values are real and whether the
+ * real vectors are in use; tbtkkpm_matrix_step_configs lists the step
+ * configurations this matrix's calls choose from (as tbtkkpm_step_configs).
+ * (No reference counterpart: the reference always uses complex<double>.) */
+TBTKKPM_API int tbtkkpm_matrix_set_real(tbtkkpm_matrix *m, int enable);
+TBTKKPM_API int tbtkkpm_matrix_real(tbtkkpm_matrix *m, int *values_real, int *in_use);
+TBTKKPM_API int tbtkkpm_matrix_step_configs(
+	tbtkkpm_matrix *m, int precision, int ldos, int *out, int cap);
+
 /* LDOS at B sites in one call: the moments <site|T_n|site> of all sites run
  * as one batched recursion, are damped and summed over the table's energy
  * grid on the device; only the [B][E] result crosses to the host.

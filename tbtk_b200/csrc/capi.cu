@@ -228,6 +228,19 @@ static int build_sell(tbtkkpm_matrix *m, cudaStream_t st) {
   count_launches(2);
   e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "SELL build");
+  // real parts for the real-vector steps, kept only for a real matrix
+  DevBuf flag;
+  if ((rc = m->sreal.reserve(8 * slots)) || (rc = flag.reserve(4))) return rc;
+  unsigned complex_flag = 0;
+  if ((e = cudaMemsetAsync(flag.ptr, 0, 4, st)) != cudaSuccess) return cuda_fail(e, "SELL build");
+  k_sell_real<<<blocks_for(slots), 256, 0, st>>>(slots, m->sval.as<double2>(), m->sreal.as<double>(),
+                                                flag.as<unsigned>());
+  count_launches(1);
+  e = cudaMemcpyAsync(&complex_flag, flag.ptr, 4, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "SELL build");
+  m->values_real = complex_flag == 0;
+  if (!m->values_real) m->sreal.release();
   return TBTKKPM_OK;
 }
 

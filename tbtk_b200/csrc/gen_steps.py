@@ -76,8 +76,42 @@ def write_multi():
     (HERE / "steps_multi.cu").write_text("\n".join(lines))
 
 
+# Real-vector steps of a real matrix at mixed precision (kpm_real.cuh):
+# (threads per row, real values per thread) shapes with register caps
+# REAL_MINBS, one table without and one with the doubling dot products.
+SHAPES_REAL = [(1, 1), (2, 1), (4, 1), (8, 1), (2, 4), (16, 1), (4, 4), (32, 1), (8, 4), (4, 8),
+               (16, 4), (8, 8), (32, 4), (16, 8), (32, 8)]
+REAL_MINBS = [1, 2, 3]
+# extra variants gathering G entries per round trip; 6 and 8 measured 14%
+# and 76% slower than the default for (8, 8) on the 2048^2 lattice (spills)
+REAL_GATHERS = []
+REAL_UNITS = [
+    ("steps_real.cu", "kStepsMixedReal", "kClassMixedReal", "false",
+     "Recursion steps on real float vectors of a real matrix with FP64 arithmetic."),
+    ("steps_real_dots.cu", "kStepsMixedRealDots", "kClassMixedRealDots", "true",
+     "Recursion steps on real float vectors of a real matrix with the doubling dot products."),
+]
+
+
+def write_real():
+    for fname, table, cls, dots, doc in REAL_UNITS:
+        lines = [f"// {doc}", "// Written by gen_steps.py.", '#include "kpm_steps.cuh"', "",
+                 "namespace tbtkkpm {", "", f"const StepEntry {table}[] = {{"]
+        for (t, p) in SHAPES_REAL:
+            for mb in REAL_MINBS:
+                lines.append(f"    TBTKKPM_REAL_ENTRY({cls}, {t}, {p}, {dots}, {mb}, 0),")
+            if p >= 4:
+                # a whole tight-binding row per round trip at the cap of 2
+                for g in REAL_GATHERS:
+                    lines.append(f"    TBTKKPM_REAL_ENTRY({cls}, {t}, {p}, {dots}, 2, {g}),")
+        lines += ["};", f"const int kNum{table[1:]} = sizeof({table}) / sizeof({table}[0]);", "",
+                  "}  // namespace tbtkkpm", ""]
+        (HERE / fname).write_text("\n".join(lines))
+
+
 def main():
     write_multi()
+    write_real()
     for fname, table, cls, V, AR, dots, shapes, doc in UNITS:
         lines = [f"// {doc}", "// Written by gen_steps.py: every configuration the driver and the",
                  "// autotuner can pick.", '#include "kpm_steps.cuh"', "", "namespace tbtkkpm {", "",

@@ -86,6 +86,11 @@ struct tbtkkpm_matrix {
   // SELL-32 copy the recursion reads: slice_ptr[nslices+1] (chunk offsets),
   // scol/sval[chunks*32]
   tbtkkpm::DevBuf slice_ptr, scol, sval;
+  // real matrix (every scaled value has a zero imaginary part): the real
+  // parts in SELL order, read by the real-vector steps of the mixed path
+  bool values_real = false;
+  bool use_real = true;  // tbtkkpm_matrix_set_real
+  tbtkkpm::DevBuf sreal;
   uint32_t nslices = 0;
   uint64_t chunks = 0;
   tbtkkpm::Workspace ws;
@@ -101,6 +106,7 @@ struct tbtkkpm_matrix {
     slice_ptr.release();
     scol.release();
     sval.release();
+    sreal.release();
     ws.release();
     timer.destroy();
   }

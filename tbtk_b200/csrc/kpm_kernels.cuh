@@ -171,6 +171,7 @@ struct Sell {
   const uint32_t *col;        // [chunks * 32], kPad in padding slots
   const double2 *val;         // [chunks * 32], 2H/s
   uint32_t N, nslices;
+  const double *vre;          // [chunks * 32] real parts of val for a real matrix, else null
 };
 
 // ---------------------------------------------------------------- arithmetic
@@ -644,6 +645,17 @@ static __global__ void k_sell_fill(uint32_t N, uint32_t nslices, const uint32_t 
       sval[slot] = make_double2(0.0, 0.0);
     }
   }
+}
+
+// Real parts of the SELL values, and a flag set when some value has a
+// nonzero imaginary part.
+static __global__ void k_sell_real(uint64_t slots, const double2 *sval, double *sreal,
+                                   unsigned *complex_flag) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= slots) return;
+  const double2 v = sval[i];
+  sreal[i] = v.x;
+  if (v.y != 0.0) atomicOr(complex_flag, 1u);
 }
 
 // ---------------------------------------------------------------- damping

@@ -6,6 +6,7 @@
 
 #include "kpm_async.cuh"
 #include "kpm_bulk.cuh"
+#include "kpm_real.cuh"
 #include "kpm_host.h"
 #include "kpm_kernels.cuh"
 
@@ -13,8 +14,15 @@
 
 namespace tbtkkpm {
 
-// Vector classes of the step kernels.
-enum StepClass : int { kClassFP64 = 0, kClassMixed = 1, kClassMixedDots = 2 };
+// Vector classes of the step kernels (Real: real float vectors of a real
+// matrix at mixed precision, see kpm_real.cuh).
+enum StepClass : int {
+  kClassFP64 = 0,
+  kClassMixed = 1,
+  kClassMixedDots = 2,
+  kClassMixedReal = 3,
+  kClassMixedRealDots = 4
+};
 
 struct StepArgs {
   Sell A;
@@ -98,6 +106,37 @@ void launch_step(cudaStream_t st, int device, unsigned max_grid, const StepArgs 
   {CLS, T, P, MB, &launch_step<V, AR, T, P, true, D, MB>,                           \
    &launch_step<V, AR, T, P, false, D, MB>}
 
+template <int TPR, int VPT, bool FIRST, bool DOTS, int MINB, int G>
+void launch_real(cudaStream_t st, int device, unsigned max_grid, const StepArgs &a,
+                 unsigned *grid) {
+  auto kern = kpm_step_real<TPR, VPT, FIRST, DOTS, MINB, G>;
+  static int per_sm[64] = {0};
+  const int d = device & 63;
+  if (per_sm[d] == 0) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kBlock, 0) != cudaSuccess ||
+        nb < 1) {
+      cudaGetLastError();
+      nb = 1;
+    }
+    per_sm[d] = nb;
+  }
+  constexpr int RPB = kBlock / TPR;
+  const uint64_t tiles = ((uint64_t)a.A.nslices * 32 + RPB - 1) / RPB;
+  uint64_t g = std::min<uint64_t>(tiles, (uint64_t)per_sm[d] * sm_count(device));
+  if (max_grid) g = std::min<uint64_t>(g, max_grid);
+  g = std::max<uint64_t>(g, 1);
+  *grid = (unsigned)g;
+  kern<<<(unsigned)g, kBlock, 0, st>>>(a.A, a.Bp, static_cast<const float *>(a.x),
+                                       static_cast<float *>(a.y), a.tg, a.n_out, a.dots);
+}
+
+// variant MB + 10*G: register cap MB, G entries gathered per round trip
+// (G 0: the default for the shape)
+#define TBTKKPM_REAL_ENTRY(CLS, T, P, D, MB, G)                                     \
+  {CLS, T, P, MB + 10 * G, &launch_real<T, P, true, D, MB, G>,                      \
+   &launch_real<T, P, false, D, MB, G>}
+
 template <int VPT, bool FIRST, bool DOTS, int S, int WMAX, int WPB>
 void launch_async(cudaStream_t st, int device, unsigned max_grid, const StepArgs &a,
                   unsigned *grid) {
@@ -136,5 +175,9 @@ extern const StepEntry kStepsMixed[];
 extern const int kNumStepsMixed;
 extern const StepEntry kStepsMixedDots[];
 extern const int kNumStepsMixedDots;
+extern const StepEntry kStepsMixedReal[];
+extern const int kNumStepsMixedReal;
+extern const StepEntry kStepsMixedRealDots[];
+extern const int kNumStepsMixedRealDots;
 
 }  // namespace tbtkkpm

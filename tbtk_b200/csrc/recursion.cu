@@ -32,7 +32,24 @@ constexpr uint32_t kMaxBatchMixed = 256;
 
 bool is_mixed(int precision) { return precision != TBTKKPM_FP64; }
 
-Shape shape_for(int precision, uint32_t B) {
+// Mixed-precision batches of a real matrix run on real float vectors
+// (kpm_real.cuh) unless the caller turned that off.
+bool real_mode(const tbtkkpm_matrix *m, int precision) {
+  return is_mixed(precision) && m->values_real && m->use_real;
+}
+
+Shape shape_for(int precision, uint32_t B, bool real = false) {
+  if (real) {
+    if (B <= 1) return {1, 1};
+    if (B <= 2) return {2, 1};
+    if (B <= 4) return {4, 1};
+    if (B <= 8) return {2, 4};
+    if (B <= 16) return {4, 4};
+    if (B <= 32) return {8, 4};
+    if (B <= 64) return {16, 4};
+    if (B <= 128) return {32, 4};
+    return {32, 8};
+  }
   if (!is_mixed(precision)) {
     if (B <= 1) return {1, 1};
     if (B <= 2) return {2, 1};
@@ -54,8 +71,9 @@ Shape shape_for(int precision, uint32_t B) {
   return {32, 8};
 }
 
-int step_class(int precision, bool dots) {
+int step_class(int precision, bool dots, bool real = false) {
   if (!is_mixed(precision)) return kClassFP64;
+  if (real) return dots ? kClassMixedRealDots : kClassMixedReal;
   return dots ? kClassMixedDots : kClassMixed;
 }
 
@@ -66,9 +84,15 @@ void step_table(int cls, const StepEntry **t, int *n) {
   } else if (cls == kClassMixed) {
     *t = kStepsMixed;
     *n = kNumStepsMixed;
-  } else {
+  } else if (cls == kClassMixedDots) {
     *t = kStepsMixedDots;
     *n = kNumStepsMixedDots;
+  } else if (cls == kClassMixedReal) {
+    *t = kStepsMixedReal;
+    *n = kNumStepsMixedReal;
+  } else {
+    *t = kStepsMixedRealDots;
+    *n = kNumStepsMixedRealDots;
   }
 }
 
@@ -100,8 +124,9 @@ ShapeKey shape_key(const tbtkkpm_matrix *m, int cls, uint32_t Bp) {
 const StepEntry *pick_step(const tbtkkpm_matrix *m, int precision, bool dots, uint32_t B,
                            const StepEntry *force) {
   if (force) return force;
-  const int cls = step_class(precision, dots);
-  const Shape s = shape_for(precision, B);
+  const bool real = real_mode(m, precision);
+  const int cls = step_class(precision, dots, real);
+  const Shape s = shape_for(precision, B, real);
   auto it = m->tuned.find(tune_key(cls, s.bp()));
   if (it != m->tuned.end()) {
     const StepEntry *e = find_step(cls, it->second[0], it->second[1], it->second[2]);
@@ -139,7 +164,8 @@ int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &fro
   if (!fn) return fail(TBTKKPM_ERR_UNSUPPORTED, "no recursion kernel for batch %u", B);
   const uint32_t Bp = (uint32_t)(fn->tpr * fn->vpt);
   if (Bp < B) return fail(TBTKKPM_ERR_ARGUMENT, "configuration of %u columns for %u sources", Bp, B);
-  const size_t esize = is_mixed(precision) ? sizeof(float2) : sizeof(double2);
+  const bool real = fn->cls == kClassMixedReal || fn->cls == kClassMixedRealDots;
+  const size_t esize = real ? sizeof(float) : (is_mixed(precision) ? sizeof(float2) : sizeof(double2));
   const size_t vbytes = (size_t)m->N * Bp * esize;
   const size_t words = ((size_t)m->N + 31) / 32;
   const uint32_t T = (uint32_t)tl.row.size();
@@ -190,7 +216,10 @@ int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &fro
   tg.mu = doubling ? ws.mu_direct.as<double2>() : ws.mu.as<double2>();
   tg.ld = ld_direct;
   const unsigned ib = blocks_for(std::max(B, T));
-  if (is_mixed(precision))
+  if (real)
+    kpm_init_sources_real<<<ib, 256, 0, st>>>(B, Bp, ws.from.as<uint32_t>(), ws.vec[0].as<float>(),
+                                              tg);
+  else if (is_mixed(precision))
     kpm_init_sources<float2><<<ib, 256, 0, st>>>(B, Bp, ws.from.as<uint32_t>(),
                                                 ws.vec[0].as<float2>(), tg);
   else
@@ -202,6 +231,7 @@ int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &fro
   a.A.val = m->sval.as<double2>();
   a.A.N = m->N;
   a.A.nslices = m->nslices;
+  a.A.vre = m->values_real ? m->sreal.as<double>() : nullptr;
   a.Bp = Bp;
   a.tg = tg;
   a.dots = doubling ? ws.dots.as<double2>() : nullptr;
@@ -700,8 +730,9 @@ extern "C" int tbtkkpm_matrix_autotune(tbtkkpm_matrix *m, uint32_t B, int precis
   std::lock_guard<std::mutex> lk(m->lock);
   DeviceGuard g(m->device);
   const bool doubling = ldos && precision == TBTKKPM_MIXED;
-  const int cls = step_class(precision, doubling);
-  const uint32_t Bp = shape_for(precision, B).bp();
+  const bool real = real_mode(m, precision);
+  const int cls = step_class(precision, doubling, real);
+  const uint32_t Bp = shape_for(precision, B, real).bp();
   const uint32_t M = doubling ? 2 * probe_steps : probe_steps + 1;
   std::vector<uint32_t> fr(B);
   for (uint32_t b = 0; b < B; b++) fr[b] = (uint32_t)((uint64_t)b * m->N / B);
@@ -771,8 +802,9 @@ extern "C" int tbtkkpm_matrix_set_config(tbtkkpm_matrix *m, uint32_t B, int prec
   if (rc) return rc;
   if (!m) return fail(TBTKKPM_ERR_ARGUMENT, "matrix_set_config: NULL matrix");
   const bool doubling = ldos && precision == TBTKKPM_MIXED;
-  const int cls = step_class(precision, doubling);
-  const uint32_t Bp = shape_for(precision, std::max(B, 1u)).bp();
+  const bool real = real_mode(m, precision);
+  const int cls = step_class(precision, doubling, real);
+  const uint32_t Bp = shape_for(precision, std::max(B, 1u), real).bp();
   if ((uint32_t)(tpr * vpt) != Bp || !find_step(cls, tpr, vpt, minb))
     return fail(TBTKKPM_ERR_ARGUMENT, "matrix_set_config: no compiled configuration %d x %d / %d "
                 "for %u columns", tpr, vpt, minb, Bp);
@@ -795,4 +827,35 @@ extern "C" int tbtkkpm_step_configs(int precision, int ldos, int *out, int cap) 
     out[3 * i + 2] = t[i].minb;
   }
   return n;
+}
+
+// As tbtkkpm_step_configs for the kernels this matrix uses (real-vector
+// kernels for a real matrix at mixed precision).
+extern "C" int tbtkkpm_matrix_step_configs(tbtkkpm_matrix *m, int precision, int ldos, int *out,
+                                           int cap) {
+  if (!m || check_precision(precision)) return -1;
+  const StepEntry *t;
+  int n;
+  step_table(step_class(precision, ldos && precision == TBTKKPM_MIXED, real_mode(m, precision)),
+             &t, &n);
+  for (int i = 0; i < n && i < cap && out; i++) {
+    out[3 * i] = t[i].tpr;
+    out[3 * i + 1] = t[i].vpt;
+    out[3 * i + 2] = t[i].minb;
+  }
+  return n;
+}
+
+extern "C" int tbtkkpm_matrix_set_real(tbtkkpm_matrix *m, int enable) {
+  if (!m) return fail(TBTKKPM_ERR_ARGUMENT, "matrix_set_real: NULL matrix");
+  std::lock_guard<std::mutex> lk(m->lock);
+  m->use_real = enable != 0;
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_matrix_real(tbtkkpm_matrix *m, int *values_real, int *in_use) {
+  if (!m) return fail(TBTKKPM_ERR_ARGUMENT, "matrix_real: NULL matrix");
+  if (values_real) *values_real = m->values_real ? 1 : 0;
+  if (in_use) *in_use = (m->values_real && m->use_real) ? 1 : 0;
+  return TBTKKPM_OK;
 }

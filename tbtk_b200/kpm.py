@@ -85,6 +85,9 @@ SIGNATURES = [
     ("tbtkkpm_matrix_autotune", _i, [_p, _u32, _i, _i, _u32, _p, _p, _p, _p]),
     ("tbtkkpm_matrix_set_config", _i, [_p, _u32, _i, _i, _i, _i, _i]),
     ("tbtkkpm_step_configs", _i, [_i, _i, _p, _i]),
+    ("tbtkkpm_matrix_set_real", _i, [_p, _i]),
+    ("tbtkkpm_matrix_real", _i, [_p, _p, _p]),
+    ("tbtkkpm_matrix_step_configs", _i, [_p, _i, _i, _p, _i]),
     ("tbtkkpm_server_create", _i, [_u32, _p, _u32, _u64, _u32, _d, _p]),
     ("tbtkkpm_server_add_model", _i, [_p, _p, _p, _p, _u32, _d, _u32, _p]),
     ("tbtkkpm_server_submit", _i, [_p, _u32, _p, _u32, _u32, _d, _p]),
@@ -249,6 +252,28 @@ class Matrix:
             self._h, int(B), int(precision), int(bool(ldos)), int(probe_steps),
             ctypes.byref(t), ctypes.byref(v), ctypes.byref(mb), ctypes.byref(ms)))
         return t.value, v.value, mb.value, ms.value
+
+    def set_real(self, enable=True):
+        """Allow (default) or forbid real float vectors at mixed precision."""
+        _check(load_library().tbtkkpm_matrix_set_real(self._h, int(bool(enable))))
+
+    def real(self):
+        """(values are real, real vectors in use at mixed precision)."""
+        vr, use = ctypes.c_int(), ctypes.c_int()
+        _check(load_library().tbtkkpm_matrix_real(self._h, ctypes.byref(vr), ctypes.byref(use)))
+        return bool(vr.value), bool(use.value)
+
+    def configs_for(self, B, precision, ldos=True):
+        """The compiled (tpr, vpt, variant) this matrix's calls for B sources
+        choose from (real-vector kernels for a real matrix at mixed
+        precision)."""
+        lib = load_library()
+        n = lib.tbtkkpm_matrix_step_configs(self._h, int(precision), int(bool(ldos)), None, 0)
+        out = np.zeros(3 * max(n, 0), dtype=np.int32)
+        lib.tbtkkpm_matrix_step_configs(self._h, int(precision), int(bool(ldos)), _ptr(out), n)
+        w = padded_width(B, precision)
+        return [tuple(int(v) for v in out[3 * i:3 * i + 3]) for i in range(n)
+                if out[3 * i] * out[3 * i + 1] == w]
 
     def set_config(self, B, precision, tpr, vpt, minb, ldos=True):
         _check(load_library().tbtkkpm_matrix_set_config(

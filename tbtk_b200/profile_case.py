@@ -11,7 +11,8 @@ recursion (CUDA events on the handle's stream) and its bandwidth in
 algorithmic bytes (matrix once per step plus three vector passes per
 source).  --sweep times every compiled step configuration for the batch;
 --autotune lets the library's autotuner choose first; --config T,V,MB forces
-one.
+one.  Without --rashba the model is real and the mixed precisions run on
+real float vectors; --complex-vectors keeps complex64 ones.
 """
 from __future__ import annotations
 
@@ -21,8 +22,8 @@ import time
 from tbtk_b200 import kpm, workloads
 
 
-def step_bytes(N, nnz, B, s_vec):
-    return nnz * 20 + 4 * (N + 1) + 3 * N * B * s_vec
+def step_bytes(N, nnz, B, s_vec, s_val=16):
+    return nnz * (s_val + 4) + 4 * (N + 1) + 3 * N * B * s_vec
 
 
 def main():
@@ -37,6 +38,8 @@ def main():
     ap.add_argument("--sweep", action="store_true")
     ap.add_argument("--autotune", action="store_true")
     ap.add_argument("--config", default=None)
+    ap.add_argument("--complex-vectors", action="store_true",
+                    help="keep complex64 vectors for a real model (no real-vector kernels)")
     a = ap.parse_args()
     prec = {"fp64": kpm.FP64, "mixed": kpm.MIXED, "mixed_direct": kpm.MIXED_DIRECT}[a.precision]
     rowptr, col, val = workloads.square_csr(a.lattice, a.lattice, t=1.0, J=0.5, W=2.0,
@@ -46,8 +49,11 @@ def main():
     mat = kpm.Matrix.from_csr(rowptr, col, val, 12.0)
     tab = kpm.Table.create(a.moments, workloads.open_grid(12.0, a.energies), 12.0)
     mat.set_profiling(True)
-    s_vec = 16 if prec == kpm.FP64 else 8
-    bstep = step_bytes(N, nnz, a.sites, s_vec)
+    if a.complex_vectors:
+        mat.set_real(False)
+    real = prec != kpm.FP64 and mat.real()[1]
+    s_vec = 16 if prec == kpm.FP64 else (4 if real else 8)
+    bstep = step_bytes(N, nnz, a.sites, s_vec, 8 if real else 16)
 
     def run(label):
         for _ in range(a.repeat):
@@ -68,7 +74,7 @@ def main():
         t, v, mb, ms = mat.autotune(a.sites, prec, ldos=True, probe_steps=8)
         print(f"autotune: tpr={t} vpt={v} minb={mb} {ms:.4f} ms/step", flush=True)
     if a.sweep:
-        for (t, v, mb) in kpm.configs_for(a.sites, prec):
+        for (t, v, mb) in mat.configs_for(a.sites, prec):
             mat.set_config(a.sites, prec, t, v, mb)
             mat.ldos_sites(tab, sites, 1e-3, prec)  # warm
             mat.profile()

@@ -289,6 +289,54 @@ def test_every_mixed_config_same_result(gpu, B):
         assert rel_err(out, fp64) <= 1e-6, (t, v, mb)
 
 
+def test_real_matrix_detected(gpu):
+    """A real Hamiltonian runs the mixed precisions on real vectors; a
+    complex one (Rashba spin-orbit) and a forbidding caller keep complex64."""
+    real = L.square(8, 6, t=1.0, J=0.5, W=2.0, periodic=True, seed=7)
+    cplx = L.square(8, 6, t=1.0, J=0.5, W=2.0, alpha=0.3, periodic=True, seed=7)
+    m = gpu.Matrix.from_csr(*real.csr(), 12.0)
+    assert m.real() == (True, True)
+    m.set_real(False)
+    assert m.real() == (True, False)
+    assert gpu.Matrix.from_csr(*cplx.csr(), 12.0).real() == (False, False)
+
+
+@pytest.mark.parametrize("B", [1, 20, 64, 200])
+def test_real_vectors_match_complex_vectors(gpu, B):
+    """Real float vectors give the complex64 path's values: directly gathered
+    moments bit for bit for every compiled real configuration; doubling LDOS
+    up to the grouping of the dot-product sums; and within the mixed bar of
+    the FP64 path."""
+    lat = L.square(13, 11, t=1.0, J=0.5, W=2.0, periodic=True, seed=41)
+    rowptr, col, val = lat.csr()
+    s, M = 12.0, 64
+    frm = L.random_sites(lat, min(B, 286), seed=4)[:B]
+    B = frm.size
+    cm = gpu.Matrix.from_csr(rowptr, col, val, s)
+    cm.set_real(False)
+    ref, _ = cm.moments_batched(frm, frm, np.arange(B), M, 1e-3, gpu.MIXED)
+    configs = gpu.Matrix.from_csr(rowptr, col, val, s).configs_for(B, gpu.MIXED, ldos=False)
+    assert configs
+    for (t, v, mb) in configs:
+        m = gpu.Matrix.from_csr(rowptr, col, val, s)
+        assert m.real()[1]
+        m.set_config(B, gpu.MIXED, t, v, mb, ldos=False)
+        mu, _ = m.moments_batched(frm, frm, np.arange(B), M, 1e-3, gpu.MIXED)
+        assert np.array_equal(mu, ref), (t, v, mb)
+    energies = gpu.tbtk_range(-12.0, 12.0, 80, False, False)
+    tab = gpu.Table.create(M, energies, s)
+    direct_c, _ = cm.ldos_sites(tab, frm, 1e-3, gpu.MIXED_DIRECT)
+    dbl_c, _ = cm.ldos_sites(tab, frm, 1e-3, gpu.MIXED)
+    rm = gpu.Matrix.from_csr(rowptr, col, val, s)
+    direct_r, _ = rm.ldos_sites(tab, frm, 1e-3, gpu.MIXED_DIRECT)
+    dbl_r, _ = rm.ldos_sites(tab, frm, 1e-3, gpu.MIXED)
+    fp64, _ = rm.ldos_sites(tab, frm, 1e-3, gpu.FP64)
+    assert np.array_equal(direct_r, direct_c)
+    assert rel_err(dbl_r, dbl_c) <= 1e-10
+    assert rel_err(dbl_r, fp64) <= 1e-6
+    assert rel_err(direct_r, fp64) <= 1e-6
+
+
 def test_ring_ldos_integral(gpu):
     g = golden("ring")
     solver = gpu.ChebyshevExpander()
