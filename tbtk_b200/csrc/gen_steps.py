@@ -85,6 +85,10 @@ REAL_MINBS = [1, 2, 3]
 # extra variants gathering G entries per round trip; 6 and 8 measured 14%
 # and 76% slower than the default for (8, 8) on the 2048^2 lattice (spills)
 REAL_GATHERS = []
+# shape -> OPT variants at the cap of 2 (kpm_step_real: bit 0 bounds with the
+# entries, bit 1 j_{n-1} at the start of its row); none compiled: for (8, 8)
+# and (16, 4) on the 2048^2 lattice the defaults measured fastest or within 3%
+REAL_OPTS = {}
 REAL_UNITS = [
     ("steps_real.cu", "kStepsMixedReal", "kClassMixedReal", "false",
      "Recursion steps on real float vectors of a real matrix with FP64 arithmetic."),
@@ -104,6 +108,8 @@ def write_real():
                 # a whole tight-binding row per round trip at the cap of 2
                 for g in REAL_GATHERS:
                     lines.append(f"    TBTKKPM_REAL_ENTRY({cls}, {t}, {p}, {dots}, 2, {g}),")
+            for opt in REAL_OPTS.get((t, p), []):
+                lines.append(f"    TBTKKPM_REAL_ENTRY_OPT({cls}, {t}, {p}, {dots}, 2, {opt}),")
         lines += ["};", f"const int kNum{table[1:]} = sizeof({table}) / sizeof({table}[0]);", "",
                   "}  // namespace tbtkkpm", ""]
         (HERE / fname).write_text("\n".join(lines))

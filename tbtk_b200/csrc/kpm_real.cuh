@@ -73,7 +73,7 @@ template <int TPR, int VPT, int PF> struct RRowFetch {
   L yr[RPack<TPR, VPT>::NL];
 };
 
-template <int TPR, int VPT, int PF, bool FIRST>
+template <int TPR, int VPT, int PF, bool FIRST, bool PFY = true>
 __device__ __forceinline__ void rfetch_row(const Sell &A, uint32_t Bp, const float *y,
                                            uint64_t tile, int grp, int sub, RowBounds b,
                                            RRowFetch<TPR, VPT, PF> &f) {
@@ -94,12 +94,14 @@ __device__ __forceinline__ void rfetch_row(const Sell &A, uint32_t Bp, const flo
     if constexpr (TPR > 1)
       f.vv[q] = f.cc[q] != kPad ? __ldcs(A.vre + (uint64_t)(f.cb + k) * 32 + f.l) : 0.0;
   }
-  if constexpr (!FIRST)
+  if constexpr (!FIRST && PFY)
     if (f.live) RPack<TPR, VPT>::load_rw(y + (uint64_t)f.row * Bp, sub, f.yr);
 }
 
 // GIN: entries gathered per round trip (0: entries_in_flight's choice).
-template <int TPR, int VPT, bool FIRST, bool DOTS, int MINB, int GIN = 0>
+// OPT bit 0: load the slice bounds with the entries (not a tile ahead);
+// bit 1: load j_{n-1} at the start of its row (not a row ahead).
+template <int TPR, int VPT, bool FIRST, bool DOTS, int MINB, int GIN = 0, int OPT = 0>
 __global__ void __launch_bounds__(kBlock, MINB)
 kpm_step_real(Sell A, uint32_t Bp, const float *__restrict__ x, float *__restrict__ y,
               Targets tg, uint32_t n_out, double2 *__restrict__ dots) {
@@ -107,6 +109,7 @@ kpm_step_real(Sell A, uint32_t Bp, const float *__restrict__ x, float *__restric
   using L = typename P::L;
   constexpr int NL = P::NL;
   constexpr int G = GIN ? GIN : entries_in_flight<float, VPT, MINB>();
+  constexpr bool PFY = !(OPT & 2);
   constexpr int RPB = kBlock / TPR;
   constexpr int PF = TPR == 1 ? G : 1;
   const int sub = threadIdx.x % TPR;
@@ -117,34 +120,43 @@ kpm_step_real(Sell A, uint32_t Bp, const float *__restrict__ x, float *__restric
 #pragma unroll
     for (int j = 0; j < VPT; j++) d_nn[j] = d_np[j] = 0.0;
   }
-  // slice bounds a tile ahead of the entries for thread shares below 64 B
-  constexpr bool PB = sizeof(float) * VPT < 64;
+  // slice bounds a tile ahead of the entries for thread shares below 32 B
+  // (for (8, 8) loading them with the entries measured 3% faster)
+  constexpr bool PB = sizeof(float) * VPT < 32 && !(OPT & 1);
   const uint64_t ntiles = ((uint64_t)A.nslices * 32 + RPB - 1) / RPB;
   RRowFetch<TPR, VPT, PF> cur, nxt;
   RowBounds bn{0, 0};
   if (blockIdx.x < ntiles)
-    rfetch_row<TPR, VPT, PF, FIRST>(A, Bp, y, blockIdx.x, grp, sub,
-                                    load_bounds<TPR>(A, blockIdx.x, grp), cur);
+    rfetch_row<TPR, VPT, PF, FIRST, PFY>(A, Bp, y, blockIdx.x, grp, sub,
+                                         load_bounds<TPR>(A, blockIdx.x, grp), cur);
   if constexpr (PB)
     if (blockIdx.x + gridDim.x < ntiles) bn = load_bounds<TPR>(A, blockIdx.x + gridDim.x, grp);
   for (uint64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     const uint64_t tnext = tile + gridDim.x, tnext2 = tnext + gridDim.x;
     RowBounds bn2{0, 0};
     if constexpr (PB) {
-      if (tnext < ntiles) rfetch_row<TPR, VPT, PF, FIRST>(A, Bp, y, tnext, grp, sub, bn, nxt);
+      if (tnext < ntiles)
+        rfetch_row<TPR, VPT, PF, FIRST, PFY>(A, Bp, y, tnext, grp, sub, bn, nxt);
       if (tnext2 < ntiles) bn2 = load_bounds<TPR>(A, tnext2, grp);
     } else {
       if (tnext < ntiles)
-        rfetch_row<TPR, VPT, PF, FIRST>(A, Bp, y, tnext, grp, sub,
-                                        load_bounds<TPR>(A, tnext, grp), nxt);
+        rfetch_row<TPR, VPT, PF, FIRST, PFY>(A, Bp, y, tnext, grp, sub,
+                                             load_bounds<TPR>(A, tnext, grp), nxt);
     }
     if (cur.ok) {
       const uint32_t row = cur.row, l = cur.l, cb = cur.cb, w = cur.ce - cur.cb;
       double acc[VPT];
+      if constexpr (FIRST) {
 #pragma unroll
-      for (int j = 0; j < VPT; j++) {
-        if constexpr (FIRST) acc[j] = 0.0;
-        else acc[j] = cur.live ? -(double)P::getf(cur.yr, j) : 0.0;
+        for (int j = 0; j < VPT; j++) acc[j] = 0.0;
+      } else if constexpr (PFY) {
+#pragma unroll
+        for (int j = 0; j < VPT; j++) acc[j] = cur.live ? -(double)P::getf(cur.yr, j) : 0.0;
+      } else {
+        L yv[NL];
+        if (cur.live) P::load_rw(y + (uint64_t)row * Bp, sub, yv);
+#pragma unroll
+        for (int j = 0; j < VPT; j++) acc[j] = cur.live ? -(double)P::getf(yv, j) : 0.0;
       }
       if constexpr (TPR == 1) {
         for (uint32_t kb = 0; kb < w; kb += G) {

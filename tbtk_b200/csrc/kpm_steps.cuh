@@ -106,10 +106,10 @@ void launch_step(cudaStream_t st, int device, unsigned max_grid, const StepArgs 
   {CLS, T, P, MB, &launch_step<V, AR, T, P, true, D, MB>,                           \
    &launch_step<V, AR, T, P, false, D, MB>}
 
-template <int TPR, int VPT, bool FIRST, bool DOTS, int MINB, int G>
+template <int TPR, int VPT, bool FIRST, bool DOTS, int MINB, int G, int OPT = 0>
 void launch_real(cudaStream_t st, int device, unsigned max_grid, const StepArgs &a,
                  unsigned *grid) {
-  auto kern = kpm_step_real<TPR, VPT, FIRST, DOTS, MINB, G>;
+  auto kern = kpm_step_real<TPR, VPT, FIRST, DOTS, MINB, G, OPT>;
   static int per_sm[64] = {0};
   const int d = device & 63;
   if (per_sm[d] == 0) {
@@ -136,6 +136,10 @@ void launch_real(cudaStream_t st, int device, unsigned max_grid, const StepArgs 
 #define TBTKKPM_REAL_ENTRY(CLS, T, P, D, MB, G)                                     \
   {CLS, T, P, MB + 10 * G, &launch_real<T, P, true, D, MB, G>,                      \
    &launch_real<T, P, false, D, MB, G>}
+// variant MB + 100*OPT: the OPT bits of kpm_step_real
+#define TBTKKPM_REAL_ENTRY_OPT(CLS, T, P, D, MB, OPT)                               \
+  {CLS, T, P, MB + 100 * OPT, &launch_real<T, P, true, D, MB, 0, OPT>,              \
+   &launch_real<T, P, false, D, MB, 0, OPT>}
 
 template <int VPT, bool FIRST, bool DOTS, int S, int WMAX, int WPB>
 void launch_async(cudaStream_t st, int device, unsigned max_grid, const StepArgs &a,
