@@ -342,6 +342,11 @@ TBTKKPM_API int tbtkkpm_server_autotune(
 TBTKKPM_API int tbtkkpm_server_set_config(
 	tbtkkpm_server *s, uint32_t width, int tpr, int vpt, int minb);
 
+/* Models added after set_real(s, 0) keep complex64 lanes even when their
+ * Hamiltonian is real; by default (1) a real model's lanes hold real float
+ * vectors (tbtkkpm_matrix_set_real), with the same results. */
+TBTKKPM_API int tbtkkpm_server_set_real(tbtkkpm_server *s, int enable);
+
 /* Stops the worker (requests still queued or in flight are dropped) and
  * frees the server. */
 TBTKKPM_API int tbtkkpm_server_destroy(tbtkkpm_server *s);

@@ -61,6 +61,9 @@ MULTI_SHAPES = {1: [(1, 1)], 2: [(2, 1)], 4: [(4, 1), (2, 2)], 8: [(4, 2), (2, 4
                 16: [(8, 2), (4, 4), (2, 8)], 32: [(16, 2), (8, 4), (4, 8)],
                 64: [(32, 2), (16, 4), (8, 8)]}
 MULTI_MINBS = [1, 2]
+# the same for real float vectors (values per thread are real floats)
+MULTI_REAL_SHAPES = {1: [(1, 1)], 2: [(2, 1)], 4: [(4, 1), (1, 4)], 8: [(2, 4), (8, 1)],
+                     16: [(4, 4), (2, 8)], 32: [(8, 4), (4, 8)], 64: [(16, 4), (8, 8)]}
 
 
 def write_multi():
@@ -74,6 +77,17 @@ def write_multi():
     lines += ["};", "const int kNumMultiSteps = sizeof(kMultiSteps) / sizeof(kMultiSteps[0]);", "",
               "}  // namespace tbtkkpm", ""]
     (HERE / "steps_multi.cu").write_text("\n".join(lines))
+    lines = ["// Multi-model recursion steps on real float vectors, every lane width.",
+             "// Written by gen_steps.py.", '#include "kpm_multi_real.cuh"', "",
+             "namespace tbtkkpm {", "", "const MultiEntry kMultiStepsReal[] = {"]
+    for w, shapes in MULTI_REAL_SHAPES.items():
+        for (t, p) in shapes:
+            for mb in MULTI_MINBS:
+                lines.append(f"    TBTKKPM_MULTI_REAL_ENTRY({t}, {p}, {mb}),")
+    lines += ["};",
+              "const int kNumMultiStepsReal = sizeof(kMultiStepsReal) / sizeof(kMultiStepsReal[0]);",
+              "", "}  // namespace tbtkkpm", ""]
+    (HERE / "steps_multi_real.cu").write_text("\n".join(lines))
 
 
 # Real-vector steps of a real matrix at mixed precision (kpm_real.cuh):

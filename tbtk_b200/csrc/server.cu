@@ -17,6 +17,7 @@
 #include "tbtkkpm.h"
 #include "kpm_host.h"
 #include "kpm_multi.cuh"
+#include "kpm_multi_real.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -67,9 +68,11 @@ struct Model {
   tbtkkpm_table *table = nullptr;  // the server's table of this scale
   uint32_t N = 0, W = 0;
   double scale = 1;
+  bool real = false;  // real Hamiltonian: lanes hold real float vectors
   bool resident = false;
   uint64_t bytes = 0;
   uint64_t last_tick = 0;
+  size_t esize() const { return real ? sizeof(float) : sizeof(float2); }
   DevBuf vec[2], dots, mu, mu_direct, base, laneM, bitmap, tlist;
   std::vector<int32_t> base_h;
   std::vector<uint32_t> M_h;
@@ -88,22 +91,35 @@ struct Model {
 
 // Lane memory of a model: vectors, fixed-point sums, moments, lane tables,
 // target bitmap and list.
-uint64_t lane_bytes(uint32_t N, uint32_t W, uint32_t Mmax, uint32_t ld) {
-  return 2ull * N * W * sizeof(float2) + 2ull * W * sizeof(long long) +
+uint64_t lane_bytes(uint32_t N, uint32_t W, uint32_t Mmax, uint32_t ld, size_t esize) {
+  return 2ull * N * W * esize + 2ull * W * sizeof(long long) +
          (uint64_t)W * Mmax * sizeof(double2) + (uint64_t)W * ld * sizeof(double2) +
          8ull * W + 4ull * ((N + 31) / 32) + 8ull * W;
 }
 
-const MultiEntry *find_multi(int tpr, int vpt, int minb) {
-  for (int i = 0; i < kNumMultiSteps; i++)
-    if (kMultiSteps[i].tpr == tpr && kMultiSteps[i].vpt == vpt && kMultiSteps[i].minb == minb)
-      return &kMultiSteps[i];
+// The step kernels of one class: complex64 lanes or real float lanes.
+const MultiEntry *find_multi(int tpr, int vpt, int minb, bool real) {
+  const MultiEntry *t = real ? kMultiStepsReal : kMultiSteps;
+  const int n = real ? kNumMultiStepsReal : kNumMultiSteps;
+  for (int i = 0; i < n; i++)
+    if (t[i].tpr == tpr && t[i].vpt == vpt && t[i].minb == minb) return &t[i];
   return nullptr;
 }
 
-// Default shape per width (measured choice of the single-model kernels:
-// few threads per row, several values each).
-std::array<int, 3> default_config(uint32_t W) {
+// Default shape per width and class (measured choices of the single-model
+// kernels: few threads per row, several values each).
+std::array<int, 3> default_config(uint32_t W, bool real) {
+  if (real) {
+    switch (W) {
+      case 1: return {1, 1, 2};
+      case 2: return {2, 1, 2};
+      case 4: return {4, 1, 2};
+      case 8: return {2, 4, 2};
+      case 16: return {4, 4, 2};
+      case 32: return {8, 4, 2};
+      default: return {8, 8, 2};
+    }
+  }
   switch (W) {
     case 1: return {1, 1, 2};
     case 2: return {2, 1, 2};
@@ -134,7 +150,8 @@ struct tbtkkpm_server {
   std::deque<std::unique_ptr<Model>> models;
   std::map<double, tbtkkpm_table *> tables;                         // Mmax rows per scale
   std::map<std::pair<uint32_t, double>, tbtkkpm_table *> exact;     // FP64 reruns
-  std::map<uint32_t, std::array<int, 3>> config;                    // width -> tpr, vpt, minb
+  std::map<uint32_t, std::array<int, 3>> config;  // width | real << 16 -> tpr, vpt, minb
+  bool use_real = true;                           // real lanes for real models added later
   std::deque<uint64_t> pending;
   std::map<uint64_t, std::unique_ptr<Request>> requests;
   uint64_t next_id = 1;
@@ -154,9 +171,10 @@ struct tbtkkpm_server {
   double step_s = 0, step_bytes = 0, finish_s = 0, rerun_s = 0;
   cudaEvent_t ev[2] = {nullptr, nullptr};  // around the steps of a tick
 
-  const std::array<int, 3> &config_for(uint32_t W) {
-    auto it = config.find(W);
-    if (it == config.end()) it = config.emplace(W, default_config(W)).first;
+  const std::array<int, 3> &config_for(uint32_t W, bool real) {
+    const uint32_t key = W | (real ? 1u << 16 : 0u);
+    auto it = config.find(key);
+    if (it == config.end()) it = config.emplace(key, default_config(W, real)).first;
     return it->second;
   }
 };
@@ -170,8 +188,9 @@ int make_resident(tbtkkpm_server *s, Model *m) {
   const uint32_t W = m->W, N = m->N;
   const size_t words = (N + 31) / 32;
   int rc;
-  if ((rc = m->vec[0].reserve(sizeof(float2) * (size_t)N * W)) ||
-      (rc = m->vec[1].reserve(sizeof(float2) * (size_t)N * W)) ||
+  const size_t es = m->esize();
+  if ((rc = m->vec[0].reserve(es * (size_t)N * W)) ||
+      (rc = m->vec[1].reserve(es * (size_t)N * W)) ||
       (rc = m->dots.reserve(2 * sizeof(long long) * W)) ||
       (rc = m->mu.reserve(sizeof(double2) * (size_t)W * s->Mmax)) ||
       (rc = m->mu_direct.reserve(sizeof(double2) * (size_t)W * s->ld)) ||
@@ -181,8 +200,8 @@ int make_resident(tbtkkpm_server *s, Model *m) {
     return rc;
   }
   cudaError_t e;
-  if ((e = cudaMemsetAsync(m->vec[0].ptr, 0, sizeof(float2) * (size_t)N * W, s->stream)) ||
-      (e = cudaMemsetAsync(m->vec[1].ptr, 0, sizeof(float2) * (size_t)N * W, s->stream)) ||
+  if ((e = cudaMemsetAsync(m->vec[0].ptr, 0, es * (size_t)N * W, s->stream)) ||
+      (e = cudaMemsetAsync(m->vec[1].ptr, 0, es * (size_t)N * W, s->stream)) ||
       (e = cudaMemsetAsync(m->dots.ptr, 0, 2 * sizeof(long long) * W, s->stream))) {
     m->release_lanes();
     return cuda_fail(e, "server: lane memory");
@@ -265,6 +284,7 @@ int admit(tbtkkpm_server *s, std::vector<MultiJoin> &joins) {
       j.col = c;
       j.site = site;
       j.W = m->W;
+      j.real = m->real ? 1u : 0u;
       joins.push_back(j);
     }
     m->busy += K;
@@ -322,6 +342,7 @@ MultiModel describe(const tbtkkpm_server *s, const Model *m) {
   d.A.slice_ptr = m->mat->slice_ptr.as<uint32_t>();
   d.A.col = m->mat->scol.as<uint32_t>();
   d.A.val = m->mat->sval.as<double2>();
+  d.A.vre = m->real ? m->mat->sreal.as<double>() : nullptr;
   d.A.N = m->N;
   d.A.nslices = m->mat->nslices;
   d.vec[0] = m->vec[0].as<float2>();
@@ -339,8 +360,8 @@ MultiModel describe(const tbtkkpm_server *s, const Model *m) {
   return d;
 }
 
-// Builds the per-width launch plans of all models with busy lanes (under
-// s->mu).
+// Builds the launch plans, one per (lane width, real or complex lanes), of
+// all models with busy lanes (under s->mu).
 int plan_tick(tbtkkpm_server *s, std::vector<ClassPlan> &plans) {
   std::map<uint32_t, size_t> index;
   for (auto &p : s->models) {
@@ -349,15 +370,16 @@ int plan_tick(tbtkkpm_server *s, std::vector<ClassPlan> &plans) {
     int rc = upload_lanes(s, m);
     if (rc) return rc;
     m->last_tick = s->tick_no;
-    auto it = index.find(m->W);
+    const uint32_t key = m->W | (m->real ? 1u << 16 : 0u);
+    auto it = index.find(key);
     if (it == index.end()) {
-      const auto &cfg = s->config_for(m->W);
+      const auto &cfg = s->config_for(m->W, m->real);
       ClassPlan cp;
       cp.W = m->W;
-      cp.entry = find_multi(cfg[0], cfg[1], cfg[2]);
+      cp.entry = find_multi(cfg[0], cfg[1], cfg[2], m->real);
       if (!cp.entry)
         return fail(TBTKKPM_ERR_UNSUPPORTED, "server: no step kernel for width %u", m->W);
-      it = index.emplace(m->W, plans.size()).first;
+      it = index.emplace(key, plans.size()).first;
       plans.push_back(std::move(cp));
     }
     ClassPlan &cp = plans[it->second];
@@ -368,7 +390,8 @@ int plan_tick(tbtkkpm_server *s, std::vector<ClassPlan> &plans) {
     cp.total_tiles += d.ntiles;
     // matrix once (value + column index, row pointers) and three vector
     // passes of the lanes
-    cp.bytes += 20.0 * m->mat->nnz + 4.0 * (m->N + 1) + 3.0 * m->N * m->W * sizeof(float2);
+    cp.bytes += (m->real ? 12.0 : 20.0) * m->mat->nnz + 4.0 * (m->N + 1) +
+                3.0 * m->N * m->W * m->esize();
     cp.models.push_back(d);
   }
   return TBTKKPM_OK;
@@ -753,11 +776,12 @@ extern "C" int tbtkkpm_server_add_model(tbtkkpm_server *s, const uint32_t *rowpt
   const int prev = swap_selected_device(s->device);
   int rc = tbtkkpm_matrix_create_csr(rowptr, col, val, N, scale, &m->mat);
   tbtkkpm_table *t = nullptr;
-  bool new_table = false;
+  bool new_table = false, use_real = true;
   if (!rc) {
     std::lock_guard<std::mutex> lk(s->mu);
     auto it = s->tables.find(scale);
     if (it != s->tables.end()) t = it->second;
+    use_real = s->use_real;
   }
   if (!rc && !t) {
     rc = tbtkkpm_table_create(s->Mmax, s->energies.data(), s->E, scale, &t);
@@ -771,7 +795,8 @@ extern "C" int tbtkkpm_server_add_model(tbtkkpm_server *s, const uint32_t *rowpt
   m->N = N;
   m->W = width;
   m->scale = scale;
-  m->bytes = lane_bytes(N, width, s->Mmax, s->ld);
+  m->real = use_real && m->mat->values_real;
+  m->bytes = lane_bytes(N, width, s->Mmax, s->ld, m->esize());
   if (m->bytes > s->budget) {
     tbtkkpm_matrix_destroy(m->mat);
     if (new_table) tbtkkpm_table_destroy(t);
@@ -888,12 +913,23 @@ extern "C" int tbtkkpm_server_stats(tbtkkpm_server *s, double *out, uint32_t n) 
 extern "C" int tbtkkpm_server_set_config(tbtkkpm_server *s, uint32_t width, int tpr, int vpt,
                                          int minb) {
   if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_set_config: NULL server");
-  if (!valid_width(width) || tpr * vpt != (int)width || !find_multi(tpr, vpt, minb))
+  const bool cplx = find_multi(tpr, vpt, minb, false) != nullptr;
+  const bool real = find_multi(tpr, vpt, minb, true) != nullptr;
+  if (!valid_width(width) || tpr * vpt != (int)width || !(cplx || real))
     return fail(TBTKKPM_ERR_UNSUPPORTED,
                 "server_set_config: no compiled step (tpr=%d, vpt=%d, minb=%d) for width %u", tpr,
                 vpt, minb, width);
   std::lock_guard<std::mutex> lk(s->mu);
-  s->config[width] = {tpr, vpt, minb};
+  // the lane class(es) this shape is compiled for
+  if (cplx) s->config[width] = {tpr, vpt, minb};
+  if (real) s->config[width | 1u << 16] = {tpr, vpt, minb};
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_server_set_real(tbtkkpm_server *s, int enable) {
+  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_set_real: NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->use_real = enable != 0;
   return TBTKKPM_OK;
 }
 
@@ -916,10 +952,12 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
   cudaStream_t st = s->stream;
   // a private copy of the lane state: every lane busy from global step 1
   const uint32_t W = width, N = probe->N, Mp = 2 * probe_steps + 2, ldp = Mp / 2 + 1;
+  const bool real = probe->real;  // the class of the probe model is tuned
+  const size_t es = probe->esize();
   DevBuf vec[2], dots, mu, mud, base, laneM, bitmap, tlist, dm, dh, tmap;
   int rc;
-  if ((rc = vec[0].reserve(sizeof(float2) * (size_t)N * W)) ||
-      (rc = vec[1].reserve(sizeof(float2) * (size_t)N * W)) ||
+  if ((rc = vec[0].reserve(es * (size_t)N * W)) ||
+      (rc = vec[1].reserve(es * (size_t)N * W)) ||
       (rc = dots.reserve(2 * sizeof(long long) * W)) || (rc = mu.reserve(sizeof(double2) * W * Mp)) ||
       (rc = mud.reserve(sizeof(double2) * W * ldp)) || (rc = base.reserve(4 * W)) ||
       (rc = laneM.reserve(4 * W)) || (rc = bitmap.reserve(4 * (size_t)((N + 31) / 32))) ||
@@ -935,7 +973,7 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
     t.push_back({site, c});
     bm[site >> 5] |= 1u << (site & 31);
     joins.push_back({vec[0].as<float2>(), mu.as<double2>() + (size_t)c * Mp,
-                     mud.as<double2>() + (size_t)c * ldp, N, c, site, W});
+                     mud.as<double2>() + (size_t)c * ldp, N, c, site, W, real ? 1u : 0u});
   }
   std::sort(t.begin(), t.end());
   for (uint32_t i = 0; i < W; i++) {
@@ -945,7 +983,7 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
   cudaError_t e;
   DevBuf dj;
   if ((rc = dj.reserve(sizeof(MultiJoin) * W))) return rc;
-  if ((e = cudaMemsetAsync(vec[1].ptr, 0, sizeof(float2) * (size_t)N * W, st)) ||
+  if ((e = cudaMemsetAsync(vec[1].ptr, 0, es * (size_t)N * W, st)) ||
       (e = cudaMemsetAsync(dots.ptr, 0, 2 * sizeof(long long) * W, st)) ||
       (e = cudaMemcpyAsync(base.ptr, base_h.data(), 4 * W, cudaMemcpyHostToDevice, st)) ||
       (e = cudaMemcpyAsync(laneM.ptr, M_h.data(), 4 * W, cudaMemcpyHostToDevice, st)) ||
@@ -962,13 +1000,16 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
   const MultiEntry *best = nullptr;
   double best_ms = 0;
   int32_t n = 1;
-  for (int i = 0; i < kNumMultiSteps && !rc; i++) {
-    const MultiEntry &en = kMultiSteps[i];
+  const MultiEntry *table = real ? kMultiStepsReal : kMultiSteps;
+  const int nentries = real ? kNumMultiStepsReal : kNumMultiSteps;
+  for (int i = 0; i < nentries && !rc; i++) {
+    const MultiEntry &en = table[i];
     if ((uint32_t)(en.tpr * en.vpt) != W) continue;
     MultiModel d{};
     d.A.slice_ptr = probe->mat->slice_ptr.as<uint32_t>();
     d.A.col = probe->mat->scol.as<uint32_t>();
     d.A.val = probe->mat->sval.as<double2>();
+    d.A.vre = real ? probe->mat->sreal.as<double>() : nullptr;
     d.A.N = N;
     d.A.nslices = probe->mat->nslices;
     d.vec[0] = vec[0].as<float2>();
@@ -1024,7 +1065,7 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
   cudaStreamSynchronize(st);
   if (rc) return rc;
   if (!best) return fail(TBTKKPM_ERR_UNSUPPORTED, "server_autotune: no kernel for width %u", W);
-  s->config[W] = {best->tpr, best->vpt, best->minb};
+  s->config[W | (real ? 1u << 16 : 0u)] = {best->tpr, best->vpt, best->minb};
   if (tpr) *tpr = best->tpr;
   if (vpt) *vpt = best->vpt;
   if (minb) *minb = best->minb;

@@ -95,6 +95,7 @@ SIGNATURES = [
     ("tbtkkpm_server_stats", _i, [_p, _p, _u32]),
     ("tbtkkpm_server_autotune", _i, [_p, _u32, _u32, _p, _p, _p, _p]),
     ("tbtkkpm_server_set_config", _i, [_p, _u32, _i, _i, _i]),
+    ("tbtkkpm_server_set_real", _i, [_p, _i]),
     ("tbtkkpm_server_destroy", _i, [_p]),
 ]
 
@@ -442,6 +443,10 @@ class Server:
     def set_config(self, width, tpr, vpt, minb):
         _check(load_library().tbtkkpm_server_set_config(self._h, int(width), int(tpr), int(vpt),
                                                         int(minb)))
+
+    def set_real(self, enable=True):
+        """Real float lanes for real models added from now on (default)."""
+        _check(load_library().tbtkkpm_server_set_real(self._h, int(bool(enable))))
 
     def close(self):
         if getattr(self, "_h", None):

@@ -119,6 +119,26 @@ def test_server_result_independent_of_configuration(gpu):
 
 
 @pytest.mark.gpu
+def test_server_real_lanes_equal_complex_lanes(gpu):
+    """Real models on real float lanes give the complex64 lanes' results bit
+    for bit (the fixed-point sums make them independent of the kernel)."""
+    kpm = gpu
+    outs = []
+    for real in (True, False):
+        srv = kpm.Server(256, grid(), hbm_budget=1 << 30, tick_steps=16, tolerance=0)
+        srv.set_real(real)
+        ms = models()
+        ids = [srv.add_model(*c, S, 8) for _, c in ms]
+        reqs = [srv.submit(ids[i], np.array([3, 40 + i, 77], dtype=np.uint32), 200, 1e-3)
+                for i in range(len(ms))]
+        outs.append([srv.wait(r) for r in reqs])
+        srv.close()
+    for a, b in zip(*outs):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+
+
+@pytest.mark.gpu
 def test_server_widths(gpu):
     kpm = gpu
     _, csr = models()[3]
