@@ -248,6 +248,20 @@ TBTKKPM_API int tbtkkpm_matrix_real(tbtkkpm_matrix *m, int *values_real, int *in
 TBTKKPM_API int tbtkkpm_matrix_step_configs(
 	tbtkkpm_matrix *m, int precision, int ldos, int *out, int cap);
 
+/* FP64 head of TBTKKPM_MIXED doubling runs.  The doubled moments pick up
+ * the FP32 rounding of the first steps, while the Chebyshev vectors still
+ * sit on the few rows around their source; so a doubling run takes its
+ * first `steps` steps (default 32, at most M/2 - 1) in FP64 on the rows
+ * those steps reach, and the FP32 recursion starts from j_{q-1}, j_q.  This
+ * needs a structurally symmetric pattern (checked when the matrix is made;
+ * a Hermitian matrix has one) and a ball of at most 6144 rows (else the
+ * batch stops its head at the last step that fits).  steps = 0 turns the
+ * head off.  tbtkkpm_matrix_fp64_head reports the setting and whether the
+ * pattern allows a head.  (No reference counterpart.) */
+TBTKKPM_API int tbtkkpm_matrix_set_fp64_head(tbtkkpm_matrix *m, uint32_t steps);
+TBTKKPM_API int tbtkkpm_matrix_fp64_head(
+	tbtkkpm_matrix *m, uint32_t *steps, int *pattern_symmetric);
+
 /* LDOS at B sites in one call: the moments <site|T_n|site> of all sites run
  * as one batched recursion, are damped and summed over the table's energy
  * grid on the device; only the [B][E] result crosses to the host.
@@ -329,7 +343,8 @@ TBTKKPM_API int tbtkkpm_server_wait(
 #define TBTKKPM_STAT_STEP_BYTES 13 /* algorithmic bytes of those steps */
 #define TBTKKPM_STAT_FINISH_S 14  /* worker time in energy sums and results */
 #define TBTKKPM_STAT_RERUN_S 15   /* of which FP64 recomputations */
-#define TBTKKPM_STAT_COUNT 16
+#define TBTKKPM_STAT_JOIN_S 16    /* worker time starting lanes (FP64 heads included) */
+#define TBTKKPM_STAT_COUNT 17
 TBTKKPM_API int tbtkkpm_server_stats(tbtkkpm_server *s, double *out, uint32_t n);
 
 /* Times every compiled step configuration of lane width `width` for
@@ -346,6 +361,11 @@ TBTKKPM_API int tbtkkpm_server_set_config(
  * Hamiltonian is real; by default (1) a real model's lanes hold real float
  * vectors (tbtkkpm_matrix_set_real), with the same results. */
 TBTKKPM_API int tbtkkpm_server_set_real(tbtkkpm_server *s, int enable);
+
+/* FP64 head steps of the lanes of models added later (default 32, 0 = off;
+ * tbtkkpm_matrix_set_fp64_head).  A lane's head depends only on its model,
+ * site and M, so its result is the same alone and in any mix. */
+TBTKKPM_API int tbtkkpm_server_set_fp64_head(tbtkkpm_server *s, uint32_t steps);
 
 /* Stops the worker (requests still queued or in flight are dropped) and
  * frees the server. */

@@ -1,6 +1,7 @@
 // C ABI of the KPM path (include/tbtkkpm.h): handles, workspace, dispatch.
 #include "tbtkkpm.h"
 #include "kpm_kernels.cuh"
+#include "kpm_prefix.cuh"
 #include "kpm_host.h"
 
 #include <cub/cub.cuh>
@@ -241,6 +242,18 @@ static int build_sell(tbtkkpm_matrix *m, cudaStream_t st) {
   if (e != cudaSuccess) return cuda_fail(e, "SELL build");
   m->values_real = complex_flag == 0;
   if (!m->values_real) m->sreal.release();
+  // structural symmetry, which the FP64 head of doubling runs needs
+  unsigned asym = 0;
+  if (N > 0) {
+    if ((e = cudaMemsetAsync(flag.ptr, 0, 4, st)) != cudaSuccess) return cuda_fail(e, "SELL build");
+    k_pattern_check<<<blocks_for(N), 256, 0, st>>>(N, m->rowptr.as<uint32_t>(), m->col.as<uint32_t>(),
+                                                   flag.as<unsigned>());
+    count_launches(1);
+    e = cudaMemcpyAsync(&asym, flag.ptr, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cuda_fail(e, "SELL build");
+  }
+  m->pattern_symmetric = N > 0 && asym == 0;
   return TBTKKPM_OK;
 }
 

@@ -66,9 +66,10 @@ struct Workspace {
   DevBuf dots;        // [grid][2][Bp] per-block dot products (doubling runs)
   DevBuf col_out;     // [Bp] output slot of each batch column (doubling runs)
   DevBuf err;         // device flag of a bounded wait that ran out
+  DevBuf head, head_jobs, head_res;  // FP64 head of doubling runs (scratch, jobs, results)
   void release() {
     for (DevBuf *b : {&vec[0], &vec[1], &bitmap, &tgt, &from, &mu, &damp, &out, &mu_direct,
-                      &dots, &col_out, &err})
+                      &dots, &col_out, &err, &head, &head_jobs, &head_res})
       b->release();
   }
 };
@@ -91,6 +92,10 @@ struct tbtkkpm_matrix {
   bool values_real = false;
   bool use_real = true;  // tbtkkpm_matrix_set_real
   tbtkkpm::DevBuf sreal;
+  // structurally symmetric pattern: doubling runs may take their first
+  // head_steps steps in FP64 on the rows those steps reach
+  bool pattern_symmetric = false;
+  uint32_t head_steps = 32;  // tbtkkpm_matrix_set_fp64_head (kPrefixSteps)
   uint32_t nslices = 0;
   uint64_t chunks = 0;
   tbtkkpm::Workspace ws;

@@ -366,6 +366,8 @@ struct MultiJoin {
   uint32_t col, site;
   uint32_t W;         // the model's lane width
   uint32_t real;      // the model's vectors are real floats (x holds float)
+  float2 *x_prev;     // the model's vec[g&1] (column cleared when not null)
+  uint32_t M;         // moments of the lane's request
 };
 
 static __global__ void kpm_multi_join(const MultiJoin *__restrict__ joins, uint32_t Mmax, uint32_t ld) {
@@ -373,10 +375,13 @@ static __global__ void kpm_multi_join(const MultiJoin *__restrict__ joins, uint3
   const uint32_t W = jn.W;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < jn.rows; r += stride) {
-    if (jn.real)
+    if (jn.real) {
       reinterpret_cast<float *>(jn.x)[r * W + jn.col] = r == jn.site ? 1.0f : 0.0f;
-    else
+      if (jn.x_prev) reinterpret_cast<float *>(jn.x_prev)[r * W + jn.col] = 0.0f;
+    } else {
       jn.x[r * W + jn.col] = r == jn.site ? make_float2(1.0f, 0.0f) : make_float2(0.0f, 0.0f);
+      if (jn.x_prev) jn.x_prev[r * W + jn.col] = make_float2(0.0f, 0.0f);
+    }
   }
   for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < Mmax; k += stride) {
     jn.mu[k] = make_double2(k == 0 ? 1.0 : 0.0, 0.0);

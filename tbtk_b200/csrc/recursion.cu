@@ -3,6 +3,7 @@
 #include "kpm_host.h"
 #include "kpm_kernels.cuh"
 #include "kpm_steps.cuh"
+#include "kpm_prefix.cuh"
 
 #include <algorithm>
 #include <array>
@@ -153,10 +154,12 @@ struct TargetList {
 // ([K][M]).  doubling: every source's only target is itself (an LDOS batch);
 // the recursion stops at j_{M/2} and the moments come from the doubling
 // identities, while the directly gathered moments of steps 0..M/2 land in
-// ws.mu_direct ([K][M/2+1]) for the error estimate.
+// ws.mu_direct ([K][M/2+1]) for the error estimate.  A mixed doubling run
+// on a structurally symmetric matrix takes its first steps in FP64 on the
+// rows they reach (kpm_prefix) unless `head` is false.
 int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &from,
               const TargetList &tl, uint32_t K, uint32_t M, bool doubling,
-              const StepEntry *force = nullptr) {
+              const StepEntry *force = nullptr, bool head = true) {
   Workspace &ws = m->ws;
   cudaStream_t st = m->stream;
   const uint32_t B = (uint32_t)from.size();
@@ -207,6 +210,58 @@ int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &fro
         (e = cudaMemsetAsync(ws.mu_direct.ptr, 0, sizeof(double2) * (size_t)K * ld_direct, st)))
       return cuda_fail(e, "recursion: staging");
   }
+  StepArgs a;
+  a.A.slice_ptr = m->slice_ptr.as<uint32_t>();
+  a.A.col = m->scol.as<uint32_t>();
+  a.A.val = m->sval.as<double2>();
+  a.A.N = m->N;
+  a.A.nslices = m->nslices;
+  a.A.vre = m->values_real ? m->sreal.as<double>() : nullptr;
+  // FP64 head: j_0 .. j_q of every source on its ball, q common to the batch
+  uint32_t q = 0;
+  const uint32_t want = std::min(m->head_steps, steps >= 1 ? steps - 1 : 0u);
+  if (head && doubling && is_mixed(precision) && m->pattern_symmetric && want >= 2) {
+    std::vector<uint32_t> slot(B, kPad);
+    for (uint32_t i = 0; i < T; i++) slot[tl.col[i]] = tl.out[i];
+    if (std::find(slot.begin(), slot.end(), kPad) != slot.end())
+      return fail(TBTKKPM_ERR_ARGUMENT, "recursion: a doubling source without its own target");
+    std::vector<PrefixJob> jobs(B);
+    for (uint32_t b = 0; b < B; b++) {
+      PrefixJob &j = jobs[b];
+      j.slice_ptr = a.A.slice_ptr;
+      j.scol = a.A.col;
+      j.sval = a.A.val;
+      j.site = from[b];
+      j.steps = want;
+      j.M = M;
+      j.ld = ld_direct;
+      j.mu = ws.mu.as<double2>() + (size_t)slot[b] * M;
+      j.mu_direct = ws.mu_direct.as<double2>() + (size_t)slot[b] * ld_direct;
+      j.x_cur = ws.vec[0].ptr;
+      j.x_prev = ws.vec[1].ptr;
+      j.W = Bp;
+      j.col = b;
+      j.real = real ? 1u : 0u;
+      j.pad = 0;
+    }
+    std::vector<PrefixResult> res;
+    if ((rc = run_fp64_head(st, jobs, ws, res))) return rc;
+    q = want;
+    for (const PrefixResult &r : res) q = std::min(q, r.q);
+    if (q < want) {
+      // a ball outgrew the table: clear the buffers and run every source to
+      // the shortest head (or start plainly when that is below 2 steps)
+      if ((e = cudaMemsetAsync(ws.vec[0].ptr, 0, vbytes, st)) ||
+          (e = cudaMemsetAsync(ws.vec[1].ptr, 0, vbytes, st)))
+        return cuda_fail(e, "recursion: staging");
+      if (q >= 2) {
+        for (PrefixJob &j : jobs) j.steps = q;
+        if ((rc = run_fp64_head(st, jobs, ws, res))) return rc;
+      } else {
+        q = 0;  // the moment rows the head touched are rewritten by the plain start
+      }
+    }
+  }
   Targets tg;
   tg.bitmap = ws.bitmap.as<uint32_t>();
   tg.row = ws.tgt.as<uint32_t>();
@@ -216,22 +271,18 @@ int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &fro
   tg.mu = doubling ? ws.mu_direct.as<double2>() : ws.mu.as<double2>();
   tg.ld = ld_direct;
   const unsigned ib = blocks_for(std::max(B, T));
-  if (real)
+  if (q > 0) {
+    // the head wrote j_q, j_{q-1} and the moments through step q
+  } else if (real) {
     kpm_init_sources_real<<<ib, 256, 0, st>>>(B, Bp, ws.from.as<uint32_t>(), ws.vec[0].as<float>(),
                                               tg);
-  else if (is_mixed(precision))
+  } else if (is_mixed(precision)) {
     kpm_init_sources<float2><<<ib, 256, 0, st>>>(B, Bp, ws.from.as<uint32_t>(),
                                                 ws.vec[0].as<float2>(), tg);
-  else
+  } else {
     kpm_init_sources<double2><<<ib, 256, 0, st>>>(B, Bp, ws.from.as<uint32_t>(),
                                                  ws.vec[0].as<double2>(), tg);
-  StepArgs a;
-  a.A.slice_ptr = m->slice_ptr.as<uint32_t>();
-  a.A.col = m->scol.as<uint32_t>();
-  a.A.val = m->sval.as<double2>();
-  a.A.N = m->N;
-  a.A.nslices = m->nslices;
-  a.A.vre = m->values_real ? m->sreal.as<double>() : nullptr;
+  }
   a.Bp = Bp;
   a.tg = tg;
   a.dots = doubling ? ws.dots.as<double2>() : nullptr;
@@ -239,9 +290,9 @@ int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &fro
   void *cur = ws.vec[0].ptr, *prev = ws.vec[1].ptr;
   m->timer.mark(st, 0);
   m->timer.pending = m->timer.enabled;
-  m->timer.pending_steps = steps;
-  count_launches(1 + (uint64_t)steps * (doubling ? 2 : 1));
-  for (uint32_t n = 1; n <= steps; n++) {
+  m->timer.pending_steps = steps - q;
+  count_launches((q > 0 ? 0 : 1) + (uint64_t)(steps - q) * (doubling ? 2 : 1));
+  for (uint32_t n = q + 1; n <= steps; n++) {
     a.x = cur;
     a.y = prev;
     a.n_out = n;
@@ -754,7 +805,7 @@ extern "C" int tbtkkpm_matrix_autotune(tbtkkpm_matrix *m, uint32_t B, int precis
     double ms = 0;
     for (int rep = 0; rep < 2; rep++) {
       m->timer.recursion_ms = 0;
-      if ((rc = run_batch(m, precision, fr, tl, B, M, doubling, &t[i]))) break;
+      if ((rc = run_batch(m, precision, fr, tl, B, M, doubling, &t[i], false))) break;
       cudaError_t e = cudaStreamSynchronize(m->stream);
       if (e != cudaSuccess) {
         rc = cuda_fail(e, "matrix_autotune");
@@ -850,6 +901,20 @@ extern "C" int tbtkkpm_matrix_set_real(tbtkkpm_matrix *m, int enable) {
   if (!m) return fail(TBTKKPM_ERR_ARGUMENT, "matrix_set_real: NULL matrix");
   std::lock_guard<std::mutex> lk(m->lock);
   m->use_real = enable != 0;
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_matrix_set_fp64_head(tbtkkpm_matrix *m, uint32_t steps) {
+  if (!m) return fail(TBTKKPM_ERR_ARGUMENT, "matrix_set_fp64_head: NULL matrix");
+  std::lock_guard<std::mutex> lk(m->lock);
+  m->head_steps = steps;
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_matrix_fp64_head(tbtkkpm_matrix *m, uint32_t *steps, int *pattern_symmetric) {
+  if (!m) return fail(TBTKKPM_ERR_ARGUMENT, "matrix_fp64_head: NULL matrix");
+  if (steps) *steps = m->head_steps;
+  if (pattern_symmetric) *pattern_symmetric = m->pattern_symmetric ? 1 : 0;
   return TBTKKPM_OK;
 }
 

@@ -18,6 +18,7 @@
 #include "kpm_host.h"
 #include "kpm_multi.cuh"
 #include "kpm_multi_real.cuh"
+#include "kpm_prefix.cuh"
 
 #include <algorithm>
 #include <chrono>
@@ -69,6 +70,7 @@ struct Model {
   uint32_t N = 0, W = 0;
   double scale = 1;
   bool real = false;  // real Hamiltonian: lanes hold real float vectors
+  uint32_t head_steps = 0;  // FP64 head of a lane (0: none)
   bool resident = false;
   uint64_t bytes = 0;
   uint64_t last_tick = 0;
@@ -152,6 +154,8 @@ struct tbtkkpm_server {
   std::map<std::pair<uint32_t, double>, tbtkkpm_table *> exact;     // FP64 reruns
   std::map<uint32_t, std::array<int, 3>> config;  // width | real << 16 -> tpr, vpt, minb
   bool use_real = true;                           // real lanes for real models added later
+  uint32_t head_steps = kPrefixSteps;             // FP64 head of models added later
+  Workspace head_ws;                              // FP64 head scratch (worker thread)
   std::deque<uint64_t> pending;
   std::map<uint64_t, std::unique_ptr<Request>> requests;
   uint64_t next_id = 1;
@@ -168,7 +172,7 @@ struct tbtkkpm_server {
   // statistics
   std::vector<double> latencies_ms;
   double reruns = 0, ticks = 0, steps = 0, lane_steps = 0, evictions = 0, waited = 0, busy_s = 0;
-  double step_s = 0, step_bytes = 0, finish_s = 0, rerun_s = 0;
+  double step_s = 0, step_bytes = 0, finish_s = 0, rerun_s = 0, join_s = 0;
   cudaEvent_t ev[2] = {nullptr, nullptr};  // around the steps of a tick
 
   const std::array<int, 3> &config_for(uint32_t W, bool real) {
@@ -241,9 +245,17 @@ bool make_room(tbtkkpm_server *s, uint64_t need, const Model *keep) {
   return true;
 }
 
+// A lane joining at this step boundary.
+struct JoinRef {
+  Model *m;
+  uint32_t c;
+  Request *r;
+};
+
 // Under s->mu.  Queued requests take free lanes in arrival order; the joins
-// of this step boundary are appended.
-int admit(tbtkkpm_server *s, std::vector<MultiJoin> &joins) {
+// of this step boundary are appended (the lane bases assume no FP64 head
+// until run_joins has reported the heads).
+int admit(tbtkkpm_server *s, std::vector<MultiJoin> &joins, std::vector<JoinRef> &refs) {
   for (auto it = s->pending.begin(); it != s->pending.end();) {
     Request *r = s->requests.at(*it).get();
     Model *m = s->models[r->model].get();
@@ -285,7 +297,10 @@ int admit(tbtkkpm_server *s, std::vector<MultiJoin> &joins) {
       j.site = site;
       j.W = m->W;
       j.real = m->real ? 1u : 0u;
+      j.x_prev = m->vec[s->n_global & 1].as<float2>();
+      j.M = r->M;
       joins.push_back(j);
+      refs.push_back({m, c, r});
     }
     m->busy += K;
     m->dirty = true;
@@ -397,27 +412,68 @@ int plan_tick(tbtkkpm_server *s, std::vector<ClassPlan> &plans) {
   return TBTKKPM_OK;
 }
 
-// Launches joins and `nsteps` steps of every plan starting at global step
-// s->n_global (worker thread, no lock held).
-int run_tick(tbtkkpm_server *s, const std::vector<MultiJoin> &joins,
-             const std::vector<ClassPlan> &plans, uint32_t nsteps) {
+// Starts the lanes of `joins` at global step s->n_global (worker thread, no
+// lock held): clears their columns and moment rows, then runs the FP64 head
+// of every lane whose model has one, which writes j_q, j_{q-1} into its
+// columns; head[i] = q of join i (0: plain start from j_0).  Returns after
+// the stream has passed the joins.
+int run_joins(tbtkkpm_server *s, const std::vector<MultiJoin> &joins, const std::vector<JoinRef> &refs,
+              std::vector<uint32_t> &head) {
   cudaStream_t st = s->stream;
   int rc;
   cudaError_t e;
-  if (!joins.empty()) {
-    if ((rc = s->d_joins.reserve(sizeof(MultiJoin) * joins.size()))) return rc;
-    if ((e = cudaMemcpyAsync(s->d_joins.ptr, joins.data(), sizeof(MultiJoin) * joins.size(),
-                             cudaMemcpyHostToDevice, st)))
-      return cuda_fail(e, "server: joins");
-    uint32_t rows = 0;
-    for (const MultiJoin &j : joins) rows = std::max(rows, j.rows);
-    const unsigned bx = std::max(1u, std::min(blocks_for(std::max(rows, s->Mmax)), 512u));
-    for (size_t j0 = 0; j0 < joins.size(); j0 += 65535) {
-      const unsigned nj = (unsigned)std::min<size_t>(65535, joins.size() - j0);
-      kpm_multi_join<<<dim3(bx, nj), 256, 0, st>>>(s->d_joins.as<MultiJoin>() + j0, s->Mmax, s->ld);
-    }
-    count_launches((joins.size() + 65534) / 65535);
+  head.assign(joins.size(), 0);
+  if (joins.empty()) return TBTKKPM_OK;
+  if ((rc = s->d_joins.reserve(sizeof(MultiJoin) * joins.size()))) return rc;
+  if ((e = cudaMemcpyAsync(s->d_joins.ptr, joins.data(), sizeof(MultiJoin) * joins.size(),
+                           cudaMemcpyHostToDevice, st)))
+    return cuda_fail(e, "server: joins");
+  uint32_t rows = 0;
+  for (const MultiJoin &j : joins) rows = std::max(rows, j.rows);
+  const unsigned bx = std::max(1u, std::min(blocks_for(std::max(rows, s->Mmax)), 512u));
+  for (size_t j0 = 0; j0 < joins.size(); j0 += 65535) {
+    const unsigned nj = (unsigned)std::min<size_t>(65535, joins.size() - j0);
+    kpm_multi_join<<<dim3(bx, nj), 256, 0, st>>>(s->d_joins.as<MultiJoin>() + j0, s->Mmax, s->ld);
   }
+  count_launches((joins.size() + 65534) / 65535);
+  std::vector<PrefixJob> jobs;
+  std::vector<size_t> which;
+  for (size_t i = 0; i < joins.size(); i++) {
+    const MultiJoin &j = joins[i];
+    const Model *m = refs[i].m;
+    const uint32_t want = std::min(m->head_steps, j.M / 2 >= 1 ? j.M / 2 - 1 : 0u);
+    if (!m->mat->pattern_symmetric || want < 2) continue;
+    PrefixJob p{};
+    p.slice_ptr = m->mat->slice_ptr.as<uint32_t>();
+    p.scol = m->mat->scol.as<uint32_t>();
+    p.sval = m->mat->sval.as<double2>();
+    p.site = j.site;
+    p.steps = want;
+    p.M = j.M;
+    p.ld = s->ld;
+    p.mu = j.mu;
+    p.mu_direct = j.mu_direct;
+    p.x_cur = j.x;
+    p.x_prev = j.x_prev;
+    p.W = j.W;
+    p.col = j.col;
+    p.real = j.real;
+    jobs.push_back(p);
+    which.push_back(i);
+  }
+  std::vector<PrefixResult> res;
+  if ((rc = run_fp64_head(st, jobs, s->head_ws, res))) return rc;
+  for (size_t k = 0; k < which.size(); k++) head[which[k]] = res[k].q >= 2 ? res[k].q : 0;
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "server: joins");
+  return TBTKKPM_OK;
+}
+
+// Launches `nsteps` steps of every plan starting at global step s->n_global
+// (worker thread, no lock held).
+int run_tick(tbtkkpm_server *s, const std::vector<ClassPlan> &plans, uint32_t nsteps) {
+  cudaStream_t st = s->stream;
+  int rc;
+  cudaError_t e;
   // descriptors and headers of all plans in one upload
   size_t nm = 0;
   for (const ClassPlan &cp : plans) nm += cp.models.size();
@@ -628,7 +684,30 @@ void worker(tbtkkpm_server *s) {
     const auto t0 = Clock::now();
     s->working = true;
     std::vector<MultiJoin> joins;
-    int rc = admit(s, joins);
+    std::vector<JoinRef> refs;
+    int rc = admit(s, joins, refs);
+    if (!rc && !joins.empty()) {
+      // FP64 heads: a lane with head q starts at local step q + 1, and a
+      // request ends with its last lane
+      std::vector<uint32_t> head;
+      lk.unlock();
+      const auto j0 = Clock::now();
+      rc = run_joins(s, joins, refs, head);
+      const double js = std::chrono::duration<double>(Clock::now() - j0).count();
+      lk.lock();
+      s->join_s += js;
+      for (size_t i = 0; !rc && i < refs.size(); i++) {
+        refs[i].m->base_h[refs[i].c] -= (int32_t)head[i];
+        refs[i].m->dirty = true;
+      }
+      for (size_t i = 0; !rc && i < refs.size(); i++) {
+        Request *r = refs[i].r;
+        if (r->lanes[0] != refs[i].c) continue;
+        int32_t last = INT32_MIN;
+        for (uint32_t c : r->lanes) last = std::max(last, refs[i].m->base_h[c]);
+        r->base = last;
+      }
+    }
     std::vector<ClassPlan> plans;
     if (!rc) rc = plan_tick(s, plans);
     if (rc) {
@@ -646,16 +725,18 @@ void worker(tbtkkpm_server *s) {
     for (auto &p : s->models) {
       Model *m = p.get();
       if (!m->resident || !m->busy) continue;
-      for (uint32_t c = 0; c < m->W; c++)
-        if (m->lane_req[c]) {
-          const int64_t last = (int64_t)m->base_h[c] + m->M_h[c] / 2;  // global step of the last local step
-          const int64_t left = last - (int64_t)s->n_global + 1;
-          nsteps = (uint32_t)std::min<int64_t>(nsteps, std::max<int64_t>(left, 1));
-        }
+      for (uint32_t c = 0; c < m->W; c++) {
+        if (!m->lane_req[c]) continue;
+        const Request *r = s->requests.at(m->lane_req[c]).get();
+        if (r->lanes.empty() || r->lanes[0] != c) continue;  // one entry per request
+        const int64_t last = (int64_t)r->base + r->M / 2;  // global step of its last local step
+        const int64_t left = last - (int64_t)s->n_global + 1;
+        nsteps = (uint32_t)std::min<int64_t>(nsteps, std::max<int64_t>(left, 1));
+      }
     }
     s->tick_no += 1;
     lk.unlock();
-    rc = run_tick(s, joins, plans, nsteps);
+    rc = run_tick(s, plans, nsteps);
     cudaError_t e = cudaSuccess;
     if (!rc && (e = cudaStreamSynchronize(s->stream)) != cudaSuccess)
       rc = cuda_fail(e, "server: tick");
@@ -777,11 +858,13 @@ extern "C" int tbtkkpm_server_add_model(tbtkkpm_server *s, const uint32_t *rowpt
   int rc = tbtkkpm_matrix_create_csr(rowptr, col, val, N, scale, &m->mat);
   tbtkkpm_table *t = nullptr;
   bool new_table = false, use_real = true;
+  uint32_t head_steps = 0;
   if (!rc) {
     std::lock_guard<std::mutex> lk(s->mu);
     auto it = s->tables.find(scale);
     if (it != s->tables.end()) t = it->second;
     use_real = s->use_real;
+    head_steps = s->head_steps;
   }
   if (!rc && !t) {
     rc = tbtkkpm_table_create(s->Mmax, s->energies.data(), s->E, scale, &t);
@@ -796,6 +879,7 @@ extern "C" int tbtkkpm_server_add_model(tbtkkpm_server *s, const uint32_t *rowpt
   m->W = width;
   m->scale = scale;
   m->real = use_real && m->mat->values_real;
+  m->head_steps = head_steps;
   m->bytes = lane_bytes(N, width, s->Mmax, s->ld, m->esize());
   if (m->bytes > s->budget) {
     tbtkkpm_matrix_destroy(m->mat);
@@ -906,6 +990,7 @@ extern "C" int tbtkkpm_server_stats(tbtkkpm_server *s, double *out, uint32_t n) 
   v[TBTKKPM_STAT_STEP_BYTES] = s->step_bytes;
   v[TBTKKPM_STAT_FINISH_S] = s->finish_s;
   v[TBTKKPM_STAT_RERUN_S] = s->rerun_s;
+  v[TBTKKPM_STAT_JOIN_S] = s->join_s;
   for (uint32_t i = 0; i < n && i < TBTKKPM_STAT_COUNT; i++) out[i] = v[i];
   return TBTKKPM_OK;
 }
@@ -923,6 +1008,13 @@ extern "C" int tbtkkpm_server_set_config(tbtkkpm_server *s, uint32_t width, int 
   // the lane class(es) this shape is compiled for
   if (cplx) s->config[width] = {tpr, vpt, minb};
   if (real) s->config[width | 1u << 16] = {tpr, vpt, minb};
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_server_set_fp64_head(tbtkkpm_server *s, uint32_t steps) {
+  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_set_fp64_head: NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->head_steps = steps;
   return TBTKKPM_OK;
 }
 
@@ -1093,6 +1185,7 @@ extern "C" int tbtkkpm_server_destroy(tbtkkpm_server *s) {
     for (DevBuf *b : {&s->d_models, &s->d_hdr, &s->d_joins, &s->d_done, &s->d_stage, &s->d_damp,
                       &s->d_tiles})
       b->release();
+    s->head_ws.release();
     for (cudaEvent_t &ev : s->ev)
       if (ev) cudaEventDestroy(ev);
     cudaStreamDestroy(s->stream);

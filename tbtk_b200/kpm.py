@@ -88,6 +88,8 @@ SIGNATURES = [
     ("tbtkkpm_matrix_set_real", _i, [_p, _i]),
     ("tbtkkpm_matrix_real", _i, [_p, _p, _p]),
     ("tbtkkpm_matrix_step_configs", _i, [_p, _i, _i, _p, _i]),
+    ("tbtkkpm_matrix_set_fp64_head", _i, [_p, _u32]),
+    ("tbtkkpm_matrix_fp64_head", _i, [_p, _p, _p]),
     ("tbtkkpm_server_create", _i, [_u32, _p, _u32, _u64, _u32, _d, _p]),
     ("tbtkkpm_server_add_model", _i, [_p, _p, _p, _p, _u32, _d, _u32, _p]),
     ("tbtkkpm_server_submit", _i, [_p, _u32, _p, _u32, _u32, _d, _p]),
@@ -96,13 +98,14 @@ SIGNATURES = [
     ("tbtkkpm_server_autotune", _i, [_p, _u32, _u32, _p, _p, _p, _p]),
     ("tbtkkpm_server_set_config", _i, [_p, _u32, _i, _i, _i]),
     ("tbtkkpm_server_set_real", _i, [_p, _i]),
+    ("tbtkkpm_server_set_fp64_head", _i, [_p, _u32]),
     ("tbtkkpm_server_destroy", _i, [_p]),
 ]
 
 PENDING = 1
 STAT_NAMES = ["completed", "p50_ms", "p99_ms", "mean_ms", "reruns", "ticks", "steps",
               "lane_steps", "resident_bytes", "evictions", "waited", "busy_s", "step_s",
-              "step_bytes", "finish_s", "rerun_s"]
+              "step_bytes", "finish_s", "rerun_s", "join_s"]
 
 
 def step_configs(precision, ldos=True):
@@ -263,6 +266,16 @@ class Matrix:
         vr, use = ctypes.c_int(), ctypes.c_int()
         _check(load_library().tbtkkpm_matrix_real(self._h, ctypes.byref(vr), ctypes.byref(use)))
         return bool(vr.value), bool(use.value)
+
+    def set_fp64_head(self, steps=32):
+        """FP64 steps at the head of MIXED doubling runs (0 turns it off)."""
+        _check(load_library().tbtkkpm_matrix_set_fp64_head(self._h, int(steps)))
+
+    def fp64_head(self):
+        """(head steps setting, pattern allows a head)."""
+        st, sym = ctypes.c_uint32(), ctypes.c_int()
+        _check(load_library().tbtkkpm_matrix_fp64_head(self._h, ctypes.byref(st), ctypes.byref(sym)))
+        return st.value, bool(sym.value)
 
     def configs_for(self, B, precision, ldos=True):
         """The compiled (tpr, vpt, variant) this matrix's calls for B sources
@@ -447,6 +460,10 @@ class Server:
     def set_real(self, enable=True):
         """Real float lanes for real models added from now on (default)."""
         _check(load_library().tbtkkpm_server_set_real(self._h, int(bool(enable))))
+
+    def set_fp64_head(self, steps=32):
+        """FP64 head steps of the lanes of models added from now on."""
+        _check(load_library().tbtkkpm_server_set_fp64_head(self._h, int(steps)))
 
     def close(self):
         if getattr(self, "_h", None):

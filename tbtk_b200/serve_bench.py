@@ -71,9 +71,10 @@ def uneven(a):
     specs = workloads.cfg4_specs(a.models, seed=4)
     srv = kpm.Server(4096, energies, hbm_budget=int(a.budget_gb * 2**30), tick_steps=a.tick,
                      tolerance=a.tolerance)
+    srv.set_fp64_head(a.fp64_head)
     t0 = time.perf_counter()
     reqs, csrs = [], {}
-    rng = np.random.default_rng(44)
+    rng = np.random.default_rng(a.sample_seed)
     sample_idx = set(rng.choice(len(specs), size=min(a.samples, len(specs)), replace=False).tolist())
     rows = nnz = 0
     for i, (kind, L, J, W, ns, M, seed) in enumerate(specs):
@@ -101,8 +102,12 @@ def uneven(a):
         where.append(i)
     t_plain, ref = plain_baseline(samples, energies, 1e-3)
     errs = [float(np.abs(results[i][0][0] - r).max() / np.abs(r).max()) for i, r in zip(where, ref)]
+    # the server's error estimate of each sampled site next to its error
+    # against the FP64 path (a site recomputed in FP64 has error 0)
+    est = [(float(results[i][1][0]), e, int(results[i][2][0])) for i, e in zip(where, errs)]
     srv.close()
     return {
+        "estimate_vs_error": est,
         "workload": f"uneven batch: {a.models} models (square/honeycomb, L in [16,256]), "
                     f"1-32 sites, M in {{512..4096}}, s=12, E=1000",
         "metric": "LDOS solves/s", "value": solves / wall, "unit": "LDOS solves/s",
@@ -121,6 +126,7 @@ def serve(a):
     pool = workloads.cfg5_pool(a.models, seed=5)
     srv = kpm.Server(4096, energies, hbm_budget=int(a.budget_gb * 2**30), tick_steps=a.tick,
                      tolerance=a.tolerance)
+    srv.set_fp64_head(a.fp64_head)
     sizes, csrs = [], []
     t0 = time.perf_counter()
     for kind, L, J, W, alpha, seed in pool:
@@ -179,6 +185,10 @@ def main():
     ap.add_argument("--tick", type=int, default=64)
     ap.add_argument("--tolerance", type=float, default=1e-6)
     ap.add_argument("--samples", type=int, default=16)
+    ap.add_argument("--sample-seed", type=int, default=44,
+                    help="seed of the sampled solves checked against the FP64 path")
+    ap.add_argument("--fp64-head", type=int, default=32,
+                    help="FP64 head steps of every lane (0: none)")
     a = ap.parse_args()
     if a.models is None:
         a.models = 1000 if a.workload == "uneven" else 64
