@@ -344,7 +344,9 @@ TBTKKPM_API int tbtkkpm_server_wait(
 #define TBTKKPM_STAT_FINISH_S 14  /* worker time in energy sums and results */
 #define TBTKKPM_STAT_RERUN_S 15   /* of which FP64 recomputations */
 #define TBTKKPM_STAT_JOIN_S 16    /* worker time starting lanes (FP64 heads included) */
-#define TBTKKPM_STAT_COUNT 17
+#define TBTKKPM_STAT_PLAN_S 17    /* worker time admitting requests and planning ticks */
+#define TBTKKPM_STAT_TICK_S 18    /* worker time launching ticks and waiting for them */
+#define TBTKKPM_STAT_COUNT 19
 TBTKKPM_API int tbtkkpm_server_stats(tbtkkpm_server *s, double *out, uint32_t n);
 
 /* Times every compiled step configuration of lane width `width` for

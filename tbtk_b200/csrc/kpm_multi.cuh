@@ -391,7 +391,7 @@ static __global__ void kpm_multi_join(const MultiJoin *__restrict__ joins, uint3
 
 // The moments of a finished request, [K][M] contiguous: the direct moments
 // for n <= M/2 and the doubled ones above, damped by a[n]/b as kpm_damp
-// (raw copies of both kinds go to the error estimate).
+// (raw copies of both kinds when raw and raw_direct are not null).
 struct MultiDone {
   const double2 *mu;        // lane row [Mmax]
   const double2 *mu_direct; // lane row [ld]
@@ -407,17 +407,49 @@ static __global__ void kpm_multi_prepare(const MultiDone *__restrict__ lanes, ui
   const uint32_t half = M / 2;
   const MultiDone d = lanes[k];
   const double2 dbl = d.mu[nn];
-  raw[i] = dbl;
+  if (raw) raw[i] = dbl;
   double2 c = dbl;
   if (nn <= half) {
     c = d.mu_direct[nn];
-    raw_direct[(uint64_t)k * (half + 1) + nn] = c;
+    if (raw_direct) raw_direct[(uint64_t)k * (half + 1) + nn] = c;
   }
   if (damp) {
     const double an = a[nn];
     c = make_double2(__ddiv_rn(__dmul_rn(c.x, an), b), __ddiv_rn(__dmul_rn(c.y, an), b));
   }
   out[i] = c;
+}
+
+// Error estimate of each finished lane, the single-model doubling_error on
+// the device: 4 sqrt(2) max_{2 <= n <= M/2} |mu_n - mu_direct_n| divided by
+// max_{n < M} |mu_n| (mu the doubled row).  One block of kErrorBlock
+// threads per lane; maxima do not depend on the reduction order.
+constexpr int kErrorBlock = 256;
+static __global__ void __launch_bounds__(kErrorBlock)
+kpm_multi_error(const MultiDone *__restrict__ lanes, uint32_t M, double *__restrict__ err) {
+  __shared__ double rs[kErrorBlock], rd[kErrorBlock];
+  const MultiDone d = lanes[blockIdx.x];
+  const uint32_t ld = M / 2 + 1;
+  double sc = 0.0, dm = 0.0;
+  for (uint32_t n = threadIdx.x; n < M; n += kErrorBlock) {
+    const double2 a = d.mu[n];
+    sc = fmax(sc, hypot(a.x, a.y));
+    if (n >= 2 && n < ld) {
+      const double2 b = d.mu_direct[n];
+      dm = fmax(dm, hypot(a.x - b.x, a.y - b.y));
+    }
+  }
+  rs[threadIdx.x] = sc;
+  rd[threadIdx.x] = dm;
+  __syncthreads();
+  for (int h = kErrorBlock / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) {
+      rs[threadIdx.x] = fmax(rs[threadIdx.x], rs[threadIdx.x + h]);
+      rd[threadIdx.x] = fmax(rd[threadIdx.x], rd[threadIdx.x + h]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) err[blockIdx.x] = rs[0] > 0 ? 4.0 * sqrt(2.0) * rd[0] / rs[0] : 0.0;
 }
 
 }  // namespace tbtkkpm

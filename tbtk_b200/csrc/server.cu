@@ -59,7 +59,6 @@ struct Request {
   std::vector<double> ldos, err;
   std::vector<int32_t> rerun;
   // staging of the finish phase
-  std::vector<double2> raw, raw_direct;
   size_t stage_off = 0;
 };
 
@@ -172,7 +171,10 @@ struct tbtkkpm_server {
   // statistics
   std::vector<double> latencies_ms;
   double reruns = 0, ticks = 0, steps = 0, lane_steps = 0, evictions = 0, waited = 0, busy_s = 0;
-  double step_s = 0, step_bytes = 0, finish_s = 0, rerun_s = 0, join_s = 0;
+  double step_s = 0, step_bytes = 0, finish_s = 0, rerun_s = 0, join_s = 0, plan_s = 0, tick_s = 0;
+  DevBuf d_res;                 // finish results of a tick: [ldos K*E | err K] per request
+  double *h_res = nullptr;      // pinned host copy of d_res
+  size_t h_res_cap = 0;
   cudaEvent_t ev[2] = {nullptr, nullptr};  // around the steps of a tick
 
   const std::array<int, 3> &config_for(uint32_t W, bool real) {
@@ -545,26 +547,43 @@ tbtkkpm_table *exact_table(tbtkkpm_server *s, uint32_t M, double scale, int *rc)
 
 // Energy sums, error estimates and FP64 recomputations of the finished
 // requests (worker thread, no lock held; the requests are no longer
-// reachable by admission).
+// reachable by admission).  The device writes every request's LDOS and
+// error estimates into one results buffer, which comes back in one copy to
+// pinned memory and one synchronisation.
 int finish(tbtkkpm_server *s, const std::vector<Request *> &done,
            const std::vector<Model *> &owner) {
   if (done.empty()) return TBTKKPM_OK;
   cudaStream_t st = s->stream;
   const uint32_t E = s->E;
-  // stage layout per request: out [K][M] | raw [K][M] | raw_direct [K][M/2+1] | ldos [K][E]
-  size_t total = 0, lanes = 0, damp_len = 0;
-  for (Request *r : done) {
+  // moments stage per request: damped moments [K][M]; results per request:
+  // ldos [K][E] | err [K]
+  size_t total = 0, lanes = 0, damp_len = 0, nres = 0;
+  std::vector<size_t> res_off(done.size());
+  for (size_t i = 0; i < done.size(); i++) {
+    Request *r = done[i];
     const size_t K = r->sites.size(), M = r->M;
     r->stage_off = total;
-    total += sizeof(double2) * (2 * K * M + K * (M / 2 + 1)) + sizeof(double) * K * E;
+    total += sizeof(double2) * K * M;
     total = (total + 255) & ~(size_t)255;
+    res_off[i] = nres;
+    nres += K * E + K;
     lanes += K;
     damp_len += M;
   }
   int rc;
   if ((rc = s->d_stage.reserve(total)) || (rc = s->d_done.reserve(sizeof(MultiDone) * lanes)) ||
-      (rc = s->d_damp.reserve(sizeof(double) * damp_len)))
+      (rc = s->d_damp.reserve(sizeof(double) * damp_len)) || (rc = s->d_res.reserve(sizeof(double) * nres)))
     return rc;
+  cudaError_t e;
+  if (s->h_res_cap < nres) {
+    if (s->h_res) cudaFreeHost(s->h_res);
+    s->h_res = nullptr;
+    s->h_res_cap = 0;
+    const size_t cap = std::max(nres, (size_t)1 << 20);
+    if ((e = cudaMallocHost(&s->h_res, sizeof(double) * cap)) != cudaSuccess)
+      return cuda_fail(e, "server: pinned results");
+    s->h_res_cap = cap;
+  }
   std::vector<MultiDone> lane_ptr;
   std::vector<double> damp_all;
   std::vector<double> bvals;
@@ -581,7 +600,6 @@ int finish(tbtkkpm_server *s, const std::vector<Request *> &done,
     damp_all.insert(damp_all.end(), a.begin(), a.end());
     bvals.push_back(b);
   }
-  cudaError_t e;
   if ((e = cudaMemcpyAsync(s->d_done.ptr, lane_ptr.data(), sizeof(MultiDone) * lanes,
                            cudaMemcpyHostToDevice, st)) ||
       (e = cudaMemcpyAsync(s->d_damp.ptr, damp_all.data(), sizeof(double) * damp_len,
@@ -592,41 +610,28 @@ int finish(tbtkkpm_server *s, const std::vector<Request *> &done,
     Request *r = done[i];
     Model *m = owner[i];
     const uint32_t K = (uint32_t)r->sites.size(), M = r->M;
-    char *base = s->d_stage.as<char>() + r->stage_off;
-    double2 *out = reinterpret_cast<double2 *>(base);
-    double2 *raw = out + (size_t)K * M;
-    double2 *rawd = raw + (size_t)K * M;
-    double *ldos = reinterpret_cast<double *>(rawd + (size_t)K * (M / 2 + 1));
+    double2 *out = reinterpret_cast<double2 *>(s->d_stage.as<char>() + r->stage_off);
+    double *ldos = s->d_res.as<double>() + res_off[i];
     kpm_multi_prepare<<<blocks_for((uint64_t)K * M), 256, 0, st>>>(
         s->d_done.as<MultiDone>() + lane0, K, M, s->d_damp.as<double>() + d0, bvals[i],
-        r->broadening != 0, out, raw, rawd);
-    count_launches(1);
+        r->broadening != 0, out, nullptr, nullptr);
+    kpm_multi_error<<<K, kErrorBlock, 0, st>>>(s->d_done.as<MultiDone>() + lane0, M, ldos + (size_t)K * E);
+    count_launches(2);
     if ((rc = launch_energy_sum(st, m->table, out, K, 4, ldos, M))) return rc;
-    r->ldos.resize((size_t)K * E);
-    r->raw.resize((size_t)K * M);
-    r->raw_direct.resize((size_t)K * (M / 2 + 1));
-    if ((e = cudaMemcpyAsync(r->ldos.data(), ldos, sizeof(double) * K * E, cudaMemcpyDeviceToHost,
-                             st)) ||
-        (e = cudaMemcpyAsync(r->raw.data(), raw, sizeof(double2) * K * M, cudaMemcpyDeviceToHost,
-                             st)) ||
-        (e = cudaMemcpyAsync(r->raw_direct.data(), rawd, sizeof(double2) * K * (M / 2 + 1),
-                             cudaMemcpyDeviceToHost, st)))
-      return cuda_fail(e, "server: results");
     lane0 += K;
     d0 += M;
   }
-  if ((e = cudaStreamSynchronize(st))) return cuda_fail(e, "server: finish");
+  if ((e = cudaMemcpyAsync(s->h_res, s->d_res.ptr, sizeof(double) * nres, cudaMemcpyDeviceToHost, st)) ||
+      (e = cudaStreamSynchronize(st)))
+    return cuda_fail(e, "server: finish");
   for (size_t i = 0; i < done.size(); i++) {
     Request *r = done[i];
     Model *m = owner[i];
     const uint32_t K = (uint32_t)r->sites.size(), M = r->M;
-    r->err.assign(K, 0.0);
+    const double *res = s->h_res + res_off[i];
+    r->ldos.assign(res, res + (size_t)K * E);
+    r->err.assign(res + (size_t)K * E, res + (size_t)K * E + K);
     r->rerun.assign(K, 0);
-    doubling_error(r->raw, r->raw_direct, K, M, M / 2 + 1, r->err.data());
-    r->raw.clear();
-    r->raw.shrink_to_fit();
-    r->raw_direct.clear();
-    r->raw_direct.shrink_to_fit();
     std::vector<uint32_t> miss;
     std::vector<uint32_t> idx;
     for (uint32_t k = 0; k < K; k++)
@@ -696,6 +701,7 @@ void worker(tbtkkpm_server *s) {
       const double js = std::chrono::duration<double>(Clock::now() - j0).count();
       lk.lock();
       s->join_s += js;
+      s->plan_s -= js;  // plan_s counts the worker's own admission and planning
       for (size_t i = 0; !rc && i < refs.size(); i++) {
         refs[i].m->base_h[refs[i].c] -= (int32_t)head[i];
         refs[i].m->dirty = true;
@@ -735,12 +741,16 @@ void worker(tbtkkpm_server *s) {
       }
     }
     s->tick_no += 1;
+    const auto p1 = Clock::now();
+    s->plan_s += std::chrono::duration<double>(p1 - t0).count();
     lk.unlock();
     rc = run_tick(s, plans, nsteps);
     cudaError_t e = cudaSuccess;
     if (!rc && (e = cudaStreamSynchronize(s->stream)) != cudaSuccess)
       rc = cuda_fail(e, "server: tick");
+    const double ts = std::chrono::duration<double>(Clock::now() - p1).count();
     lk.lock();
+    s->tick_s += ts;
     if (rc) {
       fail_all(s, rc, tbtkkpm_last_error());
       break;
@@ -991,6 +1001,8 @@ extern "C" int tbtkkpm_server_stats(tbtkkpm_server *s, double *out, uint32_t n) 
   v[TBTKKPM_STAT_FINISH_S] = s->finish_s;
   v[TBTKKPM_STAT_RERUN_S] = s->rerun_s;
   v[TBTKKPM_STAT_JOIN_S] = s->join_s;
+  v[TBTKKPM_STAT_PLAN_S] = s->plan_s;
+  v[TBTKKPM_STAT_TICK_S] = s->tick_s;
   for (uint32_t i = 0; i < n && i < TBTKKPM_STAT_COUNT; i++) out[i] = v[i];
   return TBTKKPM_OK;
 }
@@ -1186,6 +1198,8 @@ extern "C" int tbtkkpm_server_destroy(tbtkkpm_server *s) {
                       &s->d_tiles})
       b->release();
     s->head_ws.release();
+    s->d_res.release();
+    if (s->h_res) cudaFreeHost(s->h_res);
     for (cudaEvent_t &ev : s->ev)
       if (ev) cudaEventDestroy(ev);
     cudaStreamDestroy(s->stream);

@@ -105,7 +105,7 @@ SIGNATURES = [
 PENDING = 1
 STAT_NAMES = ["completed", "p50_ms", "p99_ms", "mean_ms", "reruns", "ticks", "steps",
               "lane_steps", "resident_bytes", "evictions", "waited", "busy_s", "step_s",
-              "step_bytes", "finish_s", "rerun_s", "join_s"]
+              "step_bytes", "finish_s", "rerun_s", "join_s", "plan_s", "tick_s"]
 
 
 def step_configs(precision, ldos=True):
