@@ -83,9 +83,13 @@ struct Model {
   uint32_t busy = 0;
   uint32_t tcount = 0;
   bool dirty = true;
+  DevBuf lane_mem;  // one allocation; the lane buffers above are views into it
   void release_lanes() {
-    for (DevBuf *b : {&vec[0], &vec[1], &dots, &mu, &mu_direct, &base, &laneM, &bitmap, &tlist})
-      b->release();
+    for (DevBuf *b : {&vec[0], &vec[1], &dots, &mu, &mu_direct, &base, &laneM, &bitmap, &tlist}) {
+      b->ptr = nullptr;
+      b->cap = 0;
+    }
+    lane_mem.release();
     resident = false;
   }
 };
@@ -195,15 +199,24 @@ int make_resident(tbtkkpm_server *s, Model *m) {
   const size_t words = (N + 31) / 32;
   int rc;
   const size_t es = m->esize();
-  if ((rc = m->vec[0].reserve(es * (size_t)N * W)) ||
-      (rc = m->vec[1].reserve(es * (size_t)N * W)) ||
-      (rc = m->dots.reserve(2 * sizeof(long long) * W)) ||
-      (rc = m->mu.reserve(sizeof(double2) * (size_t)W * s->Mmax)) ||
-      (rc = m->mu_direct.reserve(sizeof(double2) * (size_t)W * s->ld)) ||
-      (rc = m->base.reserve(4 * (size_t)W)) || (rc = m->laneM.reserve(4 * (size_t)W)) ||
-      (rc = m->bitmap.reserve(4 * words)) || (rc = m->tlist.reserve(8 * (size_t)W))) {
+  // one allocation per model for the nine lane buffers
+  DevBuf *views[9] = {&m->vec[0], &m->vec[1], &m->dots, &m->mu, &m->mu_direct,
+                      &m->base, &m->laneM, &m->bitmap, &m->tlist};
+  const size_t sizes[9] = {es * (size_t)N * W, es * (size_t)N * W, 2 * sizeof(long long) * W,
+                           sizeof(double2) * (size_t)W * s->Mmax, sizeof(double2) * (size_t)W * s->ld,
+                           4 * (size_t)W, 4 * (size_t)W, 4 * words, 8 * (size_t)W};
+  size_t off[9], total = 0;
+  for (int i = 0; i < 9; i++) {
+    off[i] = total;
+    total += (sizes[i] + 255) & ~(size_t)255;
+  }
+  if ((rc = m->lane_mem.reserve(total))) {
     m->release_lanes();
     return rc;
+  }
+  for (int i = 0; i < 9; i++) {
+    views[i]->ptr = m->lane_mem.as<char>() + off[i];
+    views[i]->cap = sizes[i];
   }
   cudaError_t e;
   if ((e = cudaMemsetAsync(m->vec[0].ptr, 0, es * (size_t)N * W, s->stream)) ||
