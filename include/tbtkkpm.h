@@ -273,6 +273,51 @@ TBTKKPM_API int tbtkkpm_ldos_sites(
 	tbtkkpm_matrix *m, tbtkkpm_table *t, const uint32_t *sites, uint32_t B,
 	double broadening, int precision, double *ldos_out, double *err_out);
 
+/* ------------------------------------------------------------ other properties
+ *
+ * PropertyExtractor::ChebyshevExpander's spin-polarized LDOS, density,
+ * magnetization and expectation values
+ * (Lib/src/PropertyExtractor/ChebyshevExpander.cpp:297-327,584-720).  The
+ * reference computes one recursion per (to, from) pair; these run every
+ * pair of a call as targets of one batched recursion
+ * (tbtkkpm_moments_batched) and one NonPrincipal energy sum
+ * (tbtkkpm_greens), then form the property with the reference's expression
+ * and order.  Energies are the table's; occupation[e] is the equilibrium
+ * occupation at energy e (the reference's
+ * PropertyExtractor::getThermodynamicEquilibriumOccupation, from the
+ * model's statistics, temperature and chemical potential) and dE the window
+ * spacing (energyWindow[1] - energyWindow[0]).  A site with a spin subindex
+ * is given by its spin-up and spin-down basis rows.  precision as for
+ * tbtkkpm_moments_batched. */
+
+/* out [S][E][2][2] complex: entry (a, b) = -i G_NP(to = spin a, from = spin
+ * b)(E_e) / pi (calculateSP_LDOSCallback, :686-720). */
+TBTKKPM_API int tbtkkpm_spin_polarized_ldos(
+	tbtkkpm_matrix *m, tbtkkpm_table *t, const uint32_t *up,
+	const uint32_t *down, uint32_t S, double broadening, int precision,
+	double *out);
+
+/* out[s] = sum_e occupation[e] Im G_NP(s, s)(E_e) / pi dE
+ * (calculateDensityCallback, :584-616). */
+TBTKKPM_API int tbtkkpm_density(
+	tbtkkpm_matrix *m, tbtkkpm_table *t, const uint32_t *sites, uint32_t S,
+	double broadening, int precision, const double *occupation, double dE,
+	double *out);
+
+/* out [S][2][2] complex = sum_e occupation[e] (-i) G_NP(a, b)(E_e) / pi dE
+ * (calculateMAGCallback, :618-659). */
+TBTKKPM_API int tbtkkpm_magnetization(
+	tbtkkpm_matrix *m, tbtkkpm_table *t, const uint32_t *up,
+	const uint32_t *down, uint32_t S, double broadening, int precision,
+	const double *occupation, double dE, double *out);
+
+/* out [P] complex = -sum_e occupation[e] conj(i G_NP(to_p, from_p)(E_e)) dE
+ * / pi (calculateExpectationValue, :297-327). */
+TBTKKPM_API int tbtkkpm_expectation_values(
+	tbtkkpm_matrix *m, tbtkkpm_table *t, const uint32_t *to,
+	const uint32_t *from, uint32_t P, double broadening, int precision,
+	const double *occupation, double dE, double *out);
+
 /* ------------------------------------------------------------ LDOS server
  *
  * A device-resident LDOS service over many models (no reference

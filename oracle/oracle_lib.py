@@ -148,6 +148,14 @@ class Reference:
         lib.ref_greens_pe.restype = _i
         lib.ref_greens_pe.argtypes = [_p, _d, _i, _d, _d, _d, _i, _i, _i, _i,
                                       _i, _p, _p, _p]
+        lib.ref_property.restype = _i
+        lib.ref_property.argtypes = [_p, _d, _i, _d, _d, _d, _i, _i, _d, _d, _i,
+                                     _i, _p, _p]
+        lib.ref_expectation.restype = _i
+        lib.ref_expectation.argtypes = [_p, _d, _i, _d, _d, _d, _i, _i, _d, _d,
+                                        _i, _p, _p, _p]
+        lib.ref_fermi_dirac.restype = _d
+        lib.ref_fermi_dirac.argtypes = [_d, _d, _d]
 
     @staticmethod
     def available(path=REF_SO) -> bool:
@@ -159,6 +167,10 @@ class Reference:
     def range_value(self, lower, upper, res, incl_lo, incl_hi, k):
         return self.lib.ref_range_value(lower, upper, res, int(incl_lo),
                                         int(incl_hi), k)
+
+    def fermi_dirac(self, energies, mu, T):
+        """Functions::fermiDiracDistribution at each energy."""
+        return np.array([self.lib.ref_fermi_dirac(float(e), mu, T) for e in energies])
 
     def greens(self, scale, coeff, lower, upper, res, type_, use_table,
                incl_lo=True, incl_hi=True):
@@ -234,3 +246,98 @@ class RefModel:
                                    res, int(use_table), type_, to.shape[0],
                                    to.shape[1], _ptr(to), _ptr(frm), _ptr(out))
         return out
+
+    def prop(self, kind, scale, M, broadening, lower, upper, res, T, mu, index,
+             use_table=True):
+        """One site of calculateSpinPolarizedLDOS (kind 0, [res][2][2]
+        complex), calculateDensity (kind 1, scalar) or calculateMagnetization
+        (kind 2, [2][2] complex); -1 in `index` marks the spin subindex."""
+        idx = np.ascontiguousarray(np.asarray(index, dtype=np.int32))
+        n = {0: res * 8, 1: 1, 2: 8}[kind]
+        out = np.zeros(n, dtype=np.float64)
+        got = self.ref.lib.ref_property(self.h, scale, M, broadening, lower, upper,
+                                        res, int(use_table), T, mu, kind, idx.size,
+                                        _ptr(idx), _ptr(out))
+        assert got == (res if kind == 0 else 1), got
+        if kind == 1:
+            return out[0]
+        c = out.view(np.complex128)
+        return c.reshape(res, 2, 2) if kind == 0 else c.reshape(2, 2)
+
+    def expectation(self, scale, M, broadening, lower, upper, res, T, mu, to, frm,
+                    use_table=True):
+        """calculateExpectationValue(to, from)."""
+        to = np.ascontiguousarray(np.asarray(to, dtype=np.int32))
+        frm = np.ascontiguousarray(np.asarray(frm, dtype=np.int32))
+        out = np.zeros(2, dtype=np.float64)
+        self.ref.lib.ref_expectation(self.h, scale, M, broadening, lower, upper, res,
+                                     int(use_table), T, mu, to.size, _ptr(to), _ptr(frm),
+                                     _ptr(out))
+        return complex(out[0], out[1])
+
+
+# ---------------------------------------------------------------------------
+# The PropertyExtractor's other properties from NonPrincipal Green's
+# functions, restated with the reference's expressions and operation order
+# (Lib/src/PropertyExtractor/ChebyshevExpander.cpp:297-327,584-720): scalar
+# IEEE arithmetic as std::complex<double> evaluates it (products
+# (ac - bd, ad + bc), division and scaling by a real number per component),
+# sums over the energies in order.
+
+_PI = float(np.pi)
+
+
+def _cmul(a, b):
+    return complex(a.real * b.real - a.imag * b.imag, a.real * b.imag + a.imag * b.real)
+
+
+def _scale(z, x):
+    return complex(z.real * x, z.imag * x)
+
+
+def _div(z, x):
+    return complex(z.real / x, z.imag / x)
+
+
+def sp_ldos_from_greens(G4):
+    """G4 [4][E]: G_NP of (to spin n/2, from spin n%2).  Returns [E][2][2]:
+    data.at(n/2, n%2) += -i*G/M_PI (calculateSP_LDOSCallback, :686-720)."""
+    G4 = np.asarray(G4)
+    out = np.zeros((G4.shape[1], 2, 2), dtype=np.complex128)
+    mi = complex(-0.0, -1.0)
+    for n in range(4):
+        for e in range(G4.shape[1]):
+            v = _div(_cmul(mi, complex(G4[n, e])), _PI)
+            out[e, n // 2, n % 2] = complex(0.0 + v.real, 0.0 + v.imag)
+    return out
+
+
+def density_from_greens(G, occupation, dE):
+    """data += weight*imag(G)/M_PI*dE over the energies (:584-616)."""
+    d = 0.0
+    for e in range(len(G)):
+        d += occupation[e] * complex(G[e]).imag / _PI * dE
+    return d
+
+
+def magnetization_from_greens(G4, occupation, dE):
+    """data.at(n/2, n%2) += weight*(-i)*G/M_PI*dE (:618-659)."""
+    out = np.zeros((2, 2), dtype=np.complex128)
+    mi = complex(-0.0, -1.0)
+    for n in range(4):
+        v = complex(0.0, 0.0)
+        for e in range(G4.shape[1]):
+            t = _scale(_div(_cmul(_scale(mi, occupation[e]), complex(G4[n, e])), _PI), dE)
+            v = complex(v.real + t.real, v.imag + t.imag)
+        out[n // 2, n % 2] = v
+    return out
+
+
+def expectation_from_greens(G, occupation, dE):
+    """expectationValue -= weight*conj(i*G)*dE/M_PI (:297-327)."""
+    v = complex(0.0, 0.0)
+    for e in range(len(G)):
+        ig = _cmul(complex(0.0, 1.0), complex(G[e]))
+        t = _div(_scale(_scale(ig.conjugate(), occupation[e]), dE), _PI)
+        v = complex(v.real - t.real, v.imag - t.imag)
+    return v

@@ -9,12 +9,16 @@
  *   HoppingAmplitudeSet::getSparseMatrix Lib/include/Core/TBTK/HoppingAmplitudeSet.h:397-424
  *   Solver::ChebyshevExpander           Lib/src/Solver/ChebyshevExpander.cpp:103-435
  *   PropertyExtractor::calculateLDOS    Lib/src/PropertyExtractor/ChebyshevExpander.cpp:475-505
+ *   spin-polarized LDOS, density, magnetization, expectation values
+ *                                       Lib/src/PropertyExtractor/ChebyshevExpander.cpp:297-720
  */
+#include "TBTK/Functions.h"
 #include "TBTK/Model.h"
 #include "TBTK/PropertyExtractor/ChebyshevExpander.h"
 #include "TBTK/Range.h"
 #include "TBTK/Solver/ChebyshevExpander.h"
 #include "TBTK/Streams.h"
+#include "TBTK/TBTK.h"
 
 #include <complex>
 #include <cstdint>
@@ -44,6 +48,8 @@ Solver::ChebyshevExpander::Type to_type(int type){
 struct Quiet{
 	Quiet(){
 		Communicator::setGlobalVerbose(false);
+		//Units and constants (the occupation functions need k_B).
+		TBTK::Initialize();
 	}
 } quiet;
 
@@ -249,6 +255,93 @@ int ref_greens_pe(
 		}
 	}
 	return 0;
+}
+
+
+/* One site of PropertyExtractor::ChebyshevExpander's other properties,
+ * with the model at temperature T and chemical potential mu and the
+ * PropertyExtractor's inclusive window Range(lower, upper, res).  The site
+ * is `index` (idx_len entries); an entry -1 marks the spin subindex
+ * (IDX_SPIN).  kind 0: calculateSpinPolarizedLDOS, out [res][2][2][2]
+ * (complex (a, b) entries); kind 1: calculateDensity, out [1]; kind 2:
+ * calculateMagnetization, out [2][2][2]. */
+int ref_property(
+	void *model, double scale, int M, double broadening, double lower,
+	double upper, int res, int use_table, double T, double mu, int kind,
+	int idx_len, const int *index, double *out
+){
+	Model &mdl = *(Model*)model;
+	mdl.setTemperature(T);
+	mdl.setChemicalPotential(mu);
+	Solver::ChebyshevExpander solver;
+	solver.setVerbose(false);
+	solver.setModel(mdl);
+	solver.setScaleFactor(scale);
+	solver.setNumCoefficients(M);
+	solver.setBroadening(broadening);
+	solver.setUseLookupTable(use_table != 0);
+	PropertyExtractor::ChebyshevExpander pe(solver);
+	pe.setEnergyWindow(lower, upper, res);
+	Index pattern;
+	for(int k = 0; k < idx_len; k++)
+		pattern.pushBack(index[k] == -1 ? (int)IDX_SPIN : index[k]);
+	auto put = [&](const SpinMatrix &s, double *o){
+		for(int a = 0; a < 2; a++){
+			for(int b = 0; b < 2; b++){
+				o[2*(2*a + b)] = s.at(a, b).real();
+				o[2*(2*a + b) + 1] = s.at(a, b).imag();
+			}
+		}
+	};
+	if(kind == 0){
+		Property::SpinPolarizedLDOS p
+			= pe.calculateSpinPolarizedLDOS({pattern});
+		const std::vector<SpinMatrix> &d = p.getData();
+		for(int e = 0; e < res && e < (int)d.size(); e++)
+			put(d[e], out + 8*(int64_t)e);
+		return (int)d.size();
+	}
+	if(kind == 1){
+		Property::Density p = pe.calculateDensity({pattern});
+		out[0] = p.getData()[0];
+		return (int)p.getData().size();
+	}
+	Property::Magnetization p = pe.calculateMagnetization({pattern});
+	put(p.getData()[0], out);
+	return (int)p.getData().size();
+}
+
+/* PropertyExtractor::ChebyshevExpander::calculateExpectationValue(to, from)
+ * at temperature T and chemical potential mu; out [2]. */
+int ref_expectation(
+	void *model, double scale, int M, double broadening, double lower,
+	double upper, int res, int use_table, double T, double mu, int idx_len,
+	const int *to, const int *from, double *out
+){
+	Model &mdl = *(Model*)model;
+	mdl.setTemperature(T);
+	mdl.setChemicalPotential(mu);
+	Solver::ChebyshevExpander solver;
+	solver.setVerbose(false);
+	solver.setModel(mdl);
+	solver.setScaleFactor(scale);
+	solver.setNumCoefficients(M);
+	solver.setBroadening(broadening);
+	solver.setUseLookupTable(use_table != 0);
+	PropertyExtractor::ChebyshevExpander pe(solver);
+	pe.setEnergyWindow(lower, upper, res);
+	cplx v = pe.calculateExpectationValue(
+		make_index(to, idx_len), make_index(from, idx_len)
+	);
+	out[0] = v.real();
+	out[1] = v.imag();
+	return 0;
+}
+
+/* Functions::fermiDiracDistribution(energy, mu, T), the occupation the
+ * properties above weight with (PropertyExtractor.h:910-935). */
+double ref_fermi_dirac(double energy, double mu, double T){
+	return Functions::fermiDiracDistribution(energy, mu, T);
 }
 
 }

@@ -90,6 +90,10 @@ SIGNATURES = [
     ("tbtkkpm_matrix_step_configs", _i, [_p, _i, _i, _p, _i]),
     ("tbtkkpm_matrix_set_fp64_head", _i, [_p, _u32]),
     ("tbtkkpm_matrix_fp64_head", _i, [_p, _p, _p]),
+    ("tbtkkpm_spin_polarized_ldos", _i, [_p, _p, _p, _p, _u32, _d, _i, _p]),
+    ("tbtkkpm_density", _i, [_p, _p, _p, _u32, _d, _i, _p, _d, _p]),
+    ("tbtkkpm_magnetization", _i, [_p, _p, _p, _p, _u32, _d, _i, _p, _d, _p]),
+    ("tbtkkpm_expectation_values", _i, [_p, _p, _p, _p, _u32, _d, _i, _p, _d, _p]),
     ("tbtkkpm_server_create", _i, [_u32, _p, _u32, _u64, _u32, _d, _p]),
     ("tbtkkpm_server_add_model", _i, [_p, _p, _p, _p, _u32, _d, _u32, _p]),
     ("tbtkkpm_server_submit", _i, [_p, _u32, _p, _u32, _u32, _d, _p]),
@@ -341,6 +345,56 @@ class Matrix:
                                                  sites.size, float(broadening),
                                                  int(precision), _ptr(out), _ptr(err)))
         return out, err
+
+    def spin_polarized_ldos(self, table, up, down, broadening, precision=FP64):
+        """[S][E][2][2] complex: -i G_NP(spin a, spin b) / pi per site
+        (PropertyExtractor::ChebyshevExpander::calculateSpinPolarizedLDOS)."""
+        up, down = _u32a(up), _u32a(down)
+        if up.size != down.size:
+            raise ValueError("up and down need one row per site")
+        out = np.zeros((up.size, table.E, 2, 2), dtype=np.complex128)
+        _check(load_library().tbtkkpm_spin_polarized_ldos(
+            self._h, table._h, _ptr(up), _ptr(down), up.size, float(broadening),
+            int(precision), _ptr(out)))
+        return out
+
+    def density(self, table, sites, broadening, occupation, dE, precision=FP64):
+        """[S]: sum_e occupation[e] Im G_NP / pi dE (calculateDensity)."""
+        sites = _u32a(sites)
+        occ = np.ascontiguousarray(occupation, dtype=np.float64)
+        if occ.size != table.E:
+            raise ValueError("occupation needs one value per table energy")
+        out = np.zeros(sites.size, dtype=np.float64)
+        _check(load_library().tbtkkpm_density(
+            self._h, table._h, _ptr(sites), sites.size, float(broadening), int(precision),
+            _ptr(occ), float(dE), _ptr(out)))
+        return out
+
+    def magnetization(self, table, up, down, broadening, occupation, dE, precision=FP64):
+        """[S][2][2] complex: sum_e occupation[e] (-i) G_NP(a, b) / pi dE
+        (calculateMagnetization)."""
+        up, down = _u32a(up), _u32a(down)
+        occ = np.ascontiguousarray(occupation, dtype=np.float64)
+        if up.size != down.size or occ.size != table.E:
+            raise ValueError("one up and one down row per site, one occupation per energy")
+        out = np.zeros((up.size, 2, 2), dtype=np.complex128)
+        _check(load_library().tbtkkpm_magnetization(
+            self._h, table._h, _ptr(up), _ptr(down), up.size, float(broadening),
+            int(precision), _ptr(occ), float(dE), _ptr(out)))
+        return out
+
+    def expectation_values(self, table, to, frm, broadening, occupation, dE,
+                           precision=FP64):
+        """[P] complex <c_to^dagger c_from> (calculateExpectationValue)."""
+        to, frm = _u32a(to), _u32a(frm)
+        occ = np.ascontiguousarray(occupation, dtype=np.float64)
+        if to.size != frm.size or occ.size != table.E:
+            raise ValueError("one from per to, one occupation per energy")
+        out = np.zeros(to.size, dtype=np.complex128)
+        _check(load_library().tbtkkpm_expectation_values(
+            self._h, table._h, _ptr(to), _ptr(frm), to.size, float(broadening),
+            int(precision), _ptr(occ), float(dE), _ptr(out)))
+        return out
 
     def close(self):
         if getattr(self, "_h", None):

@@ -20,6 +20,7 @@
 #include "TBTK/Range.h"
 #include "TBTK/Solver/ChebyshevExpander.h"
 #include "TBTK/Streams.h"
+#include "TBTK/TBTK.h"
 
 #include <cmath>
 #include <complex>
@@ -190,6 +191,84 @@ void testLDOS(Model &model){
 		+ std::to_string(d));
 }
 
+// Bitwise equality of two lists of 2x2 spin matrices; d receives the
+// largest entry difference.
+bool sameSpinMatrices(
+	const std::vector<SpinMatrix> &a, const std::vector<SpinMatrix> &b,
+	double &d
+){
+	d = a.size() == b.size() ? 0 : INFINITY;
+	bool ok = a.size() == b.size();
+	for(size_t n = 0; n < a.size() && n < b.size(); n++){
+		for(unsigned int r = 0; r < 2; r++){
+			for(unsigned int c = 0; c < 2; c++){
+				const cplx x = a[n].at(r, c), y = b[n].at(r, c);
+				d = std::fmax(d, std::abs(x - y));
+				ok = ok && std::memcmp(&x, &y, sizeof(cplx)) == 0;
+			}
+		}
+	}
+	return ok;
+}
+
+// TBTK's other ChebyshevExpander properties (spin-polarized LDOS, density,
+// magnetization, expectation values; PropertyExtractor/ChebyshevExpander.cpp
+// :297-327,584-720) call calculateCoefficients and generateGreensFunction
+// once per (to, from) pair, so on the seam their recursions and energy sums
+// run on the device; they must match the CPU path bit for bit.
+void testProperties(Model &model){
+	model.setTemperature(300);
+	model.setChemicalPotential(0.1);
+	Solver::ChebyshevExpander cpu, gpu;
+	configure(cpu, model, 256, false);
+	configure(gpu, model, 256, true);
+	PropertyExtractor::ChebyshevExpander peCPU(cpu), peGPU(gpu);
+	peCPU.setEnergyWindow(-4, 4, 301);
+	peGPU.setEnergyWindow(-4, 4, 301);
+
+	std::vector<Index> spinPatterns = {{2, 3, IDX_SPIN}, {0, 5, IDX_SPIN}};
+	Property::SpinPolarizedLDOS sa
+		= peCPU.calculateSpinPolarizedLDOS(spinPatterns);
+	Property::SpinPolarizedLDOS sb
+		= peGPU.calculateSpinPolarizedLDOS(spinPatterns);
+	double d;
+	bool ok = sameSpinMatrices(sa.getData(), sb.getData(), d)
+		&& sb.getData().size() == 2*301;
+	report("spin_polarized_ldos", ok,
+		"values=" + std::to_string(sb.getData().size()) + " max|diff|="
+		+ std::to_string(d));
+
+	std::vector<Index> densityPatterns = {{IDX_ALL, 2, IDX_ALL}};
+	Property::Density da = peCPU.calculateDensity(densityPatterns);
+	Property::Density db = peGPU.calculateDensity(densityPatterns);
+	const std::vector<double> &xa = da.getData(), &xb = db.getData();
+	d = xa.size() == xb.size() ? 0 : INFINITY;
+	for(size_t n = 0; n < xa.size() && n < xb.size(); n++)
+		d = std::fmax(d, std::fabs(xa[n] - xb[n]));
+	ok = xa.size() == xb.size() && xa.size() == 12
+		&& std::memcmp(xa.data(), xb.data(), xa.size()*sizeof(double))
+			== 0;
+	report("density", ok,
+		"values=" + std::to_string(xb.size()) + " max|diff|="
+		+ std::to_string(d));
+
+	std::vector<Index> magPatterns = {{1, 1, IDX_SPIN}, {4, 2, IDX_SPIN}};
+	Property::Magnetization ma = peCPU.calculateMagnetization(magPatterns);
+	Property::Magnetization mb = peGPU.calculateMagnetization(magPatterns);
+	ok = sameSpinMatrices(ma.getData(), mb.getData(), d)
+		&& mb.getData().size() == 2;
+	report("magnetization", ok, "max|diff|=" + std::to_string(d));
+
+	const cplx ea = peCPU.calculateExpectationValue({2, 3, 0}, {2, 3, 1});
+	const cplx eb = peGPU.calculateExpectationValue({2, 3, 0}, {2, 3, 1});
+	const cplx fa = peCPU.calculateExpectationValue({4, 4, 1}, {4, 4, 1});
+	const cplx fb = peGPU.calculateExpectationValue({4, 4, 1}, {4, 4, 1});
+	ok = std::memcmp(&ea, &eb, sizeof(cplx)) == 0
+		&& std::memcmp(&fa, &fb, sizeof(cplx)) == 0 && fa.real() != 0;
+	report("expectation_value", ok,
+		"|diff|=" + std::to_string(std::abs(ea - eb) + std::abs(fa - fb)));
+}
+
 int exitShort(){
 	Model model;
 	model.setVerbose(false);
@@ -206,6 +285,9 @@ int exitShort(){
 
 int main(int argc, char **argv){
 	Communicator::setGlobalVerbose(false);
+	//Units and constants (the occupation of density and magnetization
+	//needs k_B), as a TBTK application starts.
+	TBTK::Initialize();
 	if(argc > 1 && std::strcmp(argv[1], "exit-short") == 0)
 		return exitShort();
 
@@ -217,6 +299,7 @@ int main(int argc, char **argv){
 	testCoefficients(model);
 	testGreens(model);
 	testLDOS(model);
+	testProperties(model);
 
 	std::printf("%d failure(s)\n", failures);
 	return failures == 0 ? 0 : 1;

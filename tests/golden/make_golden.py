@@ -119,6 +119,36 @@ def main():
             g[f"cplx_{ty}_{tab}"] = ref.greens(10.0, cc, -9.5, 9.5, 37, ty, tab, False, True)
     cases["greens"] = g
 
+    # The PropertyExtractor's other properties (spin-polarized LDOS, density,
+    # magnetization, expectation values) on a disordered Rashba lattice at
+    # T = 300 and chemical potential 0.1, with the inclusive window
+    # Range(-3.9, 3.9, 120); one reference call per site.
+    lat = L.square(6, 5, t=1.0, J=0.5, W=2.0, alpha=0.3, periodic=True, seed=11)
+    m = ref.model(lat)
+    rowptr, col, val = m.csr()
+    s, M, bro, lo, hi, res, T, mu = 8.0, 256, 1e-3, -3.9, 3.9, 120, 300.0, 0.1
+    energies = np.array([ref.range_value(lo, hi, res, True, True, k) for k in range(res)])
+    sp_sites = [(2, 3), (0, 4), (5, 1)]
+    dens_sites = [(2, 3, 0), (2, 3, 1), (4, 0, 1)]
+    pairs = [((2, 3, 0), (2, 3, 1)), ((4, 4, 1), (4, 4, 1)), ((1, 2, 0), (2, 2, 1))]
+    cases["props"] = dict(
+        rowptr=rowptr, col=col, val=val, scale=s, M=M, broadening=bro,
+        window=np.array([lo, hi, res]), energies=energies, dE=energies[1] - energies[0],
+        T=T, mu=mu, occupation=ref.fermi_dirac(energies, mu, T),
+        sp_up=np.array([lat.basis((x, y, 0)) for x, y in sp_sites], dtype=np.uint32),
+        sp_down=np.array([lat.basis((x, y, 1)) for x, y in sp_sites], dtype=np.uint32),
+        sp_ldos=np.array([m.prop(0, s, M, bro, lo, hi, res, T, mu, [x, y, -1])
+                          for x, y in sp_sites]),
+        magnetization=np.array([m.prop(2, s, M, bro, lo, hi, res, T, mu, [x, y, -1])
+                                for x, y in sp_sites]),
+        density_sites=np.array([lat.basis(d) for d in dens_sites], dtype=np.uint32),
+        density=np.array([m.prop(1, s, M, bro, lo, hi, res, T, mu, list(d))
+                          for d in dens_sites]),
+        exp_to=np.array([lat.basis(a) for a, _ in pairs], dtype=np.uint32),
+        exp_from=np.array([lat.basis(b) for _, b in pairs], dtype=np.uint32),
+        expectation=np.array([m.expectation(s, M, bro, lo, hi, res, T, mu, list(a), list(b))
+                              for a, b in pairs]))
+
     for name, arrays in cases.items():
         np.savez_compressed(HERE / f"{name}.npz", **arrays)
         print(name, sum(np.asarray(v).nbytes for v in arrays.values()), "bytes")

@@ -156,3 +156,35 @@ def test_basis_order_matches_reference(reference):
     assert m.basis_size() == lat.num_states
     for idx in [(0, 0, 0, 0), (2, 3, 1, 1), (1, 2, 0, 1)]:
         assert m.basis_index(idx) == lat.basis(idx)
+
+
+def _props_greens(oracle, g, pairs):
+    """Damped NonPrincipal G of (to, from) basis pairs on the golden window."""
+    M, s = int(g["M"]), float(g["scale"])
+    table = oracle.lookup_table(M, g["energies"], s)
+    out = []
+    for to, frm in pairs:
+        mu = oracle.damp(oracle.moments(g["rowptr"], g["col"], g["val"], s, M, int(frm), [int(to)]),
+                         float(g["broadening"]))
+        out.append(oracle.greens_table(table, 3, mu[0]))
+    return np.array(out)
+
+
+def test_properties_restatement_matches_reference(oracle):
+    """Spin-polarized LDOS, density, magnetization and expectation values from
+    the oracle's moments and Green's functions, formed as the reference's
+    PropertyExtractor forms them, equal TBTK's own results bit for bit."""
+    from oracle_lib import (density_from_greens, expectation_from_greens,
+                            magnetization_from_greens, sp_ldos_from_greens)
+    g = golden("props")
+    occ, dE = g["occupation"], float(g["dE"])
+    for k, (u, d) in enumerate(zip(g["sp_up"], g["sp_down"])):
+        G4 = _props_greens(oracle, g, [(u, u), (u, d), (d, u), (d, d)])
+        assert np.array_equal(sp_ldos_from_greens(G4), g["sp_ldos"][k])
+        assert np.array_equal(magnetization_from_greens(G4, occ, dE), g["magnetization"][k])
+    for k, site in enumerate(g["density_sites"]):
+        G = _props_greens(oracle, g, [(site, site)])[0]
+        assert density_from_greens(G, occ, dE) == g["density"][k]
+    for k, (to, frm) in enumerate(zip(g["exp_to"], g["exp_from"])):
+        G = _props_greens(oracle, g, [(to, frm)])[0]
+        assert expectation_from_greens(G, occ, dE) == g["expectation"][k]

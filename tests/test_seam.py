@@ -56,7 +56,8 @@ def test_seam_matches_tbtk_cpu_path():
         "device_table", "coefficients_many_to", "coefficients_single",
         "greens_advanced", "greens_retarded", "greens_principal",
         "greens_nonprincipal", "greens_after_table_reload",
-        "ldos_property_extractor"}
+        "ldos_property_extractor", "spin_polarized_ldos", "density",
+        "magnetization", "expectation_value"}
     assert all(l.startswith("[PASS]") for l in lines), r.stdout
 
 
