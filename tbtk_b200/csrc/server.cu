@@ -558,27 +558,35 @@ tbtkkpm_table *exact_table(tbtkkpm_server *s, uint32_t M, double scale, int *rc)
   return t;
 }
 
-// Energy sums, error estimates and FP64 recomputations of the finished
-// requests (worker thread, no lock held; the requests are no longer
-// reachable by admission).  The device writes every request's LDOS and
-// error estimates into one results buffer, which comes back in one copy to
-// pinned memory and one synchronisation.
-int finish(tbtkkpm_server *s, const std::vector<Request *> &done,
-           const std::vector<Model *> &owner) {
-  if (done.empty()) return TBTKKPM_OK;
+// The finish phase of the requests that completed in one tick, in two
+// halves: finish_launch enqueues their damping, energy sums and error
+// estimates and the copy of all results into pinned memory on the server's
+// stream (before any later join can reuse their lanes); finish_complete
+// waits for that copy, fills the requests and runs the FP64 recomputations
+// of the sites past the tolerance.  The worker runs the second half while
+// the next tick's steps are on the device.
+struct FinishBatch {
+  std::vector<Request *> done;
+  std::vector<Model *> owner;
+  std::vector<size_t> res_off;  // offset of each request's results in h_res
+  cudaEvent_t ev = nullptr;     // after the results copy
+};
+
+int finish_launch(tbtkkpm_server *s, FinishBatch &fb) {
+  if (fb.done.empty()) return TBTKKPM_OK;
   cudaStream_t st = s->stream;
   const uint32_t E = s->E;
   // moments stage per request: damped moments [K][M]; results per request:
   // ldos [K][E] | err [K]
   size_t total = 0, lanes = 0, damp_len = 0, nres = 0;
-  std::vector<size_t> res_off(done.size());
-  for (size_t i = 0; i < done.size(); i++) {
-    Request *r = done[i];
+  fb.res_off.resize(fb.done.size());
+  for (size_t i = 0; i < fb.done.size(); i++) {
+    Request *r = fb.done[i];
     const size_t K = r->sites.size(), M = r->M;
     r->stage_off = total;
     total += sizeof(double2) * K * M;
     total = (total + 255) & ~(size_t)255;
-    res_off[i] = nres;
+    fb.res_off[i] = nres;
     nres += K * E + K;
     lanes += K;
     damp_len += M;
@@ -592,7 +600,7 @@ int finish(tbtkkpm_server *s, const std::vector<Request *> &done,
     if (s->h_res) cudaFreeHost(s->h_res);
     s->h_res = nullptr;
     s->h_res_cap = 0;
-    const size_t cap = std::max(nres, (size_t)1 << 20);
+    const size_t cap = std::max(nres + nres / 2, (size_t)1 << 20);
     if ((e = cudaMallocHost(&s->h_res, sizeof(double) * cap)) != cudaSuccess)
       return cuda_fail(e, "server: pinned results");
     s->h_res_cap = cap;
@@ -600,9 +608,9 @@ int finish(tbtkkpm_server *s, const std::vector<Request *> &done,
   std::vector<MultiDone> lane_ptr;
   std::vector<double> damp_all;
   std::vector<double> bvals;
-  for (size_t i = 0; i < done.size(); i++) {
-    Request *r = done[i];
-    Model *m = owner[i];
+  for (size_t i = 0; i < fb.done.size(); i++) {
+    Request *r = fb.done[i];
+    Model *m = fb.owner[i];
     for (uint32_t c : r->lanes)
       lane_ptr.push_back({m->mu.as<double2>() + (size_t)c * s->Mmax,
                           m->mu_direct.as<double2>() + (size_t)c * s->ld});
@@ -619,12 +627,12 @@ int finish(tbtkkpm_server *s, const std::vector<Request *> &done,
                            cudaMemcpyHostToDevice, st)))
     return cuda_fail(e, "server: finish staging");
   size_t lane0 = 0, d0 = 0;
-  for (size_t i = 0; i < done.size(); i++) {
-    Request *r = done[i];
-    Model *m = owner[i];
+  for (size_t i = 0; i < fb.done.size(); i++) {
+    Request *r = fb.done[i];
+    Model *m = fb.owner[i];
     const uint32_t K = (uint32_t)r->sites.size(), M = r->M;
     double2 *out = reinterpret_cast<double2 *>(s->d_stage.as<char>() + r->stage_off);
-    double *ldos = s->d_res.as<double>() + res_off[i];
+    double *ldos = s->d_res.as<double>() + fb.res_off[i];
     kpm_multi_prepare<<<blocks_for((uint64_t)K * M), 256, 0, st>>>(
         s->d_done.as<MultiDone>() + lane0, K, M, s->d_damp.as<double>() + d0, bvals[i],
         r->broadening != 0, out, nullptr, nullptr);
@@ -634,14 +642,25 @@ int finish(tbtkkpm_server *s, const std::vector<Request *> &done,
     lane0 += K;
     d0 += M;
   }
+  if (!fb.ev && (e = cudaEventCreateWithFlags(&fb.ev, cudaEventDisableTiming)) != cudaSuccess)
+    return cuda_fail(e, "server: finish event");
   if ((e = cudaMemcpyAsync(s->h_res, s->d_res.ptr, sizeof(double) * nres, cudaMemcpyDeviceToHost, st)) ||
-      (e = cudaStreamSynchronize(st)))
+      (e = cudaEventRecord(fb.ev, st)))
     return cuda_fail(e, "server: finish");
-  for (size_t i = 0; i < done.size(); i++) {
-    Request *r = done[i];
-    Model *m = owner[i];
+  return TBTKKPM_OK;
+}
+
+int finish_complete(tbtkkpm_server *s, FinishBatch &fb) {
+  if (fb.done.empty()) return TBTKKPM_OK;
+  cudaError_t e = cudaEventSynchronize(fb.ev);
+  if (e != cudaSuccess) return cuda_fail(e, "server: finish");
+  const uint32_t E = s->E;
+  int rc;
+  for (size_t i = 0; i < fb.done.size(); i++) {
+    Request *r = fb.done[i];
+    Model *m = fb.owner[i];
     const uint32_t K = (uint32_t)r->sites.size(), M = r->M;
-    const double *res = s->h_res + res_off[i];
+    const double *res = s->h_res + fb.res_off[i];
     r->ldos.assign(res, res + (size_t)K * E);
     r->err.assign(res + (size_t)K * E, res + (size_t)K * E + K);
     r->rerun.assign(K, 0);
@@ -692,10 +711,38 @@ void worker(tbtkkpm_server *s) {
   cudaSetDevice(s->device);
   swap_selected_device(s->device);
   std::unique_lock<std::mutex> lk(s->mu);
+  FinishBatch prev;  // launched, host half pending
+  // Host half of the pending finish (lock held on entry and exit): the
+  // requests complete and their waiters wake.
+  auto complete_prev = [&]() -> int {
+    if (prev.done.empty()) return TBTKKPM_OK;
+    lk.unlock();
+    const auto f0 = Clock::now();
+    int rc = finish_complete(s, prev);
+    const auto f1 = Clock::now();
+    lk.lock();
+    s->finish_s += std::chrono::duration<double>(f1 - f0).count();
+    if (rc) return rc;
+    for (Request *r : prev.done) {
+      s->latencies_ms.push_back(std::chrono::duration<double, std::milli>(f1 - r->t_submit).count());
+      r->done = true;
+    }
+    prev.done.clear();
+    prev.owner.clear();
+    s->cv_done.notify_all();
+    return TBTKKPM_OK;
+  };
+  int rc = TBTKKPM_OK;
   while (!s->stop) {
     bool busy = false;
     for (auto &p : s->models) busy = busy || (p->resident && p->busy);
     if (!busy && s->pending.empty()) {
+      if (!prev.done.empty()) {
+        if ((rc = complete_prev())) break;
+        s->working = false;
+        continue;
+      }
+      s->working = false;
       s->cv_work.wait(lk);
       continue;
     }
@@ -703,7 +750,7 @@ void worker(tbtkkpm_server *s) {
     s->working = true;
     std::vector<MultiJoin> joins;
     std::vector<JoinRef> refs;
-    int rc = admit(s, joins, refs);
+    rc = admit(s, joins, refs);
     if (!rc && !joins.empty()) {
       // FP64 heads: a lane with head q starts at local step q + 1, and a
       // request ends with its last lane
@@ -729,17 +776,15 @@ void worker(tbtkkpm_server *s) {
     }
     std::vector<ClassPlan> plans;
     if (!rc) rc = plan_tick(s, plans);
-    if (rc) {
-      fail_all(s, rc, tbtkkpm_last_error());
-      break;
-    }
+    if (rc) break;
     if (plans.empty()) {
       // queued work that cannot start yet (it waits for memory)
+      if ((rc = complete_prev())) break;
       s->working = false;
       s->cv_work.wait_for(lk, std::chrono::milliseconds(5));
       continue;
     }
-    // steps until the first busy lane finishes, at most tick_steps
+    // steps until the first busy request finishes, at most tick_steps
     uint32_t nsteps = s->tick_steps;
     for (auto &p : s->models) {
       Model *m = p.get();
@@ -758,16 +803,19 @@ void worker(tbtkkpm_server *s) {
     s->plan_s += std::chrono::duration<double>(p1 - t0).count();
     lk.unlock();
     rc = run_tick(s, plans, nsteps);
+    lk.lock();
+    // the previous tick's requests complete while this tick runs
+    const double f_before = s->finish_s;
+    if (!rc) rc = complete_prev();
+    const double overlap = s->finish_s - f_before;
+    lk.unlock();
     cudaError_t e = cudaSuccess;
     if (!rc && (e = cudaStreamSynchronize(s->stream)) != cudaSuccess)
       rc = cuda_fail(e, "server: tick");
-    const double ts = std::chrono::duration<double>(Clock::now() - p1).count();
+    const double ts = std::chrono::duration<double>(Clock::now() - p1).count() - overlap;
     lk.lock();
     s->tick_s += ts;
-    if (rc) {
-      fail_all(s, rc, tbtkkpm_last_error());
-      break;
-    }
+    if (rc) break;
     s->n_global += (int32_t)nsteps;
     s->ticks += 1;
     s->steps += nsteps;
@@ -776,8 +824,6 @@ void worker(tbtkkpm_server *s) {
     cudaGetLastError();
     for (const ClassPlan &cp : plans) s->step_bytes += cp.bytes * nsteps;
     // finished requests: every lane past its last local step
-    std::vector<Request *> done;
-    std::vector<Model *> owner;
     for (auto &p : s->models) {
       Model *m = p.get();
       if (!m->resident || !m->busy) continue;
@@ -787,26 +833,22 @@ void worker(tbtkkpm_server *s) {
         Request *r = s->requests.at(id).get();
         if (r->lanes.empty() || r->lanes[0] != c) continue;  // one entry per request
         if ((int64_t)r->base + r->M / 2 <= (int64_t)s->n_global - 1) {
-          done.push_back(r);
-          owner.push_back(m);
+          prev.done.push_back(r);
+          prev.owner.push_back(m);
         }
       }
     }
+    // their device half goes on the stream before any join can reuse the lanes
     lk.unlock();
     const auto f0 = Clock::now();
-    rc = finish(s, done, owner);
+    rc = finish_launch(s, prev);
     const double fs = std::chrono::duration<double>(Clock::now() - f0).count();
     lk.lock();
     s->finish_s += fs;
-    if (rc) {
-      fail_all(s, rc, tbtkkpm_last_error());
-      break;
-    }
-    const auto t1 = Clock::now();
-    s->busy_s += std::chrono::duration<double>(t1 - t0).count();
-    for (size_t i = 0; i < done.size(); i++) {
-      Request *r = done[i];
-      Model *m = owner[i];
+    if (rc) break;
+    for (size_t i = 0; i < prev.done.size(); i++) {
+      Request *r = prev.done[i];
+      Model *m = prev.owner[i];
       for (uint32_t c : r->lanes) {
         m->lane_req[c] = 0;
         m->base_h[c] = kLaneIdle;
@@ -815,12 +857,11 @@ void worker(tbtkkpm_server *s) {
       m->busy -= (uint32_t)r->lanes.size();
       m->dirty = true;
       s->lane_steps += (double)r->lanes.size() * (r->M / 2);
-      s->latencies_ms.push_back(std::chrono::duration<double, std::milli>(t1 - r->t_submit).count());
-      r->done = true;
     }
-    s->working = false;
-    if (!done.empty()) s->cv_done.notify_all();
+    s->busy_s += std::chrono::duration<double>(Clock::now() - t0).count();
   }
+  if (rc) fail_all(s, rc, tbtkkpm_last_error());
+  if (prev.ev) cudaEventDestroy(prev.ev);
   s->working = false;
 }
 
