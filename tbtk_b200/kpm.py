@@ -11,8 +11,10 @@ reads like TBTK's own:
   order (what ``HoppingAmplitudeSet::getSparseMatrix`` returns).
 * :class:`PropertyExtractor` — ``PropertyExtractor::ChebyshevExpander``
   (Lib/include/TBTK/PropertyExtractor/ChebyshevExpander.h:51-178):
-  ``setEnergyWindow``, ``calculateLDOS`` and ``calculateGreensFunctions``
-  over basis indices.
+  ``setEnergyWindow``, ``calculateLDOS``, ``calculateGreensFunctions``,
+  ``calculateSpinPolarizedLDOS``, ``calculateDensity``,
+  ``calculateMagnetization`` and ``calculateExpectationValue`` over basis
+  indices (occupation weights at the window energies as an argument).
 
 Where the reference exits through TBTKAssert/TBTKExit
 (Lib/include/Utilities/TBTK/TBTKMacros.h:55-94) these classes raise
@@ -669,6 +671,44 @@ class PropertyExtractor:
         out, _ = s._get_matrix().ldos_sites(s._get_table(), sites, s.broadening,
                                             s.precision)
         return out
+
+    def _occupation(self, occupation):
+        """The occupation weights at the window energies and the spacing dE
+        (the reference's energyWindow[1] - energyWindow[0])."""
+        e = self.getEnergyWindow()
+        occ = np.ascontiguousarray(occupation, dtype=np.float64)
+        if occ.shape != e.shape:
+            raise ValueError("occupation needs one weight per window energy")
+        return occ, float(e[1] - e[0])
+
+    def calculateSpinPolarizedLDOS(self, up, down):
+        """[S][E][2][2] complex at spin sites given by their spin-up and
+        spin-down basis indices (calculateSpinPolarizedLDOS)."""
+        s = self.solver
+        return s._get_matrix().spin_polarized_ldos(s._get_table(), up, down, s.broadening,
+                                                   s.precision)
+
+    def calculateDensity(self, sites, occupation):
+        """[S] densities; occupation = the equilibrium occupation at each
+        window energy (the reference takes it from the model's statistics,
+        temperature and chemical potential)."""
+        s = self.solver
+        occ, dE = self._occupation(occupation)
+        return s._get_matrix().density(s._get_table(), sites, s.broadening, occ, dE, s.precision)
+
+    def calculateMagnetization(self, up, down, occupation):
+        """[S][2][2] complex (calculateMagnetization)."""
+        s = self.solver
+        occ, dE = self._occupation(occupation)
+        return s._get_matrix().magnetization(s._get_table(), up, down, s.broadening, occ, dE,
+                                             s.precision)
+
+    def calculateExpectationValue(self, to, frm, occupation):
+        """<c_to^dagger c_from> (calculateExpectationValue)."""
+        s = self.solver
+        occ, dE = self._occupation(occupation)
+        return complex(s._get_matrix().expectation_values(
+            s._get_table(), [to], [frm], s.broadening, occ, dE, s.precision)[0])
 
     def calculateGreensFunctions(self, to, frm, type_="Retarded"):
         s = self.solver

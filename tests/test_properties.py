@@ -78,3 +78,24 @@ def test_properties_consistent(gpu, oracle):
         m.density(t, [0], bro, occ[:-1], dE)
     with pytest.raises(gpu.TBTKError):
         m.density(t, [10 ** 6], bro, occ, dE)
+
+
+def test_property_extractor_mirror(gpu, oracle):
+    """kpm.PropertyExtractor's property methods on the golden window give
+    the golden values (device table, FP64)."""
+    g = golden("props")
+    lo, hi, res = g["window"]
+    solver = gpu.ChebyshevExpander()
+    solver.setModel((g["rowptr"], g["col"], g["val"]))
+    solver.setScaleFactor(float(g["scale"]))
+    solver.setNumCoefficients(int(g["M"]))
+    solver.setBroadening(float(g["broadening"]))
+    pe = gpu.PropertyExtractor(solver)
+    pe.setEnergyWindow(float(lo), float(hi), int(res))
+    occ = g["occupation"]
+    assert rel_err(pe.calculateSpinPolarizedLDOS(g["sp_up"], g["sp_down"]), g["sp_ldos"]) <= 1e-12
+    assert rel_err(pe.calculateDensity(g["density_sites"], occ), g["density"]) <= 1e-12
+    assert rel_err(pe.calculateMagnetization(g["sp_up"], g["sp_down"], occ),
+                   g["magnetization"]) <= 1e-12
+    ev = pe.calculateExpectationValue(int(g["exp_to"][0]), int(g["exp_from"][0]), occ)
+    assert abs(ev - g["expectation"][0]) <= 1e-12 * abs(g["expectation"][0])
