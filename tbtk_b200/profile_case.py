@@ -40,6 +40,9 @@ def main():
     ap.add_argument("--config", default=None)
     ap.add_argument("--complex-vectors", action="store_true",
                     help="keep complex64 vectors for a real model (no real-vector kernels)")
+    ap.add_argument("--fp64-head", type=int, default=0,
+                    help="FP64 head steps of doubling runs (default 0: every step of a "
+                         "doubling run is a timed FP32 step, as without a head)")
     a = ap.parse_args()
     prec = {"fp64": kpm.FP64, "mixed": kpm.MIXED, "mixed_direct": kpm.MIXED_DIRECT}[a.precision]
     rowptr, col, val = workloads.square_csr(a.lattice, a.lattice, t=1.0, J=0.5, W=2.0,
@@ -49,6 +52,7 @@ def main():
     mat = kpm.Matrix.from_csr(rowptr, col, val, 12.0)
     tab = kpm.Table.create(a.moments, workloads.open_grid(12.0, a.energies), 12.0)
     mat.set_profiling(True)
+    mat.set_fp64_head(a.fp64_head)
     if a.complex_vectors:
         mat.set_real(False)
     real = prec != kpm.FP64 and mat.real()[1]
