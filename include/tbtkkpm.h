@@ -193,6 +193,19 @@ TBTKKPM_API int tbtkkpm_table_create(
 TBTKKPM_API int tbtkkpm_table_upload(
 	uint32_t M, uint32_t E, const double *table, tbtkkpm_table **out);
 
+/* A table handle without the M x E table: the energy sums of every call
+ * that takes it (tbtkkpm_greens, tbtkkpm_ldos, tbtkkpm_ldos_sites, the
+ * properties) run Clenshaw recurrences over T_n(E/s) and U_n(E/s) per
+ * energy instead (O(M) arithmetic per vector and energy, 8 E bytes of
+ * device memory instead of 16 M E).  Results equal the table sums up to
+ * rounding (~1e-13 relative).  Same arguments and checks as
+ * tbtkkpm_table_create.  (The survey's table-free energy-sum variant; no
+ * reference counterpart: generateGreensFunctionCPU without a table,
+ * ChebyshevExpander.cpp:363-433, evaluates e^{-in acos x} per term.) */
+TBTKKPM_API int tbtkkpm_table_create_clenshaw(
+	uint32_t M, const double *energies, uint32_t E, double scale,
+	tbtkkpm_table **out);
+
 TBTKKPM_API int tbtkkpm_table_destroy(tbtkkpm_table *t);
 
 /* Green's functions G[k][e] of one type from K damped coefficient vectors

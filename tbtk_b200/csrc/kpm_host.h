@@ -121,6 +121,11 @@ struct tbtkkpm_table {
   int device = 0;
   cudaStream_t stream = nullptr;
   uint32_t M = 0, E = 0;
+  // table-free handle (tbtkkpm_table_create_clenshaw): energies and scale
+  // only, the energy sums run Clenshaw recurrences (kpm_clenshaw)
+  bool clenshaw = false;
+  double scale = 0;
+  tbtkkpm::DevBuf energies;  // [E]
   tbtkkpm::DevBuf table;   // [M][E] complex128
   tbtkkpm::DevBuf mu, out; // staging for energy sums
   std::mutex lock;

@@ -795,4 +795,90 @@ kpm_ldos(uint32_t M, uint32_t E, uint32_t K, const double2 *__restrict__ table,
   }
 }
 
+// ---------------------------------------------------------------- table-free energy sums
+// The sums of kpm_greens / kpm_ldos without the M x E table (the survey's
+// energy-sum variant for memory-light serving).  With x = E_e/s,
+// theta = acos x, q = sin theta = sqrt(1 - x^2) and the table entries
+// T[n][e] = (1/s)(-2i/q) e^{-i n theta}/(1 + delta_n0), every type is a
+// combination of
+//   C = sum_n c_n cos(n theta)/(1 + delta_n0) = sum_n a_n T_n(x)
+//   S = sum_n c_n sin(n theta)/(1 + delta_n0) = q sum_{n>=1} c_n U_{n-1}(x),
+// Retarded (-2/(s q))(S + iC), Advanced (-2/(s q))(S - iC), Principal
+// (2/(s q)) S, NonPrincipal (2/(s q)) iC, LDOS Im(G_NP)/pi; S/q is formed
+// without dividing by q.  C and S/q come from Clenshaw recurrences over
+// descending n (b_n = a_n + 2x b_{n+1} - b_{n+2}; C = b_0 - x b_1 for the T
+// series, b_0 for the U series), O(M) FMAs per (vector, energy) and no table
+// traffic.  They differ from the table sums by rounding only (~1e-13
+// relative at M = 4096).
+template <int KT>
+__global__ void __launch_bounds__(kEnergyBlock)
+kpm_clenshaw(uint32_t M, uint32_t E, uint32_t K, const double *__restrict__ energies, double scale,
+             const double2 *__restrict__ mu, int type, void *__restrict__ out) {
+  __shared__ double2 cs[KT][kEnergyChunk];
+  const uint32_t e = blockIdx.x * kEnergyBlock + threadIdx.x;
+  const uint32_t k0 = blockIdx.y * KT;
+  const double x = e < E ? energies[e] / scale : 0.0;
+  const double x2 = 2.0 * x;
+  double2 t1[KT], t2[KT], u1[KT], u2[KT];
+#pragma unroll
+  for (int j = 0; j < KT; j++) t1[j] = t2[j] = u1[j] = u2[j] = make_double2(0.0, 0.0);
+  for (int64_t top = M; top > 0; top -= kEnergyChunk) {
+    const uint32_t n0 = (uint32_t)(top > kEnergyChunk ? top - kEnergyChunk : 0);
+    const uint32_t nc = (uint32_t)top - n0;
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < KT * kEnergyChunk; i += kEnergyBlock) {
+      const uint32_t j = i / kEnergyChunk, n = i % kEnergyChunk;
+      cs[j][n] = (k0 + j < K && n < nc) ? mu[(uint64_t)(k0 + j) * M + n0 + n] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    if (e < E) {
+      for (int n = (int)nc - 1; n >= 0; n--) {
+        const uint32_t nn = n0 + (uint32_t)n;
+#pragma unroll
+        for (int j = 0; j < KT; j++) {
+          const double2 c = cs[j][n];
+          if (nn >= 1) {
+            const double2 bu = make_double2(fma(x2, u1[j].x, c.x - u2[j].x), fma(x2, u1[j].y, c.y - u2[j].y));
+            u2[j] = u1[j];
+            u1[j] = bu;
+          }
+          const double2 a = nn == 0 ? make_double2(0.5 * c.x, 0.5 * c.y) : c;
+          const double2 bt = make_double2(fma(x2, t1[j].x, a.x - t2[j].x), fma(x2, t1[j].y, a.y - t2[j].y));
+          t2[j] = t1[j];
+          t1[j] = bt;
+        }
+      }
+    }
+  }
+  if (e >= E) return;
+  const double q = sqrt(1.0 - x * x);
+  const double A = 2.0 / (scale * q), B = 2.0 / scale;  // C weight, S/q weight
+#pragma unroll
+  for (int j = 0; j < KT; j++) {
+    if (k0 + j >= K) continue;
+    const double2 C = make_double2(t1[j].x - x * t2[j].x, t1[j].y - x * t2[j].y);
+    const double2 Sq = u1[j];  // S / q
+    const uint64_t o = (uint64_t)(k0 + j) * E + e;
+    if (type == 4) {
+      static_cast<double *>(out)[o] = A * C.x / 3.14159265358979323846;
+      continue;
+    }
+    double2 g;
+    switch (type) {
+      case 0:  // Advanced: -(2/(s q)) (S - iC)
+        g = make_double2(-(B * Sq.x + A * C.y), -(B * Sq.y - A * C.x));
+        break;
+      case 1:  // Retarded: -(2/(s q)) (S + iC)
+        g = make_double2(-(B * Sq.x - A * C.y), -(B * Sq.y + A * C.x));
+        break;
+      case 2:  // Principal: (2/(s q)) S
+        g = make_double2(B * Sq.x, B * Sq.y);
+        break;
+      default:  // NonPrincipal: (2/(s q)) iC
+        g = make_double2(-A * C.y, A * C.x);
+    }
+    static_cast<double2 *>(out)[o] = g;
+  }
+}
+
 }  // namespace tbtkkpm

@@ -501,7 +501,7 @@ extern "C" int tbtkkpm_moments_batched(tbtkkpm_matrix *m, const uint32_t *from, 
 
 // ---------------------------------------------------------------- tables
 
-static int table_alloc(uint32_t M, uint32_t E, tbtkkpm_table **out) {
+static int table_alloc(uint32_t M, uint32_t E, tbtkkpm_table **out, bool with_table = true) {
   int ndev = 0;
   tbtkkpm_device_count(&ndev);
   if (ndev == 0) return fail(TBTKKPM_ERR_CUDA, "no CUDA device available");
@@ -515,7 +515,7 @@ static int table_alloc(uint32_t M, uint32_t E, tbtkkpm_table **out) {
     delete t;
     return cuda_fail(e, "cudaStreamCreate");
   }
-  int rc = t->table.reserve(sizeof(double2) * (size_t)M * E);
+  int rc = with_table ? t->table.reserve(sizeof(double2) * (size_t)M * E) : TBTKKPM_OK;
   if (rc) {
     tbtkkpm_table_destroy(t);
     return rc;
@@ -561,6 +561,43 @@ extern "C" int tbtkkpm_table_create(uint32_t M, const double *energies, uint32_t
   return TBTKKPM_OK;
 }
 
+extern "C" int tbtkkpm_table_create_clenshaw(uint32_t M, const double *energies, uint32_t E,
+                                             double scale, tbtkkpm_table **out) {
+  if (!out) return fail(TBTKKPM_ERR_ARGUMENT, "table_create_clenshaw: out is NULL");
+  *out = nullptr;
+  if (M == 0)
+    return fail(TBTKKPM_ERR_ARGUMENT, "table_create_clenshaw: numCoefficients has to be larger than 0");
+  if (E == 0 || !energies)
+    return fail(TBTKKPM_ERR_ARGUMENT,
+                "table_create_clenshaw: The energy windows resolution has to be larger than 0.");
+  if (!(scale > 0)) return fail(TBTKKPM_ERR_ARGUMENT, "table_create_clenshaw: scaleFactor must be > 0");
+  for (uint32_t e = 0; e < E; e++)
+    if (!(energies[e] > -scale && energies[e] < scale))
+      return fail(TBTKKPM_ERR_ARGUMENT,
+                  "table_create_clenshaw: energy %g is not contained in the interval (-scaleFactor, "
+                  "scaleFactor)=(%g, %g)",
+                  energies[e], -scale, scale);
+  tbtkkpm_table *t = nullptr;
+  int rc = table_alloc(M, E, &t, false);
+  if (rc) return rc;
+  DeviceGuard g(t->device);
+  t->clenshaw = true;
+  t->scale = scale;
+  if ((rc = t->energies.reserve(8 * (size_t)E))) {
+    tbtkkpm_table_destroy(t);
+    return rc;
+  }
+  cudaError_t e = cudaMemcpyAsync(t->energies.ptr, energies, 8 * (size_t)E, cudaMemcpyHostToDevice,
+                                  t->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
+  if (e != cudaSuccess) {
+    tbtkkpm_table_destroy(t);
+    return cuda_fail(e, "table_create_clenshaw");
+  }
+  *out = t;
+  return TBTKKPM_OK;
+}
+
 extern "C" int tbtkkpm_table_upload(uint32_t M, uint32_t E, const double *table,
                                     tbtkkpm_table **out) {
   if (!out) return fail(TBTKKPM_ERR_ARGUMENT, "table_upload: out is NULL");
@@ -587,6 +624,7 @@ extern "C" int tbtkkpm_table_destroy(tbtkkpm_table *t) {
     DeviceGuard g(t->device);
     if (t->stream) cudaStreamSynchronize(t->stream);
     t->table.release();
+    t->energies.release();
     t->mu.release();
     t->out.release();
     if (t->stream) cudaStreamDestroy(t->stream);
@@ -605,6 +643,19 @@ int launch_energy_sum(cudaStream_t st, const tbtkkpm_table *t, const double2 *mu
   const uint32_t M = terms ? terms : t->M, E = t->E;
   const int KT = K == 1 ? 1 : (K <= 4 ? 4 : 8);
   dim3 grid((E + kEnergyBlock - 1) / kEnergyBlock, (K + KT - 1) / KT);
+  if (t->clenshaw) {
+    const double *en = t->energies.as<double>();
+    if (KT == 1)
+      kpm_clenshaw<1><<<grid, kEnergyBlock, 0, st>>>(M, E, K, en, t->scale, mu, type, out);
+    else if (KT == 4)
+      kpm_clenshaw<4><<<grid, kEnergyBlock, 0, st>>>(M, E, K, en, t->scale, mu, type, out);
+    else
+      kpm_clenshaw<8><<<grid, kEnergyBlock, 0, st>>>(M, E, K, en, t->scale, mu, type, out);
+    count_launches(1);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "energy sum: launch");
+    return TBTKKPM_OK;
+  }
   const double2 *tb = t->table.as<double2>();
 #define TBTKKPM_G(TY, KK) \
   kpm_greens<TY, KK><<<grid, kEnergyBlock, 0, st>>>(M, E, K, tb, mu, static_cast<double2 *>(out))

@@ -80,6 +80,7 @@ SIGNATURES = [
     ("tbtkkpm_moments_batched", _i, [_p, _p, _u32, _p, _p, _u32, _u32, _d, _i, _p, _p]),
     ("tbtkkpm_table_create", _i, [_u32, _p, _u32, _d, _p]),
     ("tbtkkpm_table_upload", _i, [_u32, _u32, _p, _p]),
+    ("tbtkkpm_table_create_clenshaw", _i, [_u32, _p, _u32, _d, _p]),
     ("tbtkkpm_table_destroy", _i, [_p]),
     ("tbtkkpm_greens", _i, [_p, _p, _u32, _i, _p]),
     ("tbtkkpm_ldos", _i, [_p, _p, _u32, _p]),
@@ -420,6 +421,16 @@ class Table:
         h = ctypes.c_void_p()
         _check(load_library().tbtkkpm_table_create(M, _ptr(energies), energies.size,
                                                    float(scale), ctypes.byref(h)))
+        return cls(h, M, energies.size)
+
+    @classmethod
+    def create_clenshaw(cls, M, energies, scale):
+        """A table handle without the M x E table: energy sums by Clenshaw
+        recurrences (tbtkkpm_table_create_clenshaw)."""
+        energies = np.ascontiguousarray(energies, dtype=np.float64)
+        h = ctypes.c_void_p()
+        _check(load_library().tbtkkpm_table_create_clenshaw(M, _ptr(energies), energies.size,
+                                                            float(scale), ctypes.byref(h)))
         return cls(h, M, energies.size)
 
     @classmethod
