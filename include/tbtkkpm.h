@@ -427,6 +427,11 @@ TBTKKPM_API int tbtkkpm_server_set_real(tbtkkpm_server *s, int enable);
  * site and M, so its result is the same alone and in any mix. */
 TBTKKPM_API int tbtkkpm_server_set_fp64_head(tbtkkpm_server *s, uint32_t steps);
 
+/* Scales first used after set_table_free(s, 1) get table-free energy sums
+ * (tbtkkpm_table_create_clenshaw): 8 E bytes per scale instead of the
+ * max_moments x E table of 16-byte entries, same results up to rounding. */
+TBTKKPM_API int tbtkkpm_server_set_table_free(tbtkkpm_server *s, int enable);
+
 /* Stops the worker (requests still queued or in flight are dropped) and
  * frees the server. */
 TBTKKPM_API int tbtkkpm_server_destroy(tbtkkpm_server *s);

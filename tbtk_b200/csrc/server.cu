@@ -158,6 +158,7 @@ struct tbtkkpm_server {
   std::map<uint32_t, std::array<int, 3>> config;  // width | real << 16 -> tpr, vpt, minb
   bool use_real = true;                           // real lanes for real models added later
   uint32_t head_steps = kPrefixSteps;             // FP64 head of models added later
+  bool table_free = false;                        // Clenshaw energy sums for scales added later
   Workspace head_ws;                              // FP64 head scratch (worker thread)
   std::deque<uint64_t> pending;
   std::map<uint64_t, std::unique_ptr<Request>> requests;
@@ -551,7 +552,8 @@ tbtkkpm_table *exact_table(tbtkkpm_server *s, uint32_t M, double scale, int *rc)
   if (it != s->exact.end()) return it->second;
   tbtkkpm_table *t = nullptr;
   const int prev = swap_selected_device(s->device);
-  *rc = tbtkkpm_table_create(M, s->energies.data(), s->E, scale, &t);
+  *rc = s->table_free ? tbtkkpm_table_create_clenshaw(M, s->energies.data(), s->E, scale, &t)
+                      : tbtkkpm_table_create(M, s->energies.data(), s->E, scale, &t);
   swap_selected_device(prev);
   if (*rc) return nullptr;
   s->exact[key] = t;
@@ -921,7 +923,7 @@ extern "C" int tbtkkpm_server_add_model(tbtkkpm_server *s, const uint32_t *rowpt
   const int prev = swap_selected_device(s->device);
   int rc = tbtkkpm_matrix_create_csr(rowptr, col, val, N, scale, &m->mat);
   tbtkkpm_table *t = nullptr;
-  bool new_table = false, use_real = true;
+  bool new_table = false, use_real = true, table_free = false;
   uint32_t head_steps = 0;
   if (!rc) {
     std::lock_guard<std::mutex> lk(s->mu);
@@ -929,9 +931,11 @@ extern "C" int tbtkkpm_server_add_model(tbtkkpm_server *s, const uint32_t *rowpt
     if (it != s->tables.end()) t = it->second;
     use_real = s->use_real;
     head_steps = s->head_steps;
+    table_free = s->table_free;
   }
   if (!rc && !t) {
-    rc = tbtkkpm_table_create(s->Mmax, s->energies.data(), s->E, scale, &t);
+    rc = table_free ? tbtkkpm_table_create_clenshaw(s->Mmax, s->energies.data(), s->E, scale, &t)
+                    : tbtkkpm_table_create(s->Mmax, s->energies.data(), s->E, scale, &t);
     new_table = rc == 0;
   }
   swap_selected_device(prev);
@@ -1074,6 +1078,13 @@ extern "C" int tbtkkpm_server_set_config(tbtkkpm_server *s, uint32_t width, int 
   // the lane class(es) this shape is compiled for
   if (cplx) s->config[width] = {tpr, vpt, minb};
   if (real) s->config[width | 1u << 16] = {tpr, vpt, minb};
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_server_set_table_free(tbtkkpm_server *s, int enable) {
+  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_set_table_free: NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->table_free = enable != 0;
   return TBTKKPM_OK;
 }
 

@@ -106,6 +106,7 @@ SIGNATURES = [
     ("tbtkkpm_server_set_config", _i, [_p, _u32, _i, _i, _i]),
     ("tbtkkpm_server_set_real", _i, [_p, _i]),
     ("tbtkkpm_server_set_fp64_head", _i, [_p, _u32]),
+    ("tbtkkpm_server_set_table_free", _i, [_p, _i]),
     ("tbtkkpm_server_destroy", _i, [_p]),
 ]
 
@@ -531,6 +532,10 @@ class Server:
     def set_fp64_head(self, steps=32):
         """FP64 head steps of the lanes of models added from now on."""
         _check(load_library().tbtkkpm_server_set_fp64_head(self._h, int(steps)))
+
+    def set_table_free(self, enable=True):
+        """Clenshaw energy sums (no lookup table) for scales first used from now on."""
+        _check(load_library().tbtkkpm_server_set_table_free(self._h, int(bool(enable))))
 
     def close(self):
         if getattr(self, "_h", None):

@@ -50,3 +50,22 @@ def test_clenshaw_matches_table_sums(gpu, name):
         assert rel_err(cl.greens(mu, ty), tab.greens(mu, ty)) <= 1e-12, ty
     mixed, _ = m.ldos_sites(cl, sites, bro, gpu.MIXED)
     assert rel_err(mixed, ref) <= 1e-6
+
+
+def test_server_table_free(gpu):
+    """A server with table-free energy sums returns the table server's LDOS
+    up to rounding (same lanes, same moments)."""
+    from tbtk_b200 import workloads
+    S = 12.0
+    energies = workloads.open_grid(S, 300)
+    csr = workloads.square_csr(20, 20, J=0.5, W=2.0, alpha=0.3, seed=2)
+    sites = [3, 77, 400]
+    out = []
+    for free in (False, True):
+        srv = gpu.Server(512, energies, hbm_budget=1 << 30, tick_steps=16, tolerance=0)
+        srv.set_table_free(free)
+        mid = srv.add_model(*csr, S, 4)
+        ldos, _, _ = srv.wait(srv.submit(mid, sites, 512, 1e-3), timeout=300)
+        out.append(ldos)
+        srv.close()
+    assert rel_err(out[1], out[0]) <= 1e-12
