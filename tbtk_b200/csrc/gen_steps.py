@@ -62,7 +62,7 @@ MULTI_SHAPES = {1: [(1, 1)], 2: [(2, 1)], 4: [(4, 1), (2, 2)], 8: [(4, 2), (2, 4
                 64: [(32, 2), (16, 4), (8, 8)]}
 MULTI_MINBS = [1, 2]
 # the same for real float vectors (values per thread are real floats)
-MULTI_REAL_SHAPES = {1: [(1, 1)], 2: [(2, 1)], 4: [(4, 1), (1, 4)], 8: [(2, 4), (8, 1)],
+MULTI_REAL_SHAPES = {1: [(1, 1)], 2: [(2, 1), (1, 2)], 4: [(4, 1), (1, 4)], 8: [(2, 4), (8, 1), (1, 8)],
                      16: [(4, 4), (2, 8)], 32: [(8, 4), (4, 8)], 64: [(16, 4), (8, 8)]}
 
 
@@ -93,7 +93,7 @@ def write_multi():
 # Real-vector steps of a real matrix at mixed precision (kpm_real.cuh):
 # (threads per row, real values per thread) shapes with register caps
 # REAL_MINBS, one table without and one with the doubling dot products.
-SHAPES_REAL = [(1, 1), (2, 1), (4, 1), (8, 1), (2, 4), (16, 1), (4, 4), (32, 1), (8, 4), (4, 8),
+SHAPES_REAL = [(1, 1), (2, 1), (1, 2), (4, 1), (1, 4), (8, 1), (1, 8), (2, 4), (16, 1), (4, 4), (32, 1), (8, 4), (4, 8),
                (16, 4), (8, 8), (32, 4), (16, 8), (32, 8)]
 REAL_MINBS = [1, 2, 3]
 # extra variants gathering G entries per round trip; 6 and 8 measured 14%

@@ -117,9 +117,9 @@ std::array<int, 3> default_config(uint32_t W, bool real) {
   if (real) {
     switch (W) {
       case 1: return {1, 1, 2};
-      case 2: return {2, 1, 2};
-      case 4: return {4, 1, 2};
-      case 8: return {2, 4, 2};
+      case 2: return {1, 2, 2};
+      case 4: return {1, 4, 2};
+      case 8: return {1, 8, 2};
       case 16: return {4, 4, 2};
       case 32: return {8, 4, 2};
       default: return {8, 8, 2};

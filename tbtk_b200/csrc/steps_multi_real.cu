@@ -9,6 +9,8 @@ const MultiEntry kMultiStepsReal[] = {
     TBTKKPM_MULTI_REAL_ENTRY(1, 1, 2),
     TBTKKPM_MULTI_REAL_ENTRY(2, 1, 1),
     TBTKKPM_MULTI_REAL_ENTRY(2, 1, 2),
+    TBTKKPM_MULTI_REAL_ENTRY(1, 2, 1),
+    TBTKKPM_MULTI_REAL_ENTRY(1, 2, 2),
     TBTKKPM_MULTI_REAL_ENTRY(4, 1, 1),
     TBTKKPM_MULTI_REAL_ENTRY(4, 1, 2),
     TBTKKPM_MULTI_REAL_ENTRY(1, 4, 1),
@@ -17,6 +19,8 @@ const MultiEntry kMultiStepsReal[] = {
     TBTKKPM_MULTI_REAL_ENTRY(2, 4, 2),
     TBTKKPM_MULTI_REAL_ENTRY(8, 1, 1),
     TBTKKPM_MULTI_REAL_ENTRY(8, 1, 2),
+    TBTKKPM_MULTI_REAL_ENTRY(1, 8, 1),
+    TBTKKPM_MULTI_REAL_ENTRY(1, 8, 2),
     TBTKKPM_MULTI_REAL_ENTRY(4, 4, 1),
     TBTKKPM_MULTI_REAL_ENTRY(4, 4, 2),
     TBTKKPM_MULTI_REAL_ENTRY(2, 8, 1),
