@@ -94,7 +94,7 @@ def write_multi():
 # (threads per row, real values per thread) shapes with register caps
 # REAL_MINBS, one table without and one with the doubling dot products.
 SHAPES_REAL = [(1, 1), (2, 1), (1, 2), (4, 1), (1, 4), (8, 1), (1, 8), (2, 4), (16, 1), (4, 4), (32, 1), (8, 4), (4, 8),
-               (16, 4), (8, 8), (32, 4), (16, 8), (32, 8)]
+               (16, 4), (8, 8), (4, 16), (32, 4), (16, 8), (32, 8)]
 REAL_MINBS = [1, 2, 3]
 # extra variants gathering G entries per round trip; 6 and 8 measured 14%
 # and 76% slower than the default for (8, 8) on the 2048^2 lattice (spills)

@@ -48,10 +48,12 @@ Shape shape_for(int precision, uint32_t B, bool real = false) {
     if (B <= 2) return {1, 2};
     if (B <= 4) return {1, 4};
     if (B <= 8) return {1, 8};
+    // wider batches: the autotuner's choices on the 2048^2 lattice (B = 64:
+    // (8, 8) 3.53 ms per step against 5.15 ms for (16, 4))
     if (B <= 16) return {4, 4};
-    if (B <= 32) return {8, 4};
-    if (B <= 64) return {16, 4};
-    if (B <= 128) return {32, 4};
+    if (B <= 32) return {4, 8};
+    if (B <= 64) return {8, 8};
+    if (B <= 128) return {16, 8};
     return {32, 8};
   }
   if (!is_mixed(precision)) {
