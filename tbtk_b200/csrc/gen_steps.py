@@ -12,7 +12,7 @@ import pathlib
 HERE = pathlib.Path(__file__).resolve().parent
 
 SHAPES_FP64 = [(1, 1), (2, 1), (4, 1), (8, 1), (16, 1), (32, 1), (16, 2), (32, 2), (16, 4), (32, 4)]
-SHAPES_MIXED = [(1, 1), (2, 1), (4, 1), (4, 2), (8, 2), (16, 2), (8, 4), (32, 2), (16, 4), (8, 8),
+SHAPES_MIXED = [(1, 1), (2, 1), (1, 2), (4, 1), (1, 4), (4, 2), (8, 2), (16, 2), (8, 4), (32, 2), (16, 4), (8, 8),
                 (32, 4), (16, 8), (32, 8)]
 MINBS = [1, 2, 3, 4]
 
@@ -57,7 +57,7 @@ def bulk_smem(V, vpt, s, wpb, dots):
 
 # Multi-model (server) steps: lane width -> (threads per row, values per
 # thread) shapes, each with the register caps MULTI_MINBS.
-MULTI_SHAPES = {1: [(1, 1)], 2: [(2, 1)], 4: [(4, 1), (2, 2)], 8: [(4, 2), (2, 4), (8, 1)],
+MULTI_SHAPES = {1: [(1, 1)], 2: [(2, 1), (1, 2)], 4: [(4, 1), (2, 2), (1, 4)], 8: [(4, 2), (2, 4), (8, 1)],
                 16: [(8, 2), (4, 4), (2, 8)], 32: [(16, 2), (8, 4), (4, 8)],
                 64: [(32, 2), (16, 4), (8, 8)]}
 MULTI_MINBS = [1, 2]

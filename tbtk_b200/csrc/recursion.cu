@@ -66,13 +66,16 @@ Shape shape_for(int precision, uint32_t B, bool real = false) {
     if (B <= 64) return {32, 2};
     return {32, 4};
   }
+  // complex64 vectors: the fastest compiled shapes on the 2048^2 lattice
+  // (B = 4: (1, 4) 0.43 ms per step; B = 64: (8, 8) 5.10 ms against 6.35 ms
+  // for (32, 2))
   if (B <= 1) return {1, 1};
-  if (B <= 2) return {2, 1};
-  if (B <= 4) return {4, 1};
+  if (B <= 2) return {1, 2};
+  if (B <= 4) return {1, 4};
   if (B <= 8) return {4, 2};
   if (B <= 16) return {8, 2};
-  if (B <= 32) return {16, 2};
-  if (B <= 64) return {32, 2};
+  if (B <= 32) return {8, 4};
+  if (B <= 64) return {8, 8};
   if (B <= 128) return {32, 4};
   return {32, 8};
 }

@@ -9,10 +9,14 @@ const MultiEntry kMultiSteps[] = {
     TBTKKPM_MULTI_ENTRY(1, 1, 2),
     TBTKKPM_MULTI_ENTRY(2, 1, 1),
     TBTKKPM_MULTI_ENTRY(2, 1, 2),
+    TBTKKPM_MULTI_ENTRY(1, 2, 1),
+    TBTKKPM_MULTI_ENTRY(1, 2, 2),
     TBTKKPM_MULTI_ENTRY(4, 1, 1),
     TBTKKPM_MULTI_ENTRY(4, 1, 2),
     TBTKKPM_MULTI_ENTRY(2, 2, 1),
     TBTKKPM_MULTI_ENTRY(2, 2, 2),
+    TBTKKPM_MULTI_ENTRY(1, 4, 1),
+    TBTKKPM_MULTI_ENTRY(1, 4, 2),
     TBTKKPM_MULTI_ENTRY(4, 2, 1),
     TBTKKPM_MULTI_ENTRY(4, 2, 2),
     TBTKKPM_MULTI_ENTRY(2, 4, 1),
