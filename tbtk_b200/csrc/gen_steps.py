@@ -4,8 +4,8 @@
 
 Each listed configuration (threads per row, complex values per thread,
 register cap as min blocks per SM) is compiled into libtbtkkpm.so; the
-driver's defaults and the autotuner choose among them.  Keep the shape lists
-in step with CONFIGS_FP64 / CONFIGS_MIXED in tbtk_b200/kpm.py.
+driver's defaults and the autotuner choose among them; callers list them
+through tbtkkpm_step_configs / tbtkkpm_matrix_step_configs.
 """
 import pathlib
 
