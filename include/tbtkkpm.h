@@ -280,8 +280,12 @@ TBTKKPM_API int tbtkkpm_matrix_fp64_head(
  * grid on the device; only the [B][E] result crosses to the host.
  * Replaces the per-site loop of PropertyExtractor::ChebyshevExpander::
  * calculateLDOS (ChebyshevExpander.cpp:475-505 through
- * PropertyExtractor.h:849-894).  err_out (may be NULL) is per site as in
- * tbtkkpm_moments_batched. */
+ * PropertyExtractor.h:849-894).  err_out (may be NULL) receives per site:
+ * 0 at TBTKKPM_FP64; -1 at TBTKKPM_MIXED_DIRECT (no estimate); at
+ * TBTKKPM_MIXED (doubling) 4 sqrt(2) times the largest gap between the
+ * doubled and the directly gathered moments over 2 <= n <= M/2, relative to
+ * max_n |mu_n| (measured against the FP64 path on 240 solves of a
+ * 1000-model batch: 0.75x to 8x the LDOS's relative error). */
 TBTKKPM_API int tbtkkpm_ldos_sites(
 	tbtkkpm_matrix *m, tbtkkpm_table *t, const uint32_t *sites, uint32_t B,
 	double broadening, int precision, double *ldos_out, double *err_out);
