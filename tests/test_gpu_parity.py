@@ -335,6 +335,14 @@ def test_real_vectors_match_complex_vectors(gpu, B):
     assert rel_err(dbl_r, dbl_c) <= 1e-10
     assert rel_err(dbl_r, fp64) <= 1e-6
     assert rel_err(direct_r, fp64) <= 1e-6
+    # every compiled doubling configuration of the real vectors: the same
+    # LDOS up to the grouping of the dot-product sums by the grid
+    for (t, v, mb) in rm.configs_for(B, gpu.MIXED, ldos=True):
+        m = gpu.Matrix.from_csr(rowptr, col, val, s)
+        m.set_config(B, gpu.MIXED, t, v, mb, ldos=True)
+        out, _ = m.ldos_sites(tab, frm, 1e-3, gpu.MIXED)
+        assert rel_err(out, dbl_r) <= 1e-7, (t, v, mb)
+        assert rel_err(out, fp64) <= 1e-6, (t, v, mb)
 
 
 def test_ring_ldos_integral(gpu):
