@@ -116,10 +116,12 @@ class Clocks:
 # lattice (N = 2,097,152 rows); the traffic grows with the rows, so a launch
 # on N rows moves that figure times N.  complex64 (8, 8, 2): 3.427 GB there
 # (algorithmic bytes 3.439 GB); real float vectors (8, 8, 2): 1.721 GB,
-# (4, 16, 2): 1.808 GB (algorithmic bytes 1.744 GB).
+# (4, 16, 2): 1.808 GB, (4, 16, 802) (dot sums in shared memory): 1.713 GB
+# (algorithmic bytes 1.744 GB).
 TRAFFIC_PER_ROW = {("complex64", 64, 8, 8, 2): 3.427e9 / 2097152,
                    ("real float", 64, 8, 8, 2): 1.721e9 / 2097152,
-                   ("real float", 64, 4, 16, 2): 1.8075e9 / 2097152}
+                   ("real float", 64, 4, 16, 2): 1.8075e9 / 2097152,
+                   ("real float", 64, 4, 16, 802): 1.7130e9 / 2097152}
 
 
 def peak_hbm():

@@ -239,9 +239,12 @@ TBTKKPM_API int tbtkkpm_matrix_set_config(
 
 /* Lists the compiled step configurations of the kernels a call at this
  * precision uses as (tpr, vpt, variant) triples into out[3*cap]; returns
- * their number (-1 for an unknown precision).  variant 2..4 is the register
+ * their number (-1 for an unknown precision).  variant 1..4 is the register
  * cap (min blocks per SM) of a register-staged kernel; 100 + 10*S + W is a
- * bulk-copy kernel with a ring of S stages per warp and W warps per block.
+ * bulk-copy kernel with a ring of S stages per warp and W warps per block;
+ * 10000 + 1000*S + 10*WMAX + W a cp.async-staged kernel.  Real-vector
+ * kernels (real matrices at the mixed precisions): cap + 100*8 (802, 803)
+ * keeps the doubling dot sums in shared memory instead of registers.
  * (No reference counterpart.) */
 TBTKKPM_API int tbtkkpm_step_configs(int precision, int ldos, int *out, int cap);
 

@@ -62,6 +62,8 @@ MULTI_SHAPES = {1: [(1, 1)], 2: [(2, 1), (1, 2)], 4: [(4, 1), (2, 2), (1, 4)], 8
                 64: [(32, 2), (16, 4), (8, 8)]}
 MULTI_MINBS = [1, 2]
 # the same for real float vectors (values per thread are real floats)
+# (16 values per thread at widths 16 and 32 spilled 240-380 bytes and lost
+# to (2, 8) and (4, 8) in the server's autotuner on the uneven batch)
 MULTI_REAL_SHAPES = {1: [(1, 1)], 2: [(2, 1), (1, 2)], 4: [(4, 1), (1, 4)], 8: [(2, 4), (8, 1), (1, 8)],
                      16: [(4, 4), (2, 8)], 32: [(8, 4), (4, 8)], 64: [(16, 4), (8, 8)]}
 
@@ -99,10 +101,22 @@ REAL_MINBS = [1, 2, 3]
 # extra variants gathering G entries per round trip; 6 and 8 measured 14%
 # and 76% slower than the default for (8, 8) on the 2048^2 lattice (spills)
 REAL_GATHERS = []
-# shape -> OPT variants at the cap of 2 (kpm_step_real: bit 0 bounds with the
-# entries, bit 1 j_{n-1} at the start of its row); none compiled: for (8, 8)
-# and (16, 4) on the 2048^2 lattice the defaults measured fastest or within 3%
-REAL_OPTS = {}
+# shape -> (register cap, OPT bits) variants of the dot-product table only
+# (kpm_step_real: bit 0 bounds with the entries, bit 1 j_{n-1} at the start
+# of its row, bit 3 the dot sums in shared memory).  Bits 0 and 1 are not
+# compiled: for (8, 8) and (16, 4) on the 2048^2 lattice the defaults measured
+# fastest or within 3%.  Bit 3 frees 2*VPT doubles of registers per thread:
+# at 64 columns on the 2048^2 lattice (4, 16) went from 3.45 to 2.90 ms per
+# step and (8, 8) from 3.52 to 3.28.  Shapes absent from SHAPES_REAL are
+# compiled with bit 3 only.
+# 16 values per thread won at every width from 16 to 256 columns; 32 values
+# (128 KB of sums, one block per SM) measured 1.3-2.3x slower, caps of 1 and
+# 3 at 16 values 1.4-1.9x slower (not compiled).
+REAL_DOTS_OPTS = {
+    (4, 8): [(2, 8)], (8, 4): [(2, 8)], (16, 4): [(2, 8)], (32, 4): [(2, 8)],
+    (16, 8): [(2, 8)], (8, 8): [(2, 8), (3, 8)], (4, 16): [(2, 8)],
+    (1, 16): [(2, 8)], (2, 16): [(2, 8)], (8, 16): [(2, 8)], (16, 16): [(2, 8)],
+}
 REAL_UNITS = [
     ("steps_real.cu", "kStepsMixedReal", "kClassMixedReal", "false",
      "Recursion steps on real float vectors of a real matrix with FP64 arithmetic."),
@@ -122,8 +136,10 @@ def write_real():
                 # a whole tight-binding row per round trip at the cap of 2
                 for g in REAL_GATHERS:
                     lines.append(f"    TBTKKPM_REAL_ENTRY({cls}, {t}, {p}, {dots}, 2, {g}),")
-            for opt in REAL_OPTS.get((t, p), []):
-                lines.append(f"    TBTKKPM_REAL_ENTRY_OPT({cls}, {t}, {p}, {dots}, 2, {opt}),")
+        if dots == "true":
+            for (t, p), variants in REAL_DOTS_OPTS.items():
+                for mb, opt in variants:
+                    lines.append(f"    TBTKKPM_REAL_ENTRY_OPT({cls}, {t}, {p}, {dots}, {mb}, {opt}),")
         lines += ["};", f"const int kNum{table[1:]} = sizeof({table}) / sizeof({table}[0]);", "",
                   "}  // namespace tbtkkpm", ""]
         (HERE / fname).write_text("\n".join(lines))

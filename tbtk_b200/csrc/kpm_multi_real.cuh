@@ -27,7 +27,10 @@ kpm_multi_step_real(const MultiModel *__restrict__ models, const MultiHeader *__
   const int32_t n = hdr->n_base + (int32_t)step_offset;
   if (nmodels == 0) return;
 
-  __shared__ long long msum[2 * VPT][kBlock];
+  // per-thread fixed-point sums, [2 * VPT][kBlock] in dynamic shared memory
+  // (64 KB at 16 values per thread, above the static limit)
+  extern __shared__ long long mreal_sums[];
+  long long (*msum)[kBlock] = reinterpret_cast<long long (*)[kBlock]>(mreal_sums);
 #pragma unroll
   for (int j = 0; j < 2 * VPT; j++) msum[j][threadIdx.x] = 0;
 
@@ -223,19 +226,22 @@ template <int TPR, int VPT, int MINB>
 void launch_multi_real(cudaStream_t st, int device, const MultiModel *models,
                        const MultiHeader *hdr, uint32_t step_offset, uint32_t W, uint32_t ld) {
   auto kern = kpm_multi_step_real<TPR, VPT, MINB>;
+  constexpr uint32_t smem = 2u * VPT * kBlock * 8u;
   static int per_sm[64] = {0};
   const int d = device & 63;
   if (per_sm[d] == 0) {
+    if (smem > 48u * 1024u)
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kBlock, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kBlock, smem) != cudaSuccess ||
         nb < 1) {
       cudaGetLastError();
       nb = 1;
     }
     per_sm[d] = nb;
   }
-  kern<<<(unsigned)(per_sm[d] * sm_count(device)), kBlock, 0, st>>>(models, hdr, step_offset, W,
-                                                                    ld);
+  kern<<<(unsigned)(per_sm[d] * sm_count(device)), kBlock, smem, st>>>(models, hdr, step_offset,
+                                                                       W, ld);
 }
 
 #define TBTKKPM_MULTI_REAL_ENTRY(T, P, MB) {T, P, MB, &launch_multi_real<T, P, MB>}

@@ -100,7 +100,9 @@ __device__ __forceinline__ void rfetch_row(const Sell &A, uint32_t Bp, const flo
 
 // GIN: entries gathered per round trip (0: entries_in_flight's choice).
 // OPT bit 0: load the slice bounds with the entries (not a tile ahead);
-// bit 1: load j_{n-1} at the start of its row (not a row ahead).
+// bit 1: load j_{n-1} at the start of its row (not a row ahead); bit 3:
+// the dot-product sums in this thread's slots of dynamic shared memory
+// (2*VPT doubles per thread) instead of registers.
 template <int TPR, int VPT, bool FIRST, bool DOTS, int MINB, int GIN = 0, int OPT = 0>
 __global__ void __launch_bounds__(kBlock, MINB)
 kpm_step_real(Sell A, uint32_t Bp, const float *__restrict__ x, float *__restrict__ y,
@@ -115,10 +117,16 @@ kpm_step_real(Sell A, uint32_t Bp, const float *__restrict__ x, float *__restric
   const int sub = threadIdx.x % TPR;
   const int grp = threadIdx.x / TPR;
   const unsigned mask = 0xffffffffu;
-  double d_nn[DOTS ? VPT : 1], d_np[DOTS ? VPT : 1];
-  if constexpr (DOTS) {
+  constexpr bool SMD = DOTS && (OPT & 8);
+  extern __shared__ double real_sdots[];  // [2][VPT][kBlock] with SMD
+  double d_nn[DOTS && !SMD ? VPT : 1], d_np[DOTS && !SMD ? VPT : 1];
+  if constexpr (DOTS && !SMD) {
 #pragma unroll
     for (int j = 0; j < VPT; j++) d_nn[j] = d_np[j] = 0.0;
+  }
+  if constexpr (SMD) {
+#pragma unroll
+    for (int j = 0; j < 2 * VPT; j++) real_sdots[j * kBlock + threadIdx.x] = 0.0;
   }
   // slice bounds a tile ahead of the entries for thread shares below 32 B
   // (for (8, 8) loading them with the entries measured 3% faster)
@@ -243,8 +251,13 @@ kpm_step_real(Sell A, uint32_t Bp, const float *__restrict__ x, float *__restric
 #pragma unroll
           for (int j = 0; j < VPT; j++) {
             const float b = P::getf(self, j);
-            d_nn[j] += (double)fmaf(af[j], af[j], 0.0f);
-            d_np[j] += (double)fmaf(af[j], b, 0.0f);
+            if constexpr (SMD) {
+              real_sdots[j * kBlock + threadIdx.x] += (double)fmaf(af[j], af[j], 0.0f);
+              real_sdots[(VPT + j) * kBlock + threadIdx.x] += (double)fmaf(af[j], b, 0.0f);
+            } else {
+              d_nn[j] += (double)fmaf(af[j], af[j], 0.0f);
+              d_np[j] += (double)fmaf(af[j], b, 0.0f);
+            }
           }
         }
       }
@@ -256,8 +269,13 @@ kpm_step_real(Sell A, uint32_t Bp, const float *__restrict__ x, float *__restric
     __shared__ double red[kBlock][2];
 #pragma unroll 1
     for (int j = 0; j < VPT; j++) {
-      red[threadIdx.x][0] = d_nn[j];
-      red[threadIdx.x][1] = d_np[j];
+      if constexpr (SMD) {
+        red[threadIdx.x][0] = real_sdots[j * kBlock + threadIdx.x];
+        red[threadIdx.x][1] = real_sdots[(VPT + j) * kBlock + threadIdx.x];
+      } else {
+        red[threadIdx.x][0] = d_nn[j];
+        red[threadIdx.x][1] = d_np[j];
+      }
       __syncthreads();
       if (grp == 0) {
         double a = 0.0, b = 0.0;

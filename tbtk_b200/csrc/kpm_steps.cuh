@@ -110,11 +110,14 @@ template <int TPR, int VPT, bool FIRST, bool DOTS, int MINB, int G, int OPT = 0>
 void launch_real(cudaStream_t st, int device, unsigned max_grid, const StepArgs &a,
                  unsigned *grid) {
   auto kern = kpm_step_real<TPR, VPT, FIRST, DOTS, MINB, G, OPT>;
+  // dot-product sums in shared memory (OPT bit 3)
+  constexpr uint32_t smem = (DOTS && (OPT & 8)) ? 2u * VPT * kBlock * 8u : 0u;
   static int per_sm[64] = {0};
   const int d = device & 63;
   if (per_sm[d] == 0) {
+    if (smem) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kBlock, 0) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kBlock, smem) != cudaSuccess ||
         nb < 1) {
       cudaGetLastError();
       nb = 1;
@@ -127,8 +130,8 @@ void launch_real(cudaStream_t st, int device, unsigned max_grid, const StepArgs 
   if (max_grid) g = std::min<uint64_t>(g, max_grid);
   g = std::max<uint64_t>(g, 1);
   *grid = (unsigned)g;
-  kern<<<(unsigned)g, kBlock, 0, st>>>(a.A, a.Bp, static_cast<const float *>(a.x),
-                                       static_cast<float *>(a.y), a.tg, a.n_out, a.dots);
+  kern<<<(unsigned)g, kBlock, smem, st>>>(a.A, a.Bp, static_cast<const float *>(a.x),
+                                          static_cast<float *>(a.y), a.tg, a.n_out, a.dots);
 }
 
 // variant MB + 10*G: register cap MB, G entries gathered per round trip

@@ -25,6 +25,7 @@ inline unsigned blocks_for(uint64_t n, unsigned bs = 256) { return (unsigned)((n
 // thread).
 struct Shape {
   int tpr, vpt;
+  int minb = 2;  // variant: register cap + 100 * OPT bits
   uint32_t bp() const { return (uint32_t)(tpr * vpt); }
 };
 
@@ -39,7 +40,7 @@ bool real_mode(const tbtkkpm_matrix *m, int precision) {
   return is_mixed(precision) && m->values_real && m->use_real;
 }
 
-Shape shape_for(int precision, uint32_t B, bool real = false) {
+Shape shape_for(int precision, uint32_t B, bool real = false, bool dots = false) {
   if (real) {
     // a thread per row up to 8 values: it prefetches all of the next row's
     // entries and gathers them in one round (0.51 against 0.71 ms per step
@@ -48,6 +49,18 @@ Shape shape_for(int precision, uint32_t B, bool real = false) {
     if (B <= 2) return {1, 2};
     if (B <= 4) return {1, 4};
     if (B <= 8) return {1, 8};
+    // doubling runs: 16 values per thread with the dot sums in shared
+    // memory (variant 802), the fastest on the 2048^2 lattice at M = 128:
+    // 0.84 / 1.83 / 2.91 / 4.93 / 11.9 ms per step for B = 16 / 32 / 64 /
+    // 128 / 256 against 1.24 / 2.19 / 3.45 / 6.90 / 13.4 for the best
+    // register-only shapes
+    if (dots) {
+      if (B <= 16) return {1, 16, 802};
+      if (B <= 32) return {2, 16, 802};
+      if (B <= 64) return {4, 16, 802};
+      if (B <= 128) return {8, 16, 802};
+      return {16, 16, 802};
+    }
     // wider batches: the autotuner's choices on the 2048^2 lattice (B = 64:
     // (8, 8) 3.53 ms per step against 5.15 ms for (16, 4))
     if (B <= 16) return {4, 4};
@@ -135,7 +148,7 @@ const StepEntry *pick_step(const tbtkkpm_matrix *m, int precision, bool dots, ui
   if (force) return force;
   const bool real = real_mode(m, precision);
   const int cls = step_class(precision, dots, real);
-  const Shape s = shape_for(precision, B, real);
+  const Shape s = shape_for(precision, B, real, dots);
   auto it = m->tuned.find(tune_key(cls, s.bp()));
   if (it != m->tuned.end()) {
     const StepEntry *e = find_step(cls, it->second[0], it->second[1], it->second[2]);
@@ -149,7 +162,7 @@ const StepEntry *pick_step(const tbtkkpm_matrix *m, int precision, bool dots, ui
       if (e) return e;
     }
   }
-  return find_step(cls, s.tpr, s.vpt, 2);
+  return find_step(cls, s.tpr, s.vpt, s.minb);
 }
 
 // ------------------------------------------------------------ one batch
