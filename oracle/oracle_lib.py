@@ -156,6 +156,11 @@ class Reference:
                                         _i, _p, _p, _p]
         lib.ref_fermi_dirac.restype = _d
         lib.ref_fermi_dirac.argtypes = [_d, _d, _d]
+        lib.ref_property_json.restype = _i64
+        lib.ref_property_json.argtypes = [_p, _d, _i, _d, _d, _d, _i, _i, _d, _d, _i,
+                                          _i, _i, _i, _p, _p, _p, _i64, _p, _i64]
+        lib.ref_json_reserialize.restype = _i64
+        lib.ref_json_reserialize.argtypes = [_i, ctypes.c_char_p, _p, _i64, _p, _i64]
 
     @staticmethod
     def available(path=REF_SO) -> bool:
@@ -171,6 +176,18 @@ class Reference:
     def fermi_dirac(self, energies, mu, T):
         """Functions::fermiDiracDistribution at each energy."""
         return np.array([self.lib.ref_fermi_dirac(float(e), mu, T) for e in energies])
+
+    def reserialize(self, kind, text, n_values):
+        """TBTK's deserializing constructor on `text` (kind 0 Property::LDOS,
+        1 EnergyResolvedProperty<complex<double>>, 2 Property::Density), then
+        serialize() again.  Returns (new JSON text, the data array read, as
+        n_values doubles)."""
+        values = np.zeros(max(n_values, 1), dtype=np.float64)
+        raw = text.encode()
+        n = self.lib.ref_json_reserialize(kind, raw, None, 0, _ptr(values), n_values)
+        buf = ctypes.create_string_buffer(n + 1)
+        self.lib.ref_json_reserialize(kind, raw, buf, n + 1, _ptr(values), n_values)
+        return buf.value.decode(), values[:n_values]
 
     def greens(self, scale, coeff, lower, upper, res, type_, use_table,
                incl_lo=True, incl_hi=True):
@@ -263,6 +280,24 @@ class RefModel:
             return out[0]
         c = out.view(np.complex128)
         return c.reshape(res, 2, 2) if kind == 0 else c.reshape(2, 2)
+
+    def property_json(self, kind, scale, M, broadening, lower, upper, res, sites,
+                      frm=None, type_=3, T=300.0, mu=0.0, use_table=True):
+        """A property from the reference's PropertyExtractor and its JSON
+        serialization: kind 0 calculateLDOS(sites), 1
+        calculateGreensFunctions(sites, frm, type_), 2 calculateDensity(sites).
+        Returns (JSON text, data array; complex for kind 1)."""
+        sites = self._idx(sites)
+        frm_a = self._idx(frm if frm is not None else sites[0])
+        n_values = sites.shape[0] * (res if kind == 0 else 2 * res if kind == 1 else 1)
+        values = np.zeros(n_values, dtype=np.float64)
+        args = (self.h, scale, M, broadening, lower, upper, res, int(use_table), T, mu,
+                kind, type_, sites.shape[0], sites.shape[1], _ptr(sites), _ptr(frm_a))
+        n = self.ref.lib.ref_property_json(*args, None, 0, _ptr(values), n_values)
+        buf = ctypes.create_string_buffer(n + 1)
+        self.ref.lib.ref_property_json(*args, buf, n + 1, _ptr(values), n_values)
+        data = values.view(np.complex128) if kind == 1 else values
+        return buf.value.decode(), data
 
     def expectation(self, scale, M, broadening, lower, upper, res, T, mu, to, frm,
                     use_table=True):

@@ -14,14 +14,20 @@
  */
 #include "TBTK/Functions.h"
 #include "TBTK/Model.h"
+#include "TBTK/Property/Density.h"
+#include "TBTK/Property/EnergyResolvedProperty.h"
+#include "TBTK/Property/GreensFunction.h"
+#include "TBTK/Property/LDOS.h"
 #include "TBTK/PropertyExtractor/ChebyshevExpander.h"
 #include "TBTK/Range.h"
 #include "TBTK/Solver/ChebyshevExpander.h"
 #include "TBTK/Streams.h"
 #include "TBTK/TBTK.h"
 
+#include <algorithm>
 #include <complex>
 #include <cstdint>
+#include <string>
 #include <vector>
 
 using namespace TBTK;
@@ -342,6 +348,129 @@ int ref_expectation(
  * properties above weight with (PropertyExtractor.h:910-935). */
 double ref_fermi_dirac(double energy, double mu, double T){
 	return Functions::fermiDiracDistribution(energy, mu, T);
+}
+
+} // extern "C"
+
+namespace {
+
+/* Copies s with a terminating 0 into out when it fits in cap bytes. */
+int64_t put_string(const std::string &s, char *out, int64_t cap){
+	if(out != nullptr && (int64_t)s.size() < cap){
+		std::copy(s.begin(), s.end(), out);
+		out[s.size()] = 0;
+	}
+	return (int64_t)s.size();
+}
+
+template<typename DataType>
+void put_data(const std::vector<DataType> &d, double *values, int64_t cap);
+
+template<>
+void put_data(const std::vector<double> &d, double *values, int64_t cap){
+	for(int64_t n = 0; n < (int64_t)d.size() && n < cap; n++)
+		values[n] = d[n];
+}
+
+template<>
+void put_data(const std::vector<cplx> &d, double *values, int64_t cap){
+	for(int64_t n = 0; n < (int64_t)d.size() && 2*n + 1 < cap; n++){
+		values[2*n] = d[n].real();
+		values[2*n + 1] = d[n].imag();
+	}
+}
+
+} // namespace
+
+extern "C" {
+
+/* A property computed by the reference and its JSON serialization
+ * (Serializable::Mode::JSON):
+ *   kind 0: PropertyExtractor::calculateLDOS(sites) -> Property::LDOS
+ *           (Lib/src/Property/LDOS.cpp:121-140);
+ *   kind 1: calculateGreensFunctions(sites, from, type) ->
+ *           Property::GreensFunction, written by its EnergyResolvedProperty
+ *           base (Lib/include/TBTK/Property/EnergyResolvedProperty.h:1156-1212);
+ *   kind 2: calculateDensity(sites) at temperature T and chemical potential
+ *           mu -> Property::Density (Lib/src/Property/Density.cpp:111-130).
+ * The property's data array goes to values (complex data as (re, im)
+ * pairs, at most values_cap doubles).  Returns the length of the JSON text,
+ * written with a terminating 0 into out when it fits in cap bytes. */
+int64_t ref_property_json(
+	void *model, double scale, int M, double broadening, double lower,
+	double upper, int res, int use_table, double T, double mu, int kind,
+	int type, int n_sites, int idx_len, const int *sites, const int *from,
+	char *out, int64_t cap, double *values, int64_t values_cap
+){
+	Model &mdl = *(Model*)model;
+	mdl.setTemperature(T);
+	mdl.setChemicalPotential(mu);
+	Solver::ChebyshevExpander solver;
+	solver.setVerbose(false);
+	solver.setModel(mdl);
+	solver.setScaleFactor(scale);
+	solver.setNumCoefficients(M);
+	solver.setBroadening(broadening);
+	solver.setUseLookupTable(use_table != 0);
+	PropertyExtractor::ChebyshevExpander pe(solver);
+	pe.setEnergyWindow(lower, upper, res);
+	std::vector<Index> patterns;
+	for(int k = 0; k < n_sites; k++)
+		patterns.push_back(make_index(sites + k*idx_len, idx_len));
+	if(kind == 0){
+		Property::LDOS p = pe.calculateLDOS(patterns);
+		put_data(p.getData(), values, values_cap);
+		return put_string(p.serialize(Serializable::Mode::JSON), out, cap);
+	}
+	if(kind == 1){
+		/* one serial table build first: calculateGreensFunctions races on
+		 * the lazy build (see ref_greens_pe) */
+		solver.generateGreensFunction(
+			std::vector<cplx>(M, cplx(0, 0)),
+			Solver::ChebyshevExpander::Type::Retarded
+		);
+		Property::GreensFunction::Type t;
+		switch(type){
+		case 0: t = Property::GreensFunction::Type::Advanced; break;
+		case 1: t = Property::GreensFunction::Type::Retarded; break;
+		case 2: t = Property::GreensFunction::Type::Principal; break;
+		default: t = Property::GreensFunction::Type::NonPrincipal; break;
+		}
+		Property::GreensFunction p = pe.calculateGreensFunctions(
+			patterns, make_index(from, idx_len), t
+		);
+		put_data(p.getData(), values, values_cap);
+		return put_string(p.serialize(Serializable::Mode::JSON), out, cap);
+	}
+	Property::Density p = pe.calculateDensity(patterns);
+	put_data(p.getData(), values, values_cap);
+	return put_string(p.serialize(Serializable::Mode::JSON), out, cap);
+}
+
+/* Reads a serialization with the reference's deserializing constructor
+ * (kind 0 Property::LDOS, kind 1 EnergyResolvedProperty<complex<double>>,
+ * kind 2 Property::Density) and serializes the object again; the data
+ * array read goes to values as in ref_property_json.  Returns the length
+ * of the new serialization, written into out as above.  A text the
+ * reference cannot parse ends the process with TBTKExit's exit(1). */
+int64_t ref_json_reserialize(
+	int kind, const char *json, char *out, int64_t cap, double *values,
+	int64_t values_cap
+){
+	const std::string s(json);
+	if(kind == 0){
+		Property::LDOS p(s, Serializable::Mode::JSON);
+		put_data(p.getData(), values, values_cap);
+		return put_string(p.serialize(Serializable::Mode::JSON), out, cap);
+	}
+	if(kind == 1){
+		Property::EnergyResolvedProperty<cplx> p(s, Serializable::Mode::JSON);
+		put_data(p.getData(), values, values_cap);
+		return put_string(p.serialize(Serializable::Mode::JSON), out, cap);
+	}
+	Property::Density p(s, Serializable::Mode::JSON);
+	put_data(p.getData(), values, values_cap);
+	return put_string(p.serialize(Serializable::Mode::JSON), out, cap);
 }
 
 }

@@ -7,9 +7,10 @@ reference call: Model -> HoppingAmplitudeSet::getSparseMatrix (CSR),
 Solver::ChebyshevExpander::calculateCoefficients (moments),
 generateGreensFunction (G, table and closed form), and
 PropertyExtractor::ChebyshevExpander::calculateLDOS /
-calculateGreensFunctions.
+calculateGreensFunctions, and the JSON text of Property::LDOS,
+GreensFunction and Density (serialize(Serializable::Mode::JSON)).
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]    (default: every case)
 """
 import pathlib
 import sys
@@ -53,7 +54,44 @@ def model_case(ref, lat, s, M, bro, to, frm, ldos_sites, E, types=(0, 1, 2, 3)):
     return out
 
 
-def main():
+def export_case(ref):
+    """Serialized properties: the reference's JSON text next to the same
+    property's values per index in argument order (from the calls the other
+    fixtures use), on a disordered Rashba lattice (complex Green's
+    functions) and a honeycomb lattice (four subindices)."""
+    out = {}
+    lat = L.square(6, 5, t=1.0, J=0.5, W=2.0, alpha=0.3, periodic=True, seed=11)
+    m = ref.model(lat)
+    s, M, bro, lo, hi, res, T, mu = 8.0, 256, 1e-3, -3.9, 3.9, 40, 300.0, 0.1
+    out["window"] = np.array([lo, hi, res])
+    sites = [(2, 3, 0), (0, 4, 1), (5, 1, 0), (1, 1, 1)]
+    out["ldos_sites"] = np.array(sites, dtype=np.int32)
+    out["ldos_text"] = np.array(m.property_json(0, s, M, bro, lo, hi, res, sites)[0])
+    out["ldos"] = m.ldos(s, M, bro, lo, hi, res, sites)
+    to, frm = [(2, 3, 0), (2, 3, 1), (4, 0, 1)], (2, 3, 0)
+    out["gf_to"] = np.array(to, dtype=np.int32)
+    out["gf_from"] = np.array(frm, dtype=np.int32)
+    for ty in (1, 3):
+        out[f"gf_text_{ty}"] = np.array(
+            m.property_json(1, s, M, bro, lo, hi, res, to, frm=frm, type_=ty)[0])
+        out[f"gf_{ty}"] = m.greens_pe(s, M, bro, lo, hi, res, ty, to, frm)
+    dsites = [(2, 3, 0), (2, 3, 1), (4, 0, 1)]
+    out["density_sites"] = np.array(dsites, dtype=np.int32)
+    out["density_text"] = np.array(
+        m.property_json(2, s, M, bro, lo, hi, res, dsites, T=T, mu=mu)[0])
+    out["density"] = np.array([m.prop(1, s, M, bro, lo, hi, res, T, mu, list(d))
+                               for d in dsites])
+    lat = L.honeycomb(6, 5, t=1.0, J=0.3, W=1.5, periodic=True, seed=5)
+    m = ref.model(lat)
+    hsites = [(2, 2, 0, 0), (5, 4, 1, 1), (0, 1, 1, 0)]
+    out["hc_window"] = np.array([-11.5, 11.5, 64])
+    out["hc_sites"] = np.array(hsites, dtype=np.int32)
+    out["hc_text"] = np.array(m.property_json(0, 12.0, 200, 1e-3, -11.5, 11.5, 64, hsites)[0])
+    out["hc_ldos"] = m.ldos(12.0, 200, 1e-3, -11.5, 11.5, 64, hsites)
+    return out
+
+
+def main(only=()):
     ref = Reference()
     cases = {}
 
@@ -149,10 +187,14 @@ def main():
         expectation=np.array([m.expectation(s, M, bro, lo, hi, res, T, mu, list(a), list(b))
                               for a, b in pairs]))
 
+    cases["export"] = export_case(ref)
+
     for name, arrays in cases.items():
+        if only and name not in only:
+            continue
         np.savez_compressed(HERE / f"{name}.npz", **arrays)
         print(name, sum(np.asarray(v).nbytes for v in arrays.values()), "bytes")
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))
