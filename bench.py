@@ -411,6 +411,9 @@ def ours(args, world, rank, local):
                                                         tuned_plain))},
                    "parallelism": f"replicas x{world} (sites sharded, no collective)"},
         "gpu_launches": int(launches),
+        "vector_steps_per_s": {"value": solves * p.M / (total_ms / 1e3),
+                               "note": "sum over solves of the M moments each returns, per "
+                                       "second (doubling runs step to M/2)"},
         "plain_fp64": {"value": plain_rate, "unit": "LDOS solves/s", "ms_per_solve": plain_ms,
                        "sites": args.plain_sites},
         "speedup_vs_plain_fp64": (value / world) / plain_rate if plain_rate else None,
