@@ -199,7 +199,7 @@ TBTKKPM_API int tbtkkpm_table_upload(
  * energy instead (O(M) arithmetic per vector and energy, 8 E bytes of
  * device memory instead of 16 M E).  Results equal the table sums up to
  * rounding (~1e-13 relative).  Same arguments and checks as
- * tbtkkpm_table_create.  (The survey's table-free energy-sum variant; no
+ * tbtkkpm_table_create.  (A table-free energy-sum variant; no
  * reference counterpart: generateGreensFunctionCPU without a table,
  * ChebyshevExpander.cpp:363-433, evaluates e^{-in acos x} per term.) */
 TBTKKPM_API int tbtkkpm_table_create_clenshaw(

@@ -796,7 +796,7 @@ kpm_ldos(uint32_t M, uint32_t E, uint32_t K, const double2 *__restrict__ table,
 }
 
 // ---------------------------------------------------------------- table-free energy sums
-// The sums of kpm_greens / kpm_ldos without the M x E table (the survey's
+// The sums of kpm_greens / kpm_ldos without the M x E table (an
 // energy-sum variant for memory-light serving).  With x = E_e/s,
 // theta = acos x, q = sin theta = sqrt(1 - x^2) and the table entries
 // T[n][e] = (1/s)(-2i/q) e^{-i n theta}/(1 + delta_n0), every type is a
