@@ -278,6 +278,24 @@ TBTKKPM_API int tbtkkpm_matrix_set_fp64_head(tbtkkpm_matrix *m, uint32_t steps);
 TBTKKPM_API int tbtkkpm_matrix_fp64_head(
 	tbtkkpm_matrix *m, uint32_t *steps, int *pattern_symmetric);
 
+/* Sources per recursion batch.  tbtkkpm_moments_batched and
+ * tbtkkpm_ldos_sites split their sources into batches of at most this many
+ * and run the batches one after another; each batch reads the matrix once
+ * per step.  width 0 (the default) is the library's choice: 128 for
+ * TBTKKPM_MIXED LDOS runs on real float vectors (wider batches of that step
+ * measured slower per source), otherwise the maximum, 128 at TBTKKPM_FP64
+ * and 256 at the mixed precisions.  Widths above the maximum are rejected.
+ * Results at TBTKKPM_FP64 and the directly gathered moments do not depend
+ * on the width; doubled moments may differ in the last bits (their dot
+ * products are summed in an order set by the batch's step configuration).
+ * tbtkkpm_matrix_batch_width reports the width a call of this precision
+ * uses (ldos != 0: tbtkkpm_ldos_sites, 0: the moment calls).
+ * (No reference counterpart: the reference runs one source per recursion.) */
+TBTKKPM_API int tbtkkpm_matrix_set_batch_width(
+	tbtkkpm_matrix *m, int precision, uint32_t width);
+TBTKKPM_API int tbtkkpm_matrix_batch_width(
+	tbtkkpm_matrix *m, int precision, int ldos, uint32_t *width);
+
 /* LDOS at B sites in one call: the moments <site|T_n|site> of all sites run
  * as one batched recursion, are damped and summed over the table's energy
  * grid on the device; only the [B][E] result crosses to the host.

@@ -93,6 +93,8 @@ SIGNATURES = [
     ("tbtkkpm_matrix_step_configs", _i, [_p, _i, _i, _p, _i]),
     ("tbtkkpm_matrix_set_fp64_head", _i, [_p, _u32]),
     ("tbtkkpm_matrix_fp64_head", _i, [_p, _p, _p]),
+    ("tbtkkpm_matrix_set_batch_width", _i, [_p, _i, _u32]),
+    ("tbtkkpm_matrix_batch_width", _i, [_p, _i, _i, _p]),
     ("tbtkkpm_spin_polarized_ldos", _i, [_p, _p, _p, _p, _u32, _d, _i, _p]),
     ("tbtkkpm_density", _i, [_p, _p, _p, _u32, _d, _i, _p, _d, _p]),
     ("tbtkkpm_magnetization", _i, [_p, _p, _p, _p, _u32, _d, _i, _p, _d, _p]),
@@ -284,6 +286,20 @@ class Matrix:
         st, sym = ctypes.c_uint32(), ctypes.c_int()
         _check(load_library().tbtkkpm_matrix_fp64_head(self._h, ctypes.byref(st), ctypes.byref(sym)))
         return st.value, bool(sym.value)
+
+    def set_batch_width(self, precision, width=0):
+        """Sources per recursion batch at this precision (0: the library's
+        choice)."""
+        _check(load_library().tbtkkpm_matrix_set_batch_width(self._h, int(precision),
+                                                              int(width)))
+
+    def batch_width(self, precision, ldos=True):
+        """Sources per batch that ldos_sites (ldos=True) or the moment calls
+        use at this precision."""
+        w = ctypes.c_uint32()
+        _check(load_library().tbtkkpm_matrix_batch_width(self._h, int(precision), int(ldos),
+                                                         ctypes.byref(w)))
+        return w.value
 
     def configs_for(self, B, precision, ldos=True):
         """The compiled (tpr, vpt, variant) this matrix's calls for B sources

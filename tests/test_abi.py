@@ -52,6 +52,10 @@ def test_argument_errors_return_status(kpm):
     with pytest.raises(kpm.TBTKError) as e:
         kpm.Table.create(10, np.array([-10.0, 0.0]), 10.0)
     assert e.value.status == kpm.ERR_ARGUMENT
+    lib = kpm.load_library()
+    assert lib.tbtkkpm_matrix_set_batch_width(None, kpm.MIXED, 64) == kpm.ERR_ARGUMENT
+    assert lib.tbtkkpm_matrix_set_batch_width(None, 7, 64) == kpm.ERR_ARGUMENT
+    assert "precision" in lib.tbtkkpm_last_error().decode()
 
 
 def test_solver_setters_mirror_reference(kpm):

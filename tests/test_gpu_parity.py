@@ -339,10 +339,52 @@ def test_real_vectors_match_complex_vectors(gpu, B):
     # LDOS up to the grouping of the dot-product sums by the grid
     for (t, v, mb) in rm.configs_for(B, gpu.MIXED, ldos=True):
         m = gpu.Matrix.from_csr(rowptr, col, val, s)
+        m.set_batch_width(gpu.MIXED, 256)  # all B sources in one batch of this shape
         m.set_config(B, gpu.MIXED, t, v, mb, ldos=True)
         out, _ = m.ldos_sites(tab, frm, 1e-3, gpu.MIXED)
         assert rel_err(out, dbl_r) <= 1e-7, (t, v, mb)
         assert rel_err(out, fp64) <= 1e-6, (t, v, mb)
+
+
+def test_batch_width_splits_without_changing_results(gpu):
+    """tbtkkpm_matrix_set_batch_width splits a call's sources into batches:
+    FP64 LDOS, directly gathered moments and the MIXED_DIRECT LDOS are bit
+    for bit the same at every width, doubling LDOS agree to the 1e-7 of the
+    dot-sum grouping; real-vector doubling LDOS default to batches of 128."""
+    lat = L.square(13, 11, t=1.0, J=0.5, W=2.0, periodic=True, seed=41)
+    rowptr, col, val = lat.csr()
+    s, M = 12.0, 64
+    frm = L.random_sites(lat, 200, seed=9)
+    B = frm.size
+    tab = gpu.Table.create(M, gpu.tbtk_range(-12.0, 12.0, 80, False, False), s)
+    m = gpu.Matrix.from_csr(rowptr, col, val, s)
+    assert m.real()[1]
+    assert m.batch_width(gpu.MIXED, ldos=True) == 128
+    assert m.batch_width(gpu.MIXED, ldos=False) == 256
+    assert m.batch_width(gpu.MIXED_DIRECT) == 256 and m.batch_width(gpu.FP64) == 128
+    precs = (gpu.FP64, gpu.MIXED_DIRECT, gpu.MIXED)
+    base = {p: m.ldos_sites(tab, frm, 1e-3, p)[0] for p in precs}
+    mu_base, _ = m.moments_batched(frm, frm, np.arange(B), M, 1e-3, gpu.MIXED)
+    assert rel_err(base[gpu.MIXED], base[gpu.FP64]) <= 1e-6
+    for w in (1, 7, 64, 128, 256):
+        for p in precs:
+            if p == gpu.FP64 and w > 128:
+                with pytest.raises(gpu.TBTKError) as e:
+                    m.set_batch_width(p, w)
+                assert e.value.status == gpu.ERR_ARGUMENT
+                continue
+            m.set_batch_width(p, w)
+            assert m.batch_width(p) == w
+            out, _ = m.ldos_sites(tab, frm, 1e-3, p)
+            if p == gpu.MIXED:
+                assert rel_err(out, base[p]) <= 1e-7, w
+                assert rel_err(out, base[gpu.FP64]) <= 1e-6, w
+            else:
+                assert np.array_equal(out, base[p]), (w, p)
+        mu, _ = m.moments_batched(frm, frm, np.arange(B), M, 1e-3, gpu.MIXED)
+        assert np.array_equal(mu, mu_base), w
+    m.set_batch_width(gpu.MIXED, 0)
+    assert m.batch_width(gpu.MIXED, ldos=True) == 128
 
 
 def test_ring_ldos_integral(gpu):
