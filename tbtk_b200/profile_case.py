@@ -11,8 +11,9 @@ recursion (CUDA events on the handle's stream) and its bandwidth in
 algorithmic bytes (matrix once per step plus three vector passes per
 source).  --sweep times every compiled step configuration for the batch;
 --autotune lets the library's autotuner choose first; --config T,V,MB forces
-one.  Without --rashba the model is real and the mixed precisions run on
-real float vectors; --complex-vectors keeps complex64 ones.
+one; --batch-width splits the sites into batches of that many.  Without
+--rashba the model is real and the mixed precisions run on real float
+vectors; --complex-vectors keeps complex64 ones.
 """
 from __future__ import annotations
 
@@ -40,6 +41,8 @@ def main():
     ap.add_argument("--config", default=None)
     ap.add_argument("--complex-vectors", action="store_true",
                     help="keep complex64 vectors for a real model (no real-vector kernels)")
+    ap.add_argument("--batch-width", type=int, default=0,
+                    help="sources per recursion batch (default 0: the library's choice)")
     ap.add_argument("--fp64-head", type=int, default=0,
                     help="FP64 head steps of doubling runs (default 0: every step of a "
                          "doubling run is a timed FP32 step, as without a head)")
@@ -55,6 +58,8 @@ def main():
     mat.set_fp64_head(a.fp64_head)
     if a.complex_vectors:
         mat.set_real(False)
+    if a.batch_width:
+        mat.set_batch_width(prec, a.batch_width)
     real = prec != kpm.FP64 and mat.real()[1]
     s_vec = 16 if prec == kpm.FP64 else (4 if real else 8)
     bstep = step_bytes(N, nnz, a.sites, s_vec, 8 if real else 16)
