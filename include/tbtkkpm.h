@@ -282,9 +282,10 @@ TBTKKPM_API int tbtkkpm_matrix_fp64_head(
  * tbtkkpm_ldos_sites split their sources into batches of at most this many
  * and run the batches one after another; each batch reads the matrix once
  * per step.  width 0 (the default) is the library's choice: 128 for
- * TBTKKPM_MIXED LDOS runs on real float vectors (wider batches of that step
- * measured slower per source), otherwise the maximum, 128 at TBTKKPM_FP64
- * and 256 at the mixed precisions.  Widths above the maximum are rejected.
+ * TBTKKPM_MIXED LDOS runs (the doubling step of 256 sources measured 20%
+ * slower per source than two batches of 128, on real and complex
+ * matrices), otherwise the maximum, 128 at TBTKKPM_FP64 and 256 at the
+ * mixed precisions.  Widths above the maximum are rejected.
  * Results at TBTKKPM_FP64 and the directly gathered moments do not depend
  * on the width; doubled moments may differ in the last bits (their dot
  * products are summed in an order set by the batch's step configuration).

@@ -397,14 +397,15 @@ void doubling_error(const std::vector<double2> &mu, const std::vector<double2> &
 
 // Sources per recursion batch of a call.  A wider batch reads the matrix
 // fewer times, but past a point its step slows by more than the matrix
-// share it saves: the real-vector doubling step on the 2048^2 lattice costs
-// 0.0385 ms per source and step at 128 sources against 0.0465 ms at 256
-// (4.93 and 11.9 ms per step), so those runs split at 128.
+// share it saves.  Doubling steps per source and step: real float vectors
+// on the 2048^2 lattice 0.0385 ms at 128 sources against 0.0465 ms at 256;
+// complex64 vectors on the 1024^2 Rashba lattice 0.0261 ms at 128 against
+// 0.0327 ms at 256 (0.0303 at 64).  So doubling runs split at 128.
 uint32_t batch_width_for(const tbtkkpm_matrix *m, int precision, bool doubling) {
   const uint32_t maxb = is_mixed(precision) ? kMaxBatchMixed : kMaxBatchFP64;
   const uint32_t set = m->batch_width[precision];
   if (set) return std::min(set, maxb);
-  if (doubling && real_mode(m, precision)) return 128;
+  if (doubling) return 128;
   return maxb;
 }
 

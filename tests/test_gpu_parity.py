@@ -350,7 +350,8 @@ def test_batch_width_splits_without_changing_results(gpu):
     """tbtkkpm_matrix_set_batch_width splits a call's sources into batches:
     FP64 LDOS, directly gathered moments and the MIXED_DIRECT LDOS are bit
     for bit the same at every width, doubling LDOS agree to the 1e-7 of the
-    dot-sum grouping; real-vector doubling LDOS default to batches of 128."""
+    dot-sum grouping; doubling LDOS default to batches of 128 on real and
+    complex matrices."""
     lat = L.square(13, 11, t=1.0, J=0.5, W=2.0, periodic=True, seed=41)
     rowptr, col, val = lat.csr()
     s, M = 12.0, 64
@@ -385,6 +386,9 @@ def test_batch_width_splits_without_changing_results(gpu):
         assert np.array_equal(mu, mu_base), w
     m.set_batch_width(gpu.MIXED, 0)
     assert m.batch_width(gpu.MIXED, ldos=True) == 128
+    cm = gpu.Matrix.from_csr(*L.square(5, 4, t=1.0, J=0.5, alpha=0.3, periodic=True).csr(), s)
+    assert not cm.real()[1]
+    assert cm.batch_width(gpu.MIXED, ldos=True) == 128 and cm.batch_width(gpu.MIXED, False) == 256
 
 
 def test_ring_ldos_integral(gpu):
