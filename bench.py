@@ -168,7 +168,7 @@ def step_bytes(p, B, s_vec, s_val=16):
 
 # ------------------------------------------------------------------ CPU baselines
 
-def cpu_port_baseline(p, threads, sample_steps=(4, 12)):
+def cpu_port_baseline(p, threads, sample_steps=(4, 36)):
     """The oracle restatement (bit-identical to the reference's CPU
     recursion), one site per thread, timed at two truncated coefficient
     counts; per-site time extrapolated linearly to the full M."""
@@ -195,11 +195,14 @@ def cpu_port_baseline(p, threads, sample_steps=(4, 12)):
 
     t_lo = run(sample_steps[0])
     t_hi = run(sample_steps[1])
-    per_step = max(t_hi - t_lo, 1e-9) / (sample_steps[1] - sample_steps[0])
-    fixed = max(t_lo - per_step * sample_steps[0], 0.0)
+    slope = (t_hi - t_lo) / (sample_steps[1] - sample_steps[0])
+    if slope > 0:
+        per_step, fixed, fit = slope, max(t_lo - slope * sample_steps[0], 0.0), "linear"
+    else:
+        per_step, fixed, fit = t_hi / sample_steps[1], 0.0, "degenerate (upper bound)"
     t_site = fixed + per_step * p.M
     return {"value": len(sites) / t_site, "unit": "LDOS solves/s", "cores": len(sites),
-            "kind": "port",
+            "kind": "port", "fit": fit,
             "sample": (f"{len(sites)} sites in parallel (one thread each) at M="
                        f"{sample_steps[0]} and M={sample_steps[1]} of the same matrix; "
                        f"per-site time {fixed:.2f} s + {per_step:.3f} s/step extrapolated to "
