@@ -42,8 +42,18 @@ import math
 
 import numpy as np
 
-__all__ = ["IndexTree", "dumps", "ldos_json", "greens_function_json", "density_json",
-           "loads"]
+__all__ = ["IndexTree", "dumps", "ldos_json", "ldos_json_patterns", "expand_patterns",
+           "greens_function_json", "density_json", "loads", "IDX_ALL", "IDX_SUM_ALL"]
+
+# TBTK's wildcard subindices (Lib/include/Core/TBTK/Subindex.h:395-399), as
+# the 32-bit ints they are stored as.
+def _i32(v):
+    return v - (1 << 32) if v & 0x80000000 else v
+
+
+IDX_ALL = _i32(0xBFFFFFFF & ~0x20000000)
+IDX_SUM_ALL = _i32(0xBFFFFFFF & ~0x20000001)
+IDX_SPIN = _i32(0xBFFFFFFF & ~0x20000002)
 
 
 # --------------------------------------------------------------- JSON text
@@ -120,10 +130,11 @@ def _flatten(index):
 
 
 class IndexTree:
-    """TBTK's ``IndexTree`` (Lib/src/Core/IndexTree.cpp) for concrete
-    indices: non-negative subindices, compound indices with separators.
-    Wildcard subindices (negative values) are not accepted: the KPM path's
-    properties are written for the concrete indices they were computed at."""
+    """TBTK's ``IndexTree`` (Lib/src/Core/IndexTree.cpp): non-negative
+    subindices, compound indices with separators and, with
+    ``wildcards=True``, wildcard subindices (a node whose subindex is a
+    wildcard keeps one child, 0, and the wildcard's value as its type).
+    Without it negative subindices are rejected."""
 
     def __init__(self):
         self.children = []
@@ -134,13 +145,15 @@ class IndexTree:
         self.linear_index = -1
         self.size = -1
 
-    def add(self, index):
+    def add(self, index, wildcards=False):
         """IndexTree::add (IndexTree.cpp:166-306), with its error checks
         raised as ValueError."""
         flat = _flatten(index)
-        for v in flat:
-            if v is not None and v < 0:
-                raise ValueError(f"index {tuple(index)}: wildcard subindices are not supported")
+        if not wildcards:
+            for v in flat:
+                if v is not None and v < 0:
+                    raise ValueError(f"index {tuple(index)}: wildcard subindices are not "
+                                     f"supported")
         self._add(flat, 0, index)
 
     def _add(self, flat, sub, index):
@@ -157,6 +170,18 @@ class IndexTree:
             if self.index_separator:
                 raise ValueError(f"index {index}: conflicting index separator at "
                                  f"subindex {sub}")
+            if v < 0:
+                if not self.wildcard_index:
+                    if self.children:
+                        raise ValueError(f"index {index}: wildcard at subindex {sub} where "
+                                         f"concrete indices were added")
+                    self.wildcard_index = True
+                    self.wildcard_type = v
+                if v != self.wildcard_type:
+                    raise ValueError(f"index {index}: another wildcard type at subindex {sub}")
+                v = 0
+            elif self.wildcard_index:
+                raise ValueError(f"index {index}: a wildcard was added at subindex {sub}")
             while len(self.children) <= v:
                 self.children.append(IndexTree())
             if self.index_included:
@@ -185,11 +210,15 @@ class IndexTree:
         return i
 
     def linear_index_of(self, index):
+        """IndexTree::getLinearIndex with SearchMode::MatchWildcards: a
+        wildcard node matches any subindex."""
         node = self
         for v in _flatten(index):
             if v is None:
                 continue
-            if v >= len(node.children):
+            if node.wildcard_index:
+                v = 0
+            if v < 0 or v >= len(node.children):
                 raise KeyError(index)
             node = node.children[v]
         if not node.index_included:
@@ -207,7 +236,8 @@ class IndexTree:
                     out.append(tuple(prefix))
                 return
             for n, c in enumerate(node.children):
-                walk(c, prefix + ([None] if node.index_separator else []) + [n])
+                v = node.wildcard_type if node.wildcard_index else n
+                walk(c, prefix + ([None] if node.index_separator else []) + [v])
 
         walk(self, [])
         return out
@@ -300,6 +330,65 @@ def ldos_json(indices, ldos, lower, upper):
     (PropertyExtractor/ChebyshevExpander.cpp:475-505)."""
     tree = _tree(indices)
     erp = _energy_resolved(tree, indices, ldos, lower, upper, np.float64, _datum_real, "0")
+    return dumps({"id": "LDOS", "energyResolvedProperty": erp})
+
+
+def _matches(pattern, index):
+    return len(pattern) == len(index) and all(
+        p < 0 or p == v for p, v in zip(pattern, index))
+
+
+def expand_patterns(patterns, model_indices):
+    """The concrete indices of the model that calculateLDOS(patterns)
+    computes, in the order it visits them: every model index that matches
+    a pattern (IDX_ALL and IDX_SUM_ALL match any value), in index-tree
+    order (PropertyExtractor::generateIndexTree,
+    Lib/src/PropertyExtractor/PropertyExtractor.cpp:323-420, with the
+    summation wildcards expanded).  model_indices: every index of the model
+    (its HoppingAmplitudeSet's basis), as tuples."""
+    pats = [tuple(int(v) for v in p) for p in patterns]
+    for p in pats:
+        for v in p:
+            if v < 0 and v not in (IDX_ALL, IDX_SUM_ALL):
+                raise ValueError(f"pattern {p}: only IDX_ALL and IDX_SUM_ALL wildcards are "
+                                 f"read here")
+    model = [tuple(int(v) for v in i) for i in model_indices]
+    tree = IndexTree()
+    for p in pats:
+        for idx in model:
+            if _matches(p, idx):
+                tree.add(idx)
+    tree.generate_linear_map()
+    return tree.indices()
+
+
+def ldos_json_patterns(patterns, model_indices, ldos, lower, upper):
+    """``Property::LDOS`` text of ``calculateLDOS(patterns)``
+    (PropertyExtractor/ChebyshevExpander.cpp:475-505): entries for the
+    patterns' matches with IDX_SUM_ALL subindices kept as wildcards
+    (generateIndexTree with keepSummationWildcards), and the LDOS of each
+    concrete index added into its entry in expand_patterns order, as the
+    reference's calculate() loop does (PropertyExtractor.h:856-900).
+    ldos: mapping from each index of expand_patterns to its LDOS [E]."""
+    pats = [tuple(int(v) for v in p) for p in patterns]
+    concrete = expand_patterns(pats, model_indices)
+    layout = IndexTree()
+    for p in pats:
+        for idx in concrete:
+            if _matches(p, idx):
+                layout.add(tuple(IDX_SUM_ALL if v == IDX_SUM_ALL else idx[m]
+                                 for m, v in enumerate(p)), wildcards=True)
+    layout.generate_linear_map()
+    if not concrete:
+        raise ValueError("the patterns match no index of the model")
+    E = np.asarray(ldos[concrete[0]]).size
+    win = _window(lower, upper, E)
+    data = np.zeros((layout.size, E))
+    for idx in concrete:
+        row = layout.linear_index_of(idx)
+        data[row] += np.asarray(ldos[idx], dtype=np.float64)
+    erp = {"id": "EnergyResolvedProperty", "energyType": "Real", "energyWindow": win,
+           "abstractProperty": _abstract(layout, E, data.reshape(-1), _datum_real, "0")}
     return dumps({"id": "LDOS", "energyResolvedProperty": erp})
 
 

@@ -81,6 +81,18 @@ def export_case(ref):
         m.property_json(2, s, M, bro, lo, hi, res, dsites, T=T, mu=mu)[0])
     out["density"] = np.array([m.prop(1, s, M, bro, lo, hi, res, T, mu, list(d))
                                for d in dsites])
+    # wildcard patterns of calculateLDOS(patterns) (IDX_ALL expands,
+    # IDX_SUM_ALL sums), with the LDOS of every model index for the sums
+    from tbtk_b200 import export as X
+    S, A = X.IDX_SUM_ALL, X.IDX_ALL
+    every = [tuple(int(v) for v in np.unravel_index(b, lat.shape)) for b in range(lat.num_states)]
+    out["pat_ldos_all"] = m.ldos(s, 128, bro, lo, 3.9, 20, every)
+    out["pat_window"] = np.array([lo, 3.9, 20])
+    pattern_sets = [[(2, 3, S)], [(A, 1, 0)], [(2, 3, S), (A, 1, 0)], [(4, S, S)], [(S, S, 1)]]
+    out["pat_count"] = np.array(len(pattern_sets))
+    for k, pats in enumerate(pattern_sets):
+        out[f"pat_patterns_{k}"] = np.array(pats, dtype=np.int32)
+        out[f"pat_text_{k}"] = np.array(m.property_json(0, s, 128, bro, lo, 3.9, 20, pats)[0])
     lat = L.honeycomb(6, 5, t=1.0, J=0.3, W=1.5, periodic=True, seed=5)
     m = ref.model(lat)
     hsites = [(2, 2, 0, 0), (5, 4, 1, 1), (0, 1, 1, 0)]

@@ -82,6 +82,68 @@ def test_oracle_results_export_as_reference(oracle):
     assert X.greens_function_json(to, frm, gf, lo, hi) == str(g["gf_text_1"])
 
 
+def _every_index(shape):
+    return [tuple(int(v) for v in np.unravel_index(b, shape)) for b in range(int(np.prod(shape)))]
+
+
+def test_pattern_ldos_text_equals_reference():
+    """calculateLDOS(patterns) with IDX_ALL and IDX_SUM_ALL: the entries, the
+    wildcard nodes of the index tree and the sums over IDX_SUM_ALL give the
+    reference's text."""
+    g = golden("export")
+    lo, hi, _ = _window(g, "pat_window")
+    shape = (6, 5, 2)
+    every = _every_index(shape)
+    table = {idx: g["pat_ldos_all"][b] for b, idx in enumerate(every)}
+    for k in range(int(g["pat_count"])):
+        pats = _tuples(g[f"pat_patterns_{k}"])
+        got = X.ldos_json_patterns(pats, every, table, lo, hi)
+        assert got == _ref_text(g[f"pat_text_{k}"]), pats
+
+
+def test_pattern_ldos_from_oracle(oracle):
+    """The same texts from the oracle's LDOS at the expanded indices."""
+    g = golden("export")
+    lo, hi, res = _window(g, "pat_window")
+    lat = L.square(6, 5, t=1.0, J=0.5, W=2.0, alpha=0.3, periodic=True, seed=11)
+    rowptr, col, val = lat.csr()
+    s, M, bro = 8.0, 128, 1e-3
+    table = oracle.lookup_table(M, oracle.range(lo, hi, res), s)
+    every = _every_index(lat.shape)
+    for k in (0, 2, 3):
+        pats = _tuples(g[f"pat_patterns_{k}"])
+        ldos = {}
+        for idx in X.expand_patterns(pats, every):
+            b = lat.basis(idx)
+            mu = oracle.damp(oracle.moments(rowptr, col, val, s, M, b, [b]), bro)
+            ldos[idx] = oracle.ldos_table(table, mu[0])
+        assert X.ldos_json_patterns(pats, every, ldos, lo, hi) == _ref_text(g[f"pat_text_{k}"])
+
+
+def test_pattern_expansion_and_errors():
+    every = _every_index((3, 2, 2))
+    S, A = X.IDX_SUM_ALL, X.IDX_ALL
+    assert X.expand_patterns([(1, S, 0)], every) == [(1, 0, 0), (1, 1, 0)]
+    assert X.expand_patterns([(A, 1, 1), (0, 1, 1)], every) == [(0, 1, 1), (1, 1, 1), (2, 1, 1)]
+    tree = X.IndexTree()
+    tree.add((1, S, 0), wildcards=True)
+    tree.generate_linear_map()
+    assert tree.linear_index_of((1, 1, 0)) == 0 and tree.indices() == [(1, S, 0)]
+    with pytest.raises(ValueError, match="wildcard"):
+        X.expand_patterns([(1, -1610612739, 0)], every)  # IDX_SPIN
+    with pytest.raises(ValueError, match="match no index"):
+        X.ldos_json_patterns([(5, 0, 0)], every, {}, -1.0, 1.0)
+    t = X.IndexTree()
+    t.add((1, 0, 0))
+    with pytest.raises(ValueError, match="wildcard"):
+        t.add((1, S, 0), wildcards=True)
+    # a summed and a concrete entry under the same subindex: TBTK's
+    # IndexTree::add rejects the pair (and exits)
+    with pytest.raises(ValueError, match="wildcard"):
+        X.ldos_json_patterns([(2, S, S), (A, 0, 1)], every,
+                             {i: np.zeros(3) for i in every}, -1.0, 1.0)
+
+
 def test_reference_reads_exported_text(reference):
     """TBTK's Property::LDOS, EnergyResolvedProperty<complex<double>> and
     Property::Density constructors read the exported text and serialize
@@ -101,6 +163,12 @@ def test_reference_reads_exported_text(reference):
     dens = rng.random(4)
     text = X.density_json(sites, dens)
     back, values = reference.reserialize(2, text, 4)
+    assert back == text
+    every = _every_index((4, 3, 2))
+    table = {idx: rng.random(6) for idx in every}
+    text = X.ldos_json_patterns([(2, X.IDX_SUM_ALL, X.IDX_SUM_ALL), (1, X.IDX_ALL, 1)], every,
+                                table, -1.0, 1.0)
+    back, values = reference.reserialize(0, text, 4 * 6)
     assert back == text
 
 
