@@ -187,6 +187,12 @@ def test_loads_round_trip():
     assert r["kind"] == "GreensFunction"
     assert r["indices"] == [(0, 3, 0, None, 1, 1, 1), (2, 0, 1, None, 1, 1, 1)]
     np.testing.assert_allclose(r["data"], gf[[1, 0]], rtol=2e-5)
+    every = _every_index((3, 2, 2))
+    table = {idx: np.full(4, 0.125 * (1 + sum(idx))) for idx in every}
+    r = X.loads(X.ldos_json_patterns([(1, X.IDX_SUM_ALL, 0), (2, 1, 1)], every, table,
+                                     -1.0, 1.0))
+    assert r["indices"] == [(1, X.IDX_SUM_ALL, 0), (2, 1, 1)]
+    np.testing.assert_allclose(r["data"][:, 0], [0.25 + 0.375, 0.625])
     r = X.loads(X.density_json(sites, [0.25, 0.5, 0.75]))
     assert r["kind"] == "Density" and r["energies"] is None
     np.testing.assert_allclose(r["data"][:, 0], [0.5, 0.75, 0.25])
