@@ -122,6 +122,55 @@ def test_ring_ldos_integrates_to_one(oracle):
         assert abs(ldos.sum() * (E[1] - E[0]) - 1) < 1e-3
 
 
+def _smooth_gaussian(data, sigma, window, lower, upper):
+    """Smooth::gaussian of an LDOS block: sigma in energy units scaled to
+    bins, weights normalised over the whole window, truncated at the edges
+    (Lib/include/Utilities/TBTK/Smooth.h:86-134,237-269)."""
+    R = data.size
+    s = sigma / (upper - lower) * R
+    half = window // 2
+    norm = 1.0 / sum(np.exp(-n * n / (2 * s * s)) for n in range(-half, half + 1))
+    out = np.zeros(R)
+    for n in range(R):
+        c = np.arange(max(0, n - half), min(n + half + 1, R))
+        out[n] = (data[c] * np.exp(-(c - n) ** 2 / (2 * s * s))).sum() * norm
+    return out
+
+
+def test_ring_ldos_matches_exact_diagonalization(oracle):
+    """calculateLDOS1 (Test/include/TBTK/Test/PropertyExtractor/
+    ChebyshevExpander.h:47-104): on the 10-site ring the KPM LDOS at site 0
+    (s = 10, the Solver's default M = 1000 and broadening 1e-6, window
+    Range(-2.5, 2.5, 1000)) and the exact one agree within 10 % after both
+    pass Smooth::gaussian(sigma 0.3, window 1001).  The exact LDOS puts
+    |u_n(0)|^2 / dE of every eigenvalue strictly inside the window into bin
+    round((E_n - E_0)/dE), as the Diagonalizer's LDOS callback does
+    (Lib/src/PropertyExtractor/Diagonalizer.cpp:594-619); numpy's eigh
+    stands in for its LAPACK solver."""
+    g = golden("ring")
+    lo, hi, R = -2.5, 2.5, 1000
+    E = tbtk_range(lo, hi, R)
+    mu = oracle.damp(oracle.moments(g["rowptr"], g["col"], g["val"], 10.0, 1000, 0, [0]), 1e-6)
+    kpm = oracle.ldos_table(oracle.lookup_table(1000, E, 10.0), mu[0])
+    N = g["rowptr"].size - 1
+    H = np.zeros((N, N), dtype=np.complex128)
+    for r in range(N):
+        for k in range(g["rowptr"][r], g["rowptr"][r + 1]):
+            H[r, g["col"][k]] += g["val"][k]
+    w, v = np.linalg.eigh(H)
+    dE = E[1] - E[0]
+    exact = np.zeros(R)
+    for n in range(N):
+        if E[0] < w[n] < E[-1]:
+            e = int(np.floor((w[n] - E[0]) / dE + 0.5))  # C round(), argument >= 0
+            if 0 <= e < R:
+                exact[e] += abs(v[0, n]) ** 2 / dE
+    a = _smooth_gaussian(kpm, 0.3, 1001, lo, hi)
+    b = _smooth_gaussian(exact, 0.3, 1001, lo, hi)
+    assert np.all(np.abs(a - b) <= 0.1 * (a + b)), np.max(np.abs(a - b) / (a + b))
+    assert abs(exact.sum() * dE - 1) < 1e-9  # every eigenvalue of the ring lies in the window
+
+
 def test_range_matches_reference(reference):
     for args in [(-1, 1, 1000, True, True), (-10, 10, 1000, False, False),
                  (-9.5, 9.5, 37, False, True), (-0.1, 0.2, 10, True, False)]:
