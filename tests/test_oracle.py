@@ -43,6 +43,20 @@ def test_oracle_csr_from_triplets(oracle, name):
     assert np.array_equal(val, g["val"])
 
 
+def test_sparse_matrix_known_answer(oracle):
+    """HoppingAmplitudeSet.getSparseMatrix (Test/include/Core/TBTK/Test/
+    HoppingAmplitudeSet.h:494-541): amplitudes 1..5 from {0},{1},{2},{3},{4}
+    to {1},{0},{2},{4},{3} give one entry per column, row = to and column =
+    from; the same matrix as CSR, the layout this path reads."""
+    to = np.array([1, 0, 2, 4, 3], dtype=np.uint32)
+    frm = np.array([0, 1, 2, 3, 4], dtype=np.uint32)
+    amp = np.array([1, 2, 3, 4, 5], dtype=np.complex128)
+    rowptr, col, val = oracle.csr_from_triplets(to, frm, amp)
+    assert rowptr.tolist() == [0, 1, 2, 3, 4, 5]
+    assert col.tolist() == [1, 0, 2, 4, 3]
+    assert val.tolist() == [2, 1, 3, 5, 4]
+
+
 @pytest.mark.parametrize("name", MODEL_CASES)
 def test_oracle_moments_bit_exact(oracle, name):
     g = golden(name)
