@@ -12,7 +12,9 @@ benchmark configurations:
    2000 energies on the open grid (-12, 12).
 3. ``cfg3``  1024x1024 periodic square with spin + Rashba alpha=0.3, J=0.5,
    disorder U[-1, 1] (N = 2,097,152, 9 entries per row), s=12, M=2048,
-   256 seeded sites as one SpMM batch, 1000 energies.
+   256 seeded sites in one tbtkkpm_ldos_sites call, 1000 energies (the
+   library runs doubling calls as SpMM batches of 128 sources; a batch width
+   of 256 runs them as one).
 4. ``cfg4``  uneven batch of seeded models (square or honeycomb, L in
    [16, 256], J in [0, 1], W in [0, 3]) with 1-32 sites and M in
    {512, 1024, 2048, 4096}, s=12, 1000 energies.
