@@ -96,7 +96,9 @@ typedef struct tbtkkpm_table tbtkkpm_table;
  * entries.  The values are scaled on the device exactly as
  * calculateCoefficientsCPU scales them (`*= 1/scaleFactor` then `*= 2`,
  * Lib/src/Solver/ChebyshevExpander.cpp:147,168) and stored in sliced ELL.
- * scale must be > 0 (ChebyshevExpander.h:394-403). */
+ * scale must be > 0 (ChebyshevExpander.h:394-403).  A NaN or infinite
+ * value is rejected with TBTKKPM_ERR_ARGUMENT before any device work (the
+ * reference accepts it and returns NaN moments). */
 TBTKKPM_API int tbtkkpm_matrix_create_csr(
 	const uint32_t *rowptr, const uint32_t *col, const double *val,
 	uint32_t N, double scale, tbtkkpm_matrix **out);

@@ -361,6 +361,9 @@ extern "C" int tbtkkpm_matrix_create_csr(const uint32_t *rowptr, const uint32_t 
       if (k > rowptr[r] && col[k] <= col[k - 1])
         return fail(TBTKKPM_ERR_ARGUMENT,
                     "matrix_create_csr: columns of row %u not strictly ascending", r);
+      if (!std::isfinite(val[2 * (uint64_t)k]) || !std::isfinite(val[2 * (uint64_t)k + 1]))
+        return fail(TBTKKPM_ERR_ARGUMENT,
+                    "matrix_create_csr: value of row %u, column %u is not finite", r, col[k]);
     }
   tbtkkpm_matrix *m = nullptr;
   int rc = matrix_alloc(N, nnz, scale, &m);
@@ -405,11 +408,15 @@ extern "C" int tbtkkpm_matrix_create_triplets(const uint32_t *rows, const uint32
                 "matrix_create_triplets: the scaleFactor=%g has to be larger than 0", scale);
   if (n && (!rows || !cols || !vals))
     return fail(TBTKKPM_ERR_ARGUMENT, "matrix_create_triplets: NULL arrays");
-  for (uint64_t i = 0; i < n; i++)
+  for (uint64_t i = 0; i < n; i++) {
     if (rows[i] >= N || cols[i] >= N)
       return fail(TBTKKPM_ERR_ARGUMENT,
                   "matrix_create_triplets: entry %llu (%u, %u) outside the %u x %u basis",
                   (unsigned long long)i, rows[i], cols[i], N, N);
+    if (!std::isfinite(vals[2 * i]) || !std::isfinite(vals[2 * i + 1]))
+      return fail(TBTKKPM_ERR_ARGUMENT, "matrix_create_triplets: value of entry %llu is not finite",
+                  (unsigned long long)i);
+  }
   int ndev = 0;
   tbtkkpm_device_count(&ndev);
   if (ndev == 0) return fail(TBTKKPM_ERR_CUDA, "no CUDA device available");

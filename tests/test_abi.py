@@ -52,6 +52,14 @@ def test_argument_errors_return_status(kpm):
     with pytest.raises(kpm.TBTKError) as e:
         kpm.Table.create(10, np.array([-10.0, 0.0]), 10.0)
     assert e.value.status == kpm.ERR_ARGUMENT
+    for bad in (np.nan, np.inf):
+        with pytest.raises(kpm.TBTKError) as e:
+            kpm.Matrix.from_csr(rowptr, col, np.array([1.0, complex(0.5, bad)]), 10.0)
+        assert e.value.status == kpm.ERR_ARGUMENT and "not finite" in str(e.value)
+        with pytest.raises(kpm.TBTKError) as e:
+            kpm.Matrix.from_triplets(np.array([0, 1]), np.array([1, 0]),
+                                     np.array([bad, 1.0], dtype=np.complex128), 2, 10.0)
+        assert e.value.status == kpm.ERR_ARGUMENT and "not finite" in str(e.value)
     lib = kpm.load_library()
     assert lib.tbtkkpm_matrix_set_batch_width(None, kpm.MIXED, 64) == kpm.ERR_ARGUMENT
     assert lib.tbtkkpm_matrix_set_batch_width(None, 7, 64) == kpm.ERR_ARGUMENT
