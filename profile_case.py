@@ -1,7 +1,8 @@
-"""One small LDOS batch of the KPM path, for profiler captures and sweeps.
+"""One small LDOS batch of the KPM path, for profiler captures and sweeps (a
+measurement tool beside bench.py; the commands in profiles/ run it).
 
-    python -m tbtk_b200.profile_case --lattice 2048 --sites 1 --precision fp64 --moments 8
-    python -m tbtk_b200.profile_case --lattice 2048 --sites 64 --sweep --moments 32
+    python profile_case.py --lattice 2048 --sites 1 --precision fp64 --moments 8
+    python profile_case.py --lattice 2048 --sites 64 --sweep --moments 32
 
 Builds the periodic square lattice with spin (L x L x 2 states, t=1, J=0.5,
 disorder U[-1, 1]; Rashba spin-orbit with --rashba), a device lookup table
@@ -20,7 +21,11 @@ from __future__ import annotations
 import argparse
 import time
 
-from tbtk_b200 import kpm, workloads
+import pathlib
+import sys
+
+sys.path.insert(0, str(pathlib.Path(__file__).resolve().parent))
+from tbtk_b200 import kpm, workloads  # noqa: E402
 
 
 def step_bytes(N, nnz, B, s_vec, s_val=16):
@@ -62,7 +67,11 @@ def main():
         mat.set_batch_width(prec, a.batch_width)
     real = prec != kpm.FP64 and mat.real()[1]
     s_vec = 16 if prec == kpm.FP64 else (4 if real else 8)
-    bstep = step_bytes(N, nnz, a.sites, s_vec, 8 if real else 16)
+    # a call runs its sites in batches of the handle's width, each batch the
+    # same number of steps: the mean algorithmic bytes of one launch
+    width = mat.batch_width(prec, ldos=True)
+    batches = [min(width, a.sites - b0) for b0 in range(0, a.sites, width)]
+    bstep = sum(step_bytes(N, nnz, b, s_vec, 8 if real else 16) for b in batches) / len(batches)
 
     def run(label):
         for _ in range(a.repeat):

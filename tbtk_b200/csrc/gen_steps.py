@@ -117,6 +117,35 @@ REAL_DOTS_OPTS = {
     (16, 8): [(2, 8)], (8, 8): [(2, 8), (3, 8)], (4, 16): [(2, 8)],
     (1, 16): [(2, 8)], (2, 16): [(2, 8)], (8, 16): [(2, 8)], (16, 16): [(2, 8)],
 }
+# Tile-staged steps (kpm_tiled.cuh): (threads per row, values per thread)
+# shapes with (rows per tile, consumer warps, blocks per SM) variants.  Rows
+# of real floats are staged with 16-byte chunks, so a thread holds 4 or 8
+# values.
+TILED_VARIANTS = [(32, 8, 1), (64, 8, 1), (32, 8, 2), (16, 8, 2)]
+TILED_VARIANTS_WIDE = TILED_VARIANTS + [(16, 4, 2), (16, 4, 3), (16, 4, 4), (32, 4, 2), (32, 4, 3),
+                                        (64, 16, 1), (32, 16, 1)]
+TILED_REAL = {(4, 4): TILED_VARIANTS, (8, 4): TILED_VARIANTS, (16, 4): TILED_VARIANTS_WIDE,
+              (8, 8): TILED_VARIANTS_WIDE, (32, 4): TILED_VARIANTS, (16, 8): TILED_VARIANTS,
+              (32, 8): TILED_VARIANTS}
+TILED_CPLX_VARIANTS = [(16, 8, 1), (32, 8, 1), (16, 8, 2), (32, 8, 2)]
+TILED_CPLX_WIDE = TILED_CPLX_VARIANTS + [(16, 4, 2), (16, 4, 3), (16, 16, 1), (32, 16, 1)]
+TILED_CPLX = {(8, 2): TILED_CPLX_VARIANTS, (8, 4): TILED_CPLX_VARIANTS,
+              (16, 4): TILED_CPLX_VARIANTS, (32, 2): TILED_CPLX_VARIANTS,
+              (32, 4): TILED_CPLX_WIDE, (16, 8): TILED_CPLX_WIDE, (64, 4): TILED_CPLX_VARIANTS}
+
+
+def tiled_lines(cls, cplx, dots):
+    shapes = TILED_CPLX if cplx else TILED_REAL
+    out = []
+    for (t, p), variants in shapes.items():
+        for (r, cw, bps) in variants:
+            if (cw * 32) % t:
+                continue
+            c = "true" if cplx else "false"
+            out.append(f"    TBTKKPM_TILED_ENTRY({cls}, {c}, {t}, {p}, {dots}, {r}, {cw}, {bps}),")
+    return out
+
+
 REAL_UNITS = [
     ("steps_real.cu", "kStepsMixedReal", "kClassMixedReal", "false",
      "Recursion steps on real float vectors of a real matrix with FP64 arithmetic."),
@@ -140,6 +169,7 @@ def write_real():
             for (t, p), variants in REAL_DOTS_OPTS.items():
                 for mb, opt in variants:
                     lines.append(f"    TBTKKPM_REAL_ENTRY_OPT({cls}, {t}, {p}, {dots}, {mb}, {opt}),")
+        lines += tiled_lines(cls, False, dots)
         lines += ["};", f"const int kNum{table[1:]} = sizeof({table}) / sizeof({table}[0]);", "",
                   "}  // namespace tbtkkpm", ""]
         (HERE / fname).write_text("\n".join(lines))
@@ -160,6 +190,7 @@ def main():
                 if bulk_smem(V, p, s, wpb, dots) <= SMEM_LIMIT:
                     lines.append(f"    TBTKKPM_BULK_ENTRY({cls}, {V}, {AR}, {p}, {dots}, {s}, {wpb}),")
         if V == "float2":
+            lines += tiled_lines(cls, True, dots)
             for p in ASYNC_VPT:
                 for s in ASYNC_STAGES:
                     for wmax in ASYNC_WMAX:

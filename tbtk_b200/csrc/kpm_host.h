@@ -74,6 +74,31 @@ struct Workspace {
   }
 };
 
+// Per-tile gather plan of a matrix for tiles of R consecutive rows, read
+// by the tile-staged steps (kpm_tiled.cuh).
+struct TilePlan {
+  const uint4 *hdr;        // [ntiles] {ent_begin, run_begin, nuniq, w | nruns << 16}
+  const uint2 *runs;       // {first column, slot_start << 16 | length}
+  const uint16_t *eslot;   // [chunks][R] shared-memory slot of each entry's column
+  const void *eval;        // [chunks][R] value (double for real, double2 for complex)
+  uint32_t N, ntiles, R;
+  uint32_t umax, wmax;     // most distinct outside columns / entries per row of a tile
+};
+
+// A plan and its device arrays; ok is false when some tile has more entries
+// than the builder sorts in shared memory.
+struct TilePlanStore {
+  bool ok = false;
+  TilePlan plan{};
+  DevBuf hdr, runs, eslot, eval;
+  void release() {
+    hdr.release();
+    runs.release();
+    eslot.release();
+    eval.release();
+  }
+};
+
 }  // namespace tbtkkpm
 
 struct tbtkkpm_matrix {
@@ -106,8 +131,12 @@ struct tbtkkpm_matrix {
   // autotuned step configuration per (kernel class, padded batch width):
   // {threads per row, values per thread, min blocks per SM}
   std::map<uint64_t, std::array<int, 3>> tuned;
+  // tile plans by (rows per tile, complex values): key 2*R + complex
+  std::map<int, tbtkkpm::TilePlanStore> plans;
   std::mutex lock;
   void release_all() {
+    for (auto &p : plans) p.second.release();
+    plans.clear();
     rowptr.release();
     col.release();
     val2.release();
@@ -147,5 +176,8 @@ void damping_factors(uint32_t M, double broadening, std::vector<double> &a, doub
 // Error estimate of doubled moments against the directly gathered ones.
 void doubling_error(const std::vector<double2> &mu, const std::vector<double2> &direct,
                     uint32_t K, uint32_t M, uint32_t ld, double *err);
+// The matrix's gather plan for R-row tiles (real or complex values), built
+// on first use; *out is null when some tile is too large for the builder.
+int tile_plan(tbtkkpm_matrix *m, int R, bool cplx, const TilePlan **out);
 
 }  // namespace tbtkkpm

@@ -7,6 +7,7 @@
 #include "kpm_async.cuh"
 #include "kpm_bulk.cuh"
 #include "kpm_real.cuh"
+#include "kpm_tiled.cuh"
 #include "kpm_host.h"
 #include "kpm_kernels.cuh"
 
@@ -33,6 +34,7 @@ struct StepArgs {
   uint32_t n_out;
   double2 *dots;
   int *err;  // device flag set by a bounded wait that ran out (bulk kernels)
+  const TilePlan *plan = nullptr;  // tile-staged steps: the matrix's plan for their R
 };
 
 // Launches one step with a grid of min(tiles, resident blocks, max_grid)
@@ -175,6 +177,54 @@ void launch_async(cudaStream_t st, int device, unsigned max_grid, const StepArgs
 #define TBTKKPM_ASYNC_ENTRY(CLS, P, D, S, WMAX, WPB)                                \
   {CLS, 32, P, 10000 + 1000 * S + 10 * WMAX + WPB,                                 \
    &launch_async<P, true, D, S, WMAX, WPB>, &launch_async<P, false, D, S, WMAX, WPB>}
+
+// Shared memory a tile-staged block may use with BPS blocks per SM (the SM
+// has 228 KB; each block reserves 1 KB; one block may take at most 227 KB).
+constexpr uint32_t tiled_budget(int bps) {
+  return bps <= 1 ? 232448u : 233472u / (uint32_t)bps - 1024u;
+}
+
+// Tile-staged step variants: 100000 + 1000*R + 10*CW + BPS (R rows per
+// tile, CW consumer warps, BPS blocks per SM).
+constexpr int kTiledVariant = 100000;
+inline bool is_tiled_variant(int v) { return v >= kTiledVariant; }
+inline int tiled_rows(int v) { return (v - kTiledVariant) / 1000; }
+inline int tiled_bps(int v) { return v % 10; }
+
+template <bool CPLX, int TPR, int VPT, int R, int CW, int BPS, bool FIRST, bool DOTS>
+void launch_tiled(cudaStream_t st, int device, unsigned max_grid, const StepArgs &a,
+                  unsigned *grid) {
+  using E = typename TiledTypes<CPLX>::E;
+  using Val = typename TiledTypes<CPLX>::Val;
+  auto kern = kpm_step_tiled<CPLX, TPR, VPT, R, CW, BPS, FIRST, DOTS>;
+  *grid = 0;
+  if (!a.plan || a.plan->R != (uint32_t)R) return;
+  const TilePlan &p = *a.plan;
+  const TiledLayout ly =
+      tiled_layout(p, a.Bp * (uint32_t)sizeof(E), (uint32_t)sizeof(Val), tiled_budget(BPS));
+  if (ly.stages == 0) return;
+  static bool attr[64] = {false};
+  const int d = device & 63;
+  if (!attr[d]) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tiled_budget(BPS));
+    attr[d] = true;
+  }
+  uint64_t g = std::min<uint64_t>(p.ntiles, (uint64_t)BPS * sm_count(device));
+  if (max_grid) g = std::min<uint64_t>(g, max_grid);
+  g = std::max<uint64_t>(g, 1);
+  *grid = (unsigned)g;
+  // the ring holds the block's dot-product reduction at the end (2 doubles
+  // per consumer thread)
+  const uint32_t smem = kTiledHeader + std::max(ly.stages * ly.stage_bytes, 32u * CW * 16u);
+  kern<<<(unsigned)g, 32 * (CW + 1), smem, st>>>(
+      p, ly, a.Bp, static_cast<const E *>(a.x), static_cast<E *>(a.y), a.tg, a.n_out, a.dots,
+      a.err, kWaitLimit);
+}
+
+#define TBTKKPM_TILED_ENTRY(CLS, CPLX, T, P, D, R, CW, BPS)                         \
+  {CLS, T, P, kTiledVariant + 1000 * R + 10 * CW + BPS,                              \
+   &launch_tiled<CPLX, T, P, R, CW, BPS, true, D>,                                   \
+   &launch_tiled<CPLX, T, P, R, CW, BPS, false, D>}
 
 extern const StepEntry kStepsFP64[];
 extern const int kNumStepsFP64;

@@ -165,6 +165,34 @@ const StepEntry *pick_step(const tbtkkpm_matrix *m, int precision, bool dots, ui
   return find_step(cls, s.tpr, s.vpt, s.minb);
 }
 
+// A tile-staged entry runs with the matrix's plan for its tile height when
+// a ring of at least two stages fits its shared memory.  Otherwise a forced
+// entry is refused (TBTKKPM_ERR_UNSUPPORTED, which the autotuner skips) and
+// a chosen one gives way to the register-staged default of the batch.
+int resolve_tiled(tbtkkpm_matrix *m, int precision, bool dots, uint32_t B, bool forced,
+                  const StepEntry *&fn, const TilePlan *&plan) {
+  plan = nullptr;
+  if (!fn || !is_tiled_variant(fn->minb)) return TBTKKPM_OK;
+  const bool cplx = !(fn->cls == kClassMixedReal || fn->cls == kClassMixedRealDots);
+  const TilePlan *p = nullptr;
+  int rc = tile_plan(m, tiled_rows(fn->minb), cplx, &p);
+  if (rc) return rc;
+  const uint32_t esz = cplx ? sizeof(float2) : sizeof(float);
+  const uint32_t vsz = cplx ? sizeof(double2) : sizeof(double);
+  if (p && tiled_layout(*p, (uint32_t)(fn->tpr * fn->vpt) * esz, vsz,
+                        tiled_budget(tiled_bps(fn->minb))).stages) {
+    plan = p;
+    return TBTKKPM_OK;
+  }
+  if (forced)
+    return fail(TBTKKPM_ERR_UNSUPPORTED,
+                "recursion: the tile-staged step %d x %d / %d does not fit this matrix", fn->tpr,
+                fn->vpt, fn->minb);
+  const Shape s = shape_for(precision, B, !cplx, dots);
+  fn = find_step(fn->cls, s.tpr, s.vpt, s.minb);
+  return TBTKKPM_OK;
+}
+
 // ------------------------------------------------------------ one batch
 // The to-indices of a batch (row, batch column, output slot), sorted by row.
 struct TargetList {
@@ -185,6 +213,9 @@ int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &fro
   cudaStream_t st = m->stream;
   const uint32_t B = (uint32_t)from.size();
   const StepEntry *fn = pick_step(m, precision, doubling, B, force);
+  const TilePlan *plan = nullptr;
+  int rc0 = resolve_tiled(m, precision, doubling, B, force != nullptr, fn, plan);
+  if (rc0) return rc0;
   if (!fn) return fail(TBTKKPM_ERR_UNSUPPORTED, "no recursion kernel for batch %u", B);
   const uint32_t Bp = (uint32_t)(fn->tpr * fn->vpt);
   if (Bp < B) return fail(TBTKKPM_ERR_ARGUMENT, "configuration of %u columns for %u sources", Bp, B);
@@ -308,6 +339,7 @@ int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &fro
   a.tg = tg;
   a.dots = doubling ? ws.dots.as<double2>() : nullptr;
   a.err = ws.err.as<int>();
+  a.plan = plan;
   void *cur = ws.vec[0].ptr, *prev = ws.vec[1].ptr;
   m->timer.mark(st, 0);
   m->timer.pending = m->timer.enabled;
@@ -319,6 +351,8 @@ int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &fro
     a.n_out = n;
     unsigned grid = 0;
     (n == 1 ? fn->first : fn->rest)(st, m->device, max_grid, a, &grid);
+    if (grid == 0) return fail(TBTKKPM_ERR_UNSUPPORTED, "recursion: step %d x %d / %d not launched",
+                               fn->tpr, fn->vpt, fn->minb);
     std::swap(cur, prev);
     if (doubling) {
       if (n == 1) {
@@ -889,9 +923,17 @@ extern "C" int tbtkkpm_matrix_autotune(tbtkkpm_matrix *m, uint32_t B, int precis
   for (int i = 0; i < n; i++) {
     if ((uint32_t)(t[i].tpr * t[i].vpt) != Bp) continue;
     double ms = 0;
+    bool skip = false;
     for (int rep = 0; rep < 2; rep++) {
       m->timer.recursion_ms = 0;
-      if ((rc = run_batch(m, precision, fr, tl, B, M, doubling, &t[i], false))) break;
+      if ((rc = run_batch(m, precision, fr, tl, B, M, doubling, &t[i], false))) {
+        // a tile-staged step whose ring does not fit this matrix
+        if (rc == TBTKKPM_ERR_UNSUPPORTED && is_tiled_variant(t[i].minb)) {
+          rc = TBTKKPM_OK;
+          skip = true;
+        }
+        break;
+      }
       cudaError_t e = cudaStreamSynchronize(m->stream);
       if (e != cudaSuccess) {
         rc = cuda_fail(e, "matrix_autotune");
@@ -903,6 +945,7 @@ extern "C" int tbtkkpm_matrix_autotune(tbtkkpm_matrix *m, uint32_t B, int precis
       ms = rep == 0 ? v : std::min(ms, v);
     }
     if (rc) break;
+    if (skip) continue;
     if (!best || ms < best_ms) {
       best = &t[i];
       best_ms = ms;
