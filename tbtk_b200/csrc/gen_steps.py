@@ -118,31 +118,46 @@ REAL_DOTS_OPTS = {
     (1, 16): [(2, 8)], (2, 16): [(2, 8)], (8, 16): [(2, 8)], (16, 16): [(2, 8)],
 }
 # Tile-staged steps (kpm_tiled.cuh): (threads per row, values per thread)
-# shapes with (rows per tile, consumer warps, blocks per SM) variants.  Rows
-# of real floats are staged with 16-byte chunks, so a thread holds 4 or 8
-# values.
-TILED_VARIANTS = [(32, 8, 1), (64, 8, 1), (32, 8, 2), (16, 8, 2)]
-TILED_VARIANTS_WIDE = TILED_VARIANTS + [(16, 4, 2), (16, 4, 3), (16, 4, 4), (32, 4, 2), (32, 4, 3),
-                                        (64, 16, 1), (32, 16, 1)]
-TILED_REAL = {(4, 4): TILED_VARIANTS, (8, 4): TILED_VARIANTS, (16, 4): TILED_VARIANTS_WIDE,
-              (8, 8): TILED_VARIANTS_WIDE, (32, 4): TILED_VARIANTS, (16, 8): TILED_VARIANTS,
-              (32, 8): TILED_VARIANTS}
-TILED_CPLX_VARIANTS = [(16, 8, 1), (32, 8, 1), (16, 8, 2), (32, 8, 2)]
-TILED_CPLX_WIDE = TILED_CPLX_VARIANTS + [(16, 4, 2), (16, 4, 3), (16, 16, 1), (32, 16, 1)]
-TILED_CPLX = {(8, 2): TILED_CPLX_VARIANTS, (8, 4): TILED_CPLX_VARIANTS,
-              (16, 4): TILED_CPLX_VARIANTS, (32, 2): TILED_CPLX_VARIANTS,
-              (32, 4): TILED_CPLX_WIDE, (16, 8): TILED_CPLX_WIDE, (64, 4): TILED_CPLX_VARIANTS}
+# shapes with (rows per tile, consumer warps, blocks per SM, widening split
+# CV) variants.  Rows of real floats are staged with 16-byte chunks, so a
+# thread holds 4 or 8 values.  On the 2048^2 lattice at 64 columns (8, 8)
+# with 64-row tiles and 16 consumer warps took 1.46 ms per step, 32-row
+# tiles at two blocks per SM 1.60 ms, both with every widening on the XU
+# pipe (69% busy in the ncu capture); CV moves widenings to the integer pipe.
+def _variants(bases, cvs):
+    return [(r, cw, bps, cv) for (r, cw, bps) in bases for cv in cvs]
+
+
+TILED_REAL = {
+    (8, 8): _variants([(32, 8, 2), (64, 16, 1), (32, 4, 3), (16, 4, 4)], [0, 30, 50, 51]),
+    (16, 4): _variants([(32, 8, 2), (64, 16, 1)], [0, 51]),
+    (4, 4): _variants([(32, 8, 2), (64, 16, 1), (32, 4, 2)], [0, 51]),
+    (8, 4): _variants([(32, 8, 2), (64, 16, 1), (32, 4, 2)], [0, 51]),
+    (16, 8): _variants([(32, 8, 2), (64, 16, 1), (16, 8, 2)], [0, 51]),
+    (32, 4): _variants([(32, 8, 2), (64, 16, 1), (16, 8, 2)], [0, 51]),
+    (32, 8): _variants([(16, 8, 2), (32, 16, 1), (16, 16, 1)], [0, 51]),
+}
+TILED_CPLX = {
+    (32, 4): _variants([(16, 16, 1), (16, 8, 1), (8, 8, 1), (8, 8, 2)], [0, 40, 60, 90, 61]),
+    (16, 8): _variants([(16, 16, 1), (16, 8, 1), (8, 8, 1), (8, 8, 2)], [0, 60, 61]),
+    (64, 4): _variants([(8, 8, 1), (8, 16, 1)], [0, 60]),
+    (32, 8): _variants([(8, 8, 1), (8, 16, 1)], [0, 60]),
+    (16, 4): _variants([(16, 8, 1), (32, 8, 1), (16, 8, 2), (16, 4, 3)], [0, 60]),
+    (32, 2): _variants([(16, 8, 1), (16, 8, 2)], [0, 60]),
+    (8, 4): _variants([(16, 8, 2), (32, 8, 1), (32, 8, 2)], [0, 60]),
+    (8, 2): _variants([(32, 8, 2), (16, 8, 2)], [0, 60]),
+}
 
 
 def tiled_lines(cls, cplx, dots):
     shapes = TILED_CPLX if cplx else TILED_REAL
     out = []
     for (t, p), variants in shapes.items():
-        for (r, cw, bps) in variants:
+        for (r, cw, bps, cv) in variants:
             if (cw * 32) % t:
                 continue
             c = "true" if cplx else "false"
-            out.append(f"    TBTKKPM_TILED_ENTRY({cls}, {c}, {t}, {p}, {dots}, {r}, {cw}, {bps}),")
+            out.append(f"    TBTKKPM_TILED_ENTRY({cls}, {c}, {t}, {p}, {dots}, {r}, {cw}, {bps}, {cv}),")
     return out
 
 

@@ -184,19 +184,20 @@ constexpr uint32_t tiled_budget(int bps) {
   return bps <= 1 ? 232448u : 233472u / (uint32_t)bps - 1024u;
 }
 
-// Tile-staged step variants: 100000 + 1000*R + 10*CW + BPS (R rows per
-// tile, CW consumer warps, BPS blocks per SM).
+// Tile-staged step variants: 100000 + 1000000*CV + 1000*R + 10*CW + BPS
+// (CV the widening split of kpm_step_tiled, R rows per tile, CW consumer
+// warps, BPS blocks per SM).
 constexpr int kTiledVariant = 100000;
 inline bool is_tiled_variant(int v) { return v >= kTiledVariant; }
-inline int tiled_rows(int v) { return (v - kTiledVariant) / 1000; }
+inline int tiled_rows(int v) { return ((v - kTiledVariant) % 1000000) / 1000; }
 inline int tiled_bps(int v) { return v % 10; }
 
-template <bool CPLX, int TPR, int VPT, int R, int CW, int BPS, bool FIRST, bool DOTS>
+template <bool CPLX, int TPR, int VPT, int R, int CW, int BPS, bool FIRST, bool DOTS, int CV>
 void launch_tiled(cudaStream_t st, int device, unsigned max_grid, const StepArgs &a,
                   unsigned *grid) {
   using E = typename TiledTypes<CPLX>::E;
   using Val = typename TiledTypes<CPLX>::Val;
-  auto kern = kpm_step_tiled<CPLX, TPR, VPT, R, CW, BPS, FIRST, DOTS>;
+  auto kern = kpm_step_tiled<CPLX, TPR, VPT, R, CW, BPS, FIRST, DOTS, CV>;
   *grid = 0;
   if (!a.plan || a.plan->R != (uint32_t)R) return;
   const TilePlan &p = *a.plan;
@@ -221,10 +222,10 @@ void launch_tiled(cudaStream_t st, int device, unsigned max_grid, const StepArgs
       a.err, kWaitLimit);
 }
 
-#define TBTKKPM_TILED_ENTRY(CLS, CPLX, T, P, D, R, CW, BPS)                         \
-  {CLS, T, P, kTiledVariant + 1000 * R + 10 * CW + BPS,                              \
-   &launch_tiled<CPLX, T, P, R, CW, BPS, true, D>,                                   \
-   &launch_tiled<CPLX, T, P, R, CW, BPS, false, D>}
+#define TBTKKPM_TILED_ENTRY(CLS, CPLX, T, P, D, R, CW, BPS, CV)                     \
+  {CLS, T, P, kTiledVariant + 1000000 * CV + 1000 * R + 10 * CW + BPS,               \
+   &launch_tiled<CPLX, T, P, R, CW, BPS, true, D, CV>,                               \
+   &launch_tiled<CPLX, T, P, R, CW, BPS, false, D, CV>}
 
 extern const StepEntry kStepsFP64[];
 extern const int kNumStepsFP64;

@@ -77,6 +77,23 @@ __device__ __forceinline__ bool mbar_wait_limit(uint64_t *bar, uint32_t parity, 
   return false;
 }
 
+// Widening of a float to FP64 on the integer pipe: the float's exponent and
+// mantissa fields moved into the double's fields (shift right by 3, sign
+// kept by the arithmetic shift and a mask; the low 3 mantissa bits into the
+// low word) read the float's exponent bias 127 as the double's 1023, so the
+// double is x * 2^-896 exactly, for normal and subnormal floats alike (a
+// float subnormal becomes the double subnormal of the same scaled value),
+// and zero stays zero.  Infinite and NaN floats do not occur (finite matrix
+// values, |j_n| <= 1).  The recursion multiplies such a value by the entry
+// value scaled up by 2^896 (exact): the FMA's exact product equals v * x,
+// so the rounded result is the same as with a conversion instruction,
+// which runs on the 16-per-clock XU pipe.
+__device__ __forceinline__ double f2d_scaled(float x) {
+  const int b = __float_as_int(x);
+  return __hiloint2double((b >> 3) & (int)0x8fffffff, b << 29);
+}
+constexpr double kWideUp = 0x1p896;
+
 // Element type of a vector row and value type of an entry.
 template <bool CPLX> struct TiledTypes;
 template <> struct TiledTypes<false> {
@@ -93,7 +110,11 @@ template <> struct TiledTypes<true> {
 // producer; warps 1..CW consume.  Consumer thread `sub` of a TPR-thread
 // group owns VPT elements of its row (interleaved 16-byte chunks, as
 // RPack / Pack), and the CW*32/TPR groups take the tile's rows in passes.
-template <bool CPLX, int TPR, int VPT, int R, int CW, int BPS, bool FIRST, bool DOTS>
+// CV = 10*GA + PA splits the float -> FP64 widenings between the pipes:
+// the gathers of a row's first GA entries and, with PA, j_{n-1} and the
+// dot-product terms widen on the integer pipe (f2d_scaled), the rest by
+// conversion instructions.  Every choice gives the same stored vectors.
+template <bool CPLX, int TPR, int VPT, int R, int CW, int BPS, bool FIRST, bool DOTS, int CV = 0>
 __global__ void __launch_bounds__(32 * (CW + 1), BPS)
 kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
                const typename TiledTypes<CPLX>::E *__restrict__ x,
@@ -104,6 +125,8 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
   using Pk = typename std::conditional<CPLX, Pack<float2, TPR, VPT>, RPack<TPR, VPT>>::type;
   using L = typename Pk::L;
   constexpr int NL = Pk::NL;
+  constexpr int GA = CV / 10;
+  constexpr bool PA = CV % 10 != 0;
   constexpr int RPP = CW * 32 / TPR;  // rows per pass
   constexpr int PASSES = (R + RPP - 1) / RPP;
   static_assert(CW * 32 % TPR == 0, "a row group must divide the consumer threads");
@@ -229,8 +252,11 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
             Pk::load_rw(reinterpret_cast<const float2 *>(prev) + (size_t)lr * Bp, sub, yv);
 #pragma unroll
             for (int j = 0; j < VPT; j++) {
-              const double2 v = Pk::get(yv, j);
-              acc[j] = make_double2(-v.x, -v.y);
+              const float2 f = Pk::getf(yv, j);
+              if constexpr (PA)
+                acc[j] = make_double2(f2d_scaled(f.x) * -kWideUp, f2d_scaled(f.y) * -kWideUp);
+              else
+                acc[j] = make_double2(-(double)f.x, -(double)f.y);
             }
           }
           for (uint32_t k = 0; k < w; k++) {
@@ -240,8 +266,17 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
             if constexpr (FIRST) v = make_double2(v.x * 0.5, v.y * 0.5);
             L xr[NL];
             Pk::load_rw(reinterpret_cast<const float2 *>(xs) + (size_t)sl * Bp, sub, xr);
+            if (GA > 0 && k < (uint32_t)GA) {
+              const double2 vu = make_double2(v.x * kWideUp, v.y * kWideUp);
 #pragma unroll
-            for (int j = 0; j < VPT; j++) acc[j] = cmac<false>(acc[j], v, Pk::get(xr, j));
+              for (int j = 0; j < VPT; j++) {
+                const float2 f = Pk::getf(xr, j);
+                acc[j] = cmac<false>(acc[j], vu, make_double2(f2d_scaled(f.x), f2d_scaled(f.y)));
+              }
+            } else {
+#pragma unroll
+              for (int j = 0; j < VPT; j++) acc[j] = cmac<false>(acc[j], v, Pk::get(xr, j));
+            }
           }
           if ((bw[p] >> (row & 31)) & 1u) {
             for (uint32_t q = target_first(tg, row); q < tg.count && __ldg(tg.row + q) == row; q++) {
@@ -264,8 +299,10 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
 #pragma unroll
             for (int j = 0; j < VPT; j++) {
               const float2 b = Pk::getf(self, j);
-              d_nn[j] += (double)fmaf(af[j].x, af[j].x, af[j].y * af[j].y);
-              d_np[j] += (double)fmaf(af[j].x, b.x, af[j].y * b.y);
+              const float nn = fmaf(af[j].x, af[j].x, af[j].y * af[j].y);
+              const float np = fmaf(af[j].x, b.x, af[j].y * b.y);
+              d_nn[j] += PA ? f2d_scaled(nn) : (double)nn;
+              d_np[j] += PA ? f2d_scaled(np) : (double)np;
             }
           }
         } else {
@@ -277,7 +314,10 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
             L yv[NL];
             Pk::load_rw(reinterpret_cast<const float *>(prev) + (size_t)lr * Bp, sub, yv);
 #pragma unroll
-            for (int j = 0; j < VPT; j++) acc[j] = -(double)Pk::getf(yv, j);
+            for (int j = 0; j < VPT; j++) {
+              const float f = Pk::getf(yv, j);
+              acc[j] = PA ? f2d_scaled(f) * -kWideUp : -(double)f;
+            }
           }
           for (uint32_t k = 0; k < w; k++) {
             const uint16_t sl = slots[k * R + lr];
@@ -286,8 +326,14 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
             if constexpr (FIRST) v = v * 0.5;
             L xr[NL];
             Pk::load_rw(reinterpret_cast<const float *>(xs) + (size_t)sl * Bp, sub, xr);
+            if (GA > 0 && k < (uint32_t)GA) {
+              const double vu = v * kWideUp;
 #pragma unroll
-            for (int j = 0; j < VPT; j++) acc[j] = fma(v, (double)Pk::getf(xr, j), acc[j]);
+              for (int j = 0; j < VPT; j++) acc[j] = fma(vu, f2d_scaled(Pk::getf(xr, j)), acc[j]);
+            } else {
+#pragma unroll
+              for (int j = 0; j < VPT; j++) acc[j] = fma(v, (double)Pk::getf(xr, j), acc[j]);
+            }
           }
           if ((bw[p] >> (row & 31)) & 1u) {
             for (uint32_t q = target_first(tg, row); q < tg.count && __ldg(tg.row + q) == row; q++) {
@@ -310,8 +356,9 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
 #pragma unroll
             for (int j = 0; j < VPT; j++) {
               const float b = Pk::getf(self, j);
-              d_nn[j] += (double)fmaf(af[j], af[j], 0.0f);
-              d_np[j] += (double)fmaf(af[j], b, 0.0f);
+              const float nn = fmaf(af[j], af[j], 0.0f), np = fmaf(af[j], b, 0.0f);
+              d_nn[j] += PA ? f2d_scaled(nn) : (double)nn;
+              d_np[j] += PA ? f2d_scaled(np) : (double)np;
             }
           }
         }
@@ -329,8 +376,9 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
 #pragma unroll
     for (int j = 0; j < VPT; j++) {
       if (ct >= 0) {
-        red[2 * ct] = d_nn[j];
-        red[2 * ct + 1] = d_np[j];
+        // sums of terms widened on the integer pipe carry the 2^-896 scale
+        red[2 * ct] = PA ? d_nn[j] * kWideUp : d_nn[j];
+        red[2 * ct + 1] = PA ? d_np[j] * kWideUp : d_np[j];
       }
       __syncthreads();
       if (ct >= 0 && grp == 0) {

@@ -52,7 +52,8 @@ int build_plan(tbtkkpm_matrix *m, int R, bool cplx, TilePlanStore &p) {
       (e = cudaMemsetAsync(tw.as<uint32_t>() + ntiles, 0, 4, st)) ||
       (e = cudaMemsetAsync(truns.as<uint32_t>() + ntiles, 0, 4, st)))
     return cuda_fail(e, "tile plan: staging");
-  if (R == 16) rc = count_tiles<16>(st, m, ntiles, grid, tw, truns, tuniq, flags);
+  if (R == 8) rc = count_tiles<8>(st, m, ntiles, grid, tw, truns, tuniq, flags);
+  else if (R == 16) rc = count_tiles<16>(st, m, ntiles, grid, tw, truns, tuniq, flags);
   else if (R == 32) rc = count_tiles<32>(st, m, ntiles, grid, tw, truns, tuniq, flags);
   else if (R == 64) rc = count_tiles<64>(st, m, ntiles, grid, tw, truns, tuniq, flags);
   else return fail(TBTKKPM_ERR_UNSUPPORTED, "tile plan: no builder for %d rows per tile", R);
@@ -88,7 +89,8 @@ int build_plan(tbtkkpm_matrix *m, int R, bool cplx, TilePlanStore &p) {
 #define TBTKKPM_FILL(RR)                                                                      \
   (cplx ? fill_tiles<RR, true>(st, m, ntiles, grid, ent, run, tw, truns, tuniq, p)            \
         : fill_tiles<RR, false>(st, m, ntiles, grid, ent, run, tw, truns, tuniq, p))
-  if (R == 16) rc = TBTKKPM_FILL(16);
+  if (R == 8) rc = TBTKKPM_FILL(8);
+  else if (R == 16) rc = TBTKKPM_FILL(16);
   else if (R == 32) rc = TBTKKPM_FILL(32);
   else rc = TBTKKPM_FILL(64);
 #undef TBTKKPM_FILL
