@@ -153,22 +153,27 @@ TBTKKPM_API int tbtkkpm_moments(
 /* tbtkkpm_moments for callers that cannot allocate device memory (code
  * inside another framework's memory pool, or under a fixed device-memory
  * budget).  It allocates nothing: the matrix (CSR as for
- * tbtkkpm_matrix_create_csr, unscaled) and the output are the caller's
- * device buffers (d_to: K basis indices; d_mu_out: [K][M] complex, damped
- * as tbtkkpm_moments), and its scratch is a fixed 32 MiB array compiled into
- * the library, which every GPU that loads the library keeps until exit.
- * Sizes with 32*N + 8*M + 256 > 32 MiB are rejected (use tbtkkpm_moments).
- * The first call on a device looks the array up on the current device;
- * make it before any stream capture.  Calls share the array: each call
- * clears what it uses, and calls that overlap on the GPU race.  Work runs on
- * `stream` (NULL: the default stream) and the call returns when it is done.
- * Bad column or to indices found on the device return TBTKKPM_ERR_ARGUMENT.
- * (No counterpart in the reference.) */
+ * tbtkkpm_matrix_create_csr, unscaled: d_rowptr N+1 entries, d_col and
+ * d_val nnz entries) and the output are the caller's device buffers (d_to:
+ * K basis indices; d_mu_out: [K][M] complex, damped as tbtkkpm_moments), and
+ * its scratch is a fixed 32 MiB array compiled into the library, which a GPU
+ * holds from the first call there (when the library's device code loads)
+ * until the process exits.  Sizes with 32*N + 8*M + 256 > 32 MiB are
+ * rejected (use tbtkkpm_moments).  The first call on a device looks the
+ * array up on the current device and caches the address for the process; a
+ * cudaDeviceReset of that device invalidates it, so do not call this after
+ * resetting the device.  Calls share the array: each call clears what it
+ * uses, and calls that overlap on the GPU race.  Work runs on `stream`
+ * (NULL: the default stream); every call is synchronous (it copies host
+ * data and waits for the stream), so it cannot be captured into a CUDA
+ * graph.  The device checks d_rowptr first (rowptr[0] == 0, non-decreasing,
+ * rowptr[N] == nnz), then skips column and to indices >= N; any of these
+ * returns TBTKKPM_ERR_ARGUMENT.  (No counterpart in the reference.) */
 TBTKKPM_API int tbtkkpm_moments_noalloc(
 	const uint32_t *d_rowptr, const uint32_t *d_col, const double *d_val,
-	uint32_t N, double scale, uint32_t from, const uint32_t *d_to,
-	uint32_t K, uint32_t M, double broadening, double *d_mu_out,
-	void *stream);
+	uint32_t N, uint64_t nnz, double scale, uint32_t from,
+	const uint32_t *d_to, uint32_t K, uint32_t M, double broadening,
+	double *d_mu_out, void *stream);
 
 /* Batched moments: B source vectors (from[b]) advance together as one
  * SpMM-style recursion.  to[k] belongs to source to_owner[k]; mu_out is
@@ -277,6 +282,17 @@ TBTKKPM_API int tbtkkpm_matrix_step_configs(
  * head off.  tbtkkpm_matrix_fp64_head reports the setting and whether the
  * pattern allows a head.  (No reference counterpart.) */
 TBTKKPM_API int tbtkkpm_matrix_set_fp64_head(tbtkkpm_matrix *m, uint32_t steps);
+
+/* Bound of each wait of the tile-staged recursion steps on this handle for
+ * rows staged in shared memory (polls of the mbarrier; default
+ * TBTKKPM_WAIT_DEFAULT).  A wait that runs out ends the step early, its
+ * issued copies are waited for with the default bound, and the call returns
+ * TBTKKPM_ERR_TIMEOUT; the handle stays usable.  polls = 0 makes every
+ * such wait give up at once, which tests that path.  (No reference
+ * counterpart: the reference's device waits are unbounded,
+ * Lib/src/Utilities/GPUResourceManager.cpp:52-73.) */
+#define TBTKKPM_WAIT_DEFAULT 0xffffffffu
+TBTKKPM_API int tbtkkpm_matrix_set_wait_limit(tbtkkpm_matrix *m, uint32_t polls);
 TBTKKPM_API int tbtkkpm_matrix_fp64_head(
 	tbtkkpm_matrix *m, uint32_t *steps, int *pattern_symmetric);
 

@@ -121,6 +121,9 @@ struct tbtkkpm_matrix {
   // head_steps steps in FP64 on the rows those steps reach
   bool pattern_symmetric = false;
   uint32_t head_steps = 32;  // tbtkkpm_matrix_set_fp64_head (kPrefixSteps)
+  // tbtkkpm_matrix_set_wait_limit: polls per staged-row wait of the
+  // tile-staged steps (TBTKKPM_WAIT_DEFAULT: the library's bound)
+  uint32_t wait_limit = 0xffffffffu;
   // tbtkkpm_matrix_set_batch_width: sources per recursion batch, per
   // precision (0: the library's choice, batch_width_for in recursion.cu)
   uint32_t batch_width[3] = {0, 0, 0};

@@ -35,6 +35,7 @@ struct StepArgs {
   double2 *dots;
   int *err;  // device flag set by a bounded wait that ran out (bulk kernels)
   const TilePlan *plan = nullptr;  // tile-staged steps: the matrix's plan for their R
+  uint32_t wait_limit = kWaitLimit;  // polls per staged-row wait (tile-staged steps)
 };
 
 // Launches one step with a grid of min(tiles, resident blocks, max_grid)
@@ -219,7 +220,7 @@ void launch_tiled(cudaStream_t st, int device, unsigned max_grid, const StepArgs
   const uint32_t smem = kTiledHeader + std::max(ly.stages * ly.stage_bytes, 32u * CW * 16u);
   kern<<<(unsigned)g, 32 * (CW + 1), smem, st>>>(
       p, ly, a.Bp, static_cast<const E *>(a.x), static_cast<E *>(a.y), a.tg, a.n_out, a.dots,
-      a.err, kWaitLimit);
+      a.err, a.wait_limit);
 }
 
 #define TBTKKPM_TILED_ENTRY(CLS, CPLX, T, P, D, R, CW, BPS, CV)                     \

@@ -28,8 +28,9 @@
 // bit-identical to theirs.
 //
 // Only non-multicast bulk copies are issued.  Every mbarrier wait is
-// bounded; a wait that runs out sets *err, and before the block exits every
-// copy it issued has landed or its wait ran out too.
+// bounded (`wait_limit` polls; 0 gives up at once); a wait that runs out
+// sets *err and ends the loops, and before the block exits every copy it
+// issued has landed (waited for with the library's bound kWaitLimit).
 #pragma once
 
 #include "kpm_bulk.cuh"
@@ -208,11 +209,12 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
     }
     if (failed && lane == 0) atomicExch(err, kErrTimeout);
     // every copy issued into this block's ring has landed (or its wait ran
-    // out) before the ring is reused or the block exits
+    // out) before the ring is reused or the block exits; this wait keeps the
+    // library's bound whatever `wait_limit` the step was given
     if (lane == 0)
       for (uint32_t s = 0; s < S && s < issued; s++) {
         const uint32_t fills = (issued - 1 - s) / S + 1;
-        if (!mbar_wait_limit(&full[s], (fills - 1) & 1u, wait_limit)) atomicExch(err, kErrTimeout);
+        if (!mbar_wait_limit(&full[s], (fills - 1) & 1u, kWaitLimit)) atomicExch(err, kErrTimeout);
       }
   } else {
     // ---------------------------------------------------------- consumers

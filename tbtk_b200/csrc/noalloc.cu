@@ -7,14 +7,19 @@
 // buffers and keeps its only scratch, the two recursion vectors and the
 // damping factors, in a fixed array compiled into the library.
 //
-// The array is kNoAllocScratchBytes (32 MiB) of device memory that every GPU
-// which loads the library holds until the process exits.  Host code must not
-// pass the array's name to a kernel (on the host that name is a stand-in, not
-// a device address); the first call on a device, with that device current,
-// looks the address up with cudaGetSymbolAddress and caches it, so make that
-// first call before any stream capture.  All calls share the array and it
-// keeps the previous call's contents: each call clears the vectors it uses,
-// and calls that overlap on the GPU race (serialise them on one stream).
+// The array is kNoAllocScratchBytes (32 MiB) of device memory.  A GPU holds
+// it from the moment this code is loaded onto that device (with CUDA's lazy
+// module loading: the first call there) until the process exits.  Host code
+// must not pass the array's name to a kernel (on the host that name is a
+// stand-in, not a device address); the first call on a device, with that
+// device current, looks the address up with cudaGetSymbolAddress and caches
+// it for the process.  A cudaDeviceReset invalidates that address (and every
+// other handle of this library on the device): do not call this entry point
+// on a device after resetting it.  All calls share the array and it keeps
+// the previous call's contents: each call clears the vectors it uses, and
+// calls that overlap on the GPU race (serialise them on one stream).  Every
+// call is synchronous (it copies host data and waits for its stream), so no
+// call can be captured into a CUDA graph.
 #include "tbtkkpm.h"
 #include "kpm_host.h"
 #include "kpm_kernels.cuh"
@@ -50,19 +55,31 @@ int scratch_address(int device, unsigned char **out) {
   return TBTKKPM_OK;
 }
 
+// The caller's rowptr: rowptr[0] == 0, never decreasing, rowptr[N] == nnz;
+// a violation sets status bit 4 (checked before any recursion step runs).
+__global__ void noalloc_check_rowptr(uint32_t N, uint64_t nnz, const uint32_t *__restrict__ rowptr,
+                                     unsigned *status) {
+  const uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= N) return;
+  const uint32_t a = rowptr[row], b = rowptr[row + 1];
+  if (a > b || b > nnz || (row == 0 && a != 0) || (row == N - 1 && b != nnz))
+    atomicOr(status, 4u);
+}
+
 // One step on the caller's CSR, values scaled on the fly exactly as the
 // matrix handles store them: v1 = v*(1/s) for the first step, 2*v1 after
 // (ChebyshevExpander.cpp:147,168), each complex product in the reference's
 // operation order.  Column indices out of range set status bit 1 and are
-// skipped.
-__global__ void noalloc_step(uint32_t N, const uint32_t *__restrict__ rowptr,
+// skipped; entry ranges are clamped to [0, nnz) (rowptr is checked first).
+__global__ void noalloc_step(uint32_t N, uint64_t nnz, const uint32_t *__restrict__ rowptr,
                              const uint32_t *__restrict__ col, const double2 *__restrict__ val,
                              double inv, bool first, const double2 *__restrict__ x,
                              double2 *__restrict__ y, unsigned *status) {
   const uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
   if (row >= N) return;
   double2 acc = first ? make_double2(0.0, 0.0) : make_double2(-y[row].x, -y[row].y);
-  const uint32_t k0 = rowptr[row], k1 = rowptr[row + 1];
+  const uint32_t k1 = (uint32_t)min((uint64_t)rowptr[row + 1], nnz);
+  const uint32_t k0 = min(rowptr[row], k1);
   for (uint32_t k = k0; k < k1; k++) {
     const uint32_t c = col[k];
     if (c >= N) {
@@ -111,11 +128,14 @@ inline unsigned blocks(uint64_t n, unsigned bs) { return (unsigned)((n + bs - 1)
 using namespace tbtkkpm;
 
 extern "C" int tbtkkpm_moments_noalloc(const uint32_t *d_rowptr, const uint32_t *d_col,
-                                       const double *d_val, uint32_t N, double scale,
-                                       uint32_t from, const uint32_t *d_to, uint32_t K,
-                                       uint32_t M, double broadening, double *d_mu_out,
-                                       void *stream) {
+                                       const double *d_val, uint32_t N, uint64_t nnz,
+                                       double scale, uint32_t from, const uint32_t *d_to,
+                                       uint32_t K, uint32_t M, double broadening,
+                                       double *d_mu_out, void *stream) {
   if (!d_rowptr || N == 0) return fail(TBTKKPM_ERR_ARGUMENT, "moments_noalloc: empty matrix");
+  if (nnz > 0xffffffffull)
+    return fail(TBTKKPM_ERR_ARGUMENT, "moments_noalloc: nnz=%llu past 32-bit entry indices",
+                (unsigned long long)nnz);
   if (!(scale > 0))
     return fail(TBTKKPM_ERR_ARGUMENT,
                 "moments_noalloc: the scaleFactor=%g has to be larger than 0", scale);
@@ -124,7 +144,7 @@ extern "C" int tbtkkpm_moments_noalloc(const uint32_t *d_rowptr, const uint32_t 
     return fail(TBTKKPM_ERR_ARGUMENT, "moments_noalloc: from index %u outside the basis of size %u",
                 from, N);
   if (K == 0) return TBTKKPM_OK;
-  if (!d_to || !d_mu_out || !d_col || !d_val)
+  if (!d_to || !d_mu_out || (nnz && (!d_col || !d_val)))
     return fail(TBTKKPM_ERR_ARGUMENT, "moments_noalloc: NULL device buffer");
   if (!std::isfinite(broadening)) return fail(TBTKKPM_ERR_ARGUMENT, "moments_noalloc: broadening not finite");
   const size_t vec_bytes = sizeof(double2) * (size_t)N;
@@ -151,17 +171,29 @@ extern "C" int tbtkkpm_moments_noalloc(const uint32_t *d_rowptr, const uint32_t 
   if ((e = cudaMemsetAsync(base, 0, 2 * vec_bytes, st)) != cudaSuccess ||
       (e = cudaMemsetAsync(status, 0, sizeof(unsigned), st)) != cudaSuccess)
     return cuda_fail(e, "moments_noalloc: clear");
+  // the caller's rowptr is checked before a step reads entries through it
+  noalloc_check_rowptr<<<blocks(N, 256), 256, 0, st>>>(N, nnz, d_rowptr, status);
+  unsigned flag = 0;
+  if ((e = cudaMemcpyAsync(&flag, status, sizeof(unsigned), cudaMemcpyDeviceToHost, st)) !=
+          cudaSuccess ||
+      (e = cudaStreamSynchronize(st)) != cudaSuccess)
+    return cuda_fail(e, "moments_noalloc: rowptr check");
+  if (flag & 4u)
+    return fail(TBTKKPM_ERR_ARGUMENT,
+                "moments_noalloc: rowptr is not a CSR row pointer of nnz=%llu entries "
+                "(rowptr[0] == 0, non-decreasing, rowptr[N] == nnz)",
+                (unsigned long long)nnz);
   noalloc_seed<<<1, 1, 0, st>>>(from, v0);
   noalloc_gather<<<blocks(K, 128), 128, 0, st>>>(N, K, M, 0, d_to, v0, mu, status);
   const double inv = 1 / scale;
   double2 *cur = v0, *prev = v1;
   for (uint32_t n = 1; n < M; n++) {
-    noalloc_step<<<blocks(N, 256), 256, 0, st>>>(N, d_rowptr, d_col, val, inv, n == 1, cur, prev,
-                                                status);
+    noalloc_step<<<blocks(N, 256), 256, 0, st>>>(N, nnz, d_rowptr, d_col, val, inv, n == 1, cur,
+                                                prev, status);
     noalloc_gather<<<blocks(K, 128), 128, 0, st>>>(N, K, M, n, d_to, prev, mu, status);
     std::swap(cur, prev);
   }
-  count_launches(2 + 2 * (uint64_t)(M - 1));
+  count_launches(3 + 2 * (uint64_t)(M - 1));
   double b = 1;
   if (broadening != 0) {
     // the host's libm, exactly as ChebyshevExpander.cpp:192-195
@@ -175,7 +207,6 @@ extern "C" int tbtkkpm_moments_noalloc(const uint32_t *d_rowptr, const uint32_t 
     noalloc_damp<<<blocks((uint64_t)K * M, 256), 256, 0, st>>>(K, M, damp, b, mu);
     count_launches(1);
   }
-  unsigned flag = 0;
   if ((e = cudaMemcpyAsync(&flag, status, sizeof(unsigned), cudaMemcpyDeviceToHost, st)) !=
           cudaSuccess ||
       (e = cudaStreamSynchronize(st)) != cudaSuccess)

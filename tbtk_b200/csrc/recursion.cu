@@ -340,6 +340,7 @@ int run_batch(tbtkkpm_matrix *m, int precision, const std::vector<uint32_t> &fro
   a.dots = doubling ? ws.dots.as<double2>() : nullptr;
   a.err = ws.err.as<int>();
   a.plan = plan;
+  a.wait_limit = m->wait_limit == TBTKKPM_WAIT_DEFAULT ? kWaitLimit : m->wait_limit;
   void *cur = ws.vec[0].ptr, *prev = ws.vec[1].ptr;
   m->timer.mark(st, 0);
   m->timer.pending = m->timer.enabled;
@@ -1037,6 +1038,13 @@ extern "C" int tbtkkpm_matrix_set_fp64_head(tbtkkpm_matrix *m, uint32_t steps) {
   if (!m) return fail(TBTKKPM_ERR_ARGUMENT, "matrix_set_fp64_head: NULL matrix");
   std::lock_guard<std::mutex> lk(m->lock);
   m->head_steps = steps;
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_matrix_set_wait_limit(tbtkkpm_matrix *m, uint32_t polls) {
+  if (!m) return fail(TBTKKPM_ERR_ARGUMENT, "matrix_set_wait_limit: NULL matrix");
+  std::lock_guard<std::mutex> lk(m->lock);
+  m->wait_limit = polls;
   return TBTKKPM_OK;
 }
 

@@ -76,7 +76,7 @@ SIGNATURES = [
     ("tbtkkpm_matrix_shape", _i, [_p, _p, _p]),
     ("tbtkkpm_matrix_download_csr", _i, [_p, _p, _p, _p]),
     ("tbtkkpm_moments", _i, [_p, _u32, _p, _u32, _u32, _d, _p]),
-    ("tbtkkpm_moments_noalloc", _i, [_p, _p, _p, _u32, _d, _u32, _p, _u32, _u32, _d, _p, _p]),
+    ("tbtkkpm_moments_noalloc", _i, [_p, _p, _p, _u32, _u64, _d, _u32, _p, _u32, _u32, _d, _p, _p]),
     ("tbtkkpm_moments_batched", _i, [_p, _p, _u32, _p, _p, _u32, _u32, _d, _i, _p, _p]),
     ("tbtkkpm_table_create", _i, [_u32, _p, _u32, _d, _p]),
     ("tbtkkpm_table_upload", _i, [_u32, _u32, _p, _p]),
@@ -92,6 +92,7 @@ SIGNATURES = [
     ("tbtkkpm_matrix_real", _i, [_p, _p, _p]),
     ("tbtkkpm_matrix_step_configs", _i, [_p, _i, _i, _p, _i]),
     ("tbtkkpm_matrix_set_fp64_head", _i, [_p, _u32]),
+    ("tbtkkpm_matrix_set_wait_limit", _i, [_p, _u32]),
     ("tbtkkpm_matrix_fp64_head", _i, [_p, _p, _p]),
     ("tbtkkpm_matrix_set_batch_width", _i, [_p, _i, _u32]),
     ("tbtkkpm_matrix_batch_width", _i, [_p, _i, _i, _p]),
@@ -276,6 +277,12 @@ class Matrix:
         vr, use = ctypes.c_int(), ctypes.c_int()
         _check(load_library().tbtkkpm_matrix_real(self._h, ctypes.byref(vr), ctypes.byref(use)))
         return bool(vr.value), bool(use.value)
+
+    def set_wait_limit(self, polls=0xFFFFFFFF):
+        """Polls per staged-row wait of the tile-staged steps
+        (tbtkkpm_matrix_set_wait_limit; the default restores the library's
+        bound, 0 makes every such wait give up at once)."""
+        _check(load_library().tbtkkpm_matrix_set_wait_limit(self._h, int(polls)))
 
     def set_fp64_head(self, steps=32):
         """FP64 steps at the head of MIXED doubling runs (0 turns it off)."""
