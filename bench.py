@@ -9,12 +9,16 @@ open grid (-12, 12), LDOS at 64 seeded sites per rank.
 One step = the LDOS of the rank's 64 sites: the batched mixed-precision
 recursion (float vectors [N][64] for this real model, complex64 ones for a
 complex model; FP64 arithmetic and moments), FP64 damping and the FP64
-energy sum through the lookup table, with the result copied to the host.  ``value`` is LDOS solves/s over all ranks (sites per
-step x steps x ranks / max over ranks of the device time).  Beside it the
-line carries the plain FP64 single-vector path (one site per recursion,
-complex128, bit-exact with the reference) on the same sites and matrix,
-the LDOS error of the mixed result against that FP64 result, the roofline
-of the recursion step, and the CPU baseline.
+energy sum through the lookup table, with the result copied to the host.
+``value`` is LDOS solves/s over all ranks (sites per step x steps x ranks /
+max over ranks of the device time).  Beside it the line carries the plain
+FP64 single-vector path (one site per recursion, complex128, bit-exact with
+the reference) on the same matrix, the LDOS error of the mixed result of
+every site against the FP64 recursion (batched FP64, bit-identical per site
+to the single-vector path), the speed-up split into its mechanisms, the
+roofline of the recursion step, the CPU baseline, and two sub-results:
+the 1024x1024 Rashba lattice (complex Hamiltonian, 256 sites, M = 2048) and
+the LDOS server on a 100-model uneven batch at tolerance 1e-6.
 
 Inputs are larger than L2 (13.8 GB of matrix and vectors per recursion step
 against 126 MB of L2), so no flush is needed between steps.
@@ -51,7 +55,10 @@ def parse():
     ap.add_argument("--sites", type=int, default=64)
     ap.add_argument("--lattice", type=int, default=2048, help="lattice side L (L x L x 2 states)")
     ap.add_argument("--moments", type=int, default=4096)
-    ap.add_argument("--plain-sites", type=int, default=2)
+    ap.add_argument("--plain-sites", type=int, default=2,
+                    help="sites timed one at a time on the plain FP64 single-vector path")
+    ap.add_argument("--no-sub", action="store_true",
+                    help="skip the Rashba and server sub-results")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -118,10 +125,51 @@ class Clocks:
 # (algorithmic bytes 3.439 GB); real float vectors (8, 8, 2): 1.721 GB,
 # (4, 16, 2): 1.808 GB, (4, 16, 802) (dot sums in shared memory): 1.713 GB
 # (algorithmic bytes 1.744 GB).
-TRAFFIC_PER_ROW = {("complex64", 64, 8, 8, 2): 3.427e9 / 2097152,
+# The tile-staged step (variant >= 100000) with 64-row tiles: real float
+# vectors, (8, 8), 16 consumer warps: 1.686 GB (1.182 read + 0.504 write);
+# keyed by (vectors, B, "tiled", rows per tile).
+TRAFFIC_PER_ROW = {("real float", 64, "tiled", 64): 1.686e9 / 2097152,
+                   ("complex64", 64, 8, 8, 2): 3.427e9 / 2097152,
                    ("real float", 64, 8, 8, 2): 1.721e9 / 2097152,
                    ("real float", 64, 4, 16, 2): 1.8075e9 / 2097152,
                    ("real float", 64, 4, 16, 802): 1.7130e9 / 2097152}
+
+
+def traffic_per_row(vec_kind, B, tuned):
+    tpr, vpt, variant = tuned[:3]
+    if variant >= 100000:
+        return TRAFFIC_PER_ROW.get((vec_kind, B, "tiled", ((variant - 100000) % 1000000) // 1000))
+    return TRAFFIC_PER_ROW.get((vec_kind, B, tpr, vpt, variant))
+
+
+def kernel_name(real_vectors, tuned):
+    tpr, vpt, variant = tuned[:3]
+    if variant >= 100000:
+        v = variant - 100000
+        return (f"kpm_step_tiled<{'real' if real_vectors else 'complex64'}, tpr={tpr}, "
+                f"vpt={vpt}, rows/tile={(v % 1000000) // 1000}, consumer warps={(v % 1000) // 10}, "
+                f"blocks/SM={v % 10}, widening split={v // 1000000}>")
+    return f"{'kpm_step_real' if real_vectors else 'kpm_step<float2'}, tpr={tpr}, vpt={vpt}, minb={variant}"
+
+
+def host_cpu():
+    """Core count and model of this host (the CPU baselines' machine)."""
+    model = None
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    try:
+        lscpu = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        keep = ("Model name", "Socket(s)", "Core(s) per socket", "Thread(s) per core", "CPU(s)")
+        info = {k.strip(): v.strip() for k, v in (ln.split(":", 1) for ln in lscpu.splitlines()
+                                                  if ":" in ln) if k.strip() in keep}
+    except (OSError, subprocess.SubprocessError):
+        info = {}
+    return {"nproc": os.cpu_count(), "model": model, "lscpu": info}
 
 
 def peak_hbm():
@@ -279,7 +327,7 @@ def reference_arm(args, world, rank):
                                f"M={args.moments}, E=2000, LDOS per site",
                    "model_build_s": round(build_s, 1)},
         "cpu_baseline": {"value": value, "unit": "LDOS solves/s", "cores": threads,
-                         "kind": "reference",
+                         "kind": "reference", "host": host_cpu(),
                          "sample": (f"TBTK PropertyExtractor::calculateLDOS on {threads} threads "
                                     f"(one site each) at M={m_lo} ({len(lo_t)}x) and M={m_hi} "
                                     f"({len(hi_t)}x), minimum of each; per-site {fixed:.2f} s + "
@@ -288,6 +336,83 @@ def reference_arm(args, world, rank):
         "e2e": {"value": value, "unit": "LDOS solves/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+
+
+# ------------------------------------------------------------------ sub-results
+
+def rashba_sub(args, stream):
+    """The 1024x1024 Rashba lattice (complex Hamiltonian, 9 entries per row):
+    256 sites in one tbtkkpm_ldos_sites call at M = 2048 (two 128-source
+    complex64 SpMM recursions by default), against the plain FP64
+    single-vector path on the same matrix, with the LDOS error of 16 sites
+    spread over the batch against their FP64 recursion."""
+    import torch
+    from tbtk_b200 import kpm, workloads
+    p = workloads.cfg3()
+    mat = kpm.Matrix.from_csr(p.rowptr, p.col, p.val, p.scale)
+    tab = kpm.Table.create(p.M, p.energies, p.scale)
+    mat.set_stream(stream.cuda_stream)
+    width = mat.batch_width(kpm.MIXED, ldos=True)
+    tuned = mat.autotune(min(width, p.sites.size), kpm.MIXED, ldos=True, probe_steps=6)
+    mat.set_profiling(True)
+    with torch.cuda.stream(stream):
+        mat.ldos_sites(tab, p.sites, p.broadening, kpm.MIXED)  # warm
+        mat.profile()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        got, est = mat.ldos_sites(tab, p.sites, p.broadening, kpm.MIXED)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        rec, _, launches = mat.profile()
+        mat.ldos_sites(tab, p.sites[:1], p.broadening, kpm.FP64)  # warm
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        mat.ldos_sites(tab, p.sites[1:2], p.broadening, kpm.FP64)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms = f0.elapsed_time(f1)
+        prec, _, plaunch = mat.profile()
+        pick = np.linspace(0, p.sites.size - 1, 16).astype(int)
+        ref, _ = mat.ldos_sites(tab, p.sites[pick], p.broadening, kpm.FP64)
+    errs = [float(np.abs(got[i] - r).max() / np.abs(r).max()) for i, r in zip(pick, ref)]
+    step_ms = rec / max(launches, 1)
+    batches = [min(width, p.sites.size - b0) for b0 in range(0, p.sites.size, width)]
+    bstep = sum(step_bytes(p, b, 8) for b in batches) / len(batches)
+    peak, _ = peak_hbm()
+    rate = p.sites.size / (ms / 1e3)
+    return {
+        "workload": (f"rashba 1024x1024 spin periodic alpha=0.3 (N={p.N}, nnz={p.nnz}), W=2, "
+                     f"s=12, M={p.M}, E={p.energies.size}, {p.sites.size} sites in one call "
+                     f"(batches of {width})"),
+        "value": rate, "unit": "LDOS solves/s", "ms_per_call": ms,
+        "step_ms": step_ms, "autotuned": dict(zip(("tpr", "vpt", "variant", "ms_per_step"), tuned)),
+        "kernel": kernel_name(False, tuned),
+        "roofline": {"achieved_GBps": bstep / (step_ms / 1e3) / 1e9,
+                     "frac": bstep / (step_ms / 1e3) / 1e9 / peak, "bytes_per_launch": bstep},
+        "plain_fp64": {"ms_per_solve": plain_ms, "value": 1e3 / plain_ms,
+                       "step_ms": prec / max(plaunch, 1)},
+        "speedup_vs_plain_fp64": rate * plain_ms / 1e3,
+        "speedup_per_site_step": (prec / max(plaunch, 1)) / (step_ms / batches[0]),
+        "ldos_rel_err_vs_fp64": max(errs), "ldos_err_sites": len(errs),
+        "error_estimate_max": float(np.max(est)),
+    }
+
+
+def server_sub():
+    """The LDOS server on the first 100 models of the uneven batch at
+    tolerance 1e-6 (FP64 rerun of a site whose error estimate exceeds it)."""
+    from tbtk_b200 import serve_bench
+    a = argparse.Namespace(models=100, budget_gb=60.0, tick=64, tolerance=1e-6, samples=12,
+                           sample_seed=44, fp64_head=32)
+    r = serve_bench.uneven(a)
+    st = r["server"]
+    return {"workload": r["workload"], "value": r["value"], "unit": "LDOS solves/s",
+            "p50_ms": st.get("p50_ms"), "p99_ms": st.get("p99_ms"), "reruns": st.get("reruns"),
+            "solves": r["solves"], "wall_s": r["wall_s"],
+            "plain_fp64": r["plain_fp64"], "speedup_vs_plain_fp64": r["speedup_vs_plain_fp64"],
+            "ldos_rel_err_vs_fp64_max": r["ldos_rel_err_vs_fp64_max"],
+            "step_GBps": r["step_GBps"]}
 
 
 # ------------------------------------------------------------------ our arm
@@ -344,22 +469,25 @@ def ours(args, world, rank, local):
         step_ms = sorted(marks[i].elapsed_time(marks[i + 1]) for i in range(args.steps))
         rec_ms, energy_ms, rec_launches = mat.profile()
 
-        # plain FP64 single-vector path on the first sites: timing + FP64 LDOS
+        # plain FP64 single-vector path (complex128, one site per recursion):
+        # timing on the first sites
         plain = []
-        ref_ldos = []
         step(kpm.FP64, p.sites[:1])  # warm
+        mat.profile()
         for i in range(args.plain_sites):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            out, _ = step(kpm.FP64, p.sites[i:i + 1])
+            step(kpm.FP64, p.sites[i:i + 1])
             e1.record(stream)
             torch.cuda.synchronize()
             plain.append(e0.elapsed_time(e1))
-            ref_ldos.append(out[0])
-        mat.profile()
-    errs = [float(np.abs(results[i] - ref_ldos[i]).max() / np.abs(ref_ldos[i]).max())
-            for i in range(args.plain_sites)]
+        plain_rec, _, plain_launches = mat.profile()
+        # FP64 LDOS of every site: the batched FP64 recursion gives each
+        # site's single-vector moments bit for bit
+        ref_all, _ = step(kpm.FP64, p.sites)
+    errs = [float(np.abs(results[i] - ref_all[i]).max() / np.abs(ref_all[i]).max())
+            for i in range(B)]
 
     # end to end through the C ABI from pinned host buffers
     e2e = None
@@ -404,7 +532,7 @@ def ours(args, world, rank, local):
     bstep = step_bytes(p, B, 4, 8) if real_vectors else step_bytes(p, B, 8)
     achieved = bstep / (avg_step_ms / 1e3) / 1e9
     vec_kind = "real float" if real_vectors else "complex64"
-    traffic_row = TRAFFIC_PER_ROW.get((vec_kind, B) + tuple(tuned_mixed[:3]))
+    traffic_row = traffic_per_row(vec_kind, B, tuned_mixed)
     peak, peak_kind = peak_hbm()
     plain_ms = statistics.median(plain) if plain else None
     plain_rate = 1e3 / plain_ms if plain_ms else None
@@ -433,7 +561,18 @@ def ours(args, world, rank, local):
         "plain_fp64": {"value": plain_rate, "unit": "LDOS solves/s", "ms_per_solve": plain_ms,
                        "sites": args.plain_sites},
         "speedup_vs_plain_fp64": (value / world) / plain_rate if plain_rate else None,
+        "speedup_mechanisms": {
+            "doubling": (p.M - 1) / (p.M // 2),
+            "batch_and_vectors_per_site_step": (plain_rec / max(plain_launches, 1))
+                                               / (avg_step_ms / B),
+            "plain_step_ms": plain_rec / max(plain_launches, 1),
+            "batched_step_ms_per_site": avg_step_ms / B,
+            "note": ("doubling: M-1 single-vector steps against M/2 doubling steps; the other "
+                     "factor compares one complex128 single-vector step with one site's share of "
+                     "the batched step (real float vectors for this real model); their product "
+                     "is the speed-up before the energy sums and the FP64 head")},
         "ldos_rel_err_vs_fp64": max(errs) if errs else None,
+        "ldos_err_sites": len(errs),
         "latency_ms": {"p50": statistics.median(step_ms),
                        "p99": step_ms[min(len(step_ms) - 1, int(0.99 * len(step_ms)))],
                        "note": (f"per {B}-site batch over the {args.steps} timed steps; "
@@ -443,10 +582,8 @@ def ours(args, world, rank, local):
                      "traffic": traffic_row * p.N if traffic_row else None,
                      "traffic_source": ("ncu dram__bytes_read+write of this kernel on the "
                                         "1024x1024 lattice (N=2097152), scaled by rows to N"),
-                     "kernel": (f"{'kpm_step_real' if real_vectors else 'kpm_step<float2'}, "
-                                f"tpr={tuned_mixed[0]}, vpt={tuned_mixed[1]}, dots, "
-                                f"minb={tuned_mixed[2]} (recursion step, B={B}, {vec_kind} "
-                                f"vectors)"),
+                     "kernel": (f"{kernel_name(real_vectors, tuned_mixed)} (recursion step "
+                                f"with the doubling dot products, B={B}, {vec_kind} vectors)"),
                      "bytes_per_launch": bstep, "avg_launch_ms": avg_step_ms,
                      "peak_kind": f"{peak_kind} (copy bandwidth)"},
         "recursion_share": rec_ms / total_ms if total_ms else None,
@@ -457,9 +594,13 @@ def ours(args, world, rank, local):
                       "unit": "LDOS solves/s", "h2d_bytes_per_step": e2e["h2d"],
                       "d2h_bytes_per_step": e2e["d2h"], "steps": args.e2e_steps,
                       "includes": "CSR upload + device table + recursion + LDOS + download"}
+    if world == 1 and not args.no_sub:
+        out["rashba_cfg3"] = rashba_sub(args, stream)
+        out["server_uneven"] = server_sub()
     if world == 1 and not args.no_cpu:
-        threads = int(min(os.cpu_count() or 1, 16, B))
+        threads = int(min(os.cpu_count() or 1, B))
         out["cpu_baseline"] = cpu_port_baseline(p, threads)
+        out["cpu_baseline"]["host"] = host_cpu()
     if dist:
         dist.destroy_process_group()
     return out

@@ -40,7 +40,10 @@ bool real_mode(const tbtkkpm_matrix *m, int precision) {
   return is_mixed(precision) && m->values_real && m->use_real;
 }
 
-Shape shape_for(int precision, uint32_t B, bool real = false, bool dots = false) {
+// The register-staged shape of a batch (kpm_step / kpm_step_real): the
+// fallback of the tile-staged defaults below, and the default of widths the
+// tile-staged steps do not serve.
+Shape register_shape_for(int precision, uint32_t B, bool real, bool dots) {
   if (real) {
     // a thread per row up to 8 values: it prefetches all of the next row's
     // entries and gathers them in one round (0.51 against 0.71 ms per step
@@ -50,10 +53,9 @@ Shape shape_for(int precision, uint32_t B, bool real = false, bool dots = false)
     if (B <= 4) return {1, 4};
     if (B <= 8) return {1, 8};
     // doubling runs: 16 values per thread with the dot sums in shared
-    // memory (variant 802), the fastest on the 2048^2 lattice at M = 128:
-    // 0.84 / 1.83 / 2.91 / 4.93 / 11.9 ms per step for B = 16 / 32 / 64 /
-    // 128 / 256 against 1.24 / 2.19 / 3.45 / 6.90 / 13.4 for the best
-    // register-only shapes
+    // memory (variant 802), the fastest register-staged shapes on the
+    // 2048^2 lattice at M = 128: 0.84 / 1.83 / 2.91 / 4.93 / 11.9 ms per step
+    // for B = 16 / 32 / 64 / 128 / 256
     if (dots) {
       if (B <= 16) return {1, 16, 802};
       if (B <= 32) return {2, 16, 802};
@@ -91,6 +93,39 @@ Shape shape_for(int precision, uint32_t B, bool real = false, bool dots = false)
   if (B <= 64) return {8, 8};
   if (B <= 128) return {32, 4};
   return {32, 8};
+}
+
+// Tile-staged variant: 100000 + 1000000*CV + 1000*R + 10*CW + BPS.
+constexpr int tiled(int cv, int rows, int cw, int bps) {
+  return 100000 + 1000000 * cv + 1000 * rows + 10 * cw + bps;
+}
+
+// Default shape of a batch.  At mixed precision from 32 sources on (from 16
+// for complex vectors) the tile-staged steps are the defaults: ms per step
+// measured on the 2048^2 lattice (real float vectors, doubling dots) for
+// B = 32 / 64 / 128 / 256: 1.05 / 1.43 / 3.01 / 5.71 against 1.82 / 2.90 /
+// 4.79 / 11.8 for the register-staged defaults, and on the 1024^2 Rashba
+// lattice (complex64) for B = 16 / 32 / 64 / 128 / 256: 0.38 / 0.55 / 1.09 /
+// 2.14 / 4.27 against 1.06 / 1.25 / 1.94 / 3.33 / 8.28.  Without the dots
+// (directly gathered moments) the real B = 64 step takes 1.29 ms (0.84 of
+// the measured copy bandwidth).  A matrix whose tiles do not fit the ring
+// falls back to register_shape_for.
+Shape shape_for(int precision, uint32_t B, bool real = false, bool dots = false) {
+  if (is_mixed(precision)) {
+    if (real) {
+      if (B > 16 && B <= 32) return {8, 4, tiled(0, 64, 16, 1)};
+      if (B > 32 && B <= 64) return {8, 8, tiled(51, 64, 16, 1)};
+      if (B > 64 && B <= 128) return {16, 8, tiled(51, 16, 8, 2)};
+      if (B > 128) return {32, 8, tiled(51, 16, 16, 1)};
+    } else {
+      if (B > 8 && B <= 16) return {8, 2, tiled(0, 32, 8, 2)};
+      if (B > 16 && B <= 32) return {8, 4, tiled(0, 32, 8, 2)};
+      if (B > 32 && B <= 64) return {16, 4, tiled(0, 16, 8, 2)};
+      if (B > 64 && B <= 128) return {32, 4, tiled(0, 16, 16, 1)};
+      if (B > 128) return {64, 4, tiled(0, 8, 16, 1)};
+    }
+  }
+  return register_shape_for(precision, B, real, dots);
 }
 
 int step_class(int precision, bool dots, bool real = false) {
@@ -188,7 +223,7 @@ int resolve_tiled(tbtkkpm_matrix *m, int precision, bool dots, uint32_t B, bool 
     return fail(TBTKKPM_ERR_UNSUPPORTED,
                 "recursion: the tile-staged step %d x %d / %d does not fit this matrix", fn->tpr,
                 fn->vpt, fn->minb);
-  const Shape s = shape_for(precision, B, !cplx, dots);
+  const Shape s = register_shape_for(precision, B, !cplx, dots);
   fn = find_step(fn->cls, s.tpr, s.vpt, s.minb);
   return TBTKKPM_OK;
 }
