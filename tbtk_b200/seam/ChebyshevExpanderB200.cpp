@@ -10,10 +10,12 @@
  * setCalculateCoefficientsOnGPU / setGenerateGreensFunctionsOnGPU flags.
  *
  * Semantics kept from the reference:
- *  - the Hamiltonian is HoppingAmplitudeSet::getSparseMatrix() in CSR, built
- *    on every calculateCoefficients call as the reference does
- *    (ChebyshevExpander.cpp:142-147), so amplitude callbacks are evaluated
- *    each time;
+ *  - the Hamiltonian is the CSR of HoppingAmplitudeSet::getSparseMatrix()
+ *    (ChebyshevExpander.cpp:142-147), bit for bit; the seam keeps it on the
+ *    device per (model, scale factor, device) and rebuilds it whenever the
+ *    model's amplitudes differ from those it was built from, amplitude
+ *    callbacks evaluated on every call as in the reference
+ *    (B200::deviceMatrix, KPMSeamB200.h);
  *  - a device comes from GPUResourceManager::allocateDevice / freeDevice
  *    (ChebyshevSolver.cu:93-100,630);
  *  - the lookup table is the Solver's host table copied to every device
@@ -28,6 +30,7 @@
 #include "TBTK/Streams.h"
 #include "TBTK/TBTKMacros.h"
 
+#include "KPMSeamB200.h"
 #include "tbtkkpm.h"
 
 #include <complex>
@@ -103,7 +106,6 @@ vector<vector<complex<double>>> ChebyshevExpander::calculateCoefficientsGPU(
 
 	const HoppingAmplitudeSet &hoppingAmplitudeSet
 		= getModel().getHoppingAmplitudeSet();
-	const unsigned int basisSize = hoppingAmplitudeSet.getBasisSize();
 	const unsigned int fromBasisIndex
 		= hoppingAmplitudeSet.getBasisIndex(from);
 	vector<uint32_t> toBasisIndices;
@@ -113,50 +115,21 @@ vector<vector<complex<double>>> ChebyshevExpander::calculateCoefficientsGPU(
 		);
 	}
 
-	//The reference's matrix: getSparseMatrix() in CSR, padded to the
-	//basis size when trailing rows are empty.
-	SparseMatrix<complex<double>> sparseMatrix
-		= hoppingAmplitudeSet.getSparseMatrix();
-	sparseMatrix.setStorageFormat(
-		SparseMatrix<complex<double>>::StorageFormat::CSR
-	);
-	const unsigned int numRows = sparseMatrix.getNumRows();
-	const unsigned int *rowPointers = sparseMatrix.getCSRRowPointers();
-	const unsigned int numEntries = rowPointers[numRows];
-	vector<uint32_t> rowptr(basisSize + 1, numEntries);
-	for(unsigned int r = 0; r <= numRows && r <= basisSize; r++)
-		rowptr[r] = rowPointers[r];
-	const unsigned int *columns = sparseMatrix.getCSRColumns();
-	const complex<double> *values = sparseMatrix.getCSRValues();
-	vector<uint32_t> col(columns, columns + numEntries);
-	vector<double> val(2*(size_t)numEntries);
-	for(unsigned int k = 0; k < numEntries; k++){
-		val[2*k] = values[k].real();
-		val[2*k + 1] = values[k].imag();
-	}
-
 	GPUResourceManager &gpu = GPUResourceManager::getInstance();
 	const int device = gpu.allocateDevice();
 	check(
 		tbtkkpm_set_device(device),
 		"ChebyshevExpander::calculateCoefficientsGPU()"
 	);
-
-	tbtkkpm_matrix *matrix = nullptr;
-	check(
-		tbtkkpm_matrix_create_csr(
-			rowptr.data(),
-			col.data(),
-			val.data(),
-			basisSize,
-			scaleFactor,
-			&matrix
-		),
+	std::shared_ptr<tbtkkpm_matrix> matrix = B200::deviceMatrix(
+		getModel(),
+		scaleFactor,
+		device,
 		"ChebyshevExpander::calculateCoefficientsGPU()"
 	);
 	vector<complex<double>> flat((size_t)to.size()*numCoefficients);
 	const int status = tbtkkpm_moments(
-		matrix,
+		matrix.get(),
 		fromBasisIndex,
 		toBasisIndices.data(),
 		toBasisIndices.size(),
@@ -164,7 +137,7 @@ vector<vector<complex<double>>> ChebyshevExpander::calculateCoefficientsGPU(
 		broadening,
 		reinterpret_cast<double*>(flat.data())
 	);
-	tbtkkpm_matrix_destroy(matrix);
+	matrix.reset();
 	gpu.freeDevice(device);
 	check(status, "ChebyshevExpander::calculateCoefficientsGPU()");
 

@@ -1,12 +1,23 @@
 /* TBTK's own Solver/PropertyExtractor::ChebyshevExpander, linked against the
  * B200 seam (tbtk_b200/seam) instead of Lib/src/cuda or Lib/src/nocuda, run
  * with the reference's GPU flags and compared with the same objects on their
- * CPU path.
+ * CPU path.  The same source builds two programs (tests/cpp/Makefile):
+ * test_seam links the reference's PropertyExtractor::ChebyshevExpander
+ * (per-index recursions), test_pe_seam links the seam's batched one
+ * (tbtk_b200/seam/PropertyExtractorChebyshevExpanderB200.cpp).
  *
  *   test_seam            all parity checks; exit 0 when all pass
  *   test_seam exit-short generateGreensFunction on the GPU path with fewer
  *                        coefficients than the lookup table; must end in
  *                        TBTKExit (message on Streams::err, exit status 1)
+ *   test_seam dump cpu|gpu FILE
+ *                        every PropertyExtractor property of the 6x6 model
+ *                        (both pattern forms) on the CPU or GPU path,
+ *                        written to FILE as named blocks of doubles
+ *   test_seam time       calculateLDOS of 64 sites of a 256x256 lattice with
+ *                        spin through TBTK's API on the GPU path (one JSON
+ *                        line: seconds, and the LDOS error of the mixed
+ *                        precision against FP64)
  *
  * Expected agreement: coefficients bit-identical (the library's FP64 step
  * follows calculateCoefficientsCPU's operation order,
@@ -22,9 +33,11 @@
 #include "TBTK/Streams.h"
 #include "TBTK/TBTK.h"
 
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -269,6 +282,179 @@ void testProperties(Model &model){
 		"|diff|=" + std::to_string(std::abs(ea - eb) + std::abs(fa - fb)));
 }
 
+/* Named blocks of doubles: uint32 name length, name, uint64 count, data. */
+class Dump{
+public:
+	explicit Dump(const char *path) : f(std::fopen(path, "wb")){}
+	~Dump(){ if(f) std::fclose(f); }
+	bool ok() const{ return f != nullptr; }
+	void put(const std::string &name, const double *data, size_t count){
+		const uint32_t n = name.size();
+		const uint64_t c = count;
+		std::fwrite(&n, sizeof(n), 1, f);
+		std::fwrite(name.data(), 1, n, f);
+		std::fwrite(&c, sizeof(c), 1, f);
+		std::fwrite(data, sizeof(double), count, f);
+	}
+	void put(const std::string &name, const std::vector<double> &v){
+		put(name, v.data(), v.size());
+	}
+	void put(const std::string &name, const std::vector<cplx> &v){
+		put(name, reinterpret_cast<const double*>(v.data()), 2*v.size());
+	}
+	void put(const std::string &name, const std::vector<SpinMatrix> &v){
+		std::vector<double> flat;
+		for(const SpinMatrix &m : v)
+			for(unsigned int r = 0; r < 2; r++)
+				for(unsigned int c = 0; c < 2; c++){
+					flat.push_back(m.at(r, c).real());
+					flat.push_back(m.at(r, c).imag());
+				}
+		put(name, flat);
+	}
+private:
+	std::FILE *f;
+};
+
+/* Every property of PropertyExtractor::ChebyshevExpander on the 6x6 model,
+ * both the pattern-list and the pattern/ranges forms. */
+int dump(bool gpu, const char *path){
+	Model model;
+	model.setVerbose(false);
+	buildModel(model);
+	model.setTemperature(300);
+	model.setChemicalPotential(0.1);
+	Solver::ChebyshevExpander solver;
+	configure(solver, model, 256, gpu);
+	PropertyExtractor::ChebyshevExpander pe(solver);
+	pe.setEnergyWindow(-4, 4, 301);
+	Dump out(path);
+	if(!out.ok())
+		return 2;
+	out.put("ldos_patterns", pe.calculateLDOS({
+		{0, 0, 0}, {2, 3, 1}, {5, 1, IDX_ALL}
+	}).getData());
+	out.put("ldos_sum", pe.calculateLDOS({{IDX_SUM_ALL, 2, IDX_ALL}}).getData());
+	out.put("ldos_ranges", pe.calculateLDOS(
+		{IDX_X, 3, IDX_SUM_ALL}, {6, 1, 2}
+	).getData());
+	out.put("greens_patterns", pe.calculateGreensFunction(
+		{{{1, 1, 0}, {1, 1, IDX_ALL}}, {{2, 2, 1}, {3, 3, 1}}},
+		Property::GreensFunction::Type::Retarded
+	).getData());
+	std::vector<Index> to = {{0, 0, 0}, {4, 1, 1}, {2, 2, 0}};
+	out.put("greens_to_list", pe.calculateGreensFunctions(
+		to, {2, 2, 0}, Property::GreensFunction::Type::Principal
+	).getData());
+	out.put("greens_advanced", pe.calculateGreensFunction(
+		{3, 1, 1}, {1, 3, 0}, Property::GreensFunction::Type::Advanced
+	).getData());
+	out.put("density_patterns",
+		pe.calculateDensity({{IDX_ALL, 2, IDX_ALL}}).getData());
+	out.put("density_ranges", pe.calculateDensity(
+		{IDX_X, IDX_Y, IDX_SUM_ALL}, {6, 6, 2}
+	).getData());
+	out.put("magnetization_patterns",
+		pe.calculateMagnetization({{1, 1, IDX_SPIN}, {4, 2, IDX_SPIN}})
+			.getData());
+	out.put("magnetization_ranges", pe.calculateMagnetization(
+		{IDX_X, 2, IDX_SPIN}, {6, 1, 2}
+	).getData());
+	out.put("sp_ldos_patterns",
+		pe.calculateSpinPolarizedLDOS({{2, 3, IDX_SPIN}}).getData());
+	out.put("sp_ldos_ranges", pe.calculateSpinPolarizedLDOS(
+		{IDX_X, 0, IDX_SPIN}, {6, 1, 2}
+	).getData());
+	std::vector<cplx> ev = {
+		pe.calculateExpectationValue({2, 3, 0}, {2, 3, 1}),
+		pe.calculateExpectationValue({4, 4, 1}, {4, 4, 1})
+	};
+	out.put("expectation_values", ev);
+	return 0;
+}
+
+/* L x L square lattice with spin, periodic, hopping -1, a Zeeman term
+ * -0.5*(1 - 2s) and on-site disorder in [-1, 1] from a fixed sequence. */
+void buildLattice(Model &model, int L){
+	unsigned int state = 2024u;
+	auto next = [&state](){
+		state = state*1664525u + 1013904223u;
+		return ((state >> 8) & 0xffff)/32767.5 - 1.0;
+	};
+	for(int x = 0; x < L; x++){
+		for(int y = 0; y < L; y++){
+			const double w = next();
+			for(int s = 0; s < 2; s++){
+				model << HoppingAmplitude(
+					w - 0.5*(1 - 2*s), {x, y, s}, {x, y, s}
+				);
+				model << HoppingAmplitude(
+					-1.0, {(x + 1)%L, y, s}, {x, y, s}
+				) + HC;
+				model << HoppingAmplitude(
+					-1.0, {x, (y + 1)%L, s}, {x, y, s}
+				) + HC;
+			}
+		}
+	}
+	model.construct();
+}
+
+int timeLDOS(){
+	const int L = 256, sites = 64, M = 1024, E = 1000;
+	Model model;
+	model.setVerbose(false);
+	buildLattice(model, L);
+	Solver::ChebyshevExpander solver;
+	solver.setVerbose(false);
+	solver.setModel(model);
+	solver.setScaleFactor(10);
+	solver.setNumCoefficients(M);
+	solver.setBroadening(1e-3);
+	solver.setUseLookupTable(true);
+	solver.setCalculateCoefficientsOnGPU(true);
+	solver.setGenerateGreensFunctionsOnGPU(true);
+	PropertyExtractor::ChebyshevExpander pe(solver);
+	pe.setEnergyWindow(-9.9, 9.9, E);
+	std::vector<Index> patterns;
+	unsigned int state = 7u;
+	for(int n = 0; n < sites; n++){
+		state = state*1664525u + 1013904223u;
+		const int site = (state >> 8) % (L*L);
+		patterns.push_back({site/L, site%L, n % 2});
+	}
+	auto run = [&](const char *precision, double &seconds){
+		setenv("TBTK_B200_PRECISION", precision, 1);
+		const auto t0 = std::chrono::steady_clock::now();
+		Property::LDOS ldos = pe.calculateLDOS(patterns);
+		seconds = std::chrono::duration<double>(
+			std::chrono::steady_clock::now() - t0
+		).count();
+		return ldos.getData();
+	};
+	double warm, fp64, mixed;
+	run("fp64", warm);	//device matrix, lookup table
+	std::vector<double> a = run("fp64", fp64);
+	std::vector<double> b = run("mixed", mixed);
+	double num = 0, den = 0;
+	for(int k = 0; k < sites; k++){
+		double d = 0, m = 0;
+		for(int e = 0; e < E; e++){
+			d = std::fmax(d, std::fabs(a[(size_t)k*E + e] - b[(size_t)k*E + e]));
+			m = std::fmax(m, std::fabs(a[(size_t)k*E + e]));
+		}
+		num = std::fmax(num, m > 0 ? d/m : d);
+		den = std::fmax(den, m);
+	}
+	std::printf(
+		"{\"sites\": %d, \"N\": %d, \"M\": %d, \"E\": %d, "
+		"\"fp64_s\": %.4f, \"mixed_s\": %.4f, \"first_call_s\": %.4f, "
+		"\"mixed_rel_err\": %.3e}\n",
+		sites, 2*L*L, M, E, fp64, mixed, warm, num
+	);
+	return 0;
+}
+
 int exitShort(){
 	Model model;
 	model.setVerbose(false);
@@ -290,6 +476,10 @@ int main(int argc, char **argv){
 	TBTK::Initialize();
 	if(argc > 1 && std::strcmp(argv[1], "exit-short") == 0)
 		return exitShort();
+	if(argc > 3 && std::strcmp(argv[1], "dump") == 0)
+		return dump(std::strcmp(argv[2], "gpu") == 0, argv[3]);
+	if(argc > 1 && std::strcmp(argv[1], "time") == 0)
+		return timeLDOS();
 
 	Model model;
 	model.setVerbose(false);
