@@ -452,6 +452,10 @@ def ours(args, world, rank, local):
         torch.cuda.synchronize()
         clocks.start()
         launches0 = kpm.kernel_launches()
+        # where a launch list of this command (ncu -k regex:'^(kpm_|k_)' -s N)
+        # finds the timed region: the library's own kernels launched before it
+        print(f"[bench] library kernel launches before the timed region: {launches0}",
+              file=sys.stderr, flush=True)
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         marks = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]

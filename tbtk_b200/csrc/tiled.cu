@@ -75,7 +75,6 @@ int build_plan(tbtkkpm_matrix *m, int R, bool cplx, TilePlanStore &p) {
                                 (int64_t)ntiles + 1, st);
   cub::DeviceScan::ExclusiveSum(tmp.ptr, tb2, truns.as<uint32_t>(), run.as<uint32_t>(),
                                 (int64_t)ntiles + 1, st);
-  count_launches(2);
   uint32_t chunks = 0, nruns = 0;
   if ((e = cudaMemcpyAsync(&chunks, ent.as<uint32_t>() + ntiles, 4, cudaMemcpyDeviceToHost, st)) ||
       (e = cudaMemcpyAsync(&nruns, run.as<uint32_t>() + ntiles, 4, cudaMemcpyDeviceToHost, st)) ||
