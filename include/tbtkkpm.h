@@ -43,6 +43,7 @@ extern "C" {
 #define TBTKKPM_ERR_TIMEOUT -4    /* a bounded device wait ran out */
 #define TBTKKPM_ERR_UNSUPPORTED -5/* combination not available */
 #define TBTKKPM_ERR_STATE -6      /* handle in the wrong state */
+#define TBTKKPM_ERR_CANCELLED -7  /* a server request was cancelled */
 
 /* Message of the calling thread's last failed call ("" if none). */
 TBTKKPM_API const char *tbtkkpm_last_error(void);
@@ -375,17 +376,22 @@ TBTKKPM_API int tbtkkpm_expectation_values(
 	const uint32_t *from, uint32_t P, double broadening, int precision,
 	const double *occupation, double dE, double *out);
 
-/* ------------------------------------------------------------ LDOS server
+/* ------------------------------------------------------------ server
  *
- * A device-resident LDOS service over many models (no reference
- * counterpart: the reference answers one calculateLDOS call at a time,
- * Lib/src/PropertyExtractor/ChebyshevExpander.cpp:475-505).  Each model
- * owns `width` lanes; a request (model, up to `width` sites, M moments,
- * broadening) takes free lanes at the next step boundary, and one kernel
- * launch per step advances every lane of every resident model (continuous
- * batching).  Lanes run complex64 vectors with FP64 arithmetic, FP64
- * moments and the doubling identities; a request whose error estimate
- * exceeds `tolerance` is recomputed in FP64 (tbtkkpm_ldos_sites at
+ * A device-resident LDOS and Green's-function service over many models (no
+ * reference counterpart: the reference answers one calculateLDOS or
+ * calculateGreensFunction call at a time,
+ * Lib/src/PropertyExtractor/ChebyshevExpander.cpp:96-295,475-505).  Each
+ * model owns `width` lanes; a request (model, up to `width` sites or
+ * (to, from) pairs, M moments, broadening) takes free lanes at the next
+ * step boundary, one lane per source, and one kernel launch per step
+ * advances every lane of every resident model (continuous batching).
+ * Lanes run complex64 (or, for real models, float) vectors with FP64
+ * arithmetic and FP64 moments; LDOS requests and Green's-function requests
+ * whose pairs are all diagonal use the doubling identities, other
+ * Green's-function requests gather every moment directly.  An output whose
+ * error estimate exceeds `tolerance` is recomputed in FP64
+ * (tbtkkpm_ldos_sites, or tbtkkpm_moments_batched + tbtkkpm_greens, at
  * TBTKKPM_FP64).  Each result depends only on its own request: the same
  * bits alone or among any other requests.  Lane memory (vectors, moments)
  * of a model is allocated when it first gets a request and counts against
@@ -419,14 +425,45 @@ TBTKKPM_API int tbtkkpm_server_submit(
 	tbtkkpm_server *s, uint32_t model, const uint32_t *sites,
 	uint32_t n_sites, uint32_t M, double broadening, uint64_t *request);
 
-/* Waits up to timeout_s seconds (0: poll) for a request.  Returns
+/* Queues the Green's functions G(to[k], from[k]) of one type (TBTKKPM_*
+ * type codes) for n_pairs pairs of a model (calculateGreensFunction(s),
+ * Lib/src/PropertyExtractor/ChebyshevExpander.cpp:96-295: coefficients
+ * <to|T_n|from> of the recursion started at `from`, then
+ * generateGreensFunction of that type,
+ * Lib/src/Solver/ChebyshevExpander.cpp:277-361).  Pairs with the same
+ * from-index share one lane; 1 <= n_pairs <= width.  If every pair has
+ * to == from the lanes run the doubling recursion to M/2 as LDOS requests
+ * do; otherwise they run M - 1 steps and gather every moment directly. */
+TBTKKPM_API int tbtkkpm_server_submit_greens(
+	tbtkkpm_server *s, uint32_t model, const uint32_t *to,
+	const uint32_t *from, uint32_t n_pairs, uint32_t M, double broadening,
+	int type, uint64_t *request);
+
+/* Waits up to timeout_s seconds (0: poll) for an LDOS request.  Returns
  * TBTKKPM_OK with ldos_out [n_sites][E], err_out [n_sites] (error estimate
  * of the mixed-precision run) and rerun_out [n_sites] (1 where the FP64
  * recomputation replaced it) filled and the request released, or
- * TBTKKPM_PENDING.  Output pointers may be NULL. */
+ * TBTKKPM_PENDING.  Output pointers may be NULL.  A cancelled request
+ * returns TBTKKPM_ERR_CANCELLED and is released. */
 TBTKKPM_API int tbtkkpm_server_wait(
 	tbtkkpm_server *s, uint64_t request, double timeout_s, double *ldos_out,
 	double *err_out, int32_t *rerun_out);
+
+/* Same for a Green's-function request: G_out [n_pairs][E] complex, err_out
+ * and rerun_out [n_pairs].  The estimate of a pair gathered directly is its
+ * source's doubling gap (the error scale of moments from the same float
+ * vectors) relative to the pair's largest moment. */
+TBTKKPM_API int tbtkkpm_server_wait_greens(
+	tbtkkpm_server *s, uint64_t request, double timeout_s, double *G_out,
+	double *err_out, int32_t *rerun_out);
+
+/* Cancels a request that is queued or in its recursion: a queued one never
+ * starts, one in flight leaves its lanes at the next step boundary; its
+ * wait then returns TBTKKPM_ERR_CANCELLED.  A request whose recursion has
+ * ended (its results are being formed or are ready) is not affected:
+ * TBTKKPM_ERR_STATE.  Cancelling twice is not an error.  (No reference
+ * counterpart.) */
+TBTKKPM_API int tbtkkpm_server_cancel(tbtkkpm_server *s, uint64_t request);
 
 /* Statistics into out[n] (n <= TBTKKPM_STAT_COUNT): */
 #define TBTKKPM_STAT_COMPLETED 0  /* requests finished */

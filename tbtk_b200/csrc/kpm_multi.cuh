@@ -44,7 +44,35 @@ struct MultiModel {
   double2 *mu_direct;        // [W][ld] directly gathered moments
   uint32_t tile0;            // first tile of this model in the launch
   uint32_t ntiles;
+  double2 *pmu;              // [W][mmax] moments of Green's-function pairs (pair entries)
+  uint32_t mmax;
 };
+
+// A model's target list pairs a row with an entry word: bits 0-7 the lane
+// (the column of the vectors), and with kPairEntry set the moment of the
+// lane's local step n goes to row n of pair slot (bits 8-15) of pmu, for
+// n < the lane's M, instead of row n < ld of the lane's direct-moment row.
+constexpr uint32_t kLaneBits = 0xffu;
+constexpr uint32_t kPairEntry = 1u << 31;
+// lane_M flag of a lane whose request gathers every moment directly
+// (Green's-function pairs with to != from): it runs M - 1 steps; the
+// doubling sums of its own source still give its error estimate.
+constexpr uint32_t kDirectLane = 1u << 31;
+constexpr uint32_t kLaneMBits = ~kDirectLane;
+
+// Destination of the moment of local step nl for target entry tc of model
+// md, or nullptr when the entry takes no moment at this step.
+__device__ __forceinline__ double2 *multi_target_dst(const MultiModel *__restrict__ md, uint32_t tc,
+                                                     int32_t nl, uint32_t ld) {
+  if (nl < 1) return nullptr;
+  const uint32_t c = tc & kLaneBits;
+  if (tc & kPairEntry) {
+    if ((uint32_t)nl >= (__ldg(md->lane_M + c) & kLaneMBits)) return nullptr;
+    return md->pmu + (uint64_t)((tc >> 8) & kLaneBits) * md->mmax + nl;
+  }
+  if ((uint32_t)nl >= ld) return nullptr;
+  return md->mu_direct + (uint64_t)c * ld + nl;
+}
 
 // Per-tick launch header (device resident): the models, their tile total,
 // the global step of step offset 0 and the model of every tile.
@@ -130,7 +158,6 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
   // fields of the current model kept in registers
   const uint32_t *t_bitmap = nullptr, *t_row = nullptr, *t_col = nullptr;
   const int32_t *t_base = nullptr;
-  double2 *t_mud = nullptr;
   long long *t_dots = nullptr;
   uint32_t t_count = 0;
 
@@ -193,7 +220,6 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
       t_col = md->tcol;
       t_count = md->tcount;
       t_base = md->base;
-      t_mud = md->mu_direct;
       t_dots = md->dots;
       first = 0;
 #pragma unroll
@@ -295,14 +321,15 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
             if (__ldg(t_row + mid) < row) lo = mid + 1; else hi = mid;
           }
           for (uint32_t i = lo; i < t_count && __ldg(t_row + i) == row; i++) {
-            const uint32_t c = __ldg(t_col + i);
+            const uint32_t tc = __ldg(t_col + i);
+            const uint32_t c = tc & kLaneBits;
             const int jt = P::slot_of(sub, c);
             if (jt < 0) continue;
-            const int32_t nl = n - __ldg(t_base + c);
-            if (nl >= 1 && (uint32_t)nl < ld) {
+            double2 *dst = multi_target_dst(models + mi, tc, n - __ldg(t_base + c), ld);
+            if (dst) {
 #pragma unroll
               for (int j = 0; j < VPT; j++)
-                if (j == jt) t_mud[(uint64_t)c * ld + nl] = acc[j];
+                if (j == jt) *dst = acc[j];
             }
           }
         }
@@ -344,7 +371,7 @@ static __global__ void kpm_multi_finalize(const MultiModel *__restrict__ models,
     const int32_t base = md->base[c];
     if (base == kLaneIdle) continue;
     const int32_t m = n - base;
-    const uint32_t M = md->lane_M[c];
+    const uint32_t M = md->lane_M[c] & kLaneMBits;
     if (m < 1 || (uint32_t)m > M / 2) continue;
     double2 *row = md->mu + (uint64_t)c * Mmax;
     if (m == 1) row[1] = md->mu_direct[(uint64_t)c * ld + 1];
@@ -436,6 +463,67 @@ kpm_multi_error(const MultiDone *__restrict__ lanes, uint32_t M, double *__restr
     sc = fmax(sc, hypot(a.x, a.y));
     if (n >= 2 && n < ld) {
       const double2 b = d.mu_direct[n];
+      dm = fmax(dm, hypot(a.x - b.x, a.y - b.y));
+    }
+  }
+  rs[threadIdx.x] = sc;
+  rd[threadIdx.x] = dm;
+  __syncthreads();
+  for (int h = kErrorBlock / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) {
+      rs[threadIdx.x] = fmax(rs[threadIdx.x], rs[threadIdx.x + h]);
+      rd[threadIdx.x] = fmax(rd[threadIdx.x], rd[threadIdx.x + h]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) err[blockIdx.x] = rs[0] > 0 ? 4.0 * sqrt(2.0) * rd[0] / rs[0] : 0.0;
+}
+
+// A (to, from) pair of a finished Green's-function request whose lanes
+// gathered every moment directly: its moment row in pmu (rows n >= 1
+// written by the steps), mu_0 = <to|from>, and the diagonal moment rows of
+// its source lane (doubled and direct), which give the error estimate.
+struct MultiPair {
+  const double2 *row;         // pair slot row [Mmax]
+  double mu0;                 // 1 if to == from, else 0
+  const double2 *lane_mu;     // the source lane's doubled moments [Mmax]
+  const double2 *lane_direct; // its directly gathered moments [ld]
+};
+
+// The damped moments of K pairs, [K][M] contiguous (as kpm_multi_prepare).
+static __global__ void kpm_multi_prepare_pairs(const MultiPair *__restrict__ pairs, uint32_t K,
+                                               uint32_t M, const double *__restrict__ a, double b,
+                                               int damp, double2 *__restrict__ out) {
+  const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (uint64_t)K * M) return;
+  const uint32_t k = (uint32_t)(i / M), nn = (uint32_t)(i % M);
+  const MultiPair p = pairs[k];
+  double2 c = nn == 0 ? make_double2(p.mu0, 0.0) : p.row[nn];
+  if (damp) {
+    const double an = a[nn];
+    c = make_double2(__ddiv_rn(__dmul_rn(c.x, an), b), __ddiv_rn(__dmul_rn(c.y, an), b));
+  }
+  out[i] = c;
+}
+
+// Error estimate of each pair: the source lane's gap between doubled and
+// direct diagonal moments, 4 sqrt(2) max_{2 <= n <= M/2} |mu_n - mu_direct_n|
+// (an absolute error scale of moments from these float vectors; the pair's
+// own moments are gathered directly, which carry less rounding), relative
+// to the pair's max_n |mu_n|.  One block of kErrorBlock threads per pair.
+static __global__ void __launch_bounds__(kErrorBlock)
+kpm_pair_error(const MultiPair *__restrict__ pairs, uint32_t M, double *__restrict__ err) {
+  __shared__ double rs[kErrorBlock], rd[kErrorBlock];
+  const MultiPair p = pairs[blockIdx.x];
+  const uint32_t ld = M / 2 + 1;
+  double sc = threadIdx.x == 0 ? fabs(p.mu0) : 0.0, dm = 0.0;
+  for (uint32_t n = threadIdx.x; n < M; n += kErrorBlock) {
+    if (n >= 1) {
+      const double2 q = p.row[n];
+      sc = fmax(sc, hypot(q.x, q.y));
+    }
+    if (n >= 2 && n < ld) {
+      const double2 a = p.lane_mu[n], b = p.lane_direct[n];
       dm = fmax(dm, hypot(a.x - b.x, a.y - b.y));
     }
   }

@@ -43,7 +43,6 @@ kpm_multi_step_real(const MultiModel *__restrict__ models, const MultiHeader *__
   uint32_t first = 0;
   const uint32_t *t_bitmap = nullptr, *t_row = nullptr, *t_col = nullptr;
   const int32_t *t_base = nullptr;
-  double2 *t_mud = nullptr;
   long long *t_dots = nullptr;
   uint32_t t_count = 0;
 
@@ -102,7 +101,6 @@ kpm_multi_step_real(const MultiModel *__restrict__ models, const MultiHeader *__
       t_col = md->tcol;
       t_count = md->tcount;
       t_base = md->base;
-      t_mud = md->mu_direct;
       t_dots = md->dots;
       first = 0;
 #pragma unroll
@@ -191,14 +189,15 @@ kpm_multi_step_real(const MultiModel *__restrict__ models, const MultiHeader *__
             if (__ldg(t_row + mid) < row) lo = mid + 1; else hi = mid;
           }
           for (uint32_t i = lo; i < t_count && __ldg(t_row + i) == row; i++) {
-            const uint32_t c = __ldg(t_col + i);
+            const uint32_t tc = __ldg(t_col + i);
+            const uint32_t c = tc & kLaneBits;
             const int jt = P::slot_of(sub, c);
             if (jt < 0) continue;
-            const int32_t nl = n - __ldg(t_base + c);
-            if (nl >= 1 && (uint32_t)nl < ld) {
+            double2 *dst = multi_target_dst(models + mi, tc, n - __ldg(t_base + c), ld);
+            if (dst) {
 #pragma unroll
               for (int j = 0; j < VPT; j++)
-                if (j == jt) t_mud[(uint64_t)c * ld + nl] = make_double2(acc[j], 0.0);
+                if (j == jt) *dst = make_double2(acc[j], 0.0);
             }
           }
         }

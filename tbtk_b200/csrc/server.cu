@@ -44,22 +44,41 @@ constexpr uint32_t kMaxWidth = 64;
 
 bool valid_width(uint32_t w) { return w >= 1 && w <= kMaxWidth && (w & (w - 1)) == 0; }
 
+constexpr int kLdos = -1;  // Request::kind of an LDOS request
+
 struct Request {
   uint64_t id = 0;
   uint32_t model = 0;
+  int kind = kLdos;  // kLdos, or the Green's function type (TBTKKPM_ADVANCED..NONPRINCIPAL)
+  // the sources, one lane each: the LDOS sites, or the distinct from-indices
+  // of a Green's-function request in order of first appearance
   std::vector<uint32_t> sites;
+  // Green's-function pairs: to[k], and the source (index into sites) of pair k
+  std::vector<uint32_t> to, pair_src;
+  // some pair has to != from: every lane gathers all moments directly
+  // (M - 1 steps) into pair slots instead of stepping to M/2 with doubling
+  bool direct = false;
+  std::vector<uint32_t> slots;  // pair slot of pair k in its model (direct requests)
   uint32_t M = 0;
   double broadening = 0;
   Clock::time_point t_submit;
   std::vector<uint32_t> lanes;
   int32_t base = 0;
   bool done = false;
+  bool finishing = false;  // its results are being formed (cancel no longer applies)
+  bool cancelled = false;
   int status = TBTKKPM_OK;
   std::string message;
-  std::vector<double> ldos, err;
+  std::vector<double> ldos, err;  // LDOS [K][E], or G [K][E] complex for a GF request
   std::vector<int32_t> rerun;
   // staging of the finish phase
   size_t stage_off = 0;
+  // recursion steps of each lane
+  uint32_t steps() const { return direct ? M - 1 : M / 2; }
+  // results: one per site, or one per pair
+  uint32_t outputs() const { return kind == kLdos ? (uint32_t)sites.size() : (uint32_t)to.size(); }
+  // doubles of one result over the energy grid
+  uint32_t result_doubles(uint32_t E) const { return kind == kLdos ? E : 2 * E; }
 };
 
 struct Model {
@@ -74,18 +93,22 @@ struct Model {
   uint64_t bytes = 0;
   uint64_t last_tick = 0;
   size_t esize() const { return real ? sizeof(float) : sizeof(float2); }
-  DevBuf vec[2], dots, mu, mu_direct, base, laneM, bitmap, tlist;
+  DevBuf vec[2], dots, mu, mu_direct, base, laneM, bitmap, tlist, pmu;
   std::vector<int32_t> base_h;
   std::vector<uint32_t> M_h;
   std::vector<uint64_t> lane_req;  // request per lane, 0 when free
   std::vector<uint32_t> lane_site;
+  // per lane: (to row, pair slot) of its Green's-function pairs (direct requests)
+  std::vector<std::vector<std::pair<uint32_t, uint32_t>>> lane_pairs;
+  std::vector<uint64_t> pair_req;  // request per pair slot, 0 when free
   std::vector<uint32_t> bitmap_h;
-  uint32_t busy = 0;
+  uint32_t busy = 0, pairs_busy = 0;
   uint32_t tcount = 0;
   bool dirty = true;
   DevBuf lane_mem;  // one allocation; the lane buffers above are views into it
   void release_lanes() {
-    for (DevBuf *b : {&vec[0], &vec[1], &dots, &mu, &mu_direct, &base, &laneM, &bitmap, &tlist}) {
+    for (DevBuf *b : {&vec[0], &vec[1], &dots, &mu, &mu_direct, &base, &laneM, &bitmap, &tlist,
+                      &pmu}) {
       b->ptr = nullptr;
       b->cap = 0;
     }
@@ -95,11 +118,12 @@ struct Model {
 };
 
 // Lane memory of a model: vectors, fixed-point sums, moments, lane tables,
-// target bitmap and list.
+// target bitmap and list (a row and an entry word for each of up to W
+// lane sites and W pair targets), pair moments.
 uint64_t lane_bytes(uint32_t N, uint32_t W, uint32_t Mmax, uint32_t ld, size_t esize) {
   return 2ull * N * W * esize + 2ull * W * sizeof(long long) +
          (uint64_t)W * Mmax * sizeof(double2) + (uint64_t)W * ld * sizeof(double2) +
-         8ull * W + 4ull * ((N + 31) / 32) + 8ull * W;
+         8ull * W + 4ull * ((N + 31) / 32) + 16ull * W + (uint64_t)W * Mmax * sizeof(double2);
 }
 
 // The step kernels of one class: complex64 lanes or real float lanes.
@@ -172,7 +196,7 @@ struct tbtkkpm_server {
   int32_t n_global = 1;  // next global step
   uint64_t tick_no = 0;
   uint64_t resident = 0;
-  DevBuf d_models, d_hdr, d_joins, d_done, d_stage, d_damp, d_tiles;
+  DevBuf d_models, d_hdr, d_joins, d_done, d_pairs, d_stage, d_damp, d_tiles;
   // statistics
   std::vector<double> latencies_ms;
   double reruns = 0, ticks = 0, steps = 0, lane_steps = 0, evictions = 0, waited = 0, busy_s = 0;
@@ -200,14 +224,22 @@ int make_resident(tbtkkpm_server *s, Model *m) {
   const size_t words = (N + 31) / 32;
   int rc;
   const size_t es = m->esize();
-  // one allocation per model for the nine lane buffers
-  DevBuf *views[9] = {&m->vec[0], &m->vec[1], &m->dots, &m->mu, &m->mu_direct,
-                      &m->base, &m->laneM, &m->bitmap, &m->tlist};
-  const size_t sizes[9] = {es * (size_t)N * W, es * (size_t)N * W, 2 * sizeof(long long) * W,
-                           sizeof(double2) * (size_t)W * s->Mmax, sizeof(double2) * (size_t)W * s->ld,
-                           4 * (size_t)W, 4 * (size_t)W, 4 * words, 8 * (size_t)W};
-  size_t off[9], total = 0;
-  for (int i = 0; i < 9; i++) {
+  // one allocation per model for the ten lane buffers
+  constexpr int kViews = 10;
+  DevBuf *views[kViews] = {&m->vec[0], &m->vec[1], &m->dots,   &m->mu,    &m->mu_direct,
+                           &m->base,   &m->laneM,  &m->bitmap, &m->tlist, &m->pmu};
+  const size_t sizes[kViews] = {es * (size_t)N * W,
+                                es * (size_t)N * W,
+                                2 * sizeof(long long) * W,
+                                sizeof(double2) * (size_t)W * s->Mmax,
+                                sizeof(double2) * (size_t)W * s->ld,
+                                4 * (size_t)W,
+                                4 * (size_t)W,
+                                4 * words,
+                                16 * (size_t)W,
+                                sizeof(double2) * (size_t)W * s->Mmax};
+  size_t off[kViews], total = 0;
+  for (int i = 0; i < kViews; i++) {
     off[i] = total;
     total += (sizes[i] + 255) & ~(size_t)255;
   }
@@ -215,7 +247,7 @@ int make_resident(tbtkkpm_server *s, Model *m) {
     m->release_lanes();
     return rc;
   }
-  for (int i = 0; i < 9; i++) {
+  for (int i = 0; i < kViews; i++) {
     views[i]->ptr = m->lane_mem.as<char>() + off[i];
     views[i]->cap = sizes[i];
   }
@@ -230,8 +262,11 @@ int make_resident(tbtkkpm_server *s, Model *m) {
   m->M_h.assign(W, 0);
   m->lane_req.assign(W, 0);
   m->lane_site.assign(W, 0);
+  m->lane_pairs.assign(W, {});
+  m->pair_req.assign(W, 0);
   m->bitmap_h.assign(words, 0);
   m->busy = 0;
+  m->pairs_busy = 0;
   m->dirty = true;
   m->resident = true;
   s->resident += m->bytes;
@@ -276,7 +311,8 @@ int admit(tbtkkpm_server *s, std::vector<MultiJoin> &joins, std::vector<JoinRef>
     Request *r = s->requests.at(*it).get();
     Model *m = s->models[r->model].get();
     const uint32_t K = (uint32_t)r->sites.size();
-    if (m->resident && m->W - m->busy < K) {
+    const uint32_t npairs = r->direct ? (uint32_t)r->to.size() : 0u;
+    if (m->resident && (m->W - m->busy < K || m->W - m->pairs_busy < npairs)) {
       ++it;
       continue;
     }
@@ -301,7 +337,7 @@ int admit(tbtkkpm_server *s, std::vector<MultiJoin> &joins, std::vector<JoinRef>
       m->lane_req[c] = r->id;
       m->lane_site[c] = site;
       m->base_h[c] = r->base;
-      m->M_h[c] = r->M;
+      m->M_h[c] = r->M | (r->direct ? kDirectLane : 0u);
       m->bitmap_h[site >> 5] |= 1u << (site & 31);
       r->lanes.push_back(c);
       MultiJoin j;
@@ -318,11 +354,38 @@ int admit(tbtkkpm_server *s, std::vector<MultiJoin> &joins, std::vector<JoinRef>
       joins.push_back(j);
       refs.push_back({m, c, r});
     }
+    if (r->direct) {
+      // pair slots: pair k's moments are gathered at its to-row from its
+      // source's lane
+      r->slots.clear();
+      for (uint32_t k = 0, d = 0; k < npairs; k++) {
+        while (m->pair_req[d]) d++;
+        m->pair_req[d] = r->id;
+        m->lane_pairs[r->lanes[r->pair_src[k]]].push_back({r->to[k], d});
+        r->slots.push_back(d);
+      }
+      m->pairs_busy += npairs;
+    }
     m->busy += K;
     m->dirty = true;
     it = s->pending.erase(it);
   }
   return TBTKKPM_OK;
+}
+
+// Frees the lanes and pair slots of a request that finished or was
+// cancelled (under s->mu).
+void release_request_lanes(Model *m, Request *r) {
+  for (uint32_t c : r->lanes) {
+    m->lane_req[c] = 0;
+    m->base_h[c] = kLaneIdle;
+    m->M_h[c] = 0;
+    m->lane_pairs[c].clear();
+  }
+  for (uint32_t d : r->slots) m->pair_req[d] = 0;
+  m->pairs_busy -= (uint32_t)r->slots.size();
+  m->busy -= (uint32_t)r->lanes.size();
+  m->dirty = true;
 }
 
 // ------------------------------------------------------------ one tick
@@ -339,19 +402,22 @@ struct ClassPlan {
 // copies come from pageable memory, so the host arrays are free on return).
 int upload_lanes(tbtkkpm_server *s, Model *m) {
   if (!m->dirty) return TBTKKPM_OK;
-  // target list: busy lanes sorted by site row
+  // target list sorted by row: every busy lane at its site (direct
+  // moments of its own source), and the pair targets of direct lanes
   std::vector<std::pair<uint32_t, uint32_t>> t;
   std::fill(m->bitmap_h.begin(), m->bitmap_h.end(), 0u);
   for (uint32_t c = 0; c < m->W; c++)
     if (m->lane_req[c]) {
       t.push_back({m->lane_site[c], c});
-      m->bitmap_h[m->lane_site[c] >> 5] |= 1u << (m->lane_site[c] & 31);
+      for (const auto &pr : m->lane_pairs[c]) t.push_back({pr.first, c | (pr.second << 8) | kPairEntry});
     }
+  for (const auto &e : t) m->bitmap_h[e.first >> 5] |= 1u << (e.first & 31);
   std::sort(t.begin(), t.end());
-  std::vector<uint32_t> tl(2 * (size_t)m->W, 0);
+  const size_t cap = 2 * (size_t)m->W;
+  std::vector<uint32_t> tl(2 * cap, 0);
   for (size_t i = 0; i < t.size(); i++) {
     tl[i] = t[i].first;
-    tl[m->W + i] = t[i].second;
+    tl[cap + i] = t[i].second;
   }
   m->tcount = (uint32_t)t.size();
   cudaError_t e;
@@ -380,14 +446,15 @@ MultiModel describe(const tbtkkpm_server *s, const Model *m) {
   d.vec[1] = m->vec[1].as<float2>();
   d.bitmap = m->bitmap.as<uint32_t>();
   d.trow = m->tlist.as<uint32_t>();
-  d.tcol = m->tlist.as<uint32_t>() + m->W;
+  d.tcol = m->tlist.as<uint32_t>() + 2 * m->W;
   d.tcount = m->tcount;
   d.base = m->base.as<int32_t>();
   d.lane_M = m->laneM.as<uint32_t>();
   d.dots = m->dots.as<long long>();
   d.mu = m->mu.as<double2>();
   d.mu_direct = m->mu_direct.as<double2>();
-  (void)s;
+  d.pmu = m->pmu.as<double2>();
+  d.mmax = s->Mmax;
   return d;
 }
 
@@ -458,7 +525,9 @@ int run_joins(tbtkkpm_server *s, const std::vector<MultiJoin> &joins, const std:
     const MultiJoin &j = joins[i];
     const Model *m = refs[i].m;
     const uint32_t want = std::min(m->head_steps, j.M / 2 >= 1 ? j.M / 2 - 1 : 0u);
-    if (!m->mat->pattern_symmetric || want < 2) continue;
+    // the head writes its source's own moments only: lanes that gather
+    // pair moments start from j_0
+    if (!m->mat->pattern_symmetric || want < 2 || refs[i].r->direct) continue;
     PrefixJob p{};
     p.slice_ptr = m->mat->slice_ptr.as<uint32_t>();
     p.scol = m->mat->scol.as<uint32_t>();
@@ -578,23 +647,26 @@ int finish_launch(tbtkkpm_server *s, FinishBatch &fb) {
   if (fb.done.empty()) return TBTKKPM_OK;
   cudaStream_t st = s->stream;
   const uint32_t E = s->E;
-  // moments stage per request: damped moments [K][M]; results per request:
-  // ldos [K][E] | err [K]
-  size_t total = 0, lanes = 0, damp_len = 0, nres = 0;
+  // moments stage per request: damped moments [K][M] of its K outputs;
+  // results per request: LDOS [K][E] or G [K][E] complex, then err [K]
+  size_t total = 0, lanes = 0, pairs = 0, damp_len = 0, nres = 0;
   fb.res_off.resize(fb.done.size());
   for (size_t i = 0; i < fb.done.size(); i++) {
     Request *r = fb.done[i];
-    const size_t K = r->sites.size(), M = r->M;
+    const size_t K = r->outputs(), M = r->M;
     r->stage_off = total;
     total += sizeof(double2) * K * M;
     total = (total + 255) & ~(size_t)255;
+    nres = (nres + 1) & ~(size_t)1;  // complex results start on 16 bytes
     fb.res_off[i] = nres;
-    nres += K * E + K;
-    lanes += K;
+    nres += K * r->result_doubles(E) + K;
+    (r->direct ? pairs : lanes) += K;
     damp_len += M;
   }
   int rc;
-  if ((rc = s->d_stage.reserve(total)) || (rc = s->d_done.reserve(sizeof(MultiDone) * lanes)) ||
+  if ((rc = s->d_stage.reserve(total)) ||
+      (rc = s->d_done.reserve(sizeof(MultiDone) * std::max<size_t>(lanes, 1))) ||
+      (rc = s->d_pairs.reserve(sizeof(MultiPair) * std::max<size_t>(pairs, 1))) ||
       (rc = s->d_damp.reserve(sizeof(double) * damp_len)) || (rc = s->d_res.reserve(sizeof(double) * nres)))
     return rc;
   cudaError_t e;
@@ -607,15 +679,30 @@ int finish_launch(tbtkkpm_server *s, FinishBatch &fb) {
       return cuda_fail(e, "server: pinned results");
     s->h_res_cap = cap;
   }
+  // per output: the moment rows of its lane (LDOS sites, diagonal pairs)
+  // or its pair slot (direct requests)
   std::vector<MultiDone> lane_ptr;
+  std::vector<MultiPair> pair_ptr;
   std::vector<double> damp_all;
   std::vector<double> bvals;
   for (size_t i = 0; i < fb.done.size(); i++) {
     Request *r = fb.done[i];
     Model *m = fb.owner[i];
-    for (uint32_t c : r->lanes)
-      lane_ptr.push_back({m->mu.as<double2>() + (size_t)c * s->Mmax,
-                          m->mu_direct.as<double2>() + (size_t)c * s->ld});
+    auto lane_rows = [&](uint32_t c) {
+      return MultiDone{m->mu.as<double2>() + (size_t)c * s->Mmax,
+                       m->mu_direct.as<double2>() + (size_t)c * s->ld};
+    };
+    if (r->kind == kLdos) {
+      for (uint32_t c : r->lanes) lane_ptr.push_back(lane_rows(c));
+    } else if (!r->direct) {
+      for (uint32_t k = 0; k < r->to.size(); k++) lane_ptr.push_back(lane_rows(r->lanes[r->pair_src[k]]));
+    } else {
+      for (uint32_t k = 0; k < r->to.size(); k++) {
+        const MultiDone l = lane_rows(r->lanes[r->pair_src[k]]);
+        pair_ptr.push_back({m->pmu.as<double2>() + (size_t)r->slots[k] * s->Mmax,
+                            r->to[k] == r->sites[r->pair_src[k]] ? 1.0 : 0.0, l.mu, l.mu_direct});
+      }
+    }
     std::vector<double> a;
     double b = 1;
     if (r->broadening != 0) damping_factors(r->M, r->broadening, a, b);
@@ -623,25 +710,39 @@ int finish_launch(tbtkkpm_server *s, FinishBatch &fb) {
     damp_all.insert(damp_all.end(), a.begin(), a.end());
     bvals.push_back(b);
   }
-  if ((e = cudaMemcpyAsync(s->d_done.ptr, lane_ptr.data(), sizeof(MultiDone) * lanes,
-                           cudaMemcpyHostToDevice, st)) ||
+  if ((!lane_ptr.empty() &&
+       (e = cudaMemcpyAsync(s->d_done.ptr, lane_ptr.data(), sizeof(MultiDone) * lane_ptr.size(),
+                            cudaMemcpyHostToDevice, st))) ||
+      (!pair_ptr.empty() &&
+       (e = cudaMemcpyAsync(s->d_pairs.ptr, pair_ptr.data(), sizeof(MultiPair) * pair_ptr.size(),
+                            cudaMemcpyHostToDevice, st))) ||
       (e = cudaMemcpyAsync(s->d_damp.ptr, damp_all.data(), sizeof(double) * damp_len,
                            cudaMemcpyHostToDevice, st)))
     return cuda_fail(e, "server: finish staging");
-  size_t lane0 = 0, d0 = 0;
+  size_t lane0 = 0, pair0 = 0, d0 = 0;
   for (size_t i = 0; i < fb.done.size(); i++) {
     Request *r = fb.done[i];
     Model *m = fb.owner[i];
-    const uint32_t K = (uint32_t)r->sites.size(), M = r->M;
+    const uint32_t K = r->outputs(), M = r->M;
     double2 *out = reinterpret_cast<double2 *>(s->d_stage.as<char>() + r->stage_off);
-    double *ldos = s->d_res.as<double>() + fb.res_off[i];
-    kpm_multi_prepare<<<blocks_for((uint64_t)K * M), 256, 0, st>>>(
-        s->d_done.as<MultiDone>() + lane0, K, M, s->d_damp.as<double>() + d0, bvals[i],
-        r->broadening != 0, out, nullptr, nullptr);
-    kpm_multi_error<<<K, kErrorBlock, 0, st>>>(s->d_done.as<MultiDone>() + lane0, M, ldos + (size_t)K * E);
+    double *res = s->d_res.as<double>() + fb.res_off[i];
+    double *err = res + (size_t)K * r->result_doubles(E);
+    if (r->direct) {
+      const MultiPair *pp = s->d_pairs.as<MultiPair>() + pair0;
+      kpm_multi_prepare_pairs<<<blocks_for((uint64_t)K * M), 256, 0, st>>>(
+          pp, K, M, s->d_damp.as<double>() + d0, bvals[i], r->broadening != 0, out);
+      kpm_pair_error<<<K, kErrorBlock, 0, st>>>(pp, M, err);
+      pair0 += K;
+    } else {
+      const MultiDone *dd = s->d_done.as<MultiDone>() + lane0;
+      kpm_multi_prepare<<<blocks_for((uint64_t)K * M), 256, 0, st>>>(
+          dd, K, M, s->d_damp.as<double>() + d0, bvals[i], r->broadening != 0, out, nullptr, nullptr);
+      kpm_multi_error<<<K, kErrorBlock, 0, st>>>(dd, M, err);
+      lane0 += K;
+    }
     count_launches(2);
-    if ((rc = launch_energy_sum(st, m->table, out, K, 4, ldos, M))) return rc;
-    lane0 += K;
+    // LDOS (4) or the request's Green's function type
+    if ((rc = launch_energy_sum(st, m->table, out, K, r->kind == kLdos ? 4 : r->kind, res, M))) return rc;
     d0 += M;
   }
   if (!fb.ev && (e = cudaEventCreateWithFlags(&fb.ev, cudaEventDisableTiming)) != cudaSuccess)
@@ -649,6 +750,51 @@ int finish_launch(tbtkkpm_server *s, FinishBatch &fb) {
   if ((e = cudaMemcpyAsync(s->h_res, s->d_res.ptr, sizeof(double) * nres, cudaMemcpyDeviceToHost, st)) ||
       (e = cudaEventRecord(fb.ev, st)))
     return cuda_fail(e, "server: finish");
+  return TBTKKPM_OK;
+}
+
+// FP64 recomputation of the outputs `idx` of a finished request (worker
+// thread, no lock held): LDOS sites through tbtkkpm_ldos_sites, Green's
+// function pairs through tbtkkpm_moments_batched and tbtkkpm_greens; each
+// result replaces the mixed-precision one in r->ldos.
+int rerun_fp64(tbtkkpm_server *s, Request *r, Model *m, const std::vector<uint32_t> &idx) {
+  const uint32_t E = s->E, M = r->M;
+  int rc;
+  tbtkkpm_table *t = exact_table(s, M, m->scale, &rc);
+  if (!t) return rc;
+  const size_t rd = r->result_doubles(E);
+  std::vector<double> out(idx.size() * rd);
+  if (r->kind == kLdos) {
+    std::vector<uint32_t> miss;
+    for (uint32_t k : idx) miss.push_back(r->sites[k]);
+    if ((rc = tbtkkpm_ldos_sites(m->mat, t, miss.data(), (uint32_t)miss.size(), r->broadening,
+                                 TBTKKPM_FP64, out.data(), nullptr)))
+      return rc;
+  } else {
+    // one source per distinct from-index of the missed pairs
+    std::vector<uint32_t> from, to, owner;
+    std::map<uint32_t, uint32_t> src;
+    for (uint32_t k : idx) {
+      const uint32_t f = r->sites[r->pair_src[k]];
+      auto it = src.find(f);
+      if (it == src.end()) {
+        it = src.emplace(f, (uint32_t)from.size()).first;
+        from.push_back(f);
+      }
+      to.push_back(r->to[k]);
+      owner.push_back(it->second);
+    }
+    std::vector<double> mu(2 * (size_t)idx.size() * M);
+    if ((rc = tbtkkpm_moments_batched(m->mat, from.data(), (uint32_t)from.size(), to.data(), owner.data(),
+                                      (uint32_t)to.size(), M, r->broadening, TBTKKPM_FP64, mu.data(),
+                                      nullptr)) ||
+        (rc = tbtkkpm_greens(t, mu.data(), (uint32_t)to.size(), r->kind, out.data())))
+      return rc;
+  }
+  for (size_t q = 0; q < idx.size(); q++) {
+    std::memcpy(r->ldos.data() + (size_t)idx[q] * rd, out.data() + q * rd, sizeof(double) * rd);
+    r->rerun[idx[q]] = 1;
+  }
   return TBTKKPM_OK;
 }
 
@@ -661,31 +807,19 @@ int finish_complete(tbtkkpm_server *s, FinishBatch &fb) {
   for (size_t i = 0; i < fb.done.size(); i++) {
     Request *r = fb.done[i];
     Model *m = fb.owner[i];
-    const uint32_t K = (uint32_t)r->sites.size(), M = r->M;
+    const uint32_t K = r->outputs();
+    const size_t rd = r->result_doubles(E);
     const double *res = s->h_res + fb.res_off[i];
-    r->ldos.assign(res, res + (size_t)K * E);
-    r->err.assign(res + (size_t)K * E, res + (size_t)K * E + K);
+    r->ldos.assign(res, res + (size_t)K * rd);
+    r->err.assign(res + (size_t)K * rd, res + (size_t)K * rd + K);
     r->rerun.assign(K, 0);
-    std::vector<uint32_t> miss;
     std::vector<uint32_t> idx;
     for (uint32_t k = 0; k < K; k++)
-      if (s->tol > 0 && !(r->err[k] <= s->tol)) {
-        miss.push_back(r->sites[k]);
-        idx.push_back(k);
-      }
-    if (!miss.empty()) {
+      if (s->tol > 0 && !(r->err[k] <= s->tol)) idx.push_back(k);
+    if (!idx.empty()) {
       const auto r0 = Clock::now();
-      tbtkkpm_table *t = exact_table(s, M, m->scale, &rc);
-      if (!t) return rc;
-      std::vector<double> out((size_t)miss.size() * E);
-      if ((rc = tbtkkpm_ldos_sites(m->mat, t, miss.data(), (uint32_t)miss.size(), r->broadening,
-                                   TBTKKPM_FP64, out.data(), nullptr)))
-        return rc;
-      for (size_t q = 0; q < idx.size(); q++) {
-        std::memcpy(r->ldos.data() + (size_t)idx[q] * E, out.data() + q * E, sizeof(double) * E);
-        r->rerun[idx[q]] = 1;
-      }
-      s->reruns += (double)miss.size();
+      if ((rc = rerun_fp64(s, r, m, idx))) return rc;
+      s->reruns += (double)idx.size();
       s->rerun_s += std::chrono::duration<double>(Clock::now() - r0).count();
     }
   }
@@ -795,7 +929,11 @@ void worker(tbtkkpm_server *s) {
         if (!m->lane_req[c]) continue;
         const Request *r = s->requests.at(m->lane_req[c]).get();
         if (r->lanes.empty() || r->lanes[0] != c) continue;  // one entry per request
-        const int64_t last = (int64_t)r->base + r->M / 2;  // global step of its last local step
+        if (r->cancelled) {
+          nsteps = 1;  // its lanes leave after this step
+          continue;
+        }
+        const int64_t last = (int64_t)r->base + r->steps();  // global step of its last local step
         const int64_t left = last - (int64_t)s->n_global + 1;
         nsteps = (uint32_t)std::min<int64_t>(nsteps, std::max<int64_t>(left, 1));
       }
@@ -825,7 +963,9 @@ void worker(tbtkkpm_server *s) {
     if (cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]) == cudaSuccess) s->step_s += ms * 1e-3;
     cudaGetLastError();
     for (const ClassPlan &cp : plans) s->step_bytes += cp.bytes * nsteps;
-    // finished requests: every lane past its last local step
+    // finished requests: every lane past its last local step; cancelled
+    // ones leave their lanes now, without results
+    bool cancelled = false;
     for (auto &p : s->models) {
       Model *m = p.get();
       if (!m->resident || !m->busy) continue;
@@ -834,12 +974,20 @@ void worker(tbtkkpm_server *s) {
         if (!id) continue;
         Request *r = s->requests.at(id).get();
         if (r->lanes.empty() || r->lanes[0] != c) continue;  // one entry per request
-        if ((int64_t)r->base + r->M / 2 <= (int64_t)s->n_global - 1) {
+        if (r->cancelled) {
+          release_request_lanes(m, r);
+          r->done = true;
+          r->status = TBTKKPM_ERR_CANCELLED;
+          r->message = "request cancelled";
+          cancelled = true;
+        } else if ((int64_t)r->base + r->steps() <= (int64_t)s->n_global - 1) {
+          r->finishing = true;
           prev.done.push_back(r);
           prev.owner.push_back(m);
         }
       }
     }
+    if (cancelled) s->cv_done.notify_all();
     // their device half goes on the stream before any join can reuse the lanes
     lk.unlock();
     const auto f0 = Clock::now();
@@ -850,15 +998,8 @@ void worker(tbtkkpm_server *s) {
     if (rc) break;
     for (size_t i = 0; i < prev.done.size(); i++) {
       Request *r = prev.done[i];
-      Model *m = prev.owner[i];
-      for (uint32_t c : r->lanes) {
-        m->lane_req[c] = 0;
-        m->base_h[c] = kLaneIdle;
-        m->M_h[c] = 0;
-      }
-      m->busy -= (uint32_t)r->lanes.size();
-      m->dirty = true;
-      s->lane_steps += (double)r->lanes.size() * (r->M / 2);
+      release_request_lanes(prev.owner[i], r);
+      s->lane_steps += (double)r->lanes.size() * r->steps();
     }
     s->busy_s += std::chrono::duration<double>(Clock::now() - t0).count();
   }
@@ -968,31 +1109,22 @@ extern "C" int tbtkkpm_server_add_model(tbtkkpm_server *s, const uint32_t *rowpt
   return TBTKKPM_OK;
 }
 
-extern "C" int tbtkkpm_server_submit(tbtkkpm_server *s, uint32_t model, const uint32_t *sites,
-                                     uint32_t n_sites, uint32_t M, double broadening,
-                                     uint64_t *request) {
-  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: NULL server");
-  if (!request || (!sites && n_sites)) return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: NULL pointer");
-  std::lock_guard<std::mutex> lk(s->mu);
+namespace tbtkkpm {
+namespace {
+
+// Checks shared by both request kinds and queues the request (under s->mu).
+int queue_request(tbtkkpm_server *s, std::unique_ptr<Request> r, uint64_t *request, const char *who) {
   if (s->failed) return fail(s->failed, "server: %s", s->fail_msg.c_str());
-  if (model >= s->models.size())
-    return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: no model %u", model);
-  Model *m = s->models[model].get();
-  if (n_sites == 0 || n_sites > m->W)
-    return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: %u sites for a model of %u lanes", n_sites,
-                m->W);
-  if (M < 2 || M > s->Mmax)
-    return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: M=%u outside [2, %u]", M, s->Mmax);
-  if (!(broadening >= 0)) return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: broadening < 0");
-  for (uint32_t k = 0; k < n_sites; k++)
-    if (sites[k] >= m->N)
-      return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: site %u >= N=%u", sites[k], m->N);
-  auto r = std::make_unique<Request>();
+  if (r->model >= s->models.size()) return fail(TBTKKPM_ERR_ARGUMENT, "%s: no model %u", who, r->model);
+  const Model *m = s->models[r->model].get();
+  if (r->M < 2 || r->M > s->Mmax)
+    return fail(TBTKKPM_ERR_ARGUMENT, "%s: M=%u outside [2, %u]", who, r->M, s->Mmax);
+  if (!(r->broadening >= 0)) return fail(TBTKKPM_ERR_ARGUMENT, "%s: broadening < 0", who);
+  for (uint32_t v : r->sites)
+    if (v >= m->N) return fail(TBTKKPM_ERR_ARGUMENT, "%s: index %u >= N=%u", who, v, m->N);
+  for (uint32_t v : r->to)
+    if (v >= m->N) return fail(TBTKKPM_ERR_ARGUMENT, "%s: index %u >= N=%u", who, v, m->N);
   r->id = s->next_id++;
-  r->model = model;
-  r->sites.assign(sites, sites + n_sites);
-  r->M = M;
-  r->broadening = broadening;
   r->t_submit = Clock::now();
   *request = r->id;
   s->pending.push_back(r->id);
@@ -1001,14 +1133,20 @@ extern "C" int tbtkkpm_server_submit(tbtkkpm_server *s, uint32_t model, const ui
   return TBTKKPM_OK;
 }
 
-extern "C" int tbtkkpm_server_wait(tbtkkpm_server *s, uint64_t request, double timeout_s,
-                                   double *ldos_out, double *err_out, int32_t *rerun_out) {
-  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_wait: NULL server");
+// Waits for a request of the given kind class and copies its results
+// (shared by tbtkkpm_server_wait and tbtkkpm_server_wait_greens).
+int wait_request(tbtkkpm_server *s, uint64_t request, double timeout_s, bool greens, double *out,
+                 double *err_out, int32_t *rerun_out, const char *who) {
+  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "%s: NULL server", who);
   std::unique_lock<std::mutex> lk(s->mu);
   auto it = s->requests.find(request);
   if (it == s->requests.end())
-    return fail(TBTKKPM_ERR_ARGUMENT, "server_wait: no request %llu", (unsigned long long)request);
+    return fail(TBTKKPM_ERR_ARGUMENT, "%s: no request %llu", who, (unsigned long long)request);
   Request *r = it->second.get();
+  if ((r->kind != kLdos) != greens)
+    return fail(TBTKKPM_ERR_ARGUMENT, "%s: request %llu is %s request", who,
+                (unsigned long long)request,
+                greens ? "an LDOS (tbtkkpm_server_wait)" : "a Green's-function (tbtkkpm_server_wait_greens)");
   if (!r->done && timeout_s > 0) {
     const auto until = Clock::now() + std::chrono::duration_cast<Clock::duration>(
                                           std::chrono::duration<double>(timeout_s));
@@ -1020,11 +1158,104 @@ extern "C" int tbtkkpm_server_wait(tbtkkpm_server *s, uint64_t request, double t
     s->requests.erase(it);
     return rc;
   }
-  const size_t K = r->sites.size();
-  if (ldos_out) std::memcpy(ldos_out, r->ldos.data(), sizeof(double) * K * s->E);
+  const size_t K = r->outputs();
+  if (out) std::memcpy(out, r->ldos.data(), sizeof(double) * K * r->result_doubles(s->E));
   if (err_out) std::memcpy(err_out, r->err.data(), sizeof(double) * K);
   if (rerun_out) std::memcpy(rerun_out, r->rerun.data(), sizeof(int32_t) * K);
   s->requests.erase(it);
+  return TBTKKPM_OK;
+}
+
+}  // namespace
+}  // namespace tbtkkpm
+
+extern "C" int tbtkkpm_server_submit(tbtkkpm_server *s, uint32_t model, const uint32_t *sites,
+                                     uint32_t n_sites, uint32_t M, double broadening,
+                                     uint64_t *request) {
+  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: NULL server");
+  if (!request || (!sites && n_sites)) return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: NULL pointer");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (model < s->models.size()) {
+    const Model *m = s->models[model].get();
+    if (n_sites == 0 || n_sites > m->W)
+      return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: %u sites for a model of %u lanes", n_sites,
+                  m->W);
+  }
+  auto r = std::make_unique<Request>();
+  r->model = model;
+  r->sites.assign(sites, sites + n_sites);
+  r->M = M;
+  r->broadening = broadening;
+  return queue_request(s, std::move(r), request, "server_submit");
+}
+
+extern "C" int tbtkkpm_server_submit_greens(tbtkkpm_server *s, uint32_t model, const uint32_t *to,
+                                            const uint32_t *from, uint32_t n_pairs, uint32_t M,
+                                            double broadening, int type, uint64_t *request) {
+  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_submit_greens: NULL server");
+  if (!request || ((!to || !from) && n_pairs))
+    return fail(TBTKKPM_ERR_ARGUMENT, "server_submit_greens: NULL pointer");
+  if (type < TBTKKPM_ADVANCED || type > TBTKKPM_NONPRINCIPAL)
+    return fail(TBTKKPM_ERR_ARGUMENT, "server_submit_greens: Unkown Green's function type %d", type);
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto r = std::make_unique<Request>();
+  r->model = model;
+  r->kind = type;
+  r->M = M;
+  r->broadening = broadening;
+  std::map<uint32_t, uint32_t> src;
+  for (uint32_t k = 0; k < n_pairs; k++) {
+    auto it = src.find(from[k]);
+    if (it == src.end()) {
+      it = src.emplace(from[k], (uint32_t)r->sites.size()).first;
+      r->sites.push_back(from[k]);
+    }
+    r->to.push_back(to[k]);
+    r->pair_src.push_back(it->second);
+    r->direct = r->direct || to[k] != from[k];
+  }
+  if (model < s->models.size()) {
+    const Model *m = s->models[model].get();
+    if (n_pairs == 0 || n_pairs > m->W)
+      return fail(TBTKKPM_ERR_ARGUMENT, "server_submit_greens: %u pairs for a model of %u lanes",
+                  n_pairs, m->W);
+  }
+  return queue_request(s, std::move(r), request, "server_submit_greens");
+}
+
+extern "C" int tbtkkpm_server_wait(tbtkkpm_server *s, uint64_t request, double timeout_s,
+                                   double *ldos_out, double *err_out, int32_t *rerun_out) {
+  return wait_request(s, request, timeout_s, false, ldos_out, err_out, rerun_out, "server_wait");
+}
+
+extern "C" int tbtkkpm_server_wait_greens(tbtkkpm_server *s, uint64_t request, double timeout_s,
+                                          double *G_out, double *err_out, int32_t *rerun_out) {
+  return wait_request(s, request, timeout_s, true, G_out, err_out, rerun_out, "server_wait_greens");
+}
+
+extern "C" int tbtkkpm_server_cancel(tbtkkpm_server *s, uint64_t request) {
+  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_cancel: NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->requests.find(request);
+  if (it == s->requests.end())
+    return fail(TBTKKPM_ERR_ARGUMENT, "server_cancel: no request %llu", (unsigned long long)request);
+  Request *r = it->second.get();
+  if (r->cancelled) return TBTKKPM_OK;
+  if (r->done || r->finishing)
+    return fail(TBTKKPM_ERR_STATE, "server_cancel: request %llu has finished its recursion",
+                (unsigned long long)request);
+  r->cancelled = true;
+  auto q = std::find(s->pending.begin(), s->pending.end(), request);
+  if (q != s->pending.end()) {
+    // still queued: it never takes lanes
+    s->pending.erase(q);
+    r->done = true;
+    r->status = TBTKKPM_ERR_CANCELLED;
+    r->message = "request cancelled";
+    s->cv_done.notify_all();
+  }
+  // in flight: the worker frees its lanes at the next step boundary
+  s->cv_work.notify_one();
   return TBTKKPM_OK;
 }
 
@@ -1259,8 +1490,8 @@ extern "C" int tbtkkpm_server_destroy(tbtkkpm_server *s) {
     }
     for (auto &t : s->tables) tbtkkpm_table_destroy(t.second);
     for (auto &t : s->exact) tbtkkpm_table_destroy(t.second);
-    for (DevBuf *b : {&s->d_models, &s->d_hdr, &s->d_joins, &s->d_done, &s->d_stage, &s->d_damp,
-                      &s->d_tiles})
+    for (DevBuf *b : {&s->d_models, &s->d_hdr, &s->d_joins, &s->d_done, &s->d_pairs, &s->d_stage,
+                      &s->d_damp, &s->d_tiles})
       b->release();
     s->head_ws.release();
     s->d_res.release();

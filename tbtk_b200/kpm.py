@@ -38,6 +38,7 @@ ERR_MEMORY = -3
 ERR_TIMEOUT = -4
 ERR_UNSUPPORTED = -5
 ERR_STATE = -6
+ERR_CANCELLED = -7
 
 ADVANCED, RETARDED, PRINCIPAL, NONPRINCIPAL = 0, 1, 2, 3
 FP64, MIXED, MIXED_DIRECT = 0, 1, 2
@@ -103,7 +104,10 @@ SIGNATURES = [
     ("tbtkkpm_server_create", _i, [_u32, _p, _u32, _u64, _u32, _d, _p]),
     ("tbtkkpm_server_add_model", _i, [_p, _p, _p, _p, _u32, _d, _u32, _p]),
     ("tbtkkpm_server_submit", _i, [_p, _u32, _p, _u32, _u32, _d, _p]),
+    ("tbtkkpm_server_submit_greens", _i, [_p, _u32, _p, _p, _u32, _u32, _d, _i, _p]),
     ("tbtkkpm_server_wait", _i, [_p, _u64, _d, _p, _p, _p]),
+    ("tbtkkpm_server_wait_greens", _i, [_p, _u64, _d, _p, _p, _p]),
+    ("tbtkkpm_server_cancel", _i, [_p, _u64]),
     ("tbtkkpm_server_stats", _i, [_p, _p, _u32]),
     ("tbtkkpm_server_autotune", _i, [_p, _u32, _u32, _p, _p, _p, _p]),
     ("tbtkkpm_server_set_config", _i, [_p, _u32, _i, _i, _i]),
@@ -487,11 +491,16 @@ class Table:
 
 
 class Server:
-    """Continuous-batching LDOS service over many device-resident models
-    (the C ABI's ``tbtkkpm_server``).  ``submit`` queues the LDOS of up to
-    ``width`` sites of a registered model and returns a request id;
-    ``wait`` returns ``(ldos [K][E], err [K], rerun [K])`` once it is done
-    (``None`` on timeout).  Any thread may submit and wait."""
+    """Continuous-batching LDOS and Green's-function service over many
+    device-resident models (the C ABI's ``tbtkkpm_server``).  ``submit``
+    queues the LDOS of up to ``width`` sites of a registered model and
+    ``submit_greens`` the Green's functions of up to ``width`` (to, from)
+    pairs; both return a request id.  ``wait`` returns ``(ldos [K][E], err
+    [K], rerun [K])``, or ``(G [K][E] complex, err, rerun)`` for a
+    Green's-function request, once it is done (``None`` on timeout);
+    ``cancel`` stops a queued or running request (its ``wait`` then raises
+    ``TBTKError`` with ``ERR_CANCELLED``).  Any thread may submit and
+    wait."""
 
     def __init__(self, max_moments, energies, hbm_budget, tick_steps=64, tolerance=1e-6):
         self.energies = np.ascontiguousarray(energies, dtype=np.float64)
@@ -516,21 +525,40 @@ class Server:
         rid = ctypes.c_uint64()
         _check(load_library().tbtkkpm_server_submit(self._h, int(model), _ptr(sites), sites.size,
                                                     int(M), float(broadening), ctypes.byref(rid)))
-        self._sites[rid.value] = sites.size
+        self._sites[rid.value] = (sites.size, False)
+        return rid.value
+
+    def submit_greens(self, model, to, from_, M, broadening, type=NONPRINCIPAL):
+        """Green's functions G(to[k], from_[k]) of ``type`` (a type code or
+        its name, as ``ChebyshevExpander.Type``)."""
+        to, from_ = _u32a(to), _u32a(from_)
+        if to.size != from_.size:
+            raise TBTKError(ERR_ARGUMENT, "submit_greens: to and from differ in length")
+        type = _TYPES.get(type, type)
+        rid = ctypes.c_uint64()
+        _check(load_library().tbtkkpm_server_submit_greens(
+            self._h, int(model), _ptr(to), _ptr(from_), to.size, int(M), float(broadening),
+            int(type), ctypes.byref(rid)))
+        self._sites[rid.value] = (to.size, True)
         return rid.value
 
     def wait(self, request, timeout=600.0):
-        K = self._sites[request]
-        ldos = np.zeros((K, self.E), dtype=np.float64)
+        K, greens = self._sites[request]
+        out = np.zeros((K, self.E), dtype=np.complex128 if greens else np.float64)
         err = np.zeros(K, dtype=np.float64)
         rerun = np.zeros(K, dtype=np.int32)
-        rc = load_library().tbtkkpm_server_wait(self._h, ctypes.c_uint64(request), float(timeout),
-                                                _ptr(ldos), _ptr(err), _ptr(rerun))
+        fn = (load_library().tbtkkpm_server_wait_greens if greens
+              else load_library().tbtkkpm_server_wait)
+        rc = fn(self._h, ctypes.c_uint64(request), float(timeout), _ptr(out), _ptr(err),
+                _ptr(rerun))
         if rc == PENDING:
             return None
         del self._sites[request]
         _check(rc)
-        return ldos, err, rerun
+        return out, err, rerun
+
+    def cancel(self, request):
+        _check(load_library().tbtkkpm_server_cancel(self._h, ctypes.c_uint64(request)))
 
     def stats(self):
         out = np.zeros(len(STAT_NAMES), dtype=np.float64)

@@ -175,7 +175,7 @@ def test_server_hbm_budget_admission(gpu):
     probe.close()
     N0 = ms[0][1][0].size - 1
     N1 = ms[1][1][0].size - 1
-    need = max(2 * N * 8 * 8 + 8 * (256 + 129) * 16 + 1024 + N // 8 for N in (N0, N1))
+    need = max(2 * N * 8 * 8 + 8 * (2 * 256 + 129) * 16 + 1024 + N // 8 for N in (N0, N1))
     srv = kpm.Server(256, grid(), hbm_budget=need, tick_steps=8, tolerance=0)
     ids = [srv.add_model(*c, S, 8) for _, c in ms]
     jobs = []
@@ -265,6 +265,167 @@ def test_server_autotune(gpu):
     ldos, _, _ = srv.wait(srv.submit(mid, sites, 128, 1e-3))
     assert rel_err(ldos, fp64_ldos(kpm, csr, sites, 128, 1e-3)) <= TOL_MIXED
     srv.close()
+
+
+def fp64_greens(kpm, csr, to, frm, M, broadening, type_):
+    """G(to[k], frm[k]) through the FP64 batched recursion and the lookup
+    table (both pinned against the reference elsewhere)."""
+    m = kpm.Matrix.from_csr(*csr, S)
+    t = kpm.Table.create(M, grid(), S)
+    src = list(dict.fromkeys(int(f) for f in frm))
+    owner = [src.index(int(f)) for f in frm]
+    mu, _ = m.moments_batched(src, to, owner, M, broadening, kpm.FP64)
+    return t.greens(mu, type_)
+
+
+GF_CASES = [
+    # (model, to, from, M, type): diagonal pairs run the doubling lanes,
+    # the others gather every moment directly
+    (1, [5, 77, 300], [5, 77, 300], 384, "Retarded"),
+    (1, [6, 7, 40, 5], [5, 5, 5, 300], 256, "NonPrincipal"),
+    (0, [3, 5, 4, 51], [3, 3, 3, 3], 320, "Advanced"),
+    (2, [10, 11, 12, 13], [10, 10, 12, 12], 200, "Principal"),
+]
+
+
+@pytest.mark.gpu
+def test_server_greens_match_fp64(gpu):
+    """Green's-function requests of every type, diagonal (doubling lanes)
+    and off-diagonal (directly gathered pairs), on real and complex models,
+    within the mixed-precision bar of the FP64 recursion's G(E)."""
+    kpm = gpu
+    ms = models()
+    srv = kpm.Server(512, grid(), hbm_budget=1 << 30, tick_steps=16, tolerance=0)
+    ids = [srv.add_model(*c, S, 8) for _, c in ms]
+    jobs = [(c, srv.submit_greens(ids[c[0]], c[1], c[2], c[3], 1e-3, c[4])) for c in GF_CASES]
+    for (i, to, frm, M, ty), rid in jobs:
+        G, err, rerun = srv.wait(rid)
+        ref = fp64_greens(kpm, ms[i][1], to, frm, M, 1e-3, kpm.ChebyshevExpander.Type[ty])
+        assert G.shape == (len(to), E) and not rerun.any()
+        for k in range(len(to)):
+            assert 0 <= err[k] < 1e-3
+            if not ref[k].any():
+                # to and from in sectors the Hamiltonian does not connect
+                assert not G[k].any()
+                continue
+            e = rel_err(G[k], ref[k])
+            assert e <= TOL_MIXED, (ms[i][0], ty, k, e)
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_server_greens_alone_equals_in_mix(gpu):
+    """A Green's-function request gives the same bits alone and in a mix of
+    LDOS and other Green's-function traffic."""
+    kpm = gpu
+    ms = models()
+    alone = []
+    for i, to, frm, M, ty in GF_CASES[:2]:
+        srv = kpm.Server(512, grid(), hbm_budget=1 << 30, tick_steps=16, tolerance=0)
+        mid = srv.add_model(*ms[i][1], S, 8)
+        alone.append(srv.wait(srv.submit_greens(mid, to, frm, M, 1e-3, ty)))
+        srv.close()
+    srv = kpm.Server(512, grid(), hbm_budget=1 << 30, tick_steps=5, tolerance=0)
+    ids = [srv.add_model(*c, S, 8) for _, c in ms]
+    rng = np.random.default_rng(7)
+    bg = []
+    for r in range(10):
+        i = r % len(ms)
+        N = ms[i][1][0].size - 1
+        sites = rng.choice(N, size=int(rng.integers(1, 4)), replace=False).astype(np.uint32)
+        bg.append(srv.submit(ids[i], sites, int(rng.integers(16, 400)), 1e-3))
+        if r % 3 == 0:
+            bg.append(srv.submit_greens(ids[i], sites, sites[::-1], int(rng.integers(16, 300)),
+                                        1e-3, "Retarded"))
+    import time
+    time.sleep(0.05)
+    probes = [srv.submit_greens(ids[i], to, frm, M, 1e-3, ty) for i, to, frm, M, ty in GF_CASES[:2]]
+    mixed = [srv.wait(p) for p in probes]
+    for b in bg:
+        srv.wait(b)
+    for a, b in zip(alone, mixed):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_server_greens_fp64_rerun(gpu):
+    kpm = gpu
+    _, csr = models()[1]
+    srv = kpm.Server(512, grid(), hbm_budget=1 << 30, tick_steps=16, tolerance=1e-300)
+    mid = srv.add_model(*csr, S, 4)
+    to, frm = [6, 7, 40], [5, 5, 300]
+    G, err, rerun = srv.wait(srv.submit_greens(mid, to, frm, 256, 1e-3, "Retarded"))
+    assert rerun.all()
+    assert np.array_equal(G, fp64_greens(kpm, csr, to, frm, 256, 1e-3, kpm.RETARDED))
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_server_cancel(gpu):
+    """A cancelled request in flight frees its lanes for the next one, a
+    cancelled queued request never starts, and a finished one is not
+    affected."""
+    kpm = gpu
+    _, csr = models()[0]
+    srv = kpm.Server(4096, grid(), hbm_budget=1 << 30, tick_steps=4, tolerance=0)
+    mid = srv.add_model(*csr, S, 2)
+    long_a = srv.submit(mid, [1, 2], 4096, 1e-3)    # takes both lanes
+    queued = srv.submit(mid, [3], 64, 1e-3)         # waits for a lane
+    srv.cancel(queued)
+    srv.cancel(queued)                               # twice is not an error
+    with pytest.raises(kpm.TBTKError) as e:
+        srv.wait(queued)
+    assert e.value.status == kpm.ERR_CANCELLED
+    srv.cancel(long_a)
+    with pytest.raises(kpm.TBTKError) as e:
+        srv.wait(long_a)
+    assert e.value.status == kpm.ERR_CANCELLED
+    # the lanes are free again: a new request runs and is right
+    sites = np.array([5, 9], dtype=np.uint32)
+    rid = srv.submit(mid, sites, 128, 1e-3)
+    import time
+    while srv.stats()["completed"] < 1:
+        time.sleep(0.01)
+    with pytest.raises(kpm.TBTKError) as e:
+        srv.cancel(rid)
+    assert e.value.status == kpm.ERR_STATE
+    ldos, _, _ = srv.wait(rid)
+    assert rel_err(ldos, fp64_ldos(kpm, csr, sites, 128, 1e-3)) <= TOL_MIXED
+    with pytest.raises(kpm.TBTKError) as e:
+        srv.cancel(rid)                              # released by wait
+    assert e.value.status == kpm.ERR_ARGUMENT
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_server_greens_argument_errors(gpu):
+    kpm = gpu
+    _, csr = models()[3]
+    srv = kpm.Server(128, grid(), hbm_budget=1 << 30, tick_steps=8, tolerance=0)
+    mid = srv.add_model(*csr, S, 4)
+    with pytest.raises(kpm.TBTKError):
+        srv.submit_greens(mid, [0, 1], [0], 64, 1e-3)          # lengths differ
+    with pytest.raises(kpm.TBTKError):
+        srv.submit_greens(mid, [0] * 5, [1] * 5, 64, 1e-3)     # more pairs than lanes
+    with pytest.raises(kpm.TBTKError):
+        srv.submit_greens(mid, [0], [10 ** 6], 64, 1e-3)       # from outside the model
+    with pytest.raises(kpm.TBTKError):
+        srv.submit_greens(mid, [10 ** 6], [0], 64, 1e-3)       # to outside the model
+    with pytest.raises(kpm.TBTKError):
+        srv.submit_greens(mid, [0], [0], 64, 1e-3, 7)          # unknown type
+    srv.close()
+
+
+def test_server_calls_check_their_handle(kpm):
+    """Entry points of the server reject a NULL handle with a status."""
+    lib = kpm.load_library()
+    assert lib.tbtkkpm_server_cancel(None, 1) == kpm.ERR_ARGUMENT
+    assert lib.tbtkkpm_server_wait_greens(None, 1, 0.0, None, None, None) == kpm.ERR_ARGUMENT
+    assert lib.tbtkkpm_server_submit_greens(None, 0, None, None, 0, 64, 0.0, 1, None) \
+        == kpm.ERR_ARGUMENT
+    assert b"NULL server" in lib.tbtkkpm_last_error()
 
 
 def test_server_needs_a_device(kpm):
