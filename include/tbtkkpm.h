@@ -498,6 +498,15 @@ TBTKKPM_API int tbtkkpm_server_autotune(
 TBTKKPM_API int tbtkkpm_server_set_config(
 	tbtkkpm_server *s, uint32_t width, int tpr, int vpt, int minb);
 
+/* Lists the compiled step configurations of lane width `width` for real
+ * float lanes (real != 0) or complex64 lanes as (tpr, vpt, variant) triples
+ * into out[3*cap]; returns their number.  variant 1-2 is the register cap
+ * of a register-staged step; 100000 + 1000*R + 10*CW + BPS a tile-staged
+ * step (rows of R-row tiles staged in shared memory by bulk copies, CW
+ * consumer warps, BPS blocks per SM; real widths from 4, complex widths
+ * from 2).  Any of them gives the same results. */
+TBTKKPM_API int tbtkkpm_server_step_configs(int real, uint32_t width, int *out, int cap);
+
 /* Models added after set_real(s, 0) keep complex64 lanes even when their
  * Hamiltonian is real; by default (1) a real model's lanes hold real float
  * vectors (tbtkkpm_matrix_set_real), with the same results. */

@@ -68,6 +68,39 @@ MULTI_REAL_SHAPES = {1: [(1, 1)], 2: [(2, 1), (1, 2)], 4: [(4, 1), (1, 4)], 8: [
                      16: [(4, 4), (2, 8)], 32: [(8, 4), (4, 8)], 64: [(16, 4), (8, 8)]}
 
 
+# Tile-staged multi-model steps (kpm_multi_tiled.cuh): lane width ->
+# (threads per row, values per thread, rows per tile, consumer warps,
+# blocks per SM).  Rows of a real width below 4 or a complex width below 2
+# are under the 16 bytes a bulk copy moves at least, so those widths keep
+# the register-staged steps.
+MULTI_TILED_REAL = {4: [(1, 4, 64, 2, 4), (1, 4, 64, 2, 2)],
+                    8: [(2, 4, 64, 4, 2), (1, 8, 64, 2, 4)],
+                    16: [(4, 4, 64, 8, 2), (2, 8, 64, 4, 2)],
+                    32: [(8, 4, 64, 16, 1), (4, 8, 64, 8, 2)],
+                    64: [(8, 8, 64, 16, 1), (16, 4, 64, 16, 1)]}
+MULTI_TILED_CPLX = {2: [(1, 2, 64, 2, 4), (2, 1, 32, 2, 4)],
+                    4: [(2, 2, 64, 4, 2), (1, 4, 64, 2, 4)],
+                    8: [(4, 2, 32, 4, 2), (2, 4, 64, 4, 2)],
+                    16: [(8, 2, 32, 8, 2), (4, 4, 32, 4, 2)],
+                    32: [(8, 4, 32, 8, 2), (16, 2, 32, 16, 1)],
+                    64: [(16, 4, 16, 8, 2), (8, 8, 32, 8, 2)]}
+
+
+def write_multi_tiled():
+    lines = ["// Tile-staged multi-model recursion steps (kpm_multi_tiled.cuh).",
+             "// Written by gen_steps.py.", '#include "kpm_multi_tiled.cuh"', "", "namespace tbtkkpm {", ""]
+    for table, cplx, shapes in (("kMultiTiled", "true", MULTI_TILED_CPLX),
+                                ("kMultiTiledReal", "false", MULTI_TILED_REAL)):
+        lines.append(f"const MultiEntry {table}[] = {{")
+        for w, cfgs in shapes.items():
+            for (t, p, r, cw, bps) in cfgs:
+                assert t * p == w and cw * 32 % t == 0
+                lines.append(f"    TBTKKPM_MULTI_TILED_ENTRY({cplx}, {t}, {p}, {r}, {cw}, {bps}),")
+        lines += ["};", f"const int kNum{table[1:]} = sizeof({table}) / sizeof({table}[0]);", ""]
+    lines += ["}  // namespace tbtkkpm", ""]
+    (HERE / "steps_multi_tiled.cu").write_text("\n".join(lines))
+
+
 def write_multi():
     lines = ["// Multi-model recursion steps for every lane width the server offers.",
              "// Written by gen_steps.py.", '#include "kpm_multi.cuh"', "", "namespace tbtkkpm {", "",
@@ -192,6 +225,7 @@ def write_real():
 
 def main():
     write_multi()
+    write_multi_tiled()
     write_real()
     for fname, table, cls, V, AR, dots, shapes, doc in UNITS:
         lines = [f"// {doc}", "// Written by gen_steps.py: every configuration the driver and the",

@@ -83,6 +83,13 @@ struct TilePlan {
   const void *eval;        // [chunks][R] value (double for real, double2 for complex)
   uint32_t N, ntiles, R;
   uint32_t umax, wmax;     // most distinct outside columns / entries per row of a tile
+  uint32_t nruns;          // runs of all tiles
+};
+
+// Byte layout of one shared-memory ring stage of a tile-staged step
+// (offsets from the stage start) and the ring.
+struct TiledLayout {
+  uint32_t stages, stage_bytes, off_slots, off_xs, off_prev;
 };
 
 // A plan and its device arrays; ok is false when some tile has more entries

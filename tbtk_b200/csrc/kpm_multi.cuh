@@ -46,6 +46,13 @@ struct MultiModel {
   uint32_t ntiles;
   double2 *pmu;              // [W][mmax] moments of Green's-function pairs (pair entries)
   uint32_t mmax;
+  // tile-staged steps (kpm_multi_tiled.cuh): the model's gather plan for the
+  // launch's rows per tile, and the offset of its runs in the launch's run list
+  const uint4 *p_hdr;
+  const uint2 *p_runs;
+  const uint16_t *p_slot;
+  const void *p_val;
+  uint32_t p_nruns, run0;
 };
 
 // A model's target list pairs a row with an entry word: bits 0-7 the lane
@@ -81,6 +88,10 @@ struct MultiHeader {
   uint32_t total_tiles;
   int32_t n_base;
   const uint32_t *tile_model;  // [total_tiles]
+  // tile-staged steps: the plan header of every tile of the launch with its
+  // runs rebased into tile_runs (kpm_multi_tiled.cuh)
+  const uint4 *tile_hdr;
+  const uint2 *tile_runs;
 };
 
 // A block takes runs of kRun consecutive tiles (run r, r + gridDim.x, ...),
@@ -547,10 +558,21 @@ kpm_pair_error(const MultiPair *__restrict__ pairs, uint32_t M, double *__restri
 
 namespace tbtkkpm {
 
-using MultiFn = void (*)(cudaStream_t, int device, const MultiModel *, const MultiHeader *,
-                         uint32_t step_offset, uint32_t W, uint32_t ld);
+// Launch data of the tile-staged steps (ignored by the register-staged
+// ones): the shared-memory ring of the launch's class, the device flag a
+// staged-row wait that runs out sets, and the polls per wait.
+struct MultiLaunch {
+  TiledLayout ly;
+  int *err;
+  uint32_t wait_limit;
+};
 
-// One compiled configuration of kpm_multi_step for lane width tpr*vpt.
+using MultiFn = void (*)(cudaStream_t, int device, const MultiModel *, const MultiHeader *,
+                         uint32_t step_offset, uint32_t W, uint32_t ld, const MultiLaunch &);
+
+// One compiled configuration of a multi-model step for lane width tpr*vpt:
+// minb is the register cap of kpm_multi_step(_real), or a tile-staged
+// variant code (kTiledVariant + 1000*R + 10*CW + BPS, kpm_multi_tiled.cuh).
 struct MultiEntry {
   int tpr, vpt, minb;
   MultiFn launch;
@@ -559,7 +581,7 @@ struct MultiEntry {
 // Grid: every resident block of the device (the kernel strides over tiles).
 template <int TPR, int VPT, int MINB>
 void launch_multi(cudaStream_t st, int device, const MultiModel *models, const MultiHeader *hdr,
-                  uint32_t step_offset, uint32_t W, uint32_t ld) {
+                  uint32_t step_offset, uint32_t W, uint32_t ld, const MultiLaunch &) {
   auto kern = kpm_multi_step<TPR, VPT, MINB>;
   static int per_sm[64] = {0};
   const int d = device & 63;

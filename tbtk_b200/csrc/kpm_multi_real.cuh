@@ -223,7 +223,8 @@ kpm_multi_step_real(const MultiModel *__restrict__ models, const MultiHeader *__
 
 template <int TPR, int VPT, int MINB>
 void launch_multi_real(cudaStream_t st, int device, const MultiModel *models,
-                       const MultiHeader *hdr, uint32_t step_offset, uint32_t W, uint32_t ld) {
+                       const MultiHeader *hdr, uint32_t step_offset, uint32_t W, uint32_t ld,
+                       const MultiLaunch &) {
   auto kern = kpm_multi_step_real<TPR, VPT, MINB>;
   constexpr uint32_t smem = 2u * VPT * kBlock * 8u;
   static int per_sm[64] = {0};

@@ -179,12 +179,6 @@ void launch_async(cudaStream_t st, int device, unsigned max_grid, const StepArgs
   {CLS, 32, P, 10000 + 1000 * S + 10 * WMAX + WPB,                                 \
    &launch_async<P, true, D, S, WMAX, WPB>, &launch_async<P, false, D, S, WMAX, WPB>}
 
-// Shared memory a tile-staged block may use with BPS blocks per SM (the SM
-// has 228 KB; each block reserves 1 KB; one block may take at most 227 KB).
-constexpr uint32_t tiled_budget(int bps) {
-  return bps <= 1 ? 232448u : 233472u / (uint32_t)bps - 1024u;
-}
-
 // Tile-staged step variants: 100000 + 1000000*CV + 1000*R + 10*CW + BPS
 // (CV the widening split of kpm_step_tiled, R rows per tile, CW consumer
 // warps, BPS blocks per SM).

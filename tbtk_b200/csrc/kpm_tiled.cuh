@@ -45,12 +45,13 @@ constexpr int kPlanBlock = 256;
 constexpr uint32_t kTiledMaxStages = 8;
 constexpr uint32_t kTiledHeader = 256;  // barriers at the start of dynamic shared memory
 
-// Byte layout of one ring stage (offsets from the stage start) and the ring.
-struct TiledLayout {
-  uint32_t stages, stage_bytes, off_slots, off_xs, off_prev;
-};
-
 __host__ __device__ inline uint32_t align_up(uint32_t v, uint32_t a) { return (v + a - 1) / a * a; }
+
+// Shared memory a tile-staged block may use with BPS blocks per SM (the SM
+// has 228 KB; each block reserves 1 KB; one block may take at most 227 KB).
+constexpr uint32_t tiled_budget(int bps) {
+  return bps <= 1 ? 232448u : 233472u / (uint32_t)bps - 1024u;
+}
 
 // Layout of a stage for `rowbytes` bytes per vector row and `vbytes` per
 // value; stages = 0 when fewer than two stages fit `budget` bytes.

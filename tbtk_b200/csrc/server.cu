@@ -18,6 +18,7 @@
 #include "kpm_host.h"
 #include "kpm_multi.cuh"
 #include "kpm_multi_real.cuh"
+#include "kpm_multi_tiled.cuh"
 #include "kpm_prefix.cuh"
 
 #include <algorithm>
@@ -126,13 +127,54 @@ uint64_t lane_bytes(uint32_t N, uint32_t W, uint32_t Mmax, uint32_t ld, size_t e
          8ull * W + 4ull * ((N + 31) / 32) + 16ull * W + (uint64_t)W * Mmax * sizeof(double2);
 }
 
-// The step kernels of one class: complex64 lanes or real float lanes.
+// The step kernels of one class (complex64 lanes or real float lanes):
+// register-staged, then tile-staged entries.
+const std::vector<const MultiEntry *> &multi_entries(bool real) {
+  static const std::vector<const MultiEntry *> lists[2] = {
+      [] {
+        std::vector<const MultiEntry *> v;
+        for (int i = 0; i < kNumMultiSteps; i++) v.push_back(&kMultiSteps[i]);
+        for (int i = 0; i < kNumMultiTiled; i++) v.push_back(&kMultiTiled[i]);
+        return v;
+      }(),
+      [] {
+        std::vector<const MultiEntry *> v;
+        for (int i = 0; i < kNumMultiStepsReal; i++) v.push_back(&kMultiStepsReal[i]);
+        for (int i = 0; i < kNumMultiTiledReal; i++) v.push_back(&kMultiTiledReal[i]);
+        return v;
+      }()};
+  return lists[real ? 1 : 0];
+}
+
 const MultiEntry *find_multi(int tpr, int vpt, int minb, bool real) {
-  const MultiEntry *t = real ? kMultiStepsReal : kMultiSteps;
-  const int n = real ? kNumMultiStepsReal : kNumMultiSteps;
-  for (int i = 0; i < n; i++)
-    if (t[i].tpr == tpr && t[i].vpt == vpt && t[i].minb == minb) return &t[i];
+  for (const MultiEntry *e : multi_entries(real))
+    if (e->tpr == tpr && e->vpt == vpt && e->minb == minb) return e;
   return nullptr;
+}
+
+// Gather plan of a model for a tile-staged entry (built on first use on the
+// model's matrix handle); null when the entry is register-staged, the rows
+// of this width are too narrow for bulk copies, or the matrix has a tile the
+// plan builder cannot take.
+const TilePlan *model_plan(Model *m, const MultiEntry *e, int *rc) {
+  *rc = TBTKKPM_OK;
+  if (!is_multi_tiled(e->minb) || (m->W * m->esize()) % 16 != 0) return nullptr;
+  const TilePlan *p = nullptr;
+  *rc = tile_plan(m->mat, multi_tiled_rows(e->minb), !m->real, &p);
+  return p;
+}
+
+// Shared-memory ring of a tile-staged entry over models whose plans have
+// at most wmax entries per row and umax outside rows per tile (stages 0:
+// two stages do not fit).
+TiledLayout multi_layout(const MultiEntry *e, uint32_t W, bool real, uint32_t wmax, uint32_t umax) {
+  TilePlan p{};
+  p.R = (uint32_t)multi_tiled_rows(e->minb);
+  p.wmax = wmax;
+  p.umax = umax;
+  return tiled_layout(p, W * (uint32_t)(real ? sizeof(float) : sizeof(float2)),
+                      real ? (uint32_t)sizeof(double) : (uint32_t)sizeof(double2),
+                      tiled_budget(multi_tiled_bps(e->minb)));
 }
 
 // Default shape per width and class (measured choices of the single-model
@@ -196,7 +238,9 @@ struct tbtkkpm_server {
   int32_t n_global = 1;  // next global step
   uint64_t tick_no = 0;
   uint64_t resident = 0;
-  DevBuf d_models, d_hdr, d_joins, d_done, d_pairs, d_stage, d_damp, d_tiles;
+  DevBuf d_models, d_hdr, d_joins, d_done, d_pairs, d_stage, d_damp, d_tiles, d_thdr, d_truns;
+  DevBuf d_err;           // staged-row wait that ran out (tile-staged steps)
+  int *h_err = nullptr;   // pinned copy of d_err read after each tick
   // statistics
   std::vector<double> latencies_ms;
   double reruns = 0, ticks = 0, steps = 0, lane_steps = 0, evictions = 0, waited = 0, busy_s = 0;
@@ -392,10 +436,13 @@ void release_request_lanes(Model *m, Request *r) {
 
 struct ClassPlan {
   uint32_t W;
+  bool real = false;
   const MultiEntry *entry;
   std::vector<MultiModel> models;
   uint32_t total_tiles = 0;
-  double bytes = 0;  // algorithmic bytes of one step
+  uint32_t total_runs = 0;  // tile-staged entries: runs of the launch
+  TiledLayout ly{};         // tile-staged entries: the class's ring
+  double bytes = 0;         // algorithmic bytes of one step
 };
 
 // Uploads the lane tables and targets of changed models (under s->mu; the
@@ -459,9 +506,12 @@ MultiModel describe(const tbtkkpm_server *s, const Model *m) {
 }
 
 // Builds the launch plans, one per (lane width, real or complex lanes), of
-// all models with busy lanes (under s->mu).
+// all models with busy lanes (under s->mu).  A class whose configured entry
+// is tile-staged falls back to the default register-staged entry of its
+// width when some model has no plan for it or two ring stages do not fit.
 int plan_tick(tbtkkpm_server *s, std::vector<ClassPlan> &plans) {
   std::map<uint32_t, size_t> index;
+  std::vector<std::vector<Model *>> members;
   for (auto &p : s->models) {
     Model *m = p.get();
     if (!m->resident || !m->busy) continue;
@@ -474,23 +524,63 @@ int plan_tick(tbtkkpm_server *s, std::vector<ClassPlan> &plans) {
       const auto &cfg = s->config_for(m->W, m->real);
       ClassPlan cp;
       cp.W = m->W;
+      cp.real = m->real;
       cp.entry = find_multi(cfg[0], cfg[1], cfg[2], m->real);
       if (!cp.entry)
         return fail(TBTKKPM_ERR_UNSUPPORTED, "server: no step kernel for width %u", m->W);
       it = index.emplace(key, plans.size()).first;
       plans.push_back(std::move(cp));
+      members.emplace_back();
     }
-    ClassPlan &cp = plans[it->second];
-    MultiModel d = describe(s, m);
-    const uint32_t rpb = kBlock / cp.entry->tpr;
-    d.tile0 = cp.total_tiles;
-    d.ntiles = (uint32_t)(((uint64_t)m->mat->nslices * 32 + rpb - 1) / rpb);
-    cp.total_tiles += d.ntiles;
-    // matrix once (value + column index, row pointers) and three vector
-    // passes of the lanes
-    cp.bytes += (m->real ? 12.0 : 20.0) * m->mat->nnz + 4.0 * (m->N + 1) +
-                3.0 * m->N * m->W * m->esize();
-    cp.models.push_back(d);
+    members[it->second].push_back(m);
+  }
+  for (size_t c = 0; c < plans.size(); c++) {
+    ClassPlan &cp = plans[c];
+    std::vector<const TilePlan *> tp(members[c].size(), nullptr);
+    if (is_multi_tiled(cp.entry->minb)) {
+      uint32_t wmax = 0, umax = 0;
+      bool ok = true;
+      for (size_t i = 0; i < members[c].size() && ok; i++) {
+        int rc;
+        tp[i] = model_plan(members[c][i], cp.entry, &rc);
+        if (rc) return rc;
+        ok = tp[i] != nullptr;
+        if (ok) {
+          wmax = std::max(wmax, tp[i]->wmax);
+          umax = std::max(umax, tp[i]->umax);
+        }
+      }
+      if (ok) cp.ly = multi_layout(cp.entry, cp.W, cp.real, wmax, umax);
+      if (!ok || cp.ly.stages == 0) {
+        const auto d = default_config(cp.W, cp.real);
+        cp.entry = find_multi(d[0], d[1], d[2], cp.real);
+        std::fill(tp.begin(), tp.end(), nullptr);
+      }
+    }
+    for (size_t i = 0; i < members[c].size(); i++) {
+      const Model *m = members[c][i];
+      MultiModel d = describe(s, m);
+      d.tile0 = cp.total_tiles;
+      if (tp[i]) {
+        d.ntiles = tp[i]->ntiles;
+        d.p_hdr = tp[i]->hdr;
+        d.p_runs = tp[i]->runs;
+        d.p_slot = tp[i]->eslot;
+        d.p_val = tp[i]->eval;
+        d.p_nruns = tp[i]->nruns;
+        d.run0 = cp.total_runs;
+        cp.total_runs += tp[i]->nruns;
+      } else {
+        const uint32_t rpb = kBlock / cp.entry->tpr;
+        d.ntiles = (uint32_t)(((uint64_t)m->mat->nslices * 32 + rpb - 1) / rpb);
+      }
+      cp.total_tiles += d.ntiles;
+      // matrix once (value + column index, row pointers) and three vector
+      // passes of the lanes
+      cp.bytes += (m->real ? 12.0 : 20.0) * m->mat->nnz + 4.0 * (m->N + 1) +
+                  3.0 * m->N * m->W * m->esize();
+      cp.models.push_back(d);
+    }
   }
   return TBTKKPM_OK;
 }
@@ -565,15 +655,23 @@ int run_tick(tbtkkpm_server *s, const std::vector<ClassPlan> &plans, uint32_t ns
   std::vector<MultiModel> all;
   all.reserve(nm);
   std::vector<MultiHeader> hdr;
-  size_t tiles = 0;
-  for (const ClassPlan &cp : plans) tiles += cp.total_tiles;
-  if ((rc = s->d_tiles.reserve(sizeof(uint32_t) * std::max<size_t>(tiles, 1)))) return rc;
-  tiles = 0;
+  size_t tiles = 0, runs = 0;
+  for (const ClassPlan &cp : plans) {
+    tiles += cp.total_tiles;
+    runs += cp.total_runs;
+  }
+  if ((rc = s->d_tiles.reserve(sizeof(uint32_t) * std::max<size_t>(tiles, 1))) ||
+      (rc = s->d_thdr.reserve(sizeof(uint4) * std::max<size_t>(tiles, 1))) ||
+      (rc = s->d_truns.reserve(sizeof(uint2) * std::max<size_t>(runs, 1))))
+    return rc;
+  tiles = runs = 0;
   for (const ClassPlan &cp : plans) {
     all.insert(all.end(), cp.models.begin(), cp.models.end());
     hdr.push_back({(uint32_t)cp.models.size(), cp.total_tiles, s->n_global,
-                   s->d_tiles.as<uint32_t>() + tiles});
+                   s->d_tiles.as<uint32_t>() + tiles, s->d_thdr.as<uint4>() + tiles,
+                   s->d_truns.as<uint2>() + runs});
     tiles += cp.total_tiles;
+    runs += cp.total_runs;
   }
   if ((rc = s->d_models.reserve(sizeof(MultiModel) * std::max<size_t>(nm, 1))) ||
       (rc = s->d_hdr.reserve(sizeof(MultiHeader) * std::max<size_t>(hdr.size(), 1))))
@@ -584,13 +682,18 @@ int run_tick(tbtkkpm_server *s, const std::vector<ClassPlan> &plans, uint32_t ns
                            cudaMemcpyHostToDevice, st)))
     return cuda_fail(e, "server: descriptors");
   {
-    size_t off = 0, toff = 0;
+    size_t off = 0;
     for (size_t p = 0; p < plans.size(); p++) {
-      kpm_multi_tilemap<<<(unsigned)plans[p].models.size(), 256, 0, st>>>(
-          s->d_models.as<MultiModel>() + off, s->d_hdr.as<MultiHeader>() + p,
-          s->d_tiles.as<uint32_t>() + toff);
+      const MultiModel *dm = s->d_models.as<MultiModel>() + off;
+      const MultiHeader &h = hdr[p];
+      if (is_multi_tiled(plans[p].entry->minb))
+        kpm_multi_tilemap_tiled<<<(unsigned)plans[p].models.size(), 256, 0, st>>>(
+            dm, s->d_hdr.as<MultiHeader>() + p, const_cast<uint32_t *>(h.tile_model),
+            const_cast<uint4 *>(h.tile_hdr), const_cast<uint2 *>(h.tile_runs));
+      else
+        kpm_multi_tilemap<<<(unsigned)plans[p].models.size(), 256, 0, st>>>(
+            dm, s->d_hdr.as<MultiHeader>() + p, const_cast<uint32_t *>(h.tile_model));
       off += plans[p].models.size();
-      toff += plans[p].total_tiles;
     }
     count_launches(plans.size());
   }
@@ -601,7 +704,8 @@ int run_tick(tbtkkpm_server *s, const std::vector<ClassPlan> &plans, uint32_t ns
       const ClassPlan &cp = plans[p];
       const MultiModel *dm = s->d_models.as<MultiModel>() + off;
       const MultiHeader *dh = s->d_hdr.as<MultiHeader>() + p;
-      cp.entry->launch(st, s->device, dm, dh, k, cp.W, s->ld);
+      cp.entry->launch(st, s->device, dm, dh, k, cp.W, s->ld,
+                       MultiLaunch{cp.ly, s->d_err.as<int>(), kWaitLimit});
       kpm_multi_finalize<<<(unsigned)cp.models.size(), std::min<uint32_t>(std::max(cp.W, 32u), 64u), 0,
                            st>>>(dm, dh, k, cp.W, s->Mmax, s->ld);
       off += cp.models.size();
@@ -610,6 +714,9 @@ int run_tick(tbtkkpm_server *s, const std::vector<ClassPlan> &plans, uint32_t ns
   cudaEventRecord(s->ev[1], st);
   count_launches(2ull * nsteps * plans.size());
   if ((e = cudaGetLastError())) return cuda_fail(e, "server: step launch");
+  // the wait flag of the tile-staged steps, read after the tick
+  if ((e = cudaMemcpyAsync(s->h_err, s->d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, st)))
+    return cuda_fail(e, "server: step status");
   return TBTKKPM_OK;
 }
 
@@ -952,6 +1059,8 @@ void worker(tbtkkpm_server *s) {
     cudaError_t e = cudaSuccess;
     if (!rc && (e = cudaStreamSynchronize(s->stream)) != cudaSuccess)
       rc = cuda_fail(e, "server: tick");
+    if (!rc && *s->h_err)
+      rc = fail(TBTKKPM_ERR_TIMEOUT, "server: a staged-row wait of a recursion step ran out");
     const double ts = std::chrono::duration<double>(Clock::now() - p1).count() - overlap;
     lk.lock();
     s->tick_s += ts;
@@ -1038,10 +1147,16 @@ extern "C" int tbtkkpm_server_create(uint32_t max_moments, const double *energie
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev[0]);
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev[1]);
+    if (e == cudaSuccess) e = cudaMallocHost(&s->h_err, sizeof(int));
+    if (e == cudaSuccess && s->d_err.reserve(sizeof(int)) != TBTKKPM_OK) e = cudaErrorMemoryAllocation;
+    if (e == cudaSuccess) e = cudaMemset(s->d_err.ptr, 0, sizeof(int));
     if (e != cudaSuccess) {
+      s->d_err.release();
+      if (s->h_err) cudaFreeHost(s->h_err);
       delete s;
       return cuda_fail(e, "server_create: stream");
     }
+    *s->h_err = 0;
   }
   s->worker = std::thread(worker, s);
   *out = s;
@@ -1312,6 +1427,21 @@ extern "C" int tbtkkpm_server_set_config(tbtkkpm_server *s, uint32_t width, int 
   return TBTKKPM_OK;
 }
 
+extern "C" int tbtkkpm_server_step_configs(int real, uint32_t width, int *out, int cap) {
+  if (cap > 0 && !out) return fail(TBTKKPM_ERR_ARGUMENT, "server_step_configs: NULL out");
+  int n = 0;
+  for (const MultiEntry *e : multi_entries(real != 0)) {
+    if ((uint32_t)(e->tpr * e->vpt) != width) continue;
+    if (n < cap) {
+      out[3 * n] = e->tpr;
+      out[3 * n + 1] = e->vpt;
+      out[3 * n + 2] = e->minb;
+    }
+    n++;
+  }
+  return n;
+}
+
 extern "C" int tbtkkpm_server_set_table_free(tbtkkpm_server *s, int enable) {
   if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_set_table_free: NULL server");
   std::lock_guard<std::mutex> lk(s->mu);
@@ -1344,7 +1474,7 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
     return fail(TBTKKPM_ERR_STATE, "server_autotune: the server is busy");
   for (auto &p : s->models)
     if (p->busy) return fail(TBTKKPM_ERR_STATE, "server_autotune: the server is busy");
-  const Model *probe = nullptr;
+  Model *probe = nullptr;
   for (auto &p : s->models)
     if (p->W == width && (!probe || p->N > probe->N)) probe = p.get();
   if (!probe) return fail(TBTKKPM_ERR_STATE, "server_autotune: no model of width %u", width);
@@ -1354,7 +1484,7 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
   const uint32_t W = width, N = probe->N, Mp = 2 * probe_steps + 2, ldp = Mp / 2 + 1;
   const bool real = probe->real;  // the class of the probe model is tuned
   const size_t es = probe->esize();
-  DevBuf vec[2], dots, mu, mud, base, laneM, bitmap, tlist, dm, dh, tmap;
+  DevBuf vec[2], dots, mu, mud, base, laneM, bitmap, tlist, dm, dh, tmap, thdr, truns;
   int rc;
   if ((rc = vec[0].reserve(es * (size_t)N * W)) ||
       (rc = vec[1].reserve(es * (size_t)N * W)) ||
@@ -1400,11 +1530,19 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
   const MultiEntry *best = nullptr;
   double best_ms = 0;
   int32_t n = 1;
-  const MultiEntry *table = real ? kMultiStepsReal : kMultiSteps;
-  const int nentries = real ? kNumMultiStepsReal : kNumMultiSteps;
-  for (int i = 0; i < nentries && !rc; i++) {
-    const MultiEntry &en = table[i];
+  for (const MultiEntry *ep : multi_entries(real)) {
+    if (rc) break;
+    const MultiEntry &en = *ep;
     if ((uint32_t)(en.tpr * en.vpt) != W) continue;
+    // a tile-staged entry needs the probe's plan and a ring that fits
+    const TilePlan *plan = model_plan(probe, &en, &rc);
+    if (rc) break;
+    TiledLayout ly{};
+    if (is_multi_tiled(en.minb)) {
+      if (!plan) continue;
+      ly = multi_layout(&en, W, real, plan->wmax, plan->umax);
+      if (ly.stages == 0) continue;
+    }
     MultiModel d{};
     d.A.slice_ptr = probe->mat->slice_ptr.as<uint32_t>();
     d.A.col = probe->mat->scol.as<uint32_t>();
@@ -1424,14 +1562,21 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
     d.mu = mu.as<double2>();
     d.mu_direct = mud.as<double2>();
     d.tile0 = 0;
-    d.ntiles = (uint32_t)(((uint64_t)d.A.nslices * 32 + kBlock / en.tpr - 1) / (kBlock / en.tpr));
-    // one model: every tile maps to model 0
-    if ((rc = tmap.reserve(4 * (size_t)d.ntiles))) break;
-    if ((e = cudaMemsetAsync(tmap.ptr, 0, 4 * (size_t)d.ntiles, st))) {
-      rc = cuda_fail(e, "server_autotune: tile map");
-      break;
+    d.ntiles = plan ? plan->ntiles
+                    : (uint32_t)(((uint64_t)d.A.nslices * 32 + kBlock / en.tpr - 1) / (kBlock / en.tpr));
+    if (plan) {
+      d.p_hdr = plan->hdr;
+      d.p_runs = plan->runs;
+      d.p_slot = plan->eslot;
+      d.p_val = plan->eval;
+      d.p_nruns = plan->nruns;
+      d.run0 = 0;
     }
-    MultiHeader h{1, d.ntiles, n, tmap.as<uint32_t>()};
+    // one model: every tile maps to model 0
+    if ((rc = tmap.reserve(4 * (size_t)d.ntiles)) || (rc = thdr.reserve(16 * (size_t)d.ntiles)) ||
+        (rc = truns.reserve(8 * (size_t)std::max(d.p_nruns, 1u))))
+      break;
+    MultiHeader h{1, d.ntiles, n, tmap.as<uint32_t>(), thdr.as<uint4>(), truns.as<uint2>()};
     // parity of the buffers follows the global step, so the probe keeps
     // counting across configurations
     if ((e = cudaMemcpyAsync(dm.ptr, &d, sizeof(d), cudaMemcpyHostToDevice, st)) ||
@@ -1439,9 +1584,18 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
       rc = cuda_fail(e, "server_autotune: descriptors");
       break;
     }
+    if (plan) {
+      kpm_multi_tilemap_tiled<<<1, 256, 0, st>>>(dm.as<MultiModel>(), dh.as<MultiHeader>(),
+                                                 tmap.as<uint32_t>(), thdr.as<uint4>(), truns.as<uint2>());
+      count_launches(1);
+    } else if ((e = cudaMemsetAsync(tmap.ptr, 0, 4 * (size_t)d.ntiles, st))) {
+      rc = cuda_fail(e, "server_autotune: tile map");
+      break;
+    }
+    const MultiLaunch ml{ly, s->d_err.as<int>(), kWaitLimit};
     for (uint32_t k = 0; k < probe_steps; k++) {
       if (k == 1) cudaEventRecord(ev[0], st);
-      en.launch(st, s->device, dm.as<MultiModel>(), dh.as<MultiHeader>(), k, W, ldp);
+      en.launch(st, s->device, dm.as<MultiModel>(), dh.as<MultiHeader>(), k, W, ldp, ml);
       kpm_multi_finalize<<<1, std::min<uint32_t>(std::max(W, 32u), 64u), 0, st>>>(
           dm.as<MultiModel>(), dh.as<MultiHeader>(), k, W, Mp, ldp);
     }
@@ -1449,6 +1603,15 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
     cudaEventRecord(ev[1], st);
     if ((e = cudaEventSynchronize(ev[1])) != cudaSuccess) {
       rc = cuda_fail(e, "server_autotune: probe");
+      break;
+    }
+    int werr = 0;
+    if ((e = cudaMemcpy(&werr, s->d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) {
+      rc = cuda_fail(e, "server_autotune: probe");
+      break;
+    }
+    if (werr) {
+      rc = fail(TBTKKPM_ERR_TIMEOUT, "server_autotune: a staged-row wait ran out");
       break;
     }
     float ms = 0;
@@ -1491,11 +1654,12 @@ extern "C" int tbtkkpm_server_destroy(tbtkkpm_server *s) {
     for (auto &t : s->tables) tbtkkpm_table_destroy(t.second);
     for (auto &t : s->exact) tbtkkpm_table_destroy(t.second);
     for (DevBuf *b : {&s->d_models, &s->d_hdr, &s->d_joins, &s->d_done, &s->d_pairs, &s->d_stage,
-                      &s->d_damp, &s->d_tiles})
+                      &s->d_damp, &s->d_tiles, &s->d_thdr, &s->d_truns, &s->d_err})
       b->release();
     s->head_ws.release();
     s->d_res.release();
     if (s->h_res) cudaFreeHost(s->h_res);
+    if (s->h_err) cudaFreeHost(s->h_err);
     for (cudaEvent_t &ev : s->ev)
       if (ev) cudaEventDestroy(ev);
     cudaStreamDestroy(s->stream);

@@ -106,6 +106,7 @@ int build_plan(tbtkkpm_matrix *m, int R, bool cplx, TilePlanStore &p) {
   p.plan.R = (uint32_t)R;
   p.plan.umax = hf[0];
   p.plan.wmax = hf[1];
+  p.plan.nruns = nruns;
   p.ok = true;
   return TBTKKPM_OK;
 }

@@ -111,6 +111,7 @@ SIGNATURES = [
     ("tbtkkpm_server_stats", _i, [_p, _p, _u32]),
     ("tbtkkpm_server_autotune", _i, [_p, _u32, _u32, _p, _p, _p, _p]),
     ("tbtkkpm_server_set_config", _i, [_p, _u32, _i, _i, _i]),
+    ("tbtkkpm_server_step_configs", _i, [_i, _u32, _p, _i]),
     ("tbtkkpm_server_set_real", _i, [_p, _i]),
     ("tbtkkpm_server_set_fp64_head", _i, [_p, _u32]),
     ("tbtkkpm_server_set_table_free", _i, [_p, _i]),
@@ -571,6 +572,16 @@ class Server:
             self._h, int(width), int(probe_steps), ctypes.byref(t), ctypes.byref(v),
             ctypes.byref(m), ctypes.byref(ms)))
         return {"tpr": t.value, "vpt": v.value, "minb": m.value, "ms_per_step": ms.value}
+
+    @staticmethod
+    def step_configs(width, real):
+        """Compiled step configurations (tpr, vpt, variant) of a lane width
+        for real float lanes or complex64 lanes."""
+        lib = load_library()
+        n = lib.tbtkkpm_server_step_configs(int(bool(real)), int(width), None, 0)
+        out = np.zeros(3 * max(n, 1), dtype=np.int32)
+        lib.tbtkkpm_server_step_configs(int(bool(real)), int(width), _ptr(out), n)
+        return [tuple(int(v) for v in out[3 * i:3 * i + 3]) for i in range(n)]
 
     def set_config(self, width, tpr, vpt, minb):
         _check(load_library().tbtkkpm_server_set_config(self._h, int(width), int(tpr), int(vpt),

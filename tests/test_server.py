@@ -118,6 +118,48 @@ def test_server_result_independent_of_configuration(gpu):
             assert np.array_equal(a, b), cfg
 
 
+def _mixed_traffic(kpm, srv, ids, ms, seed):
+    """LDOS and Green's-function requests on every model; their results."""
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for r in range(8):
+        i = r % len(ms)
+        N = ms[i][1][0].size - 1
+        sites = rng.choice(N, size=int(rng.integers(1, 3)), replace=False).astype(np.uint32)
+        M = int(rng.integers(16, 200))
+        reqs.append(srv.submit(ids[i], sites, M, 1e-3))
+        reqs.append(srv.submit_greens(ids[i], sites + 1, sites, M, 1e-3, "Retarded"))
+    return [srv.wait(q) for q in reqs]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("width", [2, 4, 8, 16, 32, 64])
+def test_server_tiled_steps_equal_register_steps(gpu, width):
+    """Every compiled step configuration of a lane width, the tile-staged
+    ones (rows staged in shared memory by bulk copies) among them, gives
+    the register-staged default's results bit for bit, on real and complex
+    models, for LDOS and directly gathered Green's-function lanes."""
+    kpm = gpu
+    ms = models()
+    outs = {}
+    for real in (True, False):
+        for cfg in [None] + kpm.Server.step_configs(width, real):
+            srv = kpm.Server(256, grid(), hbm_budget=1 << 30, tick_steps=6, tolerance=0)
+            ids = [srv.add_model(*c, S, width) for _, c in ms]
+            if cfg is not None:
+                srv.set_config(width, *cfg)
+            outs[(real, cfg)] = _mixed_traffic(kpm, srv, ids, ms, 11)
+            srv.close()
+    ref = outs[(True, None)]
+    tiled = 0
+    for key, got in outs.items():
+        tiled += key[1] is not None and key[1][2] >= 100000
+        for a, b in zip(ref, got):
+            for x, y in zip(a, b):
+                assert np.array_equal(x, y), key
+    assert tiled >= 1 or width < 4
+
+
 @pytest.mark.gpu
 def test_server_real_lanes_equal_complex_lanes(gpu):
     """Real models on real float lanes give the complex64 lanes' results bit
