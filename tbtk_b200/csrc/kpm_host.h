@@ -167,6 +167,10 @@ struct tbtkkpm_table {
   // only, the energy sums run Clenshaw recurrences (kpm_clenshaw)
   bool clenshaw = false;
   double scale = 0;
+  // largest weight of the energy sum on this grid, max_e |T[1][e]| / pi =
+  // max_e 2 / (pi s sqrt(1 - (E_e/s)^2)): the scale that turns a moment
+  // error into an LDOS error (ldos_error_estimate)
+  double wmax = 0;
   tbtkkpm::DevBuf energies;  // [E]
   tbtkkpm::DevBuf table;   // [M][E] complex128
   tbtkkpm::DevBuf mu, out; // staging for energy sums
@@ -184,6 +188,13 @@ int launch_energy_sum(cudaStream_t st, const tbtkkpm_table *t, const double2 *mu
 // Lorentz damping numerators a[n] and denominator b (host libm).
 void damping_factors(uint32_t M, double broadening, std::vector<double> &a, double &b);
 // Error estimate of doubled moments against the directly gathered ones.
+// Largest energy-sum weight of a grid (tbtkkpm_table::wmax).
+double grid_weight_max(const double *energies, uint32_t E, double scale);
+// LDOS-space error estimate of a doubling run from its moment estimate
+// (doubling_error): moment_err * wmax / max_e |v_e| over the result row, v
+// the LDOS (complex false), or G / pi for a Green's function row (complex
+// true, E interleaved pairs).  0 when the row is zero.
+double ldos_error_estimate(double moment_err, double wmax, const double *row, uint32_t E, bool complex);
 void doubling_error(const std::vector<double2> &mu, const std::vector<double2> &direct,
                     uint32_t K, uint32_t M, uint32_t ld, double *err);
 // The matrix's gather plan for R-row tiles (real or complex values), built

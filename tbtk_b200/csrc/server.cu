@@ -919,6 +919,10 @@ int finish_complete(tbtkkpm_server *s, FinishBatch &fb) {
     const double *res = s->h_res + fb.res_off[i];
     r->ldos.assign(res, res + (size_t)K * rd);
     r->err.assign(res + (size_t)K * rd, res + (size_t)K * rd + K);
+    // moment estimates -> relative errors of the LDOS or G rows
+    for (uint32_t k = 0; k < K; k++)
+      r->err[k] = ldos_error_estimate(r->err[k], m->table->wmax, r->ldos.data() + (size_t)k * rd, E,
+                                      r->kind != kLdos);
     r->rerun.assign(K, 0);
     std::vector<uint32_t> idx;
     for (uint32_t k = 0; k < K; k++)

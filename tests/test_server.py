@@ -207,6 +207,46 @@ def test_server_fp64_rerun_on_miss(gpu):
 
 
 @pytest.mark.gpu
+def test_server_error_estimate_bounds_error_on_uneven_batch(gpu):
+    """The per-site error estimate is at least the actual LDOS error on
+    every sampled solve of uneven-batch models (the uneven batch's
+    distribution of lattices, disorder, site counts and coefficient counts,
+    with sides up to 96), and with the FP64 rerun at tolerance 1e-6 every
+    returned LDOS is within 1e-6 of the FP64 recursion."""
+    kpm = gpu
+    energies = workloads.open_grid(S, 1000)
+    specs = [sp for sp in workloads.cfg4_specs(1000, seed=4) if sp[1] <= 96][:40]
+    srv = kpm.Server(4096, energies, hbm_budget=8 << 30, tick_steps=64, tolerance=1e-6)
+    jobs = []
+    for kind, L, J, W, ns, M, seed in specs:
+        csr = workloads.build_model(kind, L, J, W, seed)
+        cells = 2 * L * L if kind == "honeycomb" else L * L
+        sites = workloads.sample_sites(cells, 2, ns, seed + 1)
+        w = 1 << max(ns - 1, 0).bit_length()
+        jobs.append((csr, sites, M, srv.submit(srv.add_model(*csr, S, w), sites, M, 1e-3)))
+    solves = reruns = 0
+    ratios = []
+    for csr, sites, M, rid in jobs:
+        ldos, est, rerun = srv.wait(rid, timeout=600)
+        m = kpm.Matrix.from_csr(*csr, S)
+        t = kpm.Table.create(M, energies, S)
+        ref, _ = m.ldos_sites(t, sites, 1e-3, kpm.FP64)
+        for k in range(sites.size):
+            e = rel_err(ldos[k], ref[k])
+            assert e <= 1e-6, (M, k, e, est[k], rerun[k])
+            if rerun[k]:
+                assert e == 0.0
+                reruns += 1
+            else:
+                assert est[k] >= e, (M, k, e, est[k])
+                ratios.append(est[k] / e if e > 0 else np.inf)
+            solves += 1
+    assert solves >= 200
+    assert srv.stats()["reruns"] == reruns
+    srv.close()
+
+
+@pytest.mark.gpu
 def test_server_hbm_budget_admission(gpu):
     """A budget for one model's lanes: requests to two models alternate
     through eviction and still give the right answers."""
