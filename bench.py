@@ -16,9 +16,10 @@ FP64 single-vector path (one site per recursion, complex128, bit-exact with
 the reference) on the same matrix, the LDOS error of the mixed result of
 every site against the FP64 recursion (batched FP64, bit-identical per site
 to the single-vector path), the speed-up split into its mechanisms, the
-roofline of the recursion step, the CPU baseline, and two sub-results:
-the 1024x1024 Rashba lattice (complex Hamiltonian, 256 sites, M = 2048) and
-the LDOS server on a 100-model uneven batch at tolerance 1e-6.
+roofline of the recursion step, the CPU baseline, and three sub-results:
+the 1024x1024 Rashba lattice (complex Hamiltonian, 256 sites, M = 2048),
+the LDOS server on the 1000-model uneven batch at tolerance 1e-6, and the
+server under Poisson arrivals (100 requests/s offered for 3 s).
 
 Inputs are larger than L2 (13.8 GB of matrix and vectors per recursion step
 against 126 MB of L2), so no flush is needed between steps.
@@ -400,17 +401,37 @@ def rashba_sub(args, stream):
 
 
 def server_sub():
-    """The LDOS server on the first 100 models of the uneven batch at
-    tolerance 1e-6 (FP64 rerun of a site whose error estimate exceeds it)."""
+    """The LDOS server on the uneven batch (all 1000 models, every request
+    submitted at once) at tolerance 1e-6 (FP64 rerun of a site whose error
+    estimate exceeds it)."""
     from tbtk_b200 import serve_bench
-    a = argparse.Namespace(models=100, budget_gb=60.0, tick=64, tolerance=1e-6, samples=12,
+    a = argparse.Namespace(models=1000, budget_gb=120.0, tick=64, tolerance=1e-6, samples=16,
                            sample_seed=44, fp64_head=32)
     r = serve_bench.uneven(a)
     st = r["server"]
     return {"workload": r["workload"], "value": r["value"], "unit": "LDOS solves/s",
             "p50_ms": st.get("p50_ms"), "p99_ms": st.get("p99_ms"), "reruns": st.get("reruns"),
+            "rerun_rate": st.get("reruns", 0) / max(r["solves"], 1),
             "solves": r["solves"], "wall_s": r["wall_s"],
             "plain_fp64": r["plain_fp64"], "speedup_vs_plain_fp64": r["speedup_vs_plain_fp64"],
+            "ldos_rel_err_vs_fp64_max": r["ldos_rel_err_vs_fp64_max"],
+            "step_GBps": r["step_GBps"]}
+
+
+def serving_sub():
+    """The server answering Poisson arrivals at 100 requests/s for 3 s
+    against the 64-model pool (LDOS requests of 1-16 sites, M in
+    [512, 4096]): served throughput and the latency percentiles."""
+    from tbtk_b200 import serve_bench
+    a = argparse.Namespace(models=64, budget_gb=120.0, tick=64, tolerance=1e-6, samples=8,
+                           sample_seed=44, fp64_head=32, rate=100.0, duration=3.0)
+    r = serve_bench.serve(a)
+    st = r["server"]
+    return {"workload": r["workload"], "value": r["value"], "unit": "LDOS solves/s",
+            "requests": r["requests"], "requests_per_s_served": r["requests_per_s"],
+            "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"], "reruns": st.get("reruns"),
+            "wall_s": r["wall_s"], "plain_fp64": r["plain_fp64"],
+            "speedup_vs_plain_fp64": r["speedup_vs_plain_fp64"],
             "ldos_rel_err_vs_fp64_max": r["ldos_rel_err_vs_fp64_max"],
             "step_GBps": r["step_GBps"]}
 
@@ -601,6 +622,7 @@ def ours(args, world, rank, local):
     if world == 1 and not args.no_sub:
         out["rashba_cfg3"] = rashba_sub(args, stream)
         out["server_uneven"] = server_sub()
+        out["server_serving"] = serving_sub()
     if world == 1 and not args.no_cpu:
         threads = int(min(os.cpu_count() or 1, B))
         out["cpu_baseline"] = cpu_port_baseline(p, threads)

@@ -489,8 +489,10 @@ TBTKKPM_API int tbtkkpm_server_cancel(tbtkkpm_server *s, uint64_t request);
 TBTKKPM_API int tbtkkpm_server_stats(tbtkkpm_server *s, double *out, uint32_t n);
 
 /* Times every compiled step configuration of lane width `width` for
- * probe_steps steps on the largest registered model of that width (the
- * server must be idle) and keeps the fastest; set_config installs a known
+ * probe_steps steps, for each lane class (real float lanes, complex64
+ * lanes) with a model of that width, on the largest model of the class
+ * (the server must be idle), and keeps the fastest per class; the outputs
+ * describe the class of the largest model.  set_config installs a known
  * one.  Results do not depend on the configuration. */
 TBTKKPM_API int tbtkkpm_server_autotune(
 	tbtkkpm_server *s, uint32_t width, uint32_t probe_steps, int *tpr,
@@ -501,10 +503,12 @@ TBTKKPM_API int tbtkkpm_server_set_config(
 /* Lists the compiled step configurations of lane width `width` for real
  * float lanes (real != 0) or complex64 lanes as (tpr, vpt, variant) triples
  * into out[3*cap]; returns their number.  variant 1-2 is the register cap
- * of a register-staged step; 100000 + 1000*R + 10*CW + BPS a tile-staged
- * step (rows of R-row tiles staged in shared memory by bulk copies, CW
- * consumer warps, BPS blocks per SM; real widths from 4, complex widths
- * from 2).  Any of them gives the same results. */
+ * of a register-staged step; 100000 + 1000000*CV + 1000*R + 10*CW + BPS a
+ * tile-staged step (rows of R-row tiles staged in shared memory by bulk
+ * copies, CW consumer warps, BPS blocks per SM, CV the split of the
+ * float -> FP64 widenings between the integer and conversion pipes; real
+ * widths from 4, complex widths from 2).  Any of them gives the same
+ * results. */
 TBTKKPM_API int tbtkkpm_server_step_configs(int real, uint32_t width, int *out, int cap);
 
 /* Models added after set_real(s, 0) keep complex64 lanes even when their

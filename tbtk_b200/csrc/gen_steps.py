@@ -73,17 +73,26 @@ MULTI_REAL_SHAPES = {1: [(1, 1)], 2: [(2, 1), (1, 2)], 4: [(4, 1), (1, 4)], 8: [
 # blocks per SM).  Rows of a real width below 4 or a complex width below 2
 # are under the 16 bytes a bulk copy moves at least, so those widths keep
 # the register-staged steps.
-MULTI_TILED_REAL = {4: [(1, 4, 64, 2, 4), (1, 4, 64, 2, 2)],
-                    8: [(2, 4, 64, 4, 2), (1, 8, 64, 2, 4)],
-                    16: [(4, 4, 64, 8, 2), (2, 8, 64, 4, 2)],
-                    32: [(8, 4, 64, 16, 1), (4, 8, 64, 8, 2)],
-                    64: [(8, 8, 64, 16, 1), (16, 4, 64, 16, 1)]}
-MULTI_TILED_CPLX = {2: [(1, 2, 64, 2, 4), (2, 1, 32, 2, 4)],
-                    4: [(2, 2, 64, 4, 2), (1, 4, 64, 2, 4)],
-                    8: [(4, 2, 32, 4, 2), (2, 4, 64, 4, 2)],
-                    16: [(8, 2, 32, 8, 2), (4, 4, 32, 4, 2)],
-                    32: [(8, 4, 32, 8, 2), (16, 2, 32, 16, 1)],
-                    64: [(16, 4, 16, 8, 2), (8, 8, 32, 8, 2)]}
+# The last field is the conversion split CV of kpm_multi_tiled (0: every
+# conversion an instruction of the XU pipe; 51: the first 5 gathers and
+# j_{n-1} widened on the integer pipe; 2 or 53: the doubling terms' fixed
+# point on the integer pipe too).
+MULTI_TILED_REAL = {4: [(1, 4, 64, 2, 4, 0), (1, 4, 64, 2, 2, 0)],
+                    8: [(2, 4, 64, 4, 2, 0), (1, 8, 64, 2, 4, 0), (2, 4, 64, 4, 2, 51)],
+                    16: [(4, 4, 64, 8, 2, 0), (2, 8, 64, 4, 2, 0), (4, 4, 64, 8, 2, 51),
+                         (2, 8, 64, 4, 2, 51)],
+                    32: [(8, 4, 64, 16, 1, 0), (4, 8, 64, 8, 2, 0), (8, 4, 64, 16, 1, 51),
+                         (4, 8, 64, 8, 2, 51), (4, 8, 64, 8, 2, 53), (4, 8, 64, 8, 2, 2)],
+                    64: [(8, 8, 64, 16, 1, 0), (16, 4, 64, 16, 1, 0), (8, 8, 64, 16, 1, 51),
+                         (8, 8, 64, 16, 1, 50), (8, 8, 64, 16, 1, 53), (8, 8, 64, 16, 1, 2)]}
+MULTI_TILED_CPLX = {2: [(1, 2, 64, 2, 4, 0), (2, 1, 32, 2, 4, 0)],
+                    4: [(2, 2, 64, 4, 2, 0), (1, 4, 64, 2, 4, 0)],
+                    8: [(4, 2, 32, 4, 2, 0), (2, 4, 64, 4, 2, 0)],
+                    16: [(8, 2, 32, 8, 2, 0), (4, 4, 32, 4, 2, 0), (8, 2, 32, 8, 2, 41),
+                         (8, 2, 32, 8, 2, 43)],
+                    32: [(8, 4, 32, 8, 2, 0), (16, 2, 32, 16, 1, 0), (8, 4, 32, 8, 2, 41)],
+                    64: [(16, 4, 16, 8, 2, 0), (8, 8, 32, 8, 2, 0), (16, 4, 16, 8, 2, 41),
+                         (16, 4, 16, 8, 2, 43)]}
 
 
 def write_multi_tiled():
@@ -93,9 +102,9 @@ def write_multi_tiled():
                                 ("kMultiTiledReal", "false", MULTI_TILED_REAL)):
         lines.append(f"const MultiEntry {table}[] = {{")
         for w, cfgs in shapes.items():
-            for (t, p, r, cw, bps) in cfgs:
+            for (t, p, r, cw, bps, cv) in cfgs:
                 assert t * p == w and cw * 32 % t == 0
-                lines.append(f"    TBTKKPM_MULTI_TILED_ENTRY({cplx}, {t}, {p}, {r}, {cw}, {bps}),")
+                lines.append(f"    TBTKKPM_MULTI_TILED_ENTRY({cplx}, {t}, {p}, {r}, {cw}, {bps}, {cv}),")
         lines += ["};", f"const int kNum{table[1:]} = sizeof({table}) / sizeof({table}[0]);", ""]
     lines += ["}  // namespace tbtkkpm", ""]
     (HERE / "steps_multi_tiled.cu").write_text("\n".join(lines))

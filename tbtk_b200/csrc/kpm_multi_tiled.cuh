@@ -31,32 +31,72 @@
 
 namespace tbtkkpm {
 
-// Tile-staged variant code of a multi-model entry: kTiledVariant + 1000*R +
-// 10*CW + BPS (R rows per tile, CW consumer warps, BPS blocks per SM).
+// Tile-staged variant code of a multi-model entry: kTiledVariant +
+// 1000000*CV + 1000*R + 10*CW + BPS (CV the widening split, R rows per tile,
+// CW consumer warps, BPS blocks per SM).
 constexpr int kMultiTiledVariant = 100000;
 inline bool is_multi_tiled(int minb) { return minb >= kMultiTiledVariant; }
 inline int multi_tiled_rows(int minb) { return ((minb - kMultiTiledVariant) % 1000000) / 1000; }
 inline int multi_tiled_bps(int minb) { return minb % 10; }
 
-// Per launch tile: its model and its plan header, the runs copied into the
-// launch's run list at the model's run0.  One block per model.
+// Descriptor of a launch tile, 6 x 16 bytes: [0] its plan header {entry
+// chunk, first run in the launch's run list, distinct outside rows, w |
+// runs << 16}; [1] {model | rows << 16, first row, target bits of its rows
+// (2 words)}; [2..5] its first kDescRuns runs.  The targets change only
+// between ticks, so one map serves every step of a tick.
+constexpr uint32_t kDescWords = 6;  // uint4 per descriptor
+constexpr uint32_t kDescRuns = 8;
+
+// Writes the descriptors (and the launch's run list) of every tile of the
+// launch's models: one block per model; R rows per tile (R divides 64).
 static __global__ void kpm_multi_tilemap_tiled(const MultiModel *__restrict__ models,
-                                               const MultiHeader *__restrict__ hdr,
-                                               uint32_t *tile_model, uint4 *tile_hdr,
-                                               uint2 *tile_runs) {
+                                               const MultiHeader *__restrict__ hdr, uint32_t R,
+                                               uint4 *tile_desc, uint2 *tile_runs) {
   if (blockIdx.x >= hdr->nmodels) return;
   const MultiModel &q = models[blockIdx.x];
-  const uint32_t t0 = q.tile0, nt = q.ntiles, r0 = q.run0;
+  const uint32_t t0 = q.tile0, nt = q.ntiles, ro = q.run0, N = q.A.N;
   for (uint32_t t = threadIdx.x; t < nt; t += blockDim.x) {
-    uint4 h = q.p_hdr[t];
-    h.y += r0;
-    tile_model[t0 + t] = blockIdx.x;
-    tile_hdr[t0 + t] = h;
+    const uint4 h = q.p_hdr[t];
+    uint4 *d = tile_desc + (size_t)(t0 + t) * kDescWords;
+    d[0] = make_uint4(h.x, h.y + ro, h.z, h.w);
+    const uint32_t r0 = t * R, rt = min(R, N - r0);
+    // bits of rows r0 .. r0 + rt - 1 (r0 a multiple of R)
+    unsigned long long bits = 0;
+    for (uint32_t w = r0 >> 5; w <= (r0 + rt - 1) >> 5; w++)
+      bits |= (unsigned long long)q.bitmap[w] << (32 * (w - (r0 >> 5)));
+    bits >>= (r0 & 31);
+    if (rt < 64) bits &= (1ull << rt) - 1;
+    d[1] = make_uint4(blockIdx.x | (rt << 16), r0, (uint32_t)bits, (uint32_t)(bits >> 32));
+    const uint32_t nruns = h.w >> 16;
+    uint2 rr[kDescRuns];
+#pragma unroll
+    for (uint32_t k = 0; k < kDescRuns; k++) rr[k] = k < nruns ? q.p_runs[h.y + k] : make_uint2(0, 0);
+#pragma unroll
+    for (uint32_t k = 0; k < kDescRuns; k += 2)
+      d[2 + k / 2] = make_uint4(rr[k].x, rr[k].y, rr[k + 1].x, rr[k + 1].y);
   }
-  for (uint32_t k = threadIdx.x; k < q.p_nruns; k += blockDim.x) tile_runs[r0 + k] = q.p_runs[k];
+  for (uint32_t k = threadIdx.x; k < q.p_nruns; k += blockDim.x) tile_runs[ro + k] = q.p_runs[k];
 }
 
-template <bool CPLX, int TPR, int VPT, int R, int CW, int BPS>
+// What the producer hands the consumers with each ring stage (in shared
+// memory beside the barriers, written before the stage's arrive).
+struct MultiStageMeta {
+  uint32_t model, r0, rows, w;
+  unsigned long long bits;   // target rows of the tile
+  unsigned long long first;  // lanes at their local step 1
+  void *y;                   // the model's output buffer (vec[n & 1])
+  long long *dots;           // the model's doubling sums
+};
+constexpr uint32_t kMultiHeader = 128 + kTiledMaxStages * 64;  // barriers, then a MultiStageMeta per stage
+static_assert(sizeof(MultiStageMeta) <= 64, "a stage's meta takes one 64-byte slot");
+
+// CV = 10*GA + PA splits the conversions between the pipes: the gathers of
+// a row's first GA entries and, with PA bit 0, j_{n-1} widen to FP64 on the
+// integer pipe (f2d_scaled, as in kpm_step_tiled), and with PA bit 1 the
+// doubling terms go to fixed point on the integer pipe (fix61_int); the
+// rest are conversion instructions on the XU pipe.  Every choice stores the
+// same vectors and sums the same fixed-point terms.
+template <bool CPLX, int TPR, int VPT, int R, int CW, int BPS, int CV>
 __global__ void __launch_bounds__(32 * (CW + 1), BPS)
 kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__restrict__ hdr,
                 TiledLayout LY, uint32_t step_offset, uint32_t W, uint32_t ld, int *err,
@@ -66,19 +106,24 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
   using Pk = typename std::conditional<CPLX, Pack<float2, TPR, VPT>, RPack<TPR, VPT>>::type;
   using L = typename Pk::L;
   constexpr int NL = Pk::NL;
+  constexpr int GA = CV / 10;
+  constexpr bool PA = (CV % 10) & 1;
+  constexpr bool PD = (CV % 10) & 2;
   constexpr int RPP = CW * 32 / TPR;  // rows per pass
   constexpr int PASSES = (R + RPP - 1) / RPP;
   static_assert(CW * 32 % TPR == 0, "a row group must divide the consumer threads");
+  static_assert(R <= 64 && 64 % R == 0, "a tile's target bits are one 64-bit word");
   extern __shared__ __align__(128) unsigned char tsm[];
   uint64_t *full = reinterpret_cast<uint64_t *>(tsm);
   uint64_t *empty = full + kTiledMaxStages;
-  unsigned char *ring = tsm + kTiledHeader;
+  MultiStageMeta *smeta = reinterpret_cast<MultiStageMeta *>(tsm + 128);
+  unsigned char *ring = tsm + kMultiHeader;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned fullmask = 0xffffffffu;
   const uint32_t S = LY.stages;
   const uint32_t rowbytes = W * (uint32_t)sizeof(E);
-  const uint32_t total = hdr->total_tiles;
-  const uint32_t *__restrict__ tile_model = hdr->tile_model;
-  const uint4 *__restrict__ thdr = hdr->tile_hdr;
+  const uint32_t total = hdr->total_tiles, run = hdr->run;
+  const uint4 *__restrict__ tdesc = hdr->tile_desc;
   const uint2 *__restrict__ truns = hdr->tile_runs;
   const int32_t n = hdr->n_base + (int32_t)step_offset;
   if (threadIdx.x == 0) {
@@ -89,55 +134,57 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  // the block's i-th tile: runs of kRun consecutive tiles, run b, b + grid, ...
+  // the block's i-th tile: runs of `run` consecutive tiles, run b, b + grid, ...
   auto tile_at = [&](uint32_t i) -> uint32_t {
-    return (blockIdx.x + (i / kRun) * gridDim.x) * kRun + i % kRun;
+    return (blockIdx.x + (i / run) * gridDim.x) * run + i % run;
   };
 
   if (warp == 0) {
     // ---------------------------------------------------------- producer
-    // Tile i is copied into stage i % S.  Headers and models two tiles
-    // ahead and the first 32 runs one tile ahead keep the dependent loads
-    // off the issue path; a model's pointers are reloaded when it changes.
+    // Lane l < 12 holds 8 bytes of a tile's descriptor (lanes 0-1 the
+    // header, 2-3 the meta word, 4-11 runs 0-7), loaded two tiles ahead, so
+    // a tile's copies are issued without waiting on a load; a model's
+    // pointers and first-step lanes are loaded when the model changes.
+    auto load_desc = [&](uint32_t t) -> uint2 {
+      return (t < total && lane < 12)
+                 ? __ldg(reinterpret_cast<const uint2 *>(tdesc + (size_t)t * kDescWords) + lane)
+                 : make_uint2(0, 0);
+    };
     uint32_t t0 = tile_at(0), t1 = tile_at(1);
-    uint4 h0 = make_uint4(0, 0, 0, 0), h1 = h0;
-    uint32_t q0 = 0, q1 = 0;
-    if (t0 < total) {
-      h0 = __ldg(thdr + t0);
-      q0 = __ldg(tile_model + t0);
-    }
-    if (t1 < total) {
-      h1 = __ldg(thdr + t1);
-      q1 = __ldg(tile_model + t1);
-    }
-    uint2 run0 = make_uint2(0, 0);
-    if (t0 < total && (uint32_t)lane < (h0.w >> 16)) run0 = __ldg(truns + h0.y + lane);
+    uint2 d0 = load_desc(t0), d1 = load_desc(t1);
     uint32_t cq = kPad;
     const Val *m_val = nullptr;
     const uint16_t *m_slot = nullptr;
-    const E *m_x = nullptr, *m_y = nullptr;
-    uint32_t m_t0 = 0, m_N = 0;
+    const E *m_x = nullptr;
+    E *m_y = nullptr;
+    long long *m_dots = nullptr;
+    unsigned long long m_first = 0;
     bool failed = false;
     uint32_t issued = 0;
     for (uint32_t i = 0; t0 < total; i++) {
       const uint32_t t2 = tile_at(i + 2);
-      uint4 h2 = make_uint4(0, 0, 0, 0);
-      uint32_t q2 = 0;
-      if (t2 < total) {
-        h2 = __ldg(thdr + t2);
-        q2 = __ldg(tile_model + t2);
-      }
-      uint2 run1 = make_uint2(0, 0);
-      if (t1 < total && (uint32_t)lane < (h1.w >> 16)) run1 = __ldg(truns + h1.y + lane);
+      const uint2 d2 = load_desc(t2);
+      const uint32_t h_ent = __shfl_sync(fullmask, d0.x, 0), h_run = __shfl_sync(fullmask, d0.y, 0);
+      const uint32_t nuniq = __shfl_sync(fullmask, d0.x, 1), hw = __shfl_sync(fullmask, d0.y, 1);
+      const uint32_t g_x = __shfl_sync(fullmask, d0.x, 2), r0 = __shfl_sync(fullmask, d0.y, 2);
+      const uint32_t b_lo = __shfl_sync(fullmask, d0.x, 3), b_hi = __shfl_sync(fullmask, d0.y, 3);
+      uint2 myrun;
+      myrun.x = __shfl_sync(fullmask, d0.x, (lane + 4) & 31);
+      myrun.y = __shfl_sync(fullmask, d0.y, (lane + 4) & 31);
+      const uint32_t q0 = g_x & 0xffffu, Rt = g_x >> 16;
       if (q0 != cq) {
         cq = q0;
         const MultiModel *md = models + q0;
         m_val = static_cast<const Val *>(md->p_val);
         m_slot = md->p_slot;
         m_x = reinterpret_cast<const E *>(md->vec[(n + 1) & 1]);
-        m_y = reinterpret_cast<const E *>(md->vec[n & 1]);
-        m_t0 = md->tile0;
-        m_N = md->A.N;
+        m_y = reinterpret_cast<E *>(md->vec[n & 1]);
+        m_dots = md->dots;
+        const int32_t *bs = md->base;
+        const bool f0 = (uint32_t)lane < W && n - __ldg(bs + lane) == 1;
+        const bool f1 = (uint32_t)lane + 32 < W && n - __ldg(bs + lane + 32) == 1;
+        m_first = (unsigned long long)__ballot_sync(fullmask, f0) |
+                  ((unsigned long long)__ballot_sync(fullmask, f1) << 32);
       }
       const uint32_t s = i % S;
       if (i >= S && !mbar_wait_limit(&empty[s], ((i / S) - 1) & 1u, wait_limit)) {
@@ -145,13 +192,24 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
         break;
       }
       unsigned char *st = ring + (size_t)s * LY.stage_bytes;
-      const uint32_t w = h0.w & 0xffffu, nruns = h0.w >> 16, nuniq = h0.z;
-      const uint32_t r0 = (t0 - m_t0) * R, Rt = min((uint32_t)R, m_N - r0);
+      const uint32_t w = hw & 0xffffu, nruns = hw >> 16;
       const uint32_t ebytes = w * R * (uint32_t)sizeof(Val), sbytes = w * R * 2u;
       const uint32_t bytes = (w ? ebytes + sbytes : 0u) + (2 * Rt + nuniq) * rowbytes;
-      if (lane == 0) mbar_expect_tx(&full[s], bytes);
+      if (lane == 0) {
+        MultiStageMeta &mt = smeta[s];
+        mt.model = q0;
+        mt.r0 = r0;
+        mt.rows = Rt;
+        mt.w = w;
+        mt.bits = (unsigned long long)b_lo | ((unsigned long long)b_hi << 32);
+        mt.first = m_first;
+        mt.y = m_y;
+        mt.dots = m_dots;
+        // the arrive (release) orders the meta before the consumers' wait
+        mbar_expect_tx(&full[s], bytes);
+      }
       __syncwarp();
-      const uint64_t e0 = (uint64_t)h0.x * R;
+      const uint64_t e0 = (uint64_t)h_ent * R;
       if (w) {
         if (lane == 0) bulk_load(st, m_val + e0, ebytes, &full[s]);
         if (lane == 1) bulk_load(st + LY.off_slots, m_slot + e0, sbytes, &full[s]);
@@ -159,8 +217,9 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
       if (lane == 2) bulk_load(st + LY.off_xs, m_x + (uint64_t)r0 * W, Rt * rowbytes, &full[s]);
       if (lane == 3) bulk_load(st + LY.off_prev, m_y + (uint64_t)r0 * W, Rt * rowbytes, &full[s]);
       for (uint32_t c = 0; c < nruns; c += 32) {
-        uint2 rn = run0;
-        if (c > 0) rn = (c + lane < nruns) ? __ldg(truns + h0.y + c + lane) : make_uint2(0, 0);
+        uint2 rn = myrun;
+        if (c > 0 || lane >= (int)kDescRuns)
+          rn = (c + lane < nruns) ? __ldg(truns + h_run + c + lane) : make_uint2(0, 0);
         if (c + lane < nruns) {
           const uint32_t slot = R + (rn.y >> 16), len = rn.y & 0xffffu;
           bulk_load(st + LY.off_xs + (size_t)slot * rowbytes, m_x + (uint64_t)rn.x * W,
@@ -169,12 +228,9 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
       }
       issued = i + 1;
       t0 = t1;
-      h0 = h1;
-      q0 = q1;
-      run0 = run1;
+      d0 = d1;
       t1 = t2;
-      h1 = h2;
-      q1 = q2;
+      d1 = d2;
     }
     if (failed && lane == 0) atomicExch(err, kErrTimeout);
     // every copy issued into this block's ring lands (or its wait runs out)
@@ -186,14 +242,14 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
       }
   } else {
     // ---------------------------------------------------------- consumers
+    // Everything a tile needs besides its staged rows comes with the stage
+    // (MultiStageMeta); only target rows read the model's target list.
     const int ct = threadIdx.x - 32;
     const int sub = ct % TPR, grp = ct / TPR;
     uint32_t cq = kPad;
-    const uint32_t *t_bitmap = nullptr, *t_row = nullptr, *t_col = nullptr;
-    const int32_t *t_base = nullptr;
     long long *t_dots = nullptr;
-    uint32_t t_count = 0, m_t0 = 0, m_N = 0, first = 0;
     E *m_y = nullptr;
+    uint32_t first = 0;
     long long s_nn[VPT], s_np[VPT];
 #pragma unroll
     for (int j = 0; j < VPT; j++) s_nn[j] = s_np[j] = 0;
@@ -205,8 +261,8 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
         long long a = s_nn[j], b = s_np[j];
 #pragma unroll
         for (int off = TPR; off < 32; off <<= 1) {
-          a += __shfl_xor_sync(0xffffffffu, a, off);
-          b += __shfl_xor_sync(0xffffffffu, b, off);
+          a += __shfl_xor_sync(fullmask, a, off);
+          b += __shfl_xor_sync(fullmask, b, off);
         }
         if (lane < TPR) {
           const uint32_t c = Pk::col_of(sub, j);
@@ -217,41 +273,25 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
       }
     };
     bool failed = false;
-    for (uint32_t i = 0;; i++) {
-      const uint32_t t = tile_at(i);
-      if (t >= total) break;
+    for (uint32_t i = 0; tile_at(i) < total; i++) {
       const uint32_t s = i % S;
-      const uint32_t q = __ldg(tile_model + t);
-      const uint32_t w = __ldg(thdr + t).w & 0xffffu;
-      if (q != cq) {
-        if (cq != kPad) flush();
-        cq = q;
-        const MultiModel *md = models + q;
-        t_bitmap = md->bitmap;
-        t_row = md->trow;
-        t_col = md->tcol;
-        t_count = md->tcount;
-        t_base = md->base;
-        t_dots = md->dots;
-        m_t0 = md->tile0;
-        m_N = md->A.N;
-        m_y = reinterpret_cast<E *>(md->vec[n & 1]);
-        first = 0;
-#pragma unroll
-        for (int j = 0; j < VPT; j++)
-          if (n - __ldg(t_base + Pk::col_of(sub, j)) == 1) first |= 1u << j;
-      }
-      const uint32_t r0 = (t - m_t0) * R, Rt = min((uint32_t)R, m_N - r0);
-      uint32_t bw[PASSES];
-#pragma unroll
-      for (int p = 0; p < PASSES; p++) {
-        const uint32_t lr = grp + p * RPP;
-        bw[p] = lr < Rt ? __ldg(t_bitmap + ((r0 + lr) >> 5)) : 0u;
-      }
       if (!mbar_wait_limit(&full[s], (i / S) & 1u, wait_limit)) {
         failed = true;
         break;
       }
+      const MultiStageMeta mt = smeta[s];
+      if (mt.model != cq) {
+        if (cq != kPad) flush();
+        cq = mt.model;
+        t_dots = mt.dots;
+        m_y = static_cast<E *>(mt.y);
+        first = 0;
+#pragma unroll
+        for (int j = 0; j < VPT; j++)
+          if ((mt.first >> Pk::col_of(sub, j)) & 1ull) first |= 1u << j;
+      }
+      const uint32_t w = mt.w, r0 = mt.r0, Rt = mt.rows;
+      const unsigned long long bits = mt.bits;
       const unsigned char *st = ring + (size_t)s * LY.stage_bytes;
       const Val *vals = reinterpret_cast<const Val *>(st);
       const uint16_t *slots = reinterpret_cast<const uint16_t *>(st + LY.off_slots);
@@ -262,6 +302,26 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
         const uint32_t lr = grp + p * RPP;
         if (lr >= Rt) continue;
         const uint32_t row = r0 + lr;
+        // moments of this row's targets (rare: the rows of lane sources and
+        // Green's-function to-indices)
+        auto targets = [&](auto store) {
+          const MultiModel *md = models + cq;
+          const uint32_t *t_row = md->trow, *t_col = md->tcol;
+          const uint32_t t_count = md->tcount;
+          uint32_t lo = 0, hi = t_count;
+          while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(t_row + mid) < row) lo = mid + 1; else hi = mid;
+          }
+          for (uint32_t e = lo; e < t_count && __ldg(t_row + e) == row; e++) {
+            const uint32_t tc = __ldg(t_col + e);
+            const uint32_t c = tc & kLaneBits;
+            const int jt = Pk::slot_of(sub, c);
+            if (jt < 0) continue;
+            double2 *dst = multi_target_dst(md, tc, n - __ldg(md->base + c), ld);
+            if (dst) store(dst, jt);
+          }
+        };
         if constexpr (CPLX) {
           double2 acc[VPT];
           {
@@ -269,7 +329,13 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
             Pk::load_rw(reinterpret_cast<const float2 *>(prev) + (size_t)lr * W, sub, yv);
 #pragma unroll
             for (int j = 0; j < VPT; j++) {
-              const double2 f = Pk::get(yv, j);
+              double2 f;
+              if constexpr (PA) {
+                const float2 g = Pk::getf(yv, j);
+                f = make_double2(f2d_scaled(g.x) * kWideUp, f2d_scaled(g.y) * kWideUp);
+              } else {
+                f = Pk::get(yv, j);
+              }
               acc[j] = ((first >> j) & 1u) ? make_double2(0.0, 0.0) : make_double2(-f.x, -f.y);
             }
           }
@@ -279,31 +345,27 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
             const double2 v = vals[k * R + lr];
             L xr[NL];
             Pk::load_rw(reinterpret_cast<const float2 *>(xs) + (size_t)sl * W, sub, xr);
+            if (GA > 0 && k < (uint32_t)GA) {
+              const double2 vu = make_double2(v.x * kWideUp, v.y * kWideUp);
 #pragma unroll
-            for (int j = 0; j < VPT; j++) acc[j] = cmac<false>(acc[j], v, Pk::get(xr, j));
+              for (int j = 0; j < VPT; j++) {
+                const float2 f = Pk::getf(xr, j);
+                acc[j] = cmac<false>(acc[j], vu, make_double2(f2d_scaled(f.x), f2d_scaled(f.y)));
+              }
+            } else {
+#pragma unroll
+              for (int j = 0; j < VPT; j++) acc[j] = cmac<false>(acc[j], v, Pk::get(xr, j));
+            }
           }
 #pragma unroll
           for (int j = 0; j < VPT; j++)
             if ((first >> j) & 1u) acc[j] = make_double2(acc[j].x * 0.5, acc[j].y * 0.5);
-          if ((bw[p] >> (row & 31)) & 1u) {
-            uint32_t lo = 0, hi = t_count;
-            while (lo < hi) {
-              const uint32_t mid = (lo + hi) >> 1;
-              if (__ldg(t_row + mid) < row) lo = mid + 1; else hi = mid;
-            }
-            for (uint32_t e = lo; e < t_count && __ldg(t_row + e) == row; e++) {
-              const uint32_t tc = __ldg(t_col + e);
-              const uint32_t c = tc & kLaneBits;
-              const int jt = Pk::slot_of(sub, c);
-              if (jt < 0) continue;
-              double2 *dst = multi_target_dst(models + cq, tc, n - __ldg(t_base + c), ld);
-              if (dst) {
+          if ((bits >> lr) & 1ull)
+            targets([&](double2 *dst, int jt) {
 #pragma unroll
-                for (int j = 0; j < VPT; j++)
-                  if (j == jt) *dst = acc[j];
-              }
-            }
-          }
+              for (int j = 0; j < VPT; j++)
+                if (j == jt) *dst = acc[j];
+            });
           float2 af[VPT];
 #pragma unroll
           for (int j = 0; j < VPT; j++)
@@ -314,8 +376,10 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
 #pragma unroll
           for (int j = 0; j < VPT; j++) {
             const float2 b = Pk::getf(self, j);
-            s_nn[j] += __float2ll_rn(fmaf(af[j].x, af[j].x, af[j].y * af[j].y) * kFixScale);
-            s_np[j] += __float2ll_rn(fmaf(af[j].x, b.x, af[j].y * b.y) * kFixScale);
+            const float nn = fmaf(af[j].x, af[j].x, af[j].y * af[j].y);
+            const float np = fmaf(af[j].x, b.x, af[j].y * b.y);
+            s_nn[j] += PD ? fix61_int(nn) : __float2ll_rn(nn * kFixScale);
+            s_np[j] += PD ? fix61_int(np) : __float2ll_rn(np * kFixScale);
           }
         } else {
           double acc[VPT];
@@ -323,8 +387,10 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
             L yv[NL];
             Pk::load_rw(reinterpret_cast<const float *>(prev) + (size_t)lr * W, sub, yv);
 #pragma unroll
-            for (int j = 0; j < VPT; j++)
-              acc[j] = ((first >> j) & 1u) ? 0.0 : -(double)Pk::getf(yv, j);
+            for (int j = 0; j < VPT; j++) {
+              const float f = Pk::getf(yv, j);
+              acc[j] = ((first >> j) & 1u) ? 0.0 : (PA ? f2d_scaled(f) * -kWideUp : -(double)f);
+            }
           }
           for (uint32_t k = 0; k < w; k++) {
             const uint16_t sl = slots[k * R + lr];
@@ -332,31 +398,24 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
             const double v = vals[k * R + lr];
             L xr[NL];
             Pk::load_rw(reinterpret_cast<const float *>(xs) + (size_t)sl * W, sub, xr);
+            if (GA > 0 && k < (uint32_t)GA) {
+              const double vu = v * kWideUp;
 #pragma unroll
-            for (int j = 0; j < VPT; j++) acc[j] = fma(v, (double)Pk::getf(xr, j), acc[j]);
+              for (int j = 0; j < VPT; j++) acc[j] = fma(vu, f2d_scaled(Pk::getf(xr, j)), acc[j]);
+            } else {
+#pragma unroll
+              for (int j = 0; j < VPT; j++) acc[j] = fma(v, (double)Pk::getf(xr, j), acc[j]);
+            }
           }
 #pragma unroll
           for (int j = 0; j < VPT; j++)
             if ((first >> j) & 1u) acc[j] = acc[j] * 0.5;
-          if ((bw[p] >> (row & 31)) & 1u) {
-            uint32_t lo = 0, hi = t_count;
-            while (lo < hi) {
-              const uint32_t mid = (lo + hi) >> 1;
-              if (__ldg(t_row + mid) < row) lo = mid + 1; else hi = mid;
-            }
-            for (uint32_t e = lo; e < t_count && __ldg(t_row + e) == row; e++) {
-              const uint32_t tc = __ldg(t_col + e);
-              const uint32_t c = tc & kLaneBits;
-              const int jt = Pk::slot_of(sub, c);
-              if (jt < 0) continue;
-              double2 *dst = multi_target_dst(models + cq, tc, n - __ldg(t_base + c), ld);
-              if (dst) {
+          if ((bits >> lr) & 1ull)
+            targets([&](double2 *dst, int jt) {
 #pragma unroll
-                for (int j = 0; j < VPT; j++)
-                  if (j == jt) *dst = make_double2(acc[j], 0.0);
-              }
-            }
-          }
+              for (int j = 0; j < VPT; j++)
+                if (j == jt) *dst = make_double2(acc[j], 0.0);
+            });
           float af[VPT];
 #pragma unroll
           for (int j = 0; j < VPT; j++) af[j] = __double2float_rn(acc[j]);
@@ -366,8 +425,9 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
 #pragma unroll
           for (int j = 0; j < VPT; j++) {
             const float b = Pk::getf(self, j);
-            s_nn[j] += __float2ll_rn(fmaf(af[j], af[j], 0.0f) * kFixScale);
-            s_np[j] += __float2ll_rn(fmaf(af[j], b, 0.0f) * kFixScale);
+            const float nn = fmaf(af[j], af[j], 0.0f), np = fmaf(af[j], b, 0.0f);
+            s_nn[j] += PD ? fix61_int(nn) : __float2ll_rn(nn * kFixScale);
+            s_np[j] += PD ? fix61_int(np) : __float2ll_rn(np * kFixScale);
           }
         }
       }
@@ -381,11 +441,11 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
 
 // Grid: BPS blocks per SM.  Launches nothing when the class has no layout
 // (ly.stages == 0: the host falls back to a register-staged entry).
-template <bool CPLX, int TPR, int VPT, int R, int CW, int BPS>
+template <bool CPLX, int TPR, int VPT, int R, int CW, int BPS, int CV>
 void launch_multi_tiled(cudaStream_t st, int device, const MultiModel *models,
                         const MultiHeader *hdr, uint32_t step_offset, uint32_t W, uint32_t ld,
                         const MultiLaunch &ml) {
-  auto kern = kpm_multi_tiled<CPLX, TPR, VPT, R, CW, BPS>;
+  auto kern = kpm_multi_tiled<CPLX, TPR, VPT, R, CW, BPS, CV>;
   if (ml.ly.stages == 0) return;
   static bool attr[64] = {false};
   const int d = device & 63;
@@ -393,13 +453,14 @@ void launch_multi_tiled(cudaStream_t st, int device, const MultiModel *models,
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tiled_budget(BPS));
     attr[d] = true;
   }
-  const uint32_t smem = kTiledHeader + ml.ly.stages * ml.ly.stage_bytes;
+  const uint32_t smem = kMultiHeader + ml.ly.stages * ml.ly.stage_bytes;
   kern<<<(unsigned)(BPS * sm_count(device)), 32 * (CW + 1), smem, st>>>(
       models, hdr, ml.ly, step_offset, W, ld, ml.err, ml.wait_limit);
 }
 
-#define TBTKKPM_MULTI_TILED_ENTRY(CPLX, T, P, R, CW, BPS) \
-  {T, P, kMultiTiledVariant + 1000 * R + 10 * CW + BPS, &launch_multi_tiled<CPLX, T, P, R, CW, BPS>}
+#define TBTKKPM_MULTI_TILED_ENTRY(CPLX, T, P, R, CW, BPS, CV)                          \
+  {T, P, kMultiTiledVariant + 1000000 * CV + 1000 * R + 10 * CW + BPS,                  \
+   &launch_multi_tiled<CPLX, T, P, R, CW, BPS, CV>}
 
 extern const MultiEntry kMultiTiled[];
 extern const int kNumMultiTiled;

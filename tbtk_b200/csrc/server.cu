@@ -172,9 +172,10 @@ TiledLayout multi_layout(const MultiEntry *e, uint32_t W, bool real, uint32_t wm
   p.R = (uint32_t)multi_tiled_rows(e->minb);
   p.wmax = wmax;
   p.umax = umax;
+  // the kernel's header holds a StageMeta per stage beside the barriers
   return tiled_layout(p, W * (uint32_t)(real ? sizeof(float) : sizeof(float2)),
                       real ? (uint32_t)sizeof(double) : (uint32_t)sizeof(double2),
-                      tiled_budget(multi_tiled_bps(e->minb)));
+                      tiled_budget(multi_tiled_bps(e->minb)) - (kMultiHeader - kTiledHeader));
 }
 
 // Default shape per width and class (measured choices of the single-model
@@ -238,7 +239,7 @@ struct tbtkkpm_server {
   int32_t n_global = 1;  // next global step
   uint64_t tick_no = 0;
   uint64_t resident = 0;
-  DevBuf d_models, d_hdr, d_joins, d_done, d_pairs, d_stage, d_damp, d_tiles, d_thdr, d_truns;
+  DevBuf d_models, d_hdr, d_joins, d_done, d_pairs, d_stage, d_damp, d_tiles, d_tdesc, d_truns;
   DevBuf d_err;           // staged-row wait that ran out (tile-staged steps)
   int *h_err = nullptr;   // pinned copy of d_err read after each tick
   // statistics
@@ -661,15 +662,22 @@ int run_tick(tbtkkpm_server *s, const std::vector<ClassPlan> &plans, uint32_t ns
     runs += cp.total_runs;
   }
   if ((rc = s->d_tiles.reserve(sizeof(uint32_t) * std::max<size_t>(tiles, 1))) ||
-      (rc = s->d_thdr.reserve(sizeof(uint4) * std::max<size_t>(tiles, 1))) ||
+      (rc = s->d_tdesc.reserve(sizeof(uint4) * kDescWords * std::max<size_t>(tiles, 1))) ||
       (rc = s->d_truns.reserve(sizeof(uint2) * std::max<size_t>(runs, 1))))
     return rc;
   tiles = runs = 0;
   for (const ClassPlan &cp : plans) {
     all.insert(all.end(), cp.models.begin(), cp.models.end());
+    // tile-staged launches: runs of 8-32 tiles per block, long enough that
+    // a block rarely changes model, short enough that every block has work
+    uint32_t run = kRun;
+    if (is_multi_tiled(cp.entry->minb)) {
+      const uint32_t grid = (uint32_t)multi_tiled_bps(cp.entry->minb) * (uint32_t)sm_count(s->device);
+      run = std::max(kRun, std::min(32u, cp.total_tiles / std::max(4 * grid, 1u)));
+    }
     hdr.push_back({(uint32_t)cp.models.size(), cp.total_tiles, s->n_global,
-                   s->d_tiles.as<uint32_t>() + tiles, s->d_thdr.as<uint4>() + tiles,
-                   s->d_truns.as<uint2>() + runs});
+                   s->d_tiles.as<uint32_t>() + tiles, s->d_tdesc.as<uint4>() + kDescWords * tiles,
+                   s->d_truns.as<uint2>() + runs, run});
     tiles += cp.total_tiles;
     runs += cp.total_runs;
   }
@@ -688,8 +696,8 @@ int run_tick(tbtkkpm_server *s, const std::vector<ClassPlan> &plans, uint32_t ns
       const MultiHeader &h = hdr[p];
       if (is_multi_tiled(plans[p].entry->minb))
         kpm_multi_tilemap_tiled<<<(unsigned)plans[p].models.size(), 256, 0, st>>>(
-            dm, s->d_hdr.as<MultiHeader>() + p, const_cast<uint32_t *>(h.tile_model),
-            const_cast<uint4 *>(h.tile_hdr), const_cast<uint2 *>(h.tile_runs));
+            dm, s->d_hdr.as<MultiHeader>() + p, (uint32_t)multi_tiled_rows(plans[p].entry->minb),
+            const_cast<uint4 *>(h.tile_desc), const_cast<uint2 *>(h.tile_runs));
       else
         kpm_multi_tilemap<<<(unsigned)plans[p].models.size(), 256, 0, st>>>(
             dm, s->d_hdr.as<MultiHeader>() + p, const_cast<uint32_t *>(h.tile_model));
@@ -1467,28 +1475,20 @@ extern "C" int tbtkkpm_server_set_real(tbtkkpm_server *s, int enable) {
   return TBTKKPM_OK;
 }
 
-extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32_t probe_steps,
-                                       int *tpr, int *vpt, int *minb, double *ms_per_step) {
-  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_autotune: NULL server");
-  if (!valid_width(width)) return fail(TBTKKPM_ERR_ARGUMENT, "server_autotune: bad width %u", width);
-  if (probe_steps < 2) return fail(TBTKKPM_ERR_ARGUMENT, "server_autotune: probe_steps < 2");
-  std::lock_guard<std::mutex> lk(s->mu);
-  if (s->failed) return fail(s->failed, "server: %s", s->fail_msg.c_str());
-  if (s->working || !s->pending.empty())
-    return fail(TBTKKPM_ERR_STATE, "server_autotune: the server is busy");
-  for (auto &p : s->models)
-    if (p->busy) return fail(TBTKKPM_ERR_STATE, "server_autotune: the server is busy");
-  Model *probe = nullptr;
-  for (auto &p : s->models)
-    if (p->W == width && (!probe || p->N > probe->N)) probe = p.get();
-  if (!probe) return fail(TBTKKPM_ERR_STATE, "server_autotune: no model of width %u", width);
+namespace tbtkkpm {
+namespace {
+
+// Times every compiled configuration of the probe model's lane class
+// (under s->mu, server idle) and keeps the fastest for that class.
+int tune_class(tbtkkpm_server *s, Model *probe, uint32_t width, uint32_t probe_steps,
+               const MultiEntry **best_out, double *best_ms_out) {
   DeviceGuard g(s->device);
   cudaStream_t st = s->stream;
   // a private copy of the lane state: every lane busy from global step 1
   const uint32_t W = width, N = probe->N, Mp = 2 * probe_steps + 2, ldp = Mp / 2 + 1;
   const bool real = probe->real;  // the class of the probe model is tuned
   const size_t es = probe->esize();
-  DevBuf vec[2], dots, mu, mud, base, laneM, bitmap, tlist, dm, dh, tmap, thdr, truns;
+  DevBuf vec[2], dots, mu, mud, base, laneM, bitmap, tlist, dm, dh, tmap, tdesc, truns;
   int rc;
   if ((rc = vec[0].reserve(es * (size_t)N * W)) ||
       (rc = vec[1].reserve(es * (size_t)N * W)) ||
@@ -1577,10 +1577,16 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
       d.run0 = 0;
     }
     // one model: every tile maps to model 0
-    if ((rc = tmap.reserve(4 * (size_t)d.ntiles)) || (rc = thdr.reserve(16 * (size_t)d.ntiles)) ||
+    if ((rc = tmap.reserve(4 * (size_t)d.ntiles)) ||
+        (rc = tdesc.reserve(16 * kDescWords * (size_t)d.ntiles)) ||
         (rc = truns.reserve(8 * (size_t)std::max(d.p_nruns, 1u))))
       break;
-    MultiHeader h{1, d.ntiles, n, tmap.as<uint32_t>(), thdr.as<uint4>(), truns.as<uint2>()};
+    uint32_t run = kRun;
+    if (plan) {
+      const uint32_t grid = (uint32_t)multi_tiled_bps(en.minb) * (uint32_t)sm_count(s->device);
+      run = std::max(kRun, std::min(32u, d.ntiles / std::max(4 * grid, 1u)));
+    }
+    MultiHeader h{1, d.ntiles, n, tmap.as<uint32_t>(), tdesc.as<uint4>(), truns.as<uint2>(), run};
     // parity of the buffers follows the global step, so the probe keeps
     // counting across configurations
     if ((e = cudaMemcpyAsync(dm.ptr, &d, sizeof(d), cudaMemcpyHostToDevice, st)) ||
@@ -1590,7 +1596,8 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
     }
     if (plan) {
       kpm_multi_tilemap_tiled<<<1, 256, 0, st>>>(dm.as<MultiModel>(), dh.as<MultiHeader>(),
-                                                 tmap.as<uint32_t>(), thdr.as<uint4>(), truns.as<uint2>());
+                                                 (uint32_t)multi_tiled_rows(en.minb), tdesc.as<uint4>(),
+                                                 truns.as<uint2>());
       count_launches(1);
     } else if ((e = cudaMemsetAsync(tmap.ptr, 0, 4 * (size_t)d.ntiles, st))) {
       rc = cuda_fail(e, "server_autotune: tile map");
@@ -1633,10 +1640,44 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
   if (rc) return rc;
   if (!best) return fail(TBTKKPM_ERR_UNSUPPORTED, "server_autotune: no kernel for width %u", W);
   s->config[W | (real ? 1u << 16 : 0u)] = {best->tpr, best->vpt, best->minb};
-  if (tpr) *tpr = best->tpr;
-  if (vpt) *vpt = best->vpt;
-  if (minb) *minb = best->minb;
-  if (ms_per_step) *ms_per_step = best_ms;
+  *best_out = best;
+  *best_ms_out = best_ms;
+  return TBTKKPM_OK;
+}
+
+}  // namespace
+}  // namespace tbtkkpm
+
+extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32_t probe_steps,
+                                       int *tpr, int *vpt, int *minb, double *ms_per_step) {
+  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_autotune: NULL server");
+  if (!valid_width(width)) return fail(TBTKKPM_ERR_ARGUMENT, "server_autotune: bad width %u", width);
+  if (probe_steps < 2) return fail(TBTKKPM_ERR_ARGUMENT, "server_autotune: probe_steps < 2");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->failed) return fail(s->failed, "server: %s", s->fail_msg.c_str());
+  if (s->working || !s->pending.empty())
+    return fail(TBTKKPM_ERR_STATE, "server_autotune: the server is busy");
+  for (auto &p : s->models)
+    if (p->busy) return fail(TBTKKPM_ERR_STATE, "server_autotune: the server is busy");
+  // the largest model of each lane class (real, complex) of this width
+  Model *probe[2] = {nullptr, nullptr};
+  for (auto &p : s->models) {
+    Model *&q = probe[p->real ? 1 : 0];
+    if (p->W == width && (!q || p->N > q->N)) q = p.get();
+  }
+  if (!probe[0] && !probe[1]) return fail(TBTKKPM_ERR_STATE, "server_autotune: no model of width %u", width);
+  const int main = !probe[0] || (probe[1] && probe[1]->N > probe[0]->N) ? 1 : 0;
+  const MultiEntry *best[2] = {nullptr, nullptr};
+  double best_ms[2] = {0, 0};
+  for (int c = 0; c < 2; c++) {
+    if (!probe[c]) continue;
+    const int rc = tune_class(s, probe[c], width, probe_steps, &best[c], &best_ms[c]);
+    if (rc) return rc;
+  }
+  if (tpr) *tpr = best[main]->tpr;
+  if (vpt) *vpt = best[main]->vpt;
+  if (minb) *minb = best[main]->minb;
+  if (ms_per_step) *ms_per_step = best_ms[main];
   return TBTKKPM_OK;
 }
 
@@ -1658,7 +1699,7 @@ extern "C" int tbtkkpm_server_destroy(tbtkkpm_server *s) {
     for (auto &t : s->tables) tbtkkpm_table_destroy(t.second);
     for (auto &t : s->exact) tbtkkpm_table_destroy(t.second);
     for (DevBuf *b : {&s->d_models, &s->d_hdr, &s->d_joins, &s->d_done, &s->d_pairs, &s->d_stage,
-                      &s->d_damp, &s->d_tiles, &s->d_thdr, &s->d_truns, &s->d_err})
+                      &s->d_damp, &s->d_tiles, &s->d_tdesc, &s->d_truns, &s->d_err})
       b->release();
     s->head_ws.release();
     s->d_res.release();
