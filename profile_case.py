@@ -15,6 +15,15 @@ source).  --sweep times every compiled step configuration for the batch;
 one; --batch-width splits the sites into batches of that many.  Without
 --rashba the model is real and the mixed precisions run on real float
 vectors; --complex-vectors keeps complex64 ones.
+
+    python profile_case.py --lattice 1024 --server 16 --moments 256 --config 4,4,164082
+
+--server W runs the same lattice as one model of the LDOS server with W
+lanes instead: one request of W sites at --moments moments, every step a
+float step (no FP64 head), with --config T,V,VARIANT installed (a
+configuration of tbtkkpm_server_step_configs), or each configuration of the
+width in turn with --sweep.  Prints the server's step time and bandwidth
+(algorithmic bytes, the server's own statistics).
 """
 from __future__ import annotations
 
@@ -51,7 +60,11 @@ def main():
     ap.add_argument("--fp64-head", type=int, default=0,
                     help="FP64 head steps of doubling runs (default 0: every step of a "
                          "doubling run is a timed FP32 step, as without a head)")
+    ap.add_argument("--server", type=int, default=0,
+                    help="run the lattice as one server model with this many lanes")
     a = ap.parse_args()
+    if a.server:
+        return server_case(a)
     prec = {"fp64": kpm.FP64, "mixed": kpm.MIXED, "mixed_direct": kpm.MIXED_DIRECT}[a.precision]
     rowptr, col, val = workloads.square_csr(a.lattice, a.lattice, t=1.0, J=0.5, W=2.0,
                                             alpha=a.rashba, seed=a.lattice)
@@ -99,6 +112,34 @@ def main():
             run(f"[tpr={t} vpt={v} minb={mb}]")
     else:
         run("")
+
+
+def server_case(a):
+    rowptr, col, val = workloads.square_csr(a.lattice, a.lattice, t=1.0, J=0.5, W=2.0,
+                                            alpha=a.rashba, seed=a.lattice)
+    N = rowptr.size - 1
+    W = a.server
+    sites = workloads.sample_sites(a.lattice * a.lattice, 2, W, 1 + a.lattice)
+    real = a.rashba == 0.0 and not a.complex_vectors
+    cfgs = kpm.Server.step_configs(W, real) if a.sweep else [None]
+    for cfg in cfgs:
+        srv = kpm.Server(a.moments, workloads.open_grid(12.0, a.energies), hbm_budget=64 << 30,
+                         tick_steps=64, tolerance=0)
+        srv.set_fp64_head(0)
+        srv.set_real(real)
+        mid = srv.add_model(rowptr, col, val, 12.0, W)
+        if cfg is None and a.config:
+            cfg = tuple(int(x) for x in a.config.split(","))
+        if cfg is not None:
+            srv.set_config(W, *cfg)
+        for _ in range(a.repeat):
+            srv.wait(srv.submit(mid, sites, a.moments, 1e-3))
+        st = srv.stats()
+        ms = st["step_s"] / max(st["steps"], 1) * 1e3
+        print(f"[server W={W} config={cfg}] N={N} M={a.moments}: {st['steps']:.0f} steps, "
+              f"{ms:.4f} ms/step ({st['step_bytes'] / max(st['step_s'], 1e-12) / 1e9:.0f} GB/s "
+              f"algorithmic)", flush=True)
+        srv.close()
 
 
 if __name__ == "__main__":

@@ -185,6 +185,14 @@ namespace tbtkkpm {
 // vectors [K][terms] on the device (terms 0: the table's M).
 int launch_energy_sum(cudaStream_t st, const tbtkkpm_table *t, const double2 *mu, uint32_t K,
                       int type, void *out, uint32_t terms = 0);
+// Energy sum of host moments [K][terms] into host `out` (terms 0: the
+// table's M; out_elem the bytes of one result value).
+int energy_sum_host(tbtkkpm_table *t, const double *mu, uint32_t K, int type, void *out,
+                    size_t out_elem, uint32_t terms);
+// tbtkkpm_ldos_sites for M <= the table's rows moments.
+int ldos_sites_terms(tbtkkpm_matrix *m, tbtkkpm_table *t, uint32_t M, const uint32_t *sites,
+                     uint32_t B, double broadening, int precision, double *ldos_out,
+                     double *err_out);
 // Lorentz damping numerators a[n] and denominator b (host libm).
 void damping_factors(uint32_t M, double broadening, std::vector<double> &a, double &b);
 // Error estimate of doubled moments against the directly gathered ones.

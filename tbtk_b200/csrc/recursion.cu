@@ -817,17 +817,20 @@ int launch_energy_sum(cudaStream_t st, const tbtkkpm_table *t, const double2 *mu
   return TBTKKPM_OK;
 }
 
-static int energy_sum_host(tbtkkpm_table *t, const double *mu, uint32_t K, int type, void *out,
-                           size_t out_elem) {
+// Energy sum of host moments [K][terms] (terms 0: the table's M; a table of
+// more rows serves fewer terms with the same sums) into host `out`.
+int energy_sum_host(tbtkkpm_table *t, const double *mu, uint32_t K, int type, void *out,
+                    size_t out_elem, uint32_t terms) {
   std::lock_guard<std::mutex> lk(t->lock);
   DeviceGuard g(t->device);
-  const size_t mbytes = sizeof(double2) * (size_t)K * t->M;
+  const uint32_t M = terms ? terms : t->M;
+  const size_t mbytes = sizeof(double2) * (size_t)K * M;
   const size_t obytes = out_elem * (size_t)K * t->E;
   int rc;
   if ((rc = t->mu.reserve(mbytes)) || (rc = t->out.reserve(obytes))) return rc;
   cudaError_t e = cudaMemcpyAsync(t->mu.ptr, mu, mbytes, cudaMemcpyHostToDevice, t->stream);
   if (e != cudaSuccess) return cuda_fail(e, "energy sum: upload");
-  if ((rc = launch_energy_sum(t->stream, t, t->mu.as<double2>(), K, type, t->out.ptr))) return rc;
+  if ((rc = launch_energy_sum(t->stream, t, t->mu.as<double2>(), K, type, t->out.ptr, M))) return rc;
   e = cudaMemcpyAsync(out, t->out.ptr, obytes, cudaMemcpyDeviceToHost, t->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
   if (e != cudaSuccess) return cuda_fail(e, "energy sum: download");
@@ -842,24 +845,34 @@ extern "C" int tbtkkpm_greens(tbtkkpm_table *t, const double *mu, uint32_t K, in
   if (type < 0 || type > 3) return fail(TBTKKPM_ERR_ARGUMENT, "greens: Unkown Green's function type %d", type);
   if (K == 0) return TBTKKPM_OK;
   if (!mu || !G_out) return fail(TBTKKPM_ERR_ARGUMENT, "greens: NULL buffers");
-  return energy_sum_host(t, mu, K, type, G_out, sizeof(double2));
+  return energy_sum_host(t, mu, K, type, G_out, sizeof(double2), 0);
 }
 
 extern "C" int tbtkkpm_ldos(tbtkkpm_table *t, const double *mu, uint32_t K, double *ldos_out) {
   if (!t) return fail(TBTKKPM_ERR_ARGUMENT, "ldos: NULL table");
   if (K == 0) return TBTKKPM_OK;
   if (!mu || !ldos_out) return fail(TBTKKPM_ERR_ARGUMENT, "ldos: NULL buffers");
-  return energy_sum_host(t, mu, K, 4, ldos_out, sizeof(double));
+  return energy_sum_host(t, mu, K, 4, ldos_out, sizeof(double), 0);
 }
 
 extern "C" int tbtkkpm_ldos_sites(tbtkkpm_matrix *m, tbtkkpm_table *t, const uint32_t *sites,
                                   uint32_t B, double broadening, int precision, double *ldos_out,
                                   double *err_out) {
+  if (!t) return fail(TBTKKPM_ERR_ARGUMENT, "ldos_sites: NULL table");
+  return tbtkkpm::ldos_sites_terms(m, t, t->M, sites, B, broadening, precision, ldos_out, err_out);
+}
+
+// tbtkkpm_ldos_sites with M <= the table's rows moments: a table of more
+// rows gives the same sums as one of M rows.
+int tbtkkpm::ldos_sites_terms(tbtkkpm_matrix *m, tbtkkpm_table *t, uint32_t M, const uint32_t *sites,
+                              uint32_t B, double broadening, int precision, double *ldos_out,
+                              double *err_out) {
   int rc = check_precision(precision);
   if (rc) return rc;
   if (!t) return fail(TBTKKPM_ERR_ARGUMENT, "ldos_sites: NULL table");
   if (B && !ldos_out) return fail(TBTKKPM_ERR_ARGUMENT, "ldos_sites: NULL ldos_out");
-  const uint32_t M = t->M, E = t->E;
+  if (M == 0 || M > t->M) return fail(TBTKKPM_ERR_ARGUMENT, "ldos_sites: %u moments for a table of %u", M, t->M);
+  const uint32_t E = t->E;
   if (B == 0) return TBTKKPM_OK;
   rc = check_moment_args(m, sites, B, sites, nullptr, B, M, broadening, ldos_out, "ldos_sites");
   if (rc) return rc;
@@ -926,7 +939,7 @@ extern "C" int tbtkkpm_ldos_sites(tbtkkpm_matrix *m, tbtkkpm_table *t, const uin
                                                                    ws.mu.as<double2>());
       count_launches(1);
     }
-    if ((rc = launch_energy_sum(m->stream, t, ws.mu.as<double2>(), nb, 4, ws.out.ptr))) return rc;
+    if ((rc = launch_energy_sum(m->stream, t, ws.mu.as<double2>(), nb, 4, ws.out.ptr, M))) return rc;
     m->timer.mark(m->stream, 3);
     e = cudaMemcpyAsync(ldos_out + (size_t)b0 * E, ws.out.ptr, sizeof(double) * (size_t)nb * E,
                         cudaMemcpyDeviceToHost, m->stream);

@@ -107,6 +107,8 @@ struct Model {
   uint32_t tcount = 0;
   bool dirty = true;
   DevBuf lane_mem;  // one allocation; the lane buffers above are views into it
+  // gather plans of the matrix by 2 * rows per tile + complex (null: none)
+  std::map<int, const TilePlan *> plans;
   void release_lanes() {
     for (DevBuf *b : {&vec[0], &vec[1], &dots, &mu, &mu_direct, &base, &laneM, &bitmap, &tlist,
                       &pmu}) {
@@ -116,6 +118,18 @@ struct Model {
     lane_mem.release();
     resident = false;
   }
+};
+
+// The FP64 recomputation of the outputs `idx` of a finished request, with
+// copies of what it needs: the rerun thread writes the results back under
+// the server's lock, by request id, only if the request still waits.
+struct RerunJob {
+  uint64_t id = 0;
+  Model *m = nullptr;
+  int kind = kLdos;
+  uint32_t M = 0;
+  double broadening = 0;
+  std::vector<uint32_t> sites, to, pair_src, idx;
 };
 
 // Lane memory of a model: vectors, fixed-point sums, moments, lane tables,
@@ -159,8 +173,18 @@ const MultiEntry *find_multi(int tpr, int vpt, int minb, bool real) {
 const TilePlan *model_plan(Model *m, const MultiEntry *e, int *rc) {
   *rc = TBTKKPM_OK;
   if (!is_multi_tiled(e->minb) || (m->W * m->esize()) % 16 != 0) return nullptr;
+  const int R = multi_tiled_rows(e->minb), key = 2 * R + (m->real ? 0 : 1);
+  auto it = m->plans.find(key);
+  if (it != m->plans.end()) return it->second;
+  // the first use builds it on the matrix handle (under its lock: the rerun
+  // thread may be running an FP64 recomputation on the same handle)
   const TilePlan *p = nullptr;
-  *rc = tile_plan(m->mat, multi_tiled_rows(e->minb), !m->real, &p);
+  {
+    std::lock_guard<std::mutex> lk(m->mat->lock);
+    *rc = tile_plan(m->mat, R, !m->real, &p);
+  }
+  if (*rc) return nullptr;
+  m->plans[key] = p;
   return p;
 }
 
@@ -221,7 +245,6 @@ struct tbtkkpm_server {
   std::condition_variable cv_work, cv_done;
   std::deque<std::unique_ptr<Model>> models;
   std::map<double, tbtkkpm_table *> tables;                         // Mmax rows per scale
-  std::map<std::pair<uint32_t, double>, tbtkkpm_table *> exact;     // FP64 reruns
   std::map<uint32_t, std::array<int, 3>> config;  // width | real << 16 -> tpr, vpt, minb
   bool use_real = true;                           // real lanes for real models added later
   uint32_t head_steps = kPrefixSteps;             // FP64 head of models added later
@@ -232,6 +255,12 @@ struct tbtkkpm_server {
   uint64_t next_id = 1;
   bool stop = false;
   bool working = false;  // a tick or finish phase is running
+  // FP64 recomputations run on their own thread (rerun_worker), so the
+  // worker keeps stepping the other requests meanwhile
+  std::deque<RerunJob> rerun_jobs;
+  int rerun_running = 0;
+  std::condition_variable cv_rerun;
+  std::thread rerun_thread;
   int failed = 0;
   std::string fail_msg;
   std::thread worker;
@@ -250,6 +279,12 @@ struct tbtkkpm_server {
   double *h_res = nullptr;      // pinned host copy of d_res
   size_t h_res_cap = 0;
   cudaEvent_t ev[2] = {nullptr, nullptr};  // around the steps of a tick
+  // The lane classes of a tick are independent (different models), so
+  // their steps run on their own streams, forked from and joined back into
+  // `stream`: a class of small, latency-bound steps overlaps the others.
+  static constexpr int kClassStreams = 4;
+  cudaStream_t cls_stream[kClassStreams] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[kClassStreams] = {};
 
   const std::array<int, 3> &config_for(uint32_t W, bool real) {
     const uint32_t key = W | (real ? 1u << 16 : 0u);
@@ -706,19 +741,32 @@ int run_tick(tbtkkpm_server *s, const std::vector<ClassPlan> &plans, uint32_t ns
     count_launches(plans.size());
   }
   cudaEventRecord(s->ev[0], st);
+  // class p steps on stream p % kClassStreams (in order within a class)
+  const int nstreams = (int)std::min<size_t>(plans.size(), tbtkkpm_server::kClassStreams);
+  if (nstreams > 1) {
+    if ((e = cudaEventRecord(s->ev_fork, st))) return cuda_fail(e, "server: fork");
+    for (int i = 0; i < nstreams; i++)
+      if ((e = cudaStreamWaitEvent(s->cls_stream[i], s->ev_fork, 0))) return cuda_fail(e, "server: fork");
+  }
   for (uint32_t k = 0; k < nsteps; k++) {
     size_t off = 0;
     for (size_t p = 0; p < plans.size(); p++) {
       const ClassPlan &cp = plans[p];
       const MultiModel *dm = s->d_models.as<MultiModel>() + off;
       const MultiHeader *dh = s->d_hdr.as<MultiHeader>() + p;
-      cp.entry->launch(st, s->device, dm, dh, k, cp.W, s->ld,
+      cudaStream_t cs = nstreams > 1 ? s->cls_stream[p % nstreams] : st;
+      cp.entry->launch(cs, s->device, dm, dh, k, cp.W, s->ld,
                        MultiLaunch{cp.ly, s->d_err.as<int>(), kWaitLimit});
       kpm_multi_finalize<<<(unsigned)cp.models.size(), std::min<uint32_t>(std::max(cp.W, 32u), 64u), 0,
-                           st>>>(dm, dh, k, cp.W, s->Mmax, s->ld);
+                           cs>>>(dm, dh, k, cp.W, s->Mmax, s->ld);
       off += cp.models.size();
     }
   }
+  if (nstreams > 1)
+    for (int i = 0; i < nstreams; i++)
+      if ((e = cudaEventRecord(s->ev_join[i], s->cls_stream[i])) ||
+          (e = cudaStreamWaitEvent(st, s->ev_join[i], 0)))
+        return cuda_fail(e, "server: join");
   cudaEventRecord(s->ev[1], st);
   count_launches(2ull * nsteps * plans.size());
   if ((e = cudaGetLastError())) return cuda_fail(e, "server: step launch");
@@ -729,20 +777,6 @@ int run_tick(tbtkkpm_server *s, const std::vector<ClassPlan> &plans, uint32_t ns
 }
 
 // ------------------------------------------------------------ finish
-
-tbtkkpm_table *exact_table(tbtkkpm_server *s, uint32_t M, double scale, int *rc) {
-  auto key = std::make_pair(M, scale);
-  auto it = s->exact.find(key);
-  if (it != s->exact.end()) return it->second;
-  tbtkkpm_table *t = nullptr;
-  const int prev = swap_selected_device(s->device);
-  *rc = s->table_free ? tbtkkpm_table_create_clenshaw(M, s->energies.data(), s->E, scale, &t)
-                      : tbtkkpm_table_create(M, s->energies.data(), s->E, scale, &t);
-  swap_selected_device(prev);
-  if (*rc) return nullptr;
-  s->exact[key] = t;
-  return t;
-}
 
 // The finish phase of the requests that completed in one tick, in two
 // halves: finish_launch enqueues their damping, energy sums and error
@@ -756,6 +790,10 @@ struct FinishBatch {
   std::vector<Model *> owner;
   std::vector<size_t> res_off;  // offset of each request's results in h_res
   cudaEvent_t ev = nullptr;     // after the results copy
+  // FP64 recomputations the host half found, and their requests (which
+  // complete when the rerun thread has written them back)
+  std::vector<RerunJob> reruns;
+  std::vector<Request *> rerun_req;
 };
 
 int finish_launch(tbtkkpm_server *s, FinishBatch &fb) {
@@ -868,49 +906,46 @@ int finish_launch(tbtkkpm_server *s, FinishBatch &fb) {
   return TBTKKPM_OK;
 }
 
-// FP64 recomputation of the outputs `idx` of a finished request (worker
-// thread, no lock held): LDOS sites through tbtkkpm_ldos_sites, Green's
-// function pairs through tbtkkpm_moments_batched and tbtkkpm_greens; each
-// result replaces the mixed-precision one in r->ldos.
-int rerun_fp64(tbtkkpm_server *s, Request *r, Model *m, const std::vector<uint32_t> &idx) {
-  const uint32_t E = s->E, M = r->M;
+// FP64 recomputation of a job's outputs (rerun thread, no lock held): LDOS
+// sites through the LDOS path, Green's function pairs through
+// tbtkkpm_moments_batched and the energy sum, both with the server's table
+// of max_moments rows summing the job's M terms (the same sums as a table
+// of M rows).  out receives [idx][E] LDOS or [idx][E] complex G.
+int rerun_fp64(tbtkkpm_server *s, const RerunJob &j, std::vector<double> &out) {
+  const uint32_t E = s->E, M = j.M;
   int rc;
-  tbtkkpm_table *t = exact_table(s, M, m->scale, &rc);
-  if (!t) return rc;
-  const size_t rd = r->result_doubles(E);
-  std::vector<double> out(idx.size() * rd);
-  if (r->kind == kLdos) {
+  Model *m = j.m;
+  const size_t rd = j.kind == kLdos ? E : 2 * (size_t)E;
+  out.assign(j.idx.size() * rd, 0.0);
+  const int prev = swap_selected_device(s->device);
+  if (j.kind == kLdos) {
     std::vector<uint32_t> miss;
-    for (uint32_t k : idx) miss.push_back(r->sites[k]);
-    if ((rc = tbtkkpm_ldos_sites(m->mat, t, miss.data(), (uint32_t)miss.size(), r->broadening,
-                                 TBTKKPM_FP64, out.data(), nullptr)))
-      return rc;
+    for (uint32_t k : j.idx) miss.push_back(j.sites[k]);
+    rc = ldos_sites_terms(m->mat, m->table, M, miss.data(), (uint32_t)miss.size(), j.broadening,
+                          TBTKKPM_FP64, out.data(), nullptr);
   } else {
     // one source per distinct from-index of the missed pairs
     std::vector<uint32_t> from, to, owner;
     std::map<uint32_t, uint32_t> src;
-    for (uint32_t k : idx) {
-      const uint32_t f = r->sites[r->pair_src[k]];
+    for (uint32_t k : j.idx) {
+      const uint32_t f = j.sites[j.pair_src[k]];
       auto it = src.find(f);
       if (it == src.end()) {
         it = src.emplace(f, (uint32_t)from.size()).first;
         from.push_back(f);
       }
-      to.push_back(r->to[k]);
+      to.push_back(j.to[k]);
       owner.push_back(it->second);
     }
-    std::vector<double> mu(2 * (size_t)idx.size() * M);
-    if ((rc = tbtkkpm_moments_batched(m->mat, from.data(), (uint32_t)from.size(), to.data(), owner.data(),
-                                      (uint32_t)to.size(), M, r->broadening, TBTKKPM_FP64, mu.data(),
-                                      nullptr)) ||
-        (rc = tbtkkpm_greens(t, mu.data(), (uint32_t)to.size(), r->kind, out.data())))
-      return rc;
+    std::vector<double> mu(2 * (size_t)j.idx.size() * M);
+    rc = tbtkkpm_moments_batched(m->mat, from.data(), (uint32_t)from.size(), to.data(), owner.data(),
+                                 (uint32_t)to.size(), M, j.broadening, TBTKKPM_FP64, mu.data(), nullptr);
+    if (!rc)
+      rc = energy_sum_host(m->table, mu.data(), (uint32_t)to.size(), j.kind, out.data(),
+                           sizeof(double2), M);
   }
-  for (size_t q = 0; q < idx.size(); q++) {
-    std::memcpy(r->ldos.data() + (size_t)idx[q] * rd, out.data() + q * rd, sizeof(double) * rd);
-    r->rerun[idx[q]] = 1;
-  }
-  return TBTKKPM_OK;
+  swap_selected_device(prev);
+  return rc;
 }
 
 int finish_complete(tbtkkpm_server *s, FinishBatch &fb) {
@@ -918,7 +953,6 @@ int finish_complete(tbtkkpm_server *s, FinishBatch &fb) {
   cudaError_t e = cudaEventSynchronize(fb.ev);
   if (e != cudaSuccess) return cuda_fail(e, "server: finish");
   const uint32_t E = s->E;
-  int rc;
   for (size_t i = 0; i < fb.done.size(); i++) {
     Request *r = fb.done[i];
     Model *m = fb.owner[i];
@@ -932,14 +966,20 @@ int finish_complete(tbtkkpm_server *s, FinishBatch &fb) {
       r->err[k] = ldos_error_estimate(r->err[k], m->table->wmax, r->ldos.data() + (size_t)k * rd, E,
                                       r->kind != kLdos);
     r->rerun.assign(K, 0);
-    std::vector<uint32_t> idx;
+    RerunJob j;
     for (uint32_t k = 0; k < K; k++)
-      if (s->tol > 0 && !(r->err[k] <= s->tol)) idx.push_back(k);
-    if (!idx.empty()) {
-      const auto r0 = Clock::now();
-      if ((rc = rerun_fp64(s, r, m, idx))) return rc;
-      s->reruns += (double)idx.size();
-      s->rerun_s += std::chrono::duration<double>(Clock::now() - r0).count();
+      if (s->tol > 0 && !(r->err[k] <= s->tol)) j.idx.push_back(k);
+    if (!j.idx.empty()) {
+      j.id = r->id;
+      j.m = m;
+      j.kind = r->kind;
+      j.M = r->M;
+      j.broadening = r->broadening;
+      j.sites = r->sites;
+      j.to = r->to;
+      j.pair_src = r->pair_src;
+      fb.reruns.push_back(std::move(j));
+      fb.rerun_req.push_back(r);
     }
   }
   return TBTKKPM_OK;
@@ -962,6 +1002,45 @@ void fail_all(tbtkkpm_server *s, int rc, const std::string &msg) {
   s->cv_done.notify_all();
 }
 
+// The rerun thread: FP64 recomputations of finished requests, one job at a
+// time, results written back under the lock if the request still waits.
+void rerun_worker(tbtkkpm_server *s) {
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  while (true) {
+    s->cv_rerun.wait(lk, [&] { return s->stop || !s->rerun_jobs.empty(); });
+    if (s->stop) break;
+    RerunJob j = std::move(s->rerun_jobs.front());
+    s->rerun_jobs.pop_front();
+    s->rerun_running += 1;
+    lk.unlock();
+    const auto r0 = Clock::now();
+    std::vector<double> out;
+    const int rc = rerun_fp64(s, j, out);
+    const auto r1 = Clock::now();
+    lk.lock();
+    s->rerun_running -= 1;
+    s->rerun_s += std::chrono::duration<double>(r1 - r0).count();
+    auto it = s->requests.find(j.id);
+    if (it == s->requests.end() || it->second->done) continue;  // failed or dropped meanwhile
+    Request *r = it->second.get();
+    if (rc) {
+      r->status = rc;
+      r->message = tbtkkpm_last_error();
+    } else {
+      const size_t rd = r->result_doubles(s->E);
+      for (size_t q = 0; q < j.idx.size(); q++) {
+        std::memcpy(r->ldos.data() + (size_t)j.idx[q] * rd, out.data() + q * rd, sizeof(double) * rd);
+        r->rerun[j.idx[q]] = 1;
+      }
+      s->reruns += (double)j.idx.size();
+    }
+    s->latencies_ms.push_back(std::chrono::duration<double, std::milli>(r1 - r->t_submit).count());
+    r->done = true;
+    s->cv_done.notify_all();
+  }
+}
+
 void worker(tbtkkpm_server *s) {
   cudaSetDevice(s->device);
   swap_selected_device(s->device);
@@ -978,12 +1057,21 @@ void worker(tbtkkpm_server *s) {
     lk.lock();
     s->finish_s += std::chrono::duration<double>(f1 - f0).count();
     if (rc) return rc;
+    // requests with FP64 recomputations complete on the rerun thread
+    std::sort(prev.rerun_req.begin(), prev.rerun_req.end());
     for (Request *r : prev.done) {
+      if (std::binary_search(prev.rerun_req.begin(), prev.rerun_req.end(), r)) continue;
       s->latencies_ms.push_back(std::chrono::duration<double, std::milli>(f1 - r->t_submit).count());
       r->done = true;
     }
+    if (!prev.reruns.empty()) {
+      for (RerunJob &j : prev.reruns) s->rerun_jobs.push_back(std::move(j));
+      s->cv_rerun.notify_one();
+    }
     prev.done.clear();
     prev.owner.clear();
+    prev.reruns.clear();
+    prev.rerun_req.clear();
     s->cv_done.notify_all();
     return TBTKKPM_OK;
   };
@@ -1159,18 +1247,31 @@ extern "C" int tbtkkpm_server_create(uint32_t max_moments, const double *energie
     cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev[0]);
     if (e == cudaSuccess) e = cudaEventCreate(&s->ev[1]);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming);
+    for (int i = 0; e == cudaSuccess && i < tbtkkpm_server::kClassStreams; i++) {
+      e = cudaStreamCreateWithFlags(&s->cls_stream[i], cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_join[i], cudaEventDisableTiming);
+    }
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_err, sizeof(int));
     if (e == cudaSuccess && s->d_err.reserve(sizeof(int)) != TBTKKPM_OK) e = cudaErrorMemoryAllocation;
     if (e == cudaSuccess) e = cudaMemset(s->d_err.ptr, 0, sizeof(int));
     if (e != cudaSuccess) {
       s->d_err.release();
       if (s->h_err) cudaFreeHost(s->h_err);
+      for (cudaEvent_t ev : {s->ev[0], s->ev[1], s->ev_fork})
+        if (ev) cudaEventDestroy(ev);
+      for (int i = 0; i < tbtkkpm_server::kClassStreams; i++) {
+        if (s->ev_join[i]) cudaEventDestroy(s->ev_join[i]);
+        if (s->cls_stream[i]) cudaStreamDestroy(s->cls_stream[i]);
+      }
+      if (s->stream) cudaStreamDestroy(s->stream);
       delete s;
       return cuda_fail(e, "server_create: stream");
     }
     *s->h_err = 0;
   }
   s->worker = std::thread(worker, s);
+  s->rerun_thread = std::thread(rerun_worker, s);
   *out = s;
   return TBTKKPM_OK;
 }
@@ -1655,7 +1756,7 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
   if (probe_steps < 2) return fail(TBTKKPM_ERR_ARGUMENT, "server_autotune: probe_steps < 2");
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->failed) return fail(s->failed, "server: %s", s->fail_msg.c_str());
-  if (s->working || !s->pending.empty())
+  if (s->working || !s->pending.empty() || !s->rerun_jobs.empty() || s->rerun_running)
     return fail(TBTKKPM_ERR_STATE, "server_autotune: the server is busy");
   for (auto &p : s->models)
     if (p->busy) return fail(TBTKKPM_ERR_STATE, "server_autotune: the server is busy");
@@ -1688,7 +1789,9 @@ extern "C" int tbtkkpm_server_destroy(tbtkkpm_server *s) {
     s->stop = true;
   }
   s->cv_work.notify_all();
+  s->cv_rerun.notify_all();
   if (s->worker.joinable()) s->worker.join();
+  if (s->rerun_thread.joinable()) s->rerun_thread.join();
   {
     DeviceGuard g(s->device);
     cudaStreamSynchronize(s->stream);
@@ -1697,7 +1800,6 @@ extern "C" int tbtkkpm_server_destroy(tbtkkpm_server *s) {
       tbtkkpm_matrix_destroy(p->mat);
     }
     for (auto &t : s->tables) tbtkkpm_table_destroy(t.second);
-    for (auto &t : s->exact) tbtkkpm_table_destroy(t.second);
     for (DevBuf *b : {&s->d_models, &s->d_hdr, &s->d_joins, &s->d_done, &s->d_pairs, &s->d_stage,
                       &s->d_damp, &s->d_tiles, &s->d_tdesc, &s->d_truns, &s->d_err})
       b->release();
@@ -1707,6 +1809,11 @@ extern "C" int tbtkkpm_server_destroy(tbtkkpm_server *s) {
     if (s->h_err) cudaFreeHost(s->h_err);
     for (cudaEvent_t &ev : s->ev)
       if (ev) cudaEventDestroy(ev);
+    if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+    for (int i = 0; i < tbtkkpm_server::kClassStreams; i++) {
+      if (s->ev_join[i]) cudaEventDestroy(s->ev_join[i]);
+      if (s->cls_stream[i]) cudaStreamDestroy(s->cls_stream[i]);
+    }
     cudaStreamDestroy(s->stream);
   }
   delete s;
