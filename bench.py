@@ -415,6 +415,7 @@ def server_sub():
             "solves": r["solves"], "wall_s": r["wall_s"],
             "plain_fp64": r["plain_fp64"], "speedup_vs_plain_fp64": r["speedup_vs_plain_fp64"],
             "ldos_rel_err_vs_fp64_max": r["ldos_rel_err_vs_fp64_max"],
+            "estimate_vs_error": r["estimate_vs_error"],
             "step_GBps": r["step_GBps"]}
 
 

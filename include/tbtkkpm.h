@@ -526,6 +526,14 @@ TBTKKPM_API int tbtkkpm_server_set_fp64_head(tbtkkpm_server *s, uint32_t steps);
  * max_moments x E table of 16-byte entries, same results up to rounding. */
 TBTKKPM_API int tbtkkpm_server_set_table_free(tbtkkpm_server *s, int enable);
 
+/* Bound of each wait of the server's tile-staged steps for rows staged in
+ * shared memory (polls; TBTKKPM_WAIT_DEFAULT: the library's bound), as
+ * tbtkkpm_matrix_set_wait_limit.  A wait that runs out ends that step early
+ * and fails every request of the server with TBTKKPM_ERR_TIMEOUT; the
+ * device context stays usable.  polls = 0 makes every such wait give up at
+ * once, which tests that path.  (No reference counterpart.) */
+TBTKKPM_API int tbtkkpm_server_set_wait_limit(tbtkkpm_server *s, uint32_t polls);
+
 /* Stops the worker (requests still queued or in flight are dropped) and
  * frees the server. */
 TBTKKPM_API int tbtkkpm_server_destroy(tbtkkpm_server *s);

@@ -75,24 +75,24 @@ MULTI_REAL_SHAPES = {1: [(1, 1)], 2: [(2, 1), (1, 2)], 4: [(4, 1), (1, 4)], 8: [
 # the register-staged steps.
 # The last field is the conversion split CV of kpm_multi_tiled (0: every
 # conversion an instruction of the XU pipe; 51: the first 5 gathers and
-# j_{n-1} widened on the integer pipe; 2 or 53: the doubling terms' fixed
-# point on the integer pipe too).
+# j_{n-1} widened on the integer pipe).  The doubling terms' fixed point on
+# the integer pipe too (an exact emulation of the conversion's rounding in
+# integer instructions) measured 1.4-1.5x slower on the 2048^2 and 512^2
+# lattices at 32 and 64 lanes and was dropped.
 MULTI_TILED_REAL = {4: [(1, 4, 64, 2, 4, 0), (1, 4, 64, 2, 2, 0)],
                     8: [(2, 4, 64, 4, 2, 0), (1, 8, 64, 2, 4, 0), (2, 4, 64, 4, 2, 51)],
                     16: [(4, 4, 64, 8, 2, 0), (2, 8, 64, 4, 2, 0), (4, 4, 64, 8, 2, 51),
                          (2, 8, 64, 4, 2, 51)],
                     32: [(8, 4, 64, 16, 1, 0), (4, 8, 64, 8, 2, 0), (8, 4, 64, 16, 1, 51),
-                         (4, 8, 64, 8, 2, 51), (4, 8, 64, 8, 2, 53), (4, 8, 64, 8, 2, 2)],
+                         (4, 8, 64, 8, 2, 51)],
                     64: [(8, 8, 64, 16, 1, 0), (16, 4, 64, 16, 1, 0), (8, 8, 64, 16, 1, 51),
-                         (8, 8, 64, 16, 1, 50), (8, 8, 64, 16, 1, 53), (8, 8, 64, 16, 1, 2)]}
+                         (8, 8, 64, 16, 1, 50)]}
 MULTI_TILED_CPLX = {2: [(1, 2, 64, 2, 4, 0), (2, 1, 32, 2, 4, 0)],
                     4: [(2, 2, 64, 4, 2, 0), (1, 4, 64, 2, 4, 0)],
                     8: [(4, 2, 32, 4, 2, 0), (2, 4, 64, 4, 2, 0)],
-                    16: [(8, 2, 32, 8, 2, 0), (4, 4, 32, 4, 2, 0), (8, 2, 32, 8, 2, 41),
-                         (8, 2, 32, 8, 2, 43)],
+                    16: [(8, 2, 32, 8, 2, 0), (4, 4, 32, 4, 2, 0), (8, 2, 32, 8, 2, 41)],
                     32: [(8, 4, 32, 8, 2, 0), (16, 2, 32, 16, 1, 0), (8, 4, 32, 8, 2, 41)],
-                    64: [(16, 4, 16, 8, 2, 0), (8, 8, 32, 8, 2, 0), (16, 4, 16, 8, 2, 41),
-                         (16, 4, 16, 8, 2, 43)]}
+                    64: [(16, 4, 16, 8, 2, 0), (8, 8, 32, 8, 2, 0), (16, 4, 16, 8, 2, 41)]}
 
 
 def write_multi_tiled():

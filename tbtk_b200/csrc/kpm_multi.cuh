@@ -29,28 +29,6 @@ constexpr int32_t kLaneIdle = INT32_MIN / 2;  // base step of a lane without a r
 constexpr float kFixScale = 2305843009213693952.0f;  // 2^61
 constexpr double kFixUnit = 1.0 / 2305843009213693952.0;  // 2^-61
 
-// The fixed-point term of a float x (|x| < 4) on the integer pipe: x * 2^61
-// rounded to the nearest integer, ties to even, the value
-// __float2ll_rn(x * kFixScale) gives (the product is exact for |x| < 4).  With
-// m the 24-bit significand and E the biased exponent, x * 2^61 = m * 2^(E -
-// 89): a left shift for E >= 89, else a right shift by k = 89 - E of m plus
-// (2^(k-1) - 1 + the lowest kept bit), which rounds half to even; k is
-// capped at 31, where every significand gives 0 (zero and subnormal floats
-// too).
-__device__ __forceinline__ long long fix61_int(float x) {
-  const uint32_t b = __float_as_uint(x);
-  const int sh = (int)((b >> 23) & 0xffu) - 89;
-  const uint32_t m = (b & 0x7fffffu) | 0x800000u;
-  unsigned long long r;
-  if (sh >= 0) {
-    r = (unsigned long long)m << sh;
-  } else {
-    const uint32_t k = (uint32_t)min(-sh, 31);
-    r = (m + (1u << (k - 1)) - 1u + ((m >> k) & 1u)) >> k;
-  }
-  return (b >> 31) ? -(long long)r : (long long)r;
-}
-
 // One model of a launch (device resident, rebuilt by the host per tick).
 struct MultiModel {
   Sell A;                    // model-local SELL, 2H/s

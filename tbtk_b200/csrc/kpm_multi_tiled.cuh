@@ -90,12 +90,10 @@ struct MultiStageMeta {
 constexpr uint32_t kMultiHeader = 128 + kTiledMaxStages * 64;  // barriers, then a MultiStageMeta per stage
 static_assert(sizeof(MultiStageMeta) <= 64, "a stage's meta takes one 64-byte slot");
 
-// CV = 10*GA + PA splits the conversions between the pipes: the gathers of
-// a row's first GA entries and, with PA bit 0, j_{n-1} widen to FP64 on the
-// integer pipe (f2d_scaled, as in kpm_step_tiled), and with PA bit 1 the
-// doubling terms go to fixed point on the integer pipe (fix61_int); the
-// rest are conversion instructions on the XU pipe.  Every choice stores the
-// same vectors and sums the same fixed-point terms.
+// CV = 10*GA + PA splits the float -> FP64 widenings between the pipes as
+// in kpm_step_tiled: the gathers of a row's first GA entries and, with PA,
+// j_{n-1} widen on the integer pipe (f2d_scaled), the rest by conversion
+// instructions on the XU pipe; every choice stores the same vectors.
 template <bool CPLX, int TPR, int VPT, int R, int CW, int BPS, int CV>
 __global__ void __launch_bounds__(32 * (CW + 1), BPS)
 kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__restrict__ hdr,
@@ -107,8 +105,7 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
   using L = typename Pk::L;
   constexpr int NL = Pk::NL;
   constexpr int GA = CV / 10;
-  constexpr bool PA = (CV % 10) & 1;
-  constexpr bool PD = (CV % 10) & 2;
+  constexpr bool PA = CV % 10 != 0;
   constexpr int RPP = CW * 32 / TPR;  // rows per pass
   constexpr int PASSES = (R + RPP - 1) / RPP;
   static_assert(CW * 32 % TPR == 0, "a row group must divide the consumer threads");
@@ -376,10 +373,8 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
 #pragma unroll
           for (int j = 0; j < VPT; j++) {
             const float2 b = Pk::getf(self, j);
-            const float nn = fmaf(af[j].x, af[j].x, af[j].y * af[j].y);
-            const float np = fmaf(af[j].x, b.x, af[j].y * b.y);
-            s_nn[j] += PD ? fix61_int(nn) : __float2ll_rn(nn * kFixScale);
-            s_np[j] += PD ? fix61_int(np) : __float2ll_rn(np * kFixScale);
+            s_nn[j] += __float2ll_rn(fmaf(af[j].x, af[j].x, af[j].y * af[j].y) * kFixScale);
+            s_np[j] += __float2ll_rn(fmaf(af[j].x, b.x, af[j].y * b.y) * kFixScale);
           }
         } else {
           double acc[VPT];
@@ -425,9 +420,8 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
 #pragma unroll
           for (int j = 0; j < VPT; j++) {
             const float b = Pk::getf(self, j);
-            const float nn = fmaf(af[j], af[j], 0.0f), np = fmaf(af[j], b, 0.0f);
-            s_nn[j] += PD ? fix61_int(nn) : __float2ll_rn(nn * kFixScale);
-            s_np[j] += PD ? fix61_int(np) : __float2ll_rn(np * kFixScale);
+            s_nn[j] += __float2ll_rn(fmaf(af[j], af[j], 0.0f) * kFixScale);
+            s_np[j] += __float2ll_rn(fmaf(af[j], b, 0.0f) * kFixScale);
           }
         }
       }

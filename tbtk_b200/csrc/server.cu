@@ -249,6 +249,7 @@ struct tbtkkpm_server {
   bool use_real = true;                           // real lanes for real models added later
   uint32_t head_steps = kPrefixSteps;             // FP64 head of models added later
   bool table_free = false;                        // Clenshaw energy sums for scales added later
+  uint32_t wait_limit = kWaitLimit;               // polls per staged-row wait (set_wait_limit)
   Workspace head_ws;                              // FP64 head scratch (worker thread)
   std::deque<uint64_t> pending;
   std::map<uint64_t, std::unique_ptr<Request>> requests;
@@ -756,7 +757,7 @@ int run_tick(tbtkkpm_server *s, const std::vector<ClassPlan> &plans, uint32_t ns
       const MultiHeader *dh = s->d_hdr.as<MultiHeader>() + p;
       cudaStream_t cs = nstreams > 1 ? s->cls_stream[p % nstreams] : st;
       cp.entry->launch(cs, s->device, dm, dh, k, cp.W, s->ld,
-                       MultiLaunch{cp.ly, s->d_err.as<int>(), kWaitLimit});
+                       MultiLaunch{cp.ly, s->d_err.as<int>(), s->wait_limit});
       kpm_multi_finalize<<<(unsigned)cp.models.size(), std::min<uint32_t>(std::max(cp.W, 32u), 64u), 0,
                            cs>>>(dm, dh, k, cp.W, s->Mmax, s->ld);
       off += cp.models.size();
@@ -1566,6 +1567,13 @@ extern "C" int tbtkkpm_server_set_fp64_head(tbtkkpm_server *s, uint32_t steps) {
   if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_set_fp64_head: NULL server");
   std::lock_guard<std::mutex> lk(s->mu);
   s->head_steps = steps;
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_server_set_wait_limit(tbtkkpm_server *s, uint32_t polls) {
+  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_set_wait_limit: NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->wait_limit = polls == TBTKKPM_WAIT_DEFAULT ? kWaitLimit : polls;
   return TBTKKPM_OK;
 }
 

@@ -14,14 +14,12 @@ const MultiEntry kMultiTiled[] = {
     TBTKKPM_MULTI_TILED_ENTRY(true, 8, 2, 32, 8, 2, 0),
     TBTKKPM_MULTI_TILED_ENTRY(true, 4, 4, 32, 4, 2, 0),
     TBTKKPM_MULTI_TILED_ENTRY(true, 8, 2, 32, 8, 2, 41),
-    TBTKKPM_MULTI_TILED_ENTRY(true, 8, 2, 32, 8, 2, 43),
     TBTKKPM_MULTI_TILED_ENTRY(true, 8, 4, 32, 8, 2, 0),
     TBTKKPM_MULTI_TILED_ENTRY(true, 16, 2, 32, 16, 1, 0),
     TBTKKPM_MULTI_TILED_ENTRY(true, 8, 4, 32, 8, 2, 41),
     TBTKKPM_MULTI_TILED_ENTRY(true, 16, 4, 16, 8, 2, 0),
     TBTKKPM_MULTI_TILED_ENTRY(true, 8, 8, 32, 8, 2, 0),
     TBTKKPM_MULTI_TILED_ENTRY(true, 16, 4, 16, 8, 2, 41),
-    TBTKKPM_MULTI_TILED_ENTRY(true, 16, 4, 16, 8, 2, 43),
 };
 const int kNumMultiTiled = sizeof(kMultiTiled) / sizeof(kMultiTiled[0]);
 
@@ -39,14 +37,10 @@ const MultiEntry kMultiTiledReal[] = {
     TBTKKPM_MULTI_TILED_ENTRY(false, 4, 8, 64, 8, 2, 0),
     TBTKKPM_MULTI_TILED_ENTRY(false, 8, 4, 64, 16, 1, 51),
     TBTKKPM_MULTI_TILED_ENTRY(false, 4, 8, 64, 8, 2, 51),
-    TBTKKPM_MULTI_TILED_ENTRY(false, 4, 8, 64, 8, 2, 53),
-    TBTKKPM_MULTI_TILED_ENTRY(false, 4, 8, 64, 8, 2, 2),
     TBTKKPM_MULTI_TILED_ENTRY(false, 8, 8, 64, 16, 1, 0),
     TBTKKPM_MULTI_TILED_ENTRY(false, 16, 4, 64, 16, 1, 0),
     TBTKKPM_MULTI_TILED_ENTRY(false, 8, 8, 64, 16, 1, 51),
     TBTKKPM_MULTI_TILED_ENTRY(false, 8, 8, 64, 16, 1, 50),
-    TBTKKPM_MULTI_TILED_ENTRY(false, 8, 8, 64, 16, 1, 53),
-    TBTKKPM_MULTI_TILED_ENTRY(false, 8, 8, 64, 16, 1, 2),
 };
 const int kNumMultiTiledReal = sizeof(kMultiTiledReal) / sizeof(kMultiTiledReal[0]);
 

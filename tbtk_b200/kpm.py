@@ -112,6 +112,7 @@ SIGNATURES = [
     ("tbtkkpm_server_autotune", _i, [_p, _u32, _u32, _p, _p, _p, _p]),
     ("tbtkkpm_server_set_config", _i, [_p, _u32, _i, _i, _i]),
     ("tbtkkpm_server_step_configs", _i, [_i, _u32, _p, _i]),
+    ("tbtkkpm_server_set_wait_limit", _i, [_p, _u32]),
     ("tbtkkpm_server_set_real", _i, [_p, _i]),
     ("tbtkkpm_server_set_fp64_head", _i, [_p, _u32]),
     ("tbtkkpm_server_set_table_free", _i, [_p, _i]),
@@ -586,6 +587,11 @@ class Server:
     def set_config(self, width, tpr, vpt, minb):
         _check(load_library().tbtkkpm_server_set_config(self._h, int(width), int(tpr), int(vpt),
                                                         int(minb)))
+
+    def set_wait_limit(self, polls=0xFFFFFFFF):
+        """Polls per staged-row wait of the tile-staged steps (default: the
+        library's bound; 0 makes every wait give up at once)."""
+        _check(load_library().tbtkkpm_server_set_wait_limit(self._h, int(polls)))
 
     def set_real(self, enable=True):
         """Real float lanes for real models added from now on (default)."""

@@ -47,3 +47,31 @@ def test_staged_row_wait_runs_out(gpu, alpha):
     m.set_fp64_head()
     again, _ = m.ldos_sites(tab, sites, 1e-3, gpu.MIXED)
     assert rel_err(again, ref) <= 1e-7
+
+
+def test_server_staged_row_wait_runs_out(gpu):
+    """A server whose tile-staged steps give up every staged-row wait at
+    once fails its requests with ERR_TIMEOUT, and the device still serves a
+    new server's requests correctly."""
+    from tbtk_b200 import workloads
+    csr = workloads.square_csr(24, 24, J=0.5, W=2.0, seed=1)
+    grid = workloads.open_grid(12.0, 100)
+    cfg = next(c for c in gpu.Server.step_configs(16, True) if c[2] >= 100000)
+    srv = gpu.Server(256, grid, hbm_budget=1 << 30, tick_steps=8, tolerance=0)
+    mid = srv.add_model(*csr, 12.0, 16)
+    srv.set_config(16, *cfg)
+    srv.set_fp64_head(0)
+    srv.set_wait_limit(0)
+    sites = np.arange(0, 160, 10, dtype=np.uint32)
+    with pytest.raises(gpu.TBTKError) as e:
+        srv.wait(srv.submit(mid, sites, 128, 1e-3))
+    assert e.value.status == gpu.ERR_TIMEOUT
+    srv.close()
+    good = gpu.Server(256, grid, hbm_budget=1 << 30, tick_steps=8, tolerance=0)
+    mid = good.add_model(*csr, 12.0, 16)
+    good.set_config(16, *cfg)
+    ldos, _, _ = good.wait(good.submit(mid, sites, 128, 1e-3))
+    ref, _ = gpu.Matrix.from_csr(*csr, 12.0).ldos_sites(gpu.Table.create(128, grid, 12.0), sites,
+                                                        1e-3, gpu.FP64)
+    assert rel_err(ldos, ref) <= 1e-6
+    good.close()
