@@ -485,15 +485,18 @@ TBTKKPM_API int tbtkkpm_server_cancel(tbtkkpm_server *s, uint64_t request);
 #define TBTKKPM_STAT_JOIN_S 16    /* worker time starting lanes (FP64 heads included) */
 #define TBTKKPM_STAT_PLAN_S 17    /* worker time admitting requests and planning ticks */
 #define TBTKKPM_STAT_TICK_S 18    /* worker time launching ticks and waiting for them */
-#define TBTKKPM_STAT_COUNT 19
+#define TBTKKPM_STAT_GRAPH_TICKS 19 /* ticks whose steps replayed a captured CUDA graph */
+#define TBTKKPM_STAT_COUNT 20
 TBTKKPM_API int tbtkkpm_server_stats(tbtkkpm_server *s, double *out, uint32_t n);
 
 /* Times every compiled step configuration of lane width `width` for
  * probe_steps steps, for each lane class (real float lanes, complex64
  * lanes) with a model of that width, on the largest model of the class
  * (the server must be idle), and keeps the fastest per class; the outputs
- * describe the class of the largest model.  set_config installs a known
- * one.  Results do not depend on the configuration. */
+ * describe the class of the largest model.  For a tile-staged pick it also
+ * builds the gather plans of every model of the class, so the first tick
+ * does not.  set_config installs a known one.  Results do not depend on the
+ * configuration. */
 TBTKKPM_API int tbtkkpm_server_autotune(
 	tbtkkpm_server *s, uint32_t width, uint32_t probe_steps, int *tpr,
 	int *vpt, int *minb, double *ms_per_step);
@@ -525,6 +528,13 @@ TBTKKPM_API int tbtkkpm_server_set_fp64_head(tbtkkpm_server *s, uint32_t steps);
  * (tbtkkpm_table_create_clenshaw): 8 E bytes per scale instead of the
  * max_moments x E table of 16-byte entries, same results up to rounding. */
 TBTKKPM_API int tbtkkpm_server_set_table_free(tbtkkpm_server *s, int enable);
+
+/* The steps of a tick replay a CUDA graph of one step of every lane class,
+ * captured when the tick starts (enable = 1, the default; a device counter
+ * gives each replay its step); enable = 0 launches every kernel of every
+ * step directly.  A capture that fails turns graphs off for the server.
+ * Results do not depend on it.  (No reference counterpart.) */
+TBTKKPM_API int tbtkkpm_server_set_graphs(tbtkkpm_server *s, int enable);
 
 /* Bound of each wait of the server's tile-staged steps for rows staged in
  * shared memory (polls; TBTKKPM_WAIT_DEFAULT: the library's bound), as

@@ -93,7 +93,22 @@ struct MultiHeader {
   const uint4 *tile_desc;
   const uint2 *tile_runs;
   uint32_t run;
+  // steps of the tick done so far, when the tick replays a captured graph
+  // of one step (kpm_multi_advance ends each replay); null otherwise
+  const int32_t *step;
 };
+
+// Global step of a launch: the tick's base, the launch's step offset and,
+// in a graph replay, the device counter of steps done.
+__device__ __forceinline__ int32_t multi_step_index(const MultiHeader *__restrict__ hdr,
+                                                    uint32_t step_offset) {
+  return hdr->n_base + (int32_t)step_offset + (hdr->step ? *hdr->step : 0);
+}
+
+// Ends one replay of a tick's step graph: the next replay is the next step.
+static __global__ void kpm_multi_advance(int32_t *step) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *step += 1;
+}
 
 // A block takes runs of kRun consecutive tiles (run r, r + gridDim.x, ...),
 // so it changes model (and flushes its sums) at most once per run.
@@ -151,7 +166,7 @@ kpm_multi_step(const MultiModel *__restrict__ models, const MultiHeader *__restr
   const unsigned mask = 0xffffffffu;
   const uint32_t nmodels = hdr->nmodels, total = hdr->total_tiles;
   const uint32_t *__restrict__ tile_model = hdr->tile_model;
-  const int32_t n = hdr->n_base + (int32_t)step_offset;
+  const int32_t n = multi_step_index(hdr, step_offset);
   if (nmodels == 0) return;
 
   // per-thread fixed-point sums in shared memory (see multi_flush)
@@ -375,7 +390,7 @@ static __global__ void kpm_multi_finalize(const MultiModel *__restrict__ models,
                                    uint32_t W, uint32_t Mmax, uint32_t ld) {
   if (blockIdx.x >= hdr->nmodels) return;
   const MultiModel *md = models + blockIdx.x;
-  const int32_t n = hdr->n_base + (int32_t)step_offset;
+  const int32_t n = multi_step_index(hdr, step_offset);
   for (uint32_t c = threadIdx.x; c < W; c += blockDim.x) {
     const long long a = md->dots[c], b = md->dots[W + c];
     md->dots[c] = 0;

@@ -24,7 +24,7 @@ kpm_multi_step_real(const MultiModel *__restrict__ models, const MultiHeader *__
   const unsigned mask = 0xffffffffu;
   const uint32_t nmodels = hdr->nmodels, total = hdr->total_tiles;
   const uint32_t *__restrict__ tile_model = hdr->tile_model;
-  const int32_t n = hdr->n_base + (int32_t)step_offset;
+  const int32_t n = multi_step_index(hdr, step_offset);
   if (nmodels == 0) return;
 
   // per-thread fixed-point sums, [2 * VPT][kBlock] in dynamic shared memory

@@ -122,7 +122,7 @@ kpm_multi_tiled(const MultiModel *__restrict__ models, const MultiHeader *__rest
   const uint32_t total = hdr->total_tiles, run = hdr->run;
   const uint4 *__restrict__ tdesc = hdr->tile_desc;
   const uint2 *__restrict__ truns = hdr->tile_runs;
-  const int32_t n = hdr->n_base + (int32_t)step_offset;
+  const int32_t n = multi_step_index(hdr, step_offset);
   if (threadIdx.x == 0) {
     for (uint32_t s = 0; s < S; s++) {
       mbar_init(&full[s], 1);

@@ -1,19 +1,23 @@
-// The LDOS server behind tbtkkpm_server_* (include/tbtkkpm.h): continuous
-// batching of LDOS requests over many device-resident models.
+// The server behind tbtkkpm_server_* (include/tbtkkpm.h): continuous
+// batching of LDOS and Green's-function requests over many device-resident
+// models.
 //
 // One worker thread per server repeats
-//   admit  - queued requests take free lanes of their model at the next
-//            step boundary; a model's lane memory is allocated on its first
-//            request within the HBM budget, evicting idle models (LRU);
-//   tick   - joins (column = e_site), then S steps of kpm_multi_step +
-//            kpm_multi_finalize per lane width over all models with busy
-//            lanes, S ending no later than the first lane that finishes;
-//   finish - for every finished request: moments (direct n <= M/2, doubled
-//            above) damped and summed over the energy grid on the device,
-//            the error estimate on the host, an FP64 recomputation
-//            (tbtkkpm_ldos_sites) of the sites past the tolerance, release
-//            of the lanes.
-// Submitters only queue and wait; all device work runs on the worker.
+//   admit  - queued requests take free lanes of their model (one per
+//            source) at the next step boundary; a model's lane memory is
+//            allocated on its first request within the HBM budget, evicting
+//            idle models (LRU);
+//   tick   - joins (column = e_source, or an FP64 head), then S steps of
+//            every lane class (width, real or complex lanes) over all
+//            models with busy lanes, S ending no later than the first lane
+//            that finishes: one step of every class captured as a CUDA
+//            graph and replayed S times, the classes on their own streams;
+//   finish - for every finished request: moments damped and summed over the
+//            energy grid on the device (LDOS or the request's Green's
+//            function type), the error estimate, release of the lanes.
+// A second thread runs the FP64 recomputations of outputs past the
+// tolerance, so the worker keeps stepping meanwhile.  Submitters only queue
+// and wait.
 #include "tbtkkpm.h"
 #include "kpm_host.h"
 #include "kpm_multi.cuh"
@@ -258,10 +262,13 @@ struct tbtkkpm_server {
   bool working = false;  // a tick or finish phase is running
   // FP64 recomputations run on their own thread (rerun_worker), so the
   // worker keeps stepping the other requests meanwhile
+  // (kRerunThreads threads: the FP64 recomputations of small models are
+  // launch-bound, so several run side by side on their own streams)
+  static constexpr int kRerunThreads = 4;
   std::deque<RerunJob> rerun_jobs;
   int rerun_running = 0;
   std::condition_variable cv_rerun;
-  std::thread rerun_thread;
+  std::thread rerun_threads[kRerunThreads];
   int failed = 0;
   std::string fail_msg;
   std::thread worker;
@@ -276,6 +283,7 @@ struct tbtkkpm_server {
   std::vector<double> latencies_ms;
   double reruns = 0, ticks = 0, steps = 0, lane_steps = 0, evictions = 0, waited = 0, busy_s = 0;
   double step_s = 0, step_bytes = 0, finish_s = 0, rerun_s = 0, join_s = 0, plan_s = 0, tick_s = 0;
+  double graph_ticks = 0;
   DevBuf d_res;                 // finish results of a tick: [ldos K*E | err K] per request
   double *h_res = nullptr;      // pinned host copy of d_res
   size_t h_res_cap = 0;
@@ -286,6 +294,11 @@ struct tbtkkpm_server {
   static constexpr int kClassStreams = 4;
   cudaStream_t cls_stream[kClassStreams] = {};
   cudaEvent_t ev_fork = nullptr, ev_join[kClassStreams] = {};
+  // Each tick's steps replay a captured CUDA graph of one step of every
+  // class (tick_exec; d_step counts the replays); off when a capture failed.
+  bool use_graphs = true;
+  cudaGraphExec_t tick_exec = nullptr;
+  DevBuf d_step;
 
   const std::array<int, 3> &config_for(uint32_t W, bool real) {
     const uint32_t key = W | (real ? 1u << 16 : 0u);
@@ -504,15 +517,20 @@ int upload_lanes(tbtkkpm_server *s, Model *m) {
     tl[cap + i] = t[i].second;
   }
   m->tcount = (uint32_t)t.size();
+  // the four tables are adjacent views of the lane memory: one copy of the
+  // range from base to the end of tlist (alignment gaps included)
+  char *lo = m->base.as<char>();
+  const size_t range = (size_t)(m->tlist.as<char>() - lo) + 4 * tl.size();
+  std::vector<char> buf(range, 0);
+  auto put = [&](const DevBuf &v, const void *src, size_t n) {
+    std::memcpy(buf.data() + (v.as<char>() - lo), src, n);
+  };
+  put(m->base, m->base_h.data(), 4 * (size_t)m->W);
+  put(m->laneM, m->M_h.data(), 4 * (size_t)m->W);
+  put(m->bitmap, m->bitmap_h.data(), 4 * m->bitmap_h.size());
+  put(m->tlist, tl.data(), 4 * tl.size());
   cudaError_t e;
-  if ((e = cudaMemcpyAsync(m->base.ptr, m->base_h.data(), 4 * (size_t)m->W, cudaMemcpyHostToDevice,
-                           s->stream)) ||
-      (e = cudaMemcpyAsync(m->laneM.ptr, m->M_h.data(), 4 * (size_t)m->W, cudaMemcpyHostToDevice,
-                           s->stream)) ||
-      (e = cudaMemcpyAsync(m->bitmap.ptr, m->bitmap_h.data(), 4 * m->bitmap_h.size(),
-                           cudaMemcpyHostToDevice, s->stream)) ||
-      (e = cudaMemcpyAsync(m->tlist.ptr, tl.data(), 4 * tl.size(), cudaMemcpyHostToDevice,
-                           s->stream)))
+  if ((e = cudaMemcpyAsync(lo, buf.data(), range, cudaMemcpyHostToDevice, s->stream)))
     return cuda_fail(e, "server: lane tables");
   m->dirty = false;
   return TBTKKPM_OK;
@@ -713,7 +731,7 @@ int run_tick(tbtkkpm_server *s, const std::vector<ClassPlan> &plans, uint32_t ns
     }
     hdr.push_back({(uint32_t)cp.models.size(), cp.total_tiles, s->n_global,
                    s->d_tiles.as<uint32_t>() + tiles, s->d_tdesc.as<uint4>() + kDescWords * tiles,
-                   s->d_truns.as<uint2>() + runs, run});
+                   s->d_truns.as<uint2>() + runs, run, s->use_graphs ? s->d_step.as<int32_t>() : nullptr});
     tiles += cp.total_tiles;
     runs += cp.total_runs;
   }
@@ -741,35 +759,76 @@ int run_tick(tbtkkpm_server *s, const std::vector<ClassPlan> &plans, uint32_t ns
     }
     count_launches(plans.size());
   }
-  cudaEventRecord(s->ev[0], st);
-  // class p steps on stream p % kClassStreams (in order within a class)
+  // class p steps on stream p % kClassStreams (in order within a class):
+  // the launches of `steps` steps from step offset k0, forked from st and
+  // joined back into it
   const int nstreams = (int)std::min<size_t>(plans.size(), tbtkkpm_server::kClassStreams);
-  if (nstreams > 1) {
-    if ((e = cudaEventRecord(s->ev_fork, st))) return cuda_fail(e, "server: fork");
-    for (int i = 0; i < nstreams; i++)
-      if ((e = cudaStreamWaitEvent(s->cls_stream[i], s->ev_fork, 0))) return cuda_fail(e, "server: fork");
-  }
-  for (uint32_t k = 0; k < nsteps; k++) {
-    size_t off = 0;
-    for (size_t p = 0; p < plans.size(); p++) {
-      const ClassPlan &cp = plans[p];
-      const MultiModel *dm = s->d_models.as<MultiModel>() + off;
-      const MultiHeader *dh = s->d_hdr.as<MultiHeader>() + p;
-      cudaStream_t cs = nstreams > 1 ? s->cls_stream[p % nstreams] : st;
-      cp.entry->launch(cs, s->device, dm, dh, k, cp.W, s->ld,
-                       MultiLaunch{cp.ly, s->d_err.as<int>(), s->wait_limit});
-      kpm_multi_finalize<<<(unsigned)cp.models.size(), std::min<uint32_t>(std::max(cp.W, 32u), 64u), 0,
-                           cs>>>(dm, dh, k, cp.W, s->Mmax, s->ld);
-      off += cp.models.size();
+  auto launch_steps = [&](uint32_t k0, uint32_t steps) -> cudaError_t {
+    cudaError_t ee;
+    if (nstreams > 1) {
+      if ((ee = cudaEventRecord(s->ev_fork, st))) return ee;
+      for (int i = 0; i < nstreams; i++)
+        if ((ee = cudaStreamWaitEvent(s->cls_stream[i], s->ev_fork, 0))) return ee;
     }
+    for (uint32_t k = k0; k < k0 + steps; k++) {
+      size_t off = 0;
+      for (size_t p = 0; p < plans.size(); p++) {
+        const ClassPlan &cp = plans[p];
+        const MultiModel *dm = s->d_models.as<MultiModel>() + off;
+        const MultiHeader *dh = s->d_hdr.as<MultiHeader>() + p;
+        cudaStream_t cs = nstreams > 1 ? s->cls_stream[p % nstreams] : st;
+        cp.entry->launch(cs, s->device, dm, dh, k, cp.W, s->ld,
+                         MultiLaunch{cp.ly, s->d_err.as<int>(), s->wait_limit});
+        kpm_multi_finalize<<<(unsigned)cp.models.size(), std::min<uint32_t>(std::max(cp.W, 32u), 64u),
+                             0, cs>>>(dm, dh, k, cp.W, s->Mmax, s->ld);
+        off += cp.models.size();
+      }
+    }
+    if (nstreams > 1)
+      for (int i = 0; i < nstreams; i++)
+        if ((ee = cudaEventRecord(s->ev_join[i], s->cls_stream[i])) ||
+            (ee = cudaStreamWaitEvent(st, s->ev_join[i], 0)))
+          return ee;
+    return cudaGetLastError();
+  };
+  // The tick's graph: one step of every class, captured once and replayed
+  // nsteps times (the device counter d_step gives each replay its step).
+  // A capture or instantiation that fails falls back to direct launches.
+  if (s->tick_exec) {
+    cudaGraphExecDestroy(s->tick_exec);
+    s->tick_exec = nullptr;
   }
-  if (nstreams > 1)
-    for (int i = 0; i < nstreams; i++)
-      if ((e = cudaEventRecord(s->ev_join[i], s->cls_stream[i])) ||
-          (e = cudaStreamWaitEvent(st, s->ev_join[i], 0)))
-        return cuda_fail(e, "server: join");
+  // the headers of this tick read d_step when graphs are on: it starts at 0
+  if (hdr[0].step && (e = cudaMemsetAsync(s->d_step.ptr, 0, sizeof(int32_t), st)))
+    return cuda_fail(e, "server: step counter");
+  bool replay = false;
+  if (hdr[0].step && nsteps > 1) {
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed) == cudaSuccess) {
+      cudaError_t ce = launch_steps(0, 1);
+      if (ce == cudaSuccess) {
+        kpm_multi_advance<<<1, 32, 0, st>>>(s->d_step.as<int32_t>());
+        ce = cudaGetLastError();
+      }
+      const cudaError_t ee = cudaStreamEndCapture(st, &g);
+      if (ce == cudaSuccess && ee == cudaSuccess && g &&
+          cudaGraphInstantiate(&s->tick_exec, g, 0) == cudaSuccess)
+        replay = true;
+      if (g) cudaGraphDestroy(g);
+    }
+    cudaGetLastError();
+    if (!replay) s->use_graphs = false;  // direct launches from the next tick on
+  }
+  cudaEventRecord(s->ev[0], st);
+  if (replay) {
+    for (uint32_t k = 0; k < nsteps; k++)
+      if ((e = cudaGraphLaunch(s->tick_exec, st))) return cuda_fail(e, "server: step graph");
+  } else if ((e = launch_steps(0, nsteps))) {
+    return cuda_fail(e, "server: step launch");
+  }
   cudaEventRecord(s->ev[1], st);
-  count_launches(2ull * nsteps * plans.size());
+  count_launches((2ull * plans.size() + (replay ? 1 : 0)) * nsteps);
+  if (replay) s->graph_ticks += 1;
   if ((e = cudaGetLastError())) return cuda_fail(e, "server: step launch");
   // the wait flag of the tile-staged steps, read after the tick
   if ((e = cudaMemcpyAsync(s->h_err, s->d_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, st)))
@@ -1003,8 +1062,9 @@ void fail_all(tbtkkpm_server *s, int rc, const std::string &msg) {
   s->cv_done.notify_all();
 }
 
-// The rerun thread: FP64 recomputations of finished requests, one job at a
+// A rerun thread: FP64 recomputations of finished requests, one job at a
 // time, results written back under the lock if the request still waits.
+// Jobs of one model take turns on its matrix handle (its lock).
 void rerun_worker(tbtkkpm_server *s) {
   cudaSetDevice(s->device);
   std::unique_lock<std::mutex> lk(s->mu);
@@ -1067,7 +1127,7 @@ void worker(tbtkkpm_server *s) {
     }
     if (!prev.reruns.empty()) {
       for (RerunJob &j : prev.reruns) s->rerun_jobs.push_back(std::move(j));
-      s->cv_rerun.notify_one();
+      s->cv_rerun.notify_all();
     }
     prev.done.clear();
     prev.owner.clear();
@@ -1254,10 +1314,13 @@ extern "C" int tbtkkpm_server_create(uint32_t max_moments, const double *energie
       if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->ev_join[i], cudaEventDisableTiming);
     }
     if (e == cudaSuccess) e = cudaMallocHost(&s->h_err, sizeof(int));
-    if (e == cudaSuccess && s->d_err.reserve(sizeof(int)) != TBTKKPM_OK) e = cudaErrorMemoryAllocation;
+    if (e == cudaSuccess && (s->d_err.reserve(sizeof(int)) != TBTKKPM_OK ||
+                             s->d_step.reserve(sizeof(int32_t)) != TBTKKPM_OK))
+      e = cudaErrorMemoryAllocation;
     if (e == cudaSuccess) e = cudaMemset(s->d_err.ptr, 0, sizeof(int));
     if (e != cudaSuccess) {
       s->d_err.release();
+      s->d_step.release();
       if (s->h_err) cudaFreeHost(s->h_err);
       for (cudaEvent_t ev : {s->ev[0], s->ev[1], s->ev_fork})
         if (ev) cudaEventDestroy(ev);
@@ -1272,7 +1335,7 @@ extern "C" int tbtkkpm_server_create(uint32_t max_moments, const double *energie
     *s->h_err = 0;
   }
   s->worker = std::thread(worker, s);
-  s->rerun_thread = std::thread(rerun_worker, s);
+  for (auto &t : s->rerun_threads) t = std::thread(rerun_worker, s);
   *out = s;
   return TBTKKPM_OK;
 }
@@ -1521,6 +1584,7 @@ extern "C" int tbtkkpm_server_stats(tbtkkpm_server *s, double *out, uint32_t n) 
   v[TBTKKPM_STAT_JOIN_S] = s->join_s;
   v[TBTKKPM_STAT_PLAN_S] = s->plan_s;
   v[TBTKKPM_STAT_TICK_S] = s->tick_s;
+  v[TBTKKPM_STAT_GRAPH_TICKS] = s->graph_ticks;
   for (uint32_t i = 0; i < n && i < TBTKKPM_STAT_COUNT; i++) out[i] = v[i];
   return TBTKKPM_OK;
 }
@@ -1567,6 +1631,13 @@ extern "C" int tbtkkpm_server_set_fp64_head(tbtkkpm_server *s, uint32_t steps) {
   if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_set_fp64_head: NULL server");
   std::lock_guard<std::mutex> lk(s->mu);
   s->head_steps = steps;
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_server_set_graphs(tbtkkpm_server *s, int enable) {
+  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_set_graphs: NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->use_graphs = enable != 0;
   return TBTKKPM_OK;
 }
 
@@ -1749,6 +1820,13 @@ int tune_class(tbtkkpm_server *s, Model *probe, uint32_t width, uint32_t probe_s
   if (rc) return rc;
   if (!best) return fail(TBTKKPM_ERR_UNSUPPORTED, "server_autotune: no kernel for width %u", W);
   s->config[W | (real ? 1u << 16 : 0u)] = {best->tpr, best->vpt, best->minb};
+  // a tile-staged pick: the plans of every model of the class now, not in
+  // the first tick that needs them
+  for (auto &p : s->models) {
+    if (p->W != W || p->real != real) continue;
+    model_plan(p.get(), best, &rc);
+    if (rc) return rc;
+  }
   *best_out = best;
   *best_ms_out = best_ms;
   return TBTKKPM_OK;
@@ -1799,7 +1877,8 @@ extern "C" int tbtkkpm_server_destroy(tbtkkpm_server *s) {
   s->cv_work.notify_all();
   s->cv_rerun.notify_all();
   if (s->worker.joinable()) s->worker.join();
-  if (s->rerun_thread.joinable()) s->rerun_thread.join();
+  for (auto &t : s->rerun_threads)
+    if (t.joinable()) t.join();
   {
     DeviceGuard g(s->device);
     cudaStreamSynchronize(s->stream);
@@ -1809,7 +1888,7 @@ extern "C" int tbtkkpm_server_destroy(tbtkkpm_server *s) {
     }
     for (auto &t : s->tables) tbtkkpm_table_destroy(t.second);
     for (DevBuf *b : {&s->d_models, &s->d_hdr, &s->d_joins, &s->d_done, &s->d_pairs, &s->d_stage,
-                      &s->d_damp, &s->d_tiles, &s->d_tdesc, &s->d_truns, &s->d_err})
+                      &s->d_damp, &s->d_tiles, &s->d_tdesc, &s->d_truns, &s->d_err, &s->d_step})
       b->release();
     s->head_ws.release();
     s->d_res.release();
@@ -1817,6 +1896,7 @@ extern "C" int tbtkkpm_server_destroy(tbtkkpm_server *s) {
     if (s->h_err) cudaFreeHost(s->h_err);
     for (cudaEvent_t &ev : s->ev)
       if (ev) cudaEventDestroy(ev);
+    if (s->tick_exec) cudaGraphExecDestroy(s->tick_exec);
     if (s->ev_fork) cudaEventDestroy(s->ev_fork);
     for (int i = 0; i < tbtkkpm_server::kClassStreams; i++) {
       if (s->ev_join[i]) cudaEventDestroy(s->ev_join[i]);

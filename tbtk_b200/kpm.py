@@ -113,6 +113,7 @@ SIGNATURES = [
     ("tbtkkpm_server_set_config", _i, [_p, _u32, _i, _i, _i]),
     ("tbtkkpm_server_step_configs", _i, [_i, _u32, _p, _i]),
     ("tbtkkpm_server_set_wait_limit", _i, [_p, _u32]),
+    ("tbtkkpm_server_set_graphs", _i, [_p, _i]),
     ("tbtkkpm_server_set_real", _i, [_p, _i]),
     ("tbtkkpm_server_set_fp64_head", _i, [_p, _u32]),
     ("tbtkkpm_server_set_table_free", _i, [_p, _i]),
@@ -122,7 +123,7 @@ SIGNATURES = [
 PENDING = 1
 STAT_NAMES = ["completed", "p50_ms", "p99_ms", "mean_ms", "reruns", "ticks", "steps",
               "lane_steps", "resident_bytes", "evictions", "waited", "busy_s", "step_s",
-              "step_bytes", "finish_s", "rerun_s", "join_s", "plan_s", "tick_s"]
+              "step_bytes", "finish_s", "rerun_s", "join_s", "plan_s", "tick_s", "graph_ticks"]
 
 
 def step_configs(precision, ldos=True):
@@ -283,6 +284,10 @@ class Matrix:
         vr, use = ctypes.c_int(), ctypes.c_int()
         _check(load_library().tbtkkpm_matrix_real(self._h, ctypes.byref(vr), ctypes.byref(use)))
         return bool(vr.value), bool(use.value)
+
+    def set_graphs(self, enable=True):
+        """Replay a captured CUDA graph per tick (default) or launch directly."""
+        _check(load_library().tbtkkpm_server_set_graphs(self._h, int(bool(enable))))
 
     def set_wait_limit(self, polls=0xFFFFFFFF):
         """Polls per staged-row wait of the tile-staged steps
@@ -587,6 +592,10 @@ class Server:
     def set_config(self, width, tpr, vpt, minb):
         _check(load_library().tbtkkpm_server_set_config(self._h, int(width), int(tpr), int(vpt),
                                                         int(minb)))
+
+    def set_graphs(self, enable=True):
+        """Replay a captured CUDA graph per tick (default) or launch directly."""
+        _check(load_library().tbtkkpm_server_set_graphs(self._h, int(bool(enable))))
 
     def set_wait_limit(self, polls=0xFFFFFFFF):
         """Polls per staged-row wait of the tile-staged steps (default: the

@@ -161,6 +161,26 @@ def test_server_tiled_steps_equal_register_steps(gpu, width):
 
 
 @pytest.mark.gpu
+def test_server_graph_replay_equals_direct_launches(gpu):
+    """Ticks that replay a captured graph of one step give the results of
+    direct launches bit for bit, and the graph path is the one taken."""
+    kpm = gpu
+    ms = models()
+    outs = []
+    for graphs in (True, False):
+        srv = kpm.Server(256, grid(), hbm_budget=1 << 30, tick_steps=6, tolerance=0)
+        srv.set_graphs(graphs)
+        ids = [srv.add_model(*c, S, 8) for _, c in ms]
+        outs.append(_mixed_traffic(kpm, srv, ids, ms, 17))
+        st = srv.stats()
+        assert (st["graph_ticks"] > 0) == graphs
+        srv.close()
+    for a, b in zip(*outs):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+
+
+@pytest.mark.gpu
 def test_server_real_lanes_equal_complex_lanes(gpu):
     """Real models on real float lanes give the complex64 lanes' results bit
     for bit (the fixed-point sums make them independent of the kernel)."""
@@ -392,6 +412,8 @@ def test_server_greens_match_fp64(gpu):
                 continue
             e = rel_err(G[k], ref[k])
             assert e <= TOL_MIXED, (ms[i][0], ty, k, e)
+            # the estimate bounds the error of Green's functions too
+            assert err[k] >= e, (ms[i][0], ty, k, e, err[k])
     srv.close()
 
 
