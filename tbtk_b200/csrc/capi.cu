@@ -14,6 +14,7 @@
 #include <atomic>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace tbtkkpm {
@@ -338,6 +339,39 @@ static int matrix_alloc(uint32_t N, uint64_t nnz, double scale, tbtkkpm_matrix *
   return TBTKKPM_OK;
 }
 
+namespace {
+
+// The smallest i in [0, n) for which bad(i) holds, else n.  The host checks
+// of a large matrix run in chunks on up to 16 threads (one per 2^20 items).
+template <typename F>
+uint64_t first_bad(uint64_t n, F bad) {
+  const uint64_t hw = std::max(1u, std::thread::hardware_concurrency());
+  const unsigned T = (unsigned)std::min<uint64_t>(std::min<uint64_t>(16, hw), std::max<uint64_t>(1, n >> 20));
+  if (T <= 1) {
+    for (uint64_t i = 0; i < n; i++)
+      if (bad(i)) return i;
+    return n;
+  }
+  std::vector<uint64_t> first(T, n);
+  std::vector<std::thread> th;
+  const uint64_t chunk = (n + T - 1) / T;
+  for (unsigned t = 0; t < T; t++)
+    th.emplace_back([&, t] {
+      const uint64_t a = t * chunk, b = std::min(n, a + chunk);
+      for (uint64_t i = a; i < b; i++)
+        if (bad(i)) {
+          first[t] = i;
+          return;
+        }
+    });
+  for (auto &x : th) x.join();
+  for (unsigned t = 0; t < T; t++)
+    if (first[t] < n) return first[t];
+  return n;
+}
+
+}  // namespace
+
 extern "C" int tbtkkpm_matrix_create_csr(const uint32_t *rowptr, const uint32_t *col,
                                          const double *val, uint32_t N, double scale,
                                          tbtkkpm_matrix **out) {
@@ -348,23 +382,39 @@ extern "C" int tbtkkpm_matrix_create_csr(const uint32_t *rowptr, const uint32_t 
     return fail(TBTKKPM_ERR_ARGUMENT,
                 "matrix_create_csr: the scaleFactor=%g has to be larger than 0", scale);
   if (rowptr[0] != 0) return fail(TBTKKPM_ERR_ARGUMENT, "matrix_create_csr: rowptr[0] != 0");
-  for (uint32_t r = 0; r < N; r++)
-    if (rowptr[r + 1] < rowptr[r])
-      return fail(TBTKKPM_ERR_ARGUMENT, "matrix_create_csr: rowptr decreases at row %u", r);
+  const uint64_t dec = first_bad(N, [&](uint64_t r) { return rowptr[r + 1] < rowptr[r]; });
+  if (dec < N)
+    return fail(TBTKKPM_ERR_ARGUMENT, "matrix_create_csr: rowptr decreases at row %u", (uint32_t)dec);
   const uint64_t nnz = rowptr[N];
   if (nnz && (!col || !val)) return fail(TBTKKPM_ERR_ARGUMENT, "matrix_create_csr: NULL arrays");
-  for (uint32_t r = 0; r < N; r++)
+  // the first row with a column outside the basis, columns out of order or
+  // a value that is not finite, then its message
+  auto entry_bad = [&](uint32_t r, uint32_t k) -> int {
+    if (col[k] >= N) return 1;
+    if (k > rowptr[r] && col[k] <= col[k - 1]) return 2;
+    if (!std::isfinite(val[2 * (uint64_t)k]) || !std::isfinite(val[2 * (uint64_t)k + 1])) return 3;
+    return 0;
+  };
+  const uint64_t badrow = first_bad(N, [&](uint64_t r) {
+    for (uint32_t k = rowptr[r]; k < rowptr[r + 1]; k++)
+      if (entry_bad((uint32_t)r, k)) return true;
+    return false;
+  });
+  if (badrow < N) {
+    const uint32_t r = (uint32_t)badrow;
     for (uint32_t k = rowptr[r]; k < rowptr[r + 1]; k++) {
-      if (col[k] >= N)
+      const int why = entry_bad(r, k);
+      if (why == 1)
         return fail(TBTKKPM_ERR_ARGUMENT, "matrix_create_csr: column %u of row %u >= N=%u",
                     col[k], r, N);
-      if (k > rowptr[r] && col[k] <= col[k - 1])
+      if (why == 2)
         return fail(TBTKKPM_ERR_ARGUMENT,
                     "matrix_create_csr: columns of row %u not strictly ascending", r);
-      if (!std::isfinite(val[2 * (uint64_t)k]) || !std::isfinite(val[2 * (uint64_t)k + 1]))
+      if (why == 3)
         return fail(TBTKKPM_ERR_ARGUMENT,
                     "matrix_create_csr: value of row %u, column %u is not finite", r, col[k]);
     }
+  }
   tbtkkpm_matrix *m = nullptr;
   int rc = matrix_alloc(N, nnz, scale, &m);
   if (rc) return rc;
@@ -408,14 +458,17 @@ extern "C" int tbtkkpm_matrix_create_triplets(const uint32_t *rows, const uint32
                 "matrix_create_triplets: the scaleFactor=%g has to be larger than 0", scale);
   if (n && (!rows || !cols || !vals))
     return fail(TBTKKPM_ERR_ARGUMENT, "matrix_create_triplets: NULL arrays");
-  for (uint64_t i = 0; i < n; i++) {
+  const uint64_t i = first_bad(n, [&](uint64_t k) {
+    return rows[k] >= N || cols[k] >= N || !std::isfinite(vals[2 * k]) ||
+           !std::isfinite(vals[2 * k + 1]);
+  });
+  if (i < n) {
     if (rows[i] >= N || cols[i] >= N)
       return fail(TBTKKPM_ERR_ARGUMENT,
                   "matrix_create_triplets: entry %llu (%u, %u) outside the %u x %u basis",
                   (unsigned long long)i, rows[i], cols[i], N, N);
-    if (!std::isfinite(vals[2 * i]) || !std::isfinite(vals[2 * i + 1]))
-      return fail(TBTKKPM_ERR_ARGUMENT, "matrix_create_triplets: value of entry %llu is not finite",
-                  (unsigned long long)i);
+    return fail(TBTKKPM_ERR_ARGUMENT, "matrix_create_triplets: value of entry %llu is not finite",
+                (unsigned long long)i);
   }
   int ndev = 0;
   tbtkkpm_device_count(&ndev);
