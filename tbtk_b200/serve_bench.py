@@ -131,11 +131,11 @@ def serve(a):
     t0 = time.perf_counter()
     for kind, L, J, W, alpha, seed in pool:
         csr = workloads.build_model(kind, L, J, W, seed, alpha=alpha)
-        srv.add_model(*csr, S, 16)
+        srv.add_model(*csr, S, a.width)
         sizes.append(csr[0].size - 1)
         csrs.append(csr)
     setup_s = time.perf_counter() - t0
-    tuned = srv.autotune(16, probe_steps=6)
+    tuned = srv.autotune(a.width, probe_steps=6)
     reqs = workloads.cfg5_requests(sizes, a.rate, a.duration, seed=55)
     ids = [None] * len(reqs)
     start = time.perf_counter()
@@ -162,7 +162,7 @@ def serve(a):
     srv.close()
     return {
         "workload": f"serving: {a.models} models (N log-uniform 1e3-4e6, square/honeycomb/"
-                    f"Rashba, 16 lanes), Poisson {a.rate}/s for {a.duration}s, 1-16 sites, "
+                    f"Rashba, {a.width} lanes), Poisson {a.rate}/s for {a.duration}s, 1-16 sites, "
                     f"M in [512,4096], s=12, E=1000",
         "metric": "LDOS solves/s", "value": solves / wall, "unit": "LDOS solves/s",
         "requests": len(reqs), "requests_per_s": len(reqs) / wall, "wall_s": wall,
@@ -187,6 +187,8 @@ def main():
     ap.add_argument("--samples", type=int, default=16)
     ap.add_argument("--sample-seed", type=int, default=44,
                     help="seed of the sampled solves checked against the FP64 path")
+    ap.add_argument("--width", type=int, default=16,
+                    help="lanes of every pool model (serve)")
     ap.add_argument("--fp64-head", type=int, default=32,
                     help="FP64 head steps of every lane (0: none)")
     a = ap.parse_args()
