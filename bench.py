@@ -322,7 +322,10 @@ def reference_arm(args, world, rank):
     return {
         "impl": "reference", "metric": "LDOS solves/s", "value": value, "unit": "LDOS solves/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": t_site * 1e3 / threads, "higher_is_better": True, "scaling": "weak",
+        # the timed steps are the M=68 samples; the metric extrapolates them
+        "ms_per_step": statistics.mean(hi_t) * 1e3,
+        "extrapolated_ms_per_solve": t_site * 1e3 / threads,
+        "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "complex128", "data": "synthetic (seeded lattice)",
         "config": {"workload": f"square {args.lattice}x{args.lattice} spin periodic, W=2, s=12, "
                                f"M={args.moments}, E=2000, LDOS per site",
