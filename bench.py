@@ -242,16 +242,24 @@ def cpu_port_baseline(p, threads, sample_steps=(4, 36)):
             t.join()
         return time.perf_counter() - t0
 
+    def fit(lo, hi):
+        slope = (hi - lo) / (sample_steps[1] - sample_steps[0])
+        if slope > 0:
+            return slope, max(lo - slope * sample_steps[0], 0.0), "linear"
+        return hi / sample_steps[1], 0.0, "degenerate (upper bound)"
+
     t_lo = run(sample_steps[0])
     t_hi = run(sample_steps[1])
-    slope = (t_hi - t_lo) / (sample_steps[1] - sample_steps[0])
-    if slope > 0:
-        per_step, fixed, fit = slope, max(t_lo - slope * sample_steps[0], 0.0), "linear"
-    else:
-        per_step, fixed, fit = t_hi / sample_steps[1], 0.0, "degenerate (upper bound)"
+    per_step, fixed, fit_kind = fit(t_lo, t_hi)
     t_site = fixed + per_step * p.M
+    # one site alone on one core, the same fit
+    all_sites, sites = sites, sites[:1]
+    s1, f1, _ = fit(run(sample_steps[0]), run(sample_steps[1]))
+    sites = all_sites
+    t_one = f1 + s1 * p.M
     return {"value": len(sites) / t_site, "unit": "LDOS solves/s", "cores": len(sites),
-            "kind": "port", "fit": fit,
+            "kind": "port", "fit": fit_kind,
+            "one_core": {"value": 1.0 / t_one, "unit": "LDOS solves/s", "s_per_solve": t_one},
             "sample": (f"{len(sites)} sites in parallel (one thread each) at M="
                        f"{sample_steps[0]} and M={sample_steps[1]} of the same matrix; "
                        f"per-site time {fixed:.2f} s + {per_step:.3f} s/step extrapolated to "

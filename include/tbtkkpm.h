@@ -214,6 +214,24 @@ TBTKKPM_API int tbtkkpm_table_create_clenshaw(
 	uint32_t M, const double *energies, uint32_t E, double scale,
 	tbtkkpm_table **out);
 
+/* A table handle on the grid of Chebyshev nodes: E energies (E a power of
+ * two, 1 <= E <= 4096) E_e = -s cos(pi (2e + 1) / (2E)), ascending, are
+ * written to energies_out[E].  The energy sums of every call that takes
+ * the handle run one FFT of length 2E per coefficient vector (O(E log E)
+ * arithmetic per vector instead of the table's O(M E) multiply-adds and
+ * 16 M E table bytes; 32 E bytes of device memory).  M is the most
+ * coefficients a call may pass; any M works (terms beyond 2E fold onto the
+ * transform).  Results equal the table sums on the same energies up to
+ * rounding (~1e-13 relative).  The grid is not uniform: the properties
+ * that integrate over energy with a spacing dE (density, magnetization,
+ * expectation values) assume a uniform grid and are not meant for it.
+ * (The discrete-cosine-transform energy-sum variant; no reference
+ * counterpart: the reference sums over a uniform Range,
+ * Lib/src/Solver/ChebyshevExpander.cpp:201-270,277-435.) */
+TBTKKPM_API int tbtkkpm_table_create_chebyshev(
+	uint32_t M, uint32_t E, double scale, double *energies_out,
+	tbtkkpm_table **out);
+
 TBTKKPM_API int tbtkkpm_table_destroy(tbtkkpm_table *t);
 
 /* Green's functions G[k][e] of one type from K damped coefficient vectors
@@ -413,7 +431,10 @@ TBTKKPM_API int tbtkkpm_server_create(
 	tbtkkpm_server **out);
 
 /* Registers a model from its CSR (as tbtkkpm_matrix_create_csr) with
- * `width` lanes (1, 2, 4, ..., 64).  The model id is returned in *model. */
+ * `width` lanes (1, 2, 4, ..., 64): a request of the model takes up to
+ * `width` of them, and the lane memory (two [N][width] vector buffers, moment
+ * rows) counts `width` lanes against the HBM budget.  The model id is
+ * returned in *model. */
 TBTKKPM_API int tbtkkpm_server_add_model(
 	tbtkkpm_server *s, const uint32_t *rowptr, const uint32_t *col,
 	const double *val, uint32_t N, double scale, uint32_t width,
@@ -486,17 +507,20 @@ TBTKKPM_API int tbtkkpm_server_cancel(tbtkkpm_server *s, uint64_t request);
 #define TBTKKPM_STAT_PLAN_S 17    /* worker time admitting requests and planning ticks */
 #define TBTKKPM_STAT_TICK_S 18    /* worker time launching ticks and waiting for them */
 #define TBTKKPM_STAT_GRAPH_TICKS 19 /* ticks whose steps replayed a captured CUDA graph */
-#define TBTKKPM_STAT_COUNT 20
+#define TBTKKPM_STAT_RELAYOUTS 20 /* step-width changes of models with lanes in flight */
+#define TBTKKPM_STAT_COUNT 21
 TBTKKPM_API int tbtkkpm_server_stats(tbtkkpm_server *s, double *out, uint32_t n);
 
 /* Times every compiled step configuration of lane width `width` for
  * probe_steps steps, for each lane class (real float lanes, complex64
  * lanes) with a model of that width, on the largest model of the class
  * (the server must be idle), and keeps the fastest per class; the outputs
- * describe the class of the largest model.  For a tile-staged pick it also
- * builds the gather plans of every model of the class, so the first tick
- * does not.  set_config installs a known one.  Results do not depend on the
- * configuration. */
+ * describe the class of the largest model.  With adaptive widths
+ * (tbtkkpm_server_set_adaptive_width) the narrower widths down to 4 that
+ * these models step at are tuned the same way.  For a tile-staged pick it
+ * also builds the gather plans of every model of the class, so the first
+ * tick does not.  set_config installs a known one.  Results do not depend
+ * on the configuration. */
 TBTKKPM_API int tbtkkpm_server_autotune(
 	tbtkkpm_server *s, uint32_t width, uint32_t probe_steps, int *tpr,
 	int *vpt, int *minb, double *ms_per_step);
@@ -535,6 +559,16 @@ TBTKKPM_API int tbtkkpm_server_set_table_free(tbtkkpm_server *s, int enable);
  * step directly.  A capture that fails turns graphs off for the server.
  * Results do not depend on it.  (No reference counterpart.) */
 TBTKKPM_API int tbtkkpm_server_set_graphs(tbtkkpm_server *s, int enable);
+
+/* enable = 1 (the default): a model steps at the narrowest width (a power
+ * of two, at least 4 or its lane count) that covers its highest busy lane,
+ * so a step moves the vectors of those lanes only, not of all `width`
+ * lanes; a request takes the lowest free lanes, and at a step boundary
+ * where the width changes the model's two vector buffers are restrided in
+ * place (TBTKKPM_STAT_RELAYOUTS counts these).  enable = 0: every model
+ * steps at its full lane count.  Results do not depend on it.  (No
+ * reference counterpart.) */
+TBTKKPM_API int tbtkkpm_server_set_adaptive_width(tbtkkpm_server *s, int enable);
 
 /* Bound of each wait of the server's tile-staged steps for rows staged in
  * shared memory (polls; TBTKKPM_WAIT_DEFAULT: the library's bound), as

@@ -14,7 +14,9 @@ source).  --sweep times every compiled step configuration for the batch;
 --autotune lets the library's autotuner choose first; --config T,V,MB forces
 one; --batch-width splits the sites into batches of that many.  Without
 --rashba the model is real and the mixed precisions run on real float
-vectors; --complex-vectors keeps complex64 ones.
+vectors; --complex-vectors keeps complex64 ones.  --grid picks the energy sums
+(lookup table, Clenshaw recurrences, or FFTs on the Chebyshev-node grid); the
+printed energy time is theirs.
 
     python profile_case.py --lattice 1024 --server 16 --moments 256 --config 4,4,164082
 
@@ -60,6 +62,9 @@ def main():
     ap.add_argument("--fp64-head", type=int, default=0,
                     help="FP64 head steps of doubling runs (default 0: every step of a "
                          "doubling run is a timed FP32 step, as without a head)")
+    ap.add_argument("--grid", choices=["table", "clenshaw", "chebyshev"], default="table",
+                    help="energy sums: lookup table or Clenshaw recurrences on the open "
+                         "grid, or FFTs on the Chebyshev-node grid (--energies a power of two)")
     ap.add_argument("--server", type=int, default=0,
                     help="run the lattice as one server model with this many lanes")
     a = ap.parse_args()
@@ -71,7 +76,12 @@ def main():
     N, nnz = rowptr.size - 1, int(rowptr[-1])
     sites = workloads.sample_sites(a.lattice * a.lattice, 2, a.sites, 1 + a.lattice)
     mat = kpm.Matrix.from_csr(rowptr, col, val, 12.0)
-    tab = kpm.Table.create(a.moments, workloads.open_grid(12.0, a.energies), 12.0)
+    if a.grid == "chebyshev":
+        tab = kpm.Table.create_chebyshev(a.moments, a.energies, 12.0)
+    elif a.grid == "clenshaw":
+        tab = kpm.Table.create_clenshaw(a.moments, workloads.open_grid(12.0, a.energies), 12.0)
+    else:
+        tab = kpm.Table.create(a.moments, workloads.open_grid(12.0, a.energies), 12.0)
     mat.set_profiling(True)
     mat.set_fp64_head(a.fp64_head)
     if a.complex_vectors:

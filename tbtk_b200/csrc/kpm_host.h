@@ -166,12 +166,17 @@ struct tbtkkpm_table {
   // table-free handle (tbtkkpm_table_create_clenshaw): energies and scale
   // only, the energy sums run Clenshaw recurrences (kpm_clenshaw)
   bool clenshaw = false;
+  // Chebyshev-node grid handle (tbtkkpm_table_create_chebyshev): the
+  // energy sums run one FFT per vector (kpm_chebyshev_grid) over `twiddle`,
+  // [2E] complex e^{i pi m / (2E)}
+  bool chebyshev_grid = false;
   double scale = 0;
   // largest weight of the energy sum on this grid, max_e |T[1][e]| / pi =
   // max_e 2 / (pi s sqrt(1 - (E_e/s)^2)): the scale that turns a moment
   // error into an LDOS error (ldos_error_estimate)
   double wmax = 0;
   tbtkkpm::DevBuf energies;  // [E]
+  tbtkkpm::DevBuf twiddle;   // [2E] complex128 (Chebyshev-node grid)
   tbtkkpm::DevBuf table;   // [M][E] complex128
   tbtkkpm::DevBuf mu, out; // staging for energy sums
   std::mutex lock;

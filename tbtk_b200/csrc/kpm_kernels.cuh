@@ -881,4 +881,83 @@ kpm_clenshaw(uint32_t M, uint32_t E, uint32_t K, const double *__restrict__ ener
   }
 }
 
+// ---------------------------------------------------------------- Chebyshev-node grid sums
+// The sums of kpm_clenshaw on the grid of Chebyshev nodes x_k = cos(theta_k),
+// theta_k = pi (2k + 1) / L, L = 2E (E a power of two), by one FFT per
+// coefficient vector: O(L log L) arithmetic instead of O(M E).  With
+// a_n = c_n / (1 + delta_n0),
+//   F(k) = sum_n a_n e^{i n theta_k} = sum_{j<L} b_j e^{2 pi i j k / L},
+//   b_j  = e^{i pi j / L} sum_{p} (-1)^p a_{j + p L}
+// (e^{i pi (n + L) / L} = -e^{i pi n / L} folds M > L terms onto L), so one
+// length-L DFT with a + exponent gives F(k) = sum a_n e^{+i n theta_k} at
+// k < E and sum a_n e^{-i n theta_k} at L - 1 - k (theta_{L-1-k} = 2 pi -
+// theta_k).  C = (F+ + F-)/2, S = (F+ - F-)/(2i), and the types combine as
+// in kpm_clenshaw with A = 2/(s q) on both C and S.  Output energy e is node
+// k = E - 1 - e, so the grid ascends: E_e = -s cos(pi (2e + 1) / L).
+// tw[m] = e^{i pi m / L}, m < L (host libm).  One block per vector; the
+// radix-2 decimation-in-time FFT runs in place in L complex doubles of
+// dynamic shared memory (bit-reversed load, log2 L stages).
+constexpr int kDctBlock = 512;
+constexpr uint32_t kDctMaxE = 4096;  // L * 16 bytes = 128 KB of shared memory
+
+static __global__ void __launch_bounds__(kDctBlock)
+kpm_chebyshev_grid(uint32_t M, uint32_t E, uint32_t log2L, const double2 *__restrict__ tw,
+                   double scale, const double2 *__restrict__ mu, int type, void *__restrict__ out) {
+  extern __shared__ double2 fz[];
+  const uint32_t L = 2 * E, vec = blockIdx.x;
+  const double2 *c = mu + (uint64_t)vec * M;
+  for (uint32_t j = threadIdx.x; j < L; j += kDctBlock) {
+    double2 b = make_double2(0.0, 0.0);
+    bool neg = false;
+    for (uint32_t n = j; n < M; n += L, neg = !neg) {
+      double2 a = __ldg(c + n);
+      if (n == 0) a = make_double2(0.5 * a.x, 0.5 * a.y);
+      b = neg ? make_double2(b.x - a.x, b.y - a.y) : make_double2(b.x + a.x, b.y + a.y);
+    }
+    const double2 w = __ldg(tw + j);
+    const uint32_t r = log2L ? __brev(j) >> (32 - log2L) : 0;
+    fz[r] = make_double2(b.x * w.x - b.y * w.y, b.x * w.y + b.y * w.x);
+  }
+  __syncthreads();
+  for (uint32_t lh = 0; lh < log2L; lh++) {
+    const uint32_t h = 1u << lh;
+    for (uint32_t i = threadIdx.x; i < L / 2; i += kDctBlock) {
+      const uint32_t r = i & (h - 1), i0 = ((i >> lh) << (lh + 1)) + r, i1 = i0 + h;
+      const double2 w = __ldg(tw + (r << (log2L - lh)));  // e^{i pi r / h}
+      const double2 u = fz[i0], v0 = fz[i1];
+      const double2 v = make_double2(v0.x * w.x - v0.y * w.y, v0.x * w.y + v0.y * w.x);
+      fz[i0] = make_double2(u.x + v.x, u.y + v.y);
+      fz[i1] = make_double2(u.x - v.x, u.y - v.y);
+    }
+    __syncthreads();
+  }
+  for (uint32_t k = threadIdx.x; k < E; k += kDctBlock) {
+    const double2 fp = fz[k], fm = fz[L - 1 - k];
+    const double2 C = make_double2(0.5 * (fp.x + fm.x), 0.5 * (fp.y + fm.y));
+    const double2 S = make_double2(0.5 * (fp.y - fm.y), -0.5 * (fp.x - fm.x));
+    const double q = __ldg(&tw[2 * k + 1].y);  // sin(theta_k) > 0
+    const double A = 2.0 / (scale * q);
+    const uint64_t o = (uint64_t)vec * E + (E - 1 - k);
+    if (type == 4) {
+      static_cast<double *>(out)[o] = A * C.x / 3.14159265358979323846;
+      continue;
+    }
+    double2 g;
+    switch (type) {
+      case 0:  // Advanced: -A (S - iC)
+        g = make_double2(-A * (S.x + C.y), -A * (S.y - C.x));
+        break;
+      case 1:  // Retarded: -A (S + iC)
+        g = make_double2(-A * (S.x - C.y), -A * (S.y + C.x));
+        break;
+      case 2:  // Principal: A S
+        g = make_double2(A * S.x, A * S.y);
+        break;
+      default:  // NonPrincipal: A iC
+        g = make_double2(-A * C.y, A * C.x);
+    }
+    static_cast<double2 *>(out)[o] = g;
+  }
+}
+
 }  // namespace tbtkkpm

@@ -22,6 +22,9 @@
 #pragma once
 
 #include "kpm_kernels.cuh"
+#include <algorithm>
+#include <utility>
+#include <vector>
 
 namespace tbtkkpm {
 
@@ -108,6 +111,53 @@ __device__ __forceinline__ int32_t multi_step_index(const MultiHeader *__restric
 // Ends one replay of a tick's step graph: the next replay is the next step.
 static __global__ void kpm_multi_advance(int32_t *step) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *step += 1;
+}
+
+// Changes the row stride of a lane buffer [N][W] -> [N][W2] in place for
+// rows [r0, r1): lane c < min(W, W2) of row r moves from r W + c to
+// r W2 + c, lanes [W, W2) of a widened row are zero.  A launch may only
+// cover rows whose source and destination ranges do not overlap those of
+// rows still to move (lane_relayout_ranges), so its threads need no order.
+template <typename T>
+static __global__ void kpm_lane_relayout(T *__restrict__ v, uint32_t r0, uint32_t r1, uint32_t W,
+                                         uint32_t W2) {
+  const uint64_t n = (uint64_t)(r1 - r0) * W2;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint64_t r = r0 + i / W2;
+    const uint32_t c = (uint32_t)(i % W2);
+    T x{};
+    if (c < W) x = v[r * W + c];
+    v[r * W2 + c] = x;
+  }
+}
+
+// The launches of an in-place restride [N][W] -> [N][W2] (powers of two),
+// as row ranges in launch order.  Widening (W2 = W 2^k) moves rows from the
+// end: rows [a, b) with a 2^k >= b read [a W, b W) and write [a W2, b W2),
+// which lie above every row not yet moved; row 0 goes last (its lanes
+// c < W stay in place).  Narrowing (W = W2 2^k) moves rows from the start:
+// rows [a, b) with b <= a 2^k write below their own sources and above the
+// rows already moved; row 0 stays.
+inline void lane_relayout_ranges(uint32_t N, uint32_t W, uint32_t W2,
+                                 std::vector<std::pair<uint32_t, uint32_t>> &out) {
+  out.clear();
+  if (W == W2 || N == 0) return;
+  if (W2 > W) {
+    const uint32_t f = W2 / W;
+    for (uint32_t b = N; b > 0;) {
+      const uint32_t a = b == 1 ? 0 : (uint32_t)(((uint64_t)b + f - 1) / f);
+      out.push_back({a, b});
+      b = a;
+    }
+  } else {
+    const uint64_t f = W / W2;
+    for (uint32_t a = 1; a < N;) {
+      const uint32_t b = (uint32_t)std::min<uint64_t>(N, (uint64_t)a * f);
+      out.push_back({a, b});
+      a = b;
+    }
+  }
 }
 
 // A block takes runs of kRun consecutive tiles (run r, r + gridDim.x, ...),

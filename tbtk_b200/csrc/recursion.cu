@@ -727,6 +727,51 @@ extern "C" int tbtkkpm_table_create_clenshaw(uint32_t M, const double *energies,
   return TBTKKPM_OK;
 }
 
+extern "C" int tbtkkpm_table_create_chebyshev(uint32_t M, uint32_t E, double scale,
+                                              double *energies_out, tbtkkpm_table **out) {
+  if (!out) return fail(TBTKKPM_ERR_ARGUMENT, "table_create_chebyshev: out is NULL");
+  *out = nullptr;
+  if (M == 0)
+    return fail(TBTKKPM_ERR_ARGUMENT, "table_create_chebyshev: numCoefficients has to be larger than 0");
+  if (E == 0 || (E & (E - 1)) || E > kDctMaxE)
+    return fail(TBTKKPM_ERR_ARGUMENT,
+                "table_create_chebyshev: the number of energies (%u) has to be a power of two in "
+                "[1, %u]",
+                E, kDctMaxE);
+  if (!(scale > 0)) return fail(TBTKKPM_ERR_ARGUMENT, "table_create_chebyshev: scaleFactor must be > 0");
+  if (!energies_out) return fail(TBTKKPM_ERR_ARGUMENT, "table_create_chebyshev: energies_out is NULL");
+  const uint32_t L = 2 * E;
+  std::vector<double2> tw(L);
+  for (uint32_t m = 0; m < L; m++) {
+    const double a = M_PI * (double)m / (double)L;
+    tw[m] = make_double2(std::cos(a), std::sin(a));
+  }
+  // node k = E - 1 - e at x_k = cos(pi (2k + 1) / L): ascending energies
+  std::vector<double> en(E);
+  for (uint32_t e = 0; e < E; e++) en[e] = scale * tw[2 * (E - 1 - e) + 1].x;
+  tbtkkpm_table *t = nullptr;
+  int rc = table_alloc(M, E, &t, false);
+  if (rc) return rc;
+  DeviceGuard g(t->device);
+  t->chebyshev_grid = true;
+  t->scale = scale;
+  t->wmax = grid_weight_max(en.data(), E, scale);
+  if ((rc = t->twiddle.reserve(sizeof(double2) * (size_t)L))) {
+    tbtkkpm_table_destroy(t);
+    return rc;
+  }
+  cudaError_t e = cudaMemcpyAsync(t->twiddle.ptr, tw.data(), sizeof(double2) * (size_t)L,
+                                  cudaMemcpyHostToDevice, t->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(t->stream);
+  if (e != cudaSuccess) {
+    tbtkkpm_table_destroy(t);
+    return cuda_fail(e, "table_create_chebyshev");
+  }
+  std::copy(en.begin(), en.end(), energies_out);
+  *out = t;
+  return TBTKKPM_OK;
+}
+
 extern "C" int tbtkkpm_table_upload(uint32_t M, uint32_t E, const double *table,
                                     tbtkkpm_table **out) {
   if (!out) return fail(TBTKKPM_ERR_ARGUMENT, "table_upload: out is NULL");
@@ -759,6 +804,7 @@ extern "C" int tbtkkpm_table_destroy(tbtkkpm_table *t) {
     if (t->stream) cudaStreamSynchronize(t->stream);
     t->table.release();
     t->energies.release();
+    t->twiddle.release();
     t->mu.release();
     t->out.release();
     if (t->stream) cudaStreamDestroy(t->stream);
@@ -775,6 +821,22 @@ namespace tbtkkpm {
 int launch_energy_sum(cudaStream_t st, const tbtkkpm_table *t, const double2 *mu, uint32_t K,
                       int type, void *out, uint32_t terms) {
   const uint32_t M = terms ? terms : t->M, E = t->E;
+  if (K == 0) return TBTKKPM_OK;
+  if (t->chebyshev_grid) {
+    uint32_t log2L = 0;
+    while ((1u << log2L) < 2 * E) log2L++;
+    const int smem = (int)(sizeof(double2) * 2 * E);
+    cudaError_t e = cudaSuccess;
+    if (smem > 48 * 1024)
+      e = cudaFuncSetAttribute(kpm_chebyshev_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return cuda_fail(e, "energy sum: shared memory");
+    kpm_chebyshev_grid<<<K, kDctBlock, smem, st>>>(M, E, log2L, t->twiddle.as<double2>(), t->scale,
+                                                    mu, type, out);
+    count_launches(1);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "energy sum: launch");
+    return TBTKKPM_OK;
+  }
   const int KT = K == 1 ? 1 : (K <= 4 ? 4 : 8);
   dim3 grid((E + kEnergyBlock - 1) / kEnergyBlock, (K + KT - 1) / KT);
   if (t->clenshaw) {

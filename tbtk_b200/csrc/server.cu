@@ -34,6 +34,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <string>
 #include <thread>
 #include <vector>
@@ -50,6 +51,10 @@ constexpr uint32_t kMaxWidth = 64;
 bool valid_width(uint32_t w) { return w >= 1 && w <= kMaxWidth && (w & (w - 1)) == 0; }
 
 constexpr int kLdos = -1;  // Request::kind of an LDOS request
+
+// Narrowest width a model steps at when its width follows demand: below it
+// the matrix bytes of a step dominate and a narrower row saves little.
+constexpr uint32_t kMinStepWidth = 4;
 
 struct Request {
   uint64_t id = 0;
@@ -90,7 +95,10 @@ struct Model {
   uint32_t id = 0;
   tbtkkpm_matrix *mat = nullptr;
   tbtkkpm_table *table = nullptr;  // the server's table of this scale
-  uint32_t N = 0, W = 0;
+  // Wmax lanes are allocated; the steps run at width W, the smallest power
+  // of two (at least kMinStepWidth) that covers every busy lane, or Wmax
+  // when the width does not follow demand (tbtkkpm_server_set_adaptive_width)
+  uint32_t N = 0, W = 0, Wmax = 0;
   double scale = 1;
   bool real = false;  // real Hamiltonian: lanes hold real float vectors
   uint32_t head_steps = 0;  // FP64 head of a lane (0: none)
@@ -171,12 +179,12 @@ const MultiEntry *find_multi(int tpr, int vpt, int minb, bool real) {
 }
 
 // Gather plan of a model for a tile-staged entry (built on first use on the
-// model's matrix handle); null when the entry is register-staged, the rows
-// of this width are too narrow for bulk copies, or the matrix has a tile the
-// plan builder cannot take.
-const TilePlan *model_plan(Model *m, const MultiEntry *e, int *rc) {
+// model's matrix handle); null when the entry is register-staged, rows of W
+// lanes are too narrow for bulk copies, or the matrix has a tile the plan
+// builder cannot take.
+const TilePlan *model_plan(Model *m, uint32_t W, const MultiEntry *e, int *rc) {
   *rc = TBTKKPM_OK;
-  if (!is_multi_tiled(e->minb) || (m->W * m->esize()) % 16 != 0) return nullptr;
+  if (!is_multi_tiled(e->minb) || (W * m->esize()) % 16 != 0) return nullptr;
   const int R = multi_tiled_rows(e->minb), key = 2 * R + (m->real ? 0 : 1);
   auto it = m->plans.find(key);
   if (it != m->plans.end()) return it->second;
@@ -250,10 +258,12 @@ struct tbtkkpm_server {
   std::deque<std::unique_ptr<Model>> models;
   std::map<double, tbtkkpm_table *> tables;                         // Mmax rows per scale
   std::map<uint32_t, std::array<int, 3>> config;  // width | real << 16 -> tpr, vpt, minb
+  std::set<uint32_t> tuned;                       // keys of config the autotuner measured
   bool use_real = true;                           // real lanes for real models added later
   uint32_t head_steps = kPrefixSteps;             // FP64 head of models added later
   bool table_free = false;                        // Clenshaw energy sums for scales added later
   uint32_t wait_limit = kWaitLimit;               // polls per staged-row wait (set_wait_limit)
+  bool adaptive_width = true;                     // step widths follow demand (set_adaptive_width)
   Workspace head_ws;                              // FP64 head scratch (worker thread)
   std::deque<uint64_t> pending;
   std::map<uint64_t, std::unique_ptr<Request>> requests;
@@ -283,7 +293,7 @@ struct tbtkkpm_server {
   std::vector<double> latencies_ms;
   double reruns = 0, ticks = 0, steps = 0, lane_steps = 0, evictions = 0, waited = 0, busy_s = 0;
   double step_s = 0, step_bytes = 0, finish_s = 0, rerun_s = 0, join_s = 0, plan_s = 0, tick_s = 0;
-  double graph_ticks = 0;
+  double graph_ticks = 0, relayouts = 0;
   DevBuf d_res;                 // finish results of a tick: [ldos K*E | err K] per request
   double *h_res = nullptr;      // pinned host copy of d_res
   size_t h_res_cap = 0;
@@ -314,7 +324,7 @@ namespace {
 // ------------------------------------------------------------ admission
 
 int make_resident(tbtkkpm_server *s, Model *m) {
-  const uint32_t W = m->W, N = m->N;
+  const uint32_t W = m->Wmax, N = m->N;
   const size_t words = (N + 31) / 32;
   int rc;
   const size_t es = m->esize();
@@ -361,6 +371,7 @@ int make_resident(tbtkkpm_server *s, Model *m) {
   m->bitmap_h.assign(words, 0);
   m->busy = 0;
   m->pairs_busy = 0;
+  m->W = m->Wmax;
   m->dirty = true;
   m->resident = true;
   s->resident += m->bytes;
@@ -397,16 +408,41 @@ struct JoinRef {
   Request *r;
 };
 
-// Under s->mu.  Queued requests take free lanes in arrival order; the joins
-// of this step boundary are appended (the lane bases assume no FP64 head
-// until run_joins has reported the heads).
-int admit(tbtkkpm_server *s, std::vector<MultiJoin> &joins, std::vector<JoinRef> &refs) {
+// A change of a model's step width at a step boundary: its two lane
+// buffers are restrided in place (run_relayouts) before the joins run.
+struct Relayout {
+  Model *m;
+  uint32_t from, to;
+};
+
+// The width model m steps at: the smallest power of two, at least
+// kMinStepWidth, that covers its highest busy lane (Wmax when the width does
+// not follow demand).
+uint32_t step_width(const tbtkkpm_server *s, const Model *m) {
+  if (!s->adaptive_width) return m->Wmax;
+  uint32_t hi = 0;
+  for (uint32_t c = 0; c < m->Wmax; c++)
+    if (m->lane_req[c]) hi = c + 1;
+  uint32_t w = std::min(kMinStepWidth, m->Wmax);
+  while (w < hi) w *= 2;
+  return w;
+}
+
+// Under s->mu.  Queued requests take free lanes in arrival order (the
+// lowest free lanes of their model); the joins of this step boundary are
+// appended (the lane bases assume no FP64 head until run_joins has reported
+// the heads).  Then every resident model takes its step width: `moves` gets
+// the restrides of models whose lanes already held state.
+int admit(tbtkkpm_server *s, std::vector<MultiJoin> &joins, std::vector<JoinRef> &refs,
+          std::vector<Relayout> &moves) {
+  std::vector<uint32_t> busy0(s->models.size());
+  for (size_t i = 0; i < s->models.size(); i++) busy0[i] = s->models[i]->busy;
   for (auto it = s->pending.begin(); it != s->pending.end();) {
     Request *r = s->requests.at(*it).get();
     Model *m = s->models[r->model].get();
     const uint32_t K = (uint32_t)r->sites.size();
     const uint32_t npairs = r->direct ? (uint32_t)r->to.size() : 0u;
-    if (m->resident && (m->W - m->busy < K || m->W - m->pairs_busy < npairs)) {
+    if (m->resident && (m->Wmax - m->busy < K || m->Wmax - m->pairs_busy < npairs)) {
       ++it;
       continue;
     }
@@ -425,7 +461,7 @@ int admit(tbtkkpm_server *s, std::vector<MultiJoin> &joins, std::vector<JoinRef>
       if (rc) return rc;
     }
     r->base = s->n_global - 1;
-    for (uint32_t c = 0, k = 0; c < m->W && k < K; c++) {
+    for (uint32_t c = 0, k = 0; c < m->Wmax && k < K; c++) {
       if (m->lane_req[c]) continue;
       const uint32_t site = r->sites[k++];
       m->lane_req[c] = r->id;
@@ -464,6 +500,43 @@ int admit(tbtkkpm_server *s, std::vector<MultiJoin> &joins, std::vector<JoinRef>
     m->dirty = true;
     it = s->pending.erase(it);
   }
+  for (size_t i = 0; i < s->models.size(); i++) {
+    Model *m = s->models[i].get();
+    if (!m->resident || !m->busy) continue;
+    const uint32_t w = step_width(s, m);
+    if (w == m->W) continue;
+    if (busy0[i]) moves.push_back({m, m->W, w});
+    m->W = w;
+    m->dirty = true;
+  }
+  for (size_t i = 0; i < joins.size(); i++) joins[i].W = refs[i].m->W;
+  return TBTKKPM_OK;
+}
+
+// Restrides the lane buffers of `moves` on the server's stream (worker
+// thread, no lock held; the previous tick has ended, the joins follow).
+int run_relayouts(tbtkkpm_server *s, const std::vector<Relayout> &moves) {
+  std::vector<std::pair<uint32_t, uint32_t>> ranges;
+  uint64_t launches = 0;
+  for (const Relayout &mv : moves) {
+    const Model *m = mv.m;
+    lane_relayout_ranges(m->N, mv.from, mv.to, ranges);
+    for (int b = 0; b < 2; b++)
+      for (const auto &rg : ranges) {
+        const uint64_t n = (uint64_t)(rg.second - rg.first) * mv.to;
+        const unsigned grid = (unsigned)std::min<uint64_t>(blocks_for(n), 8ull * sm_count(s->device));
+        if (m->real)
+          kpm_lane_relayout<float><<<grid, 256, 0, s->stream>>>(m->vec[b].as<float>(), rg.first,
+                                                                rg.second, mv.from, mv.to);
+        else
+          kpm_lane_relayout<float2><<<grid, 256, 0, s->stream>>>(m->vec[b].as<float2>(), rg.first,
+                                                                 rg.second, mv.from, mv.to);
+        launches += 1;
+      }
+  }
+  count_launches(launches);
+  const cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "server: lane restride");
   return TBTKKPM_OK;
 }
 
@@ -503,14 +576,14 @@ int upload_lanes(tbtkkpm_server *s, Model *m) {
   // moments of its own source), and the pair targets of direct lanes
   std::vector<std::pair<uint32_t, uint32_t>> t;
   std::fill(m->bitmap_h.begin(), m->bitmap_h.end(), 0u);
-  for (uint32_t c = 0; c < m->W; c++)
+  for (uint32_t c = 0; c < m->Wmax; c++)
     if (m->lane_req[c]) {
       t.push_back({m->lane_site[c], c});
       for (const auto &pr : m->lane_pairs[c]) t.push_back({pr.first, c | (pr.second << 8) | kPairEntry});
     }
   for (const auto &e : t) m->bitmap_h[e.first >> 5] |= 1u << (e.first & 31);
   std::sort(t.begin(), t.end());
-  const size_t cap = 2 * (size_t)m->W;
+  const size_t cap = 2 * (size_t)m->Wmax;
   std::vector<uint32_t> tl(2 * cap, 0);
   for (size_t i = 0; i < t.size(); i++) {
     tl[i] = t[i].first;
@@ -525,8 +598,8 @@ int upload_lanes(tbtkkpm_server *s, Model *m) {
   auto put = [&](const DevBuf &v, const void *src, size_t n) {
     std::memcpy(buf.data() + (v.as<char>() - lo), src, n);
   };
-  put(m->base, m->base_h.data(), 4 * (size_t)m->W);
-  put(m->laneM, m->M_h.data(), 4 * (size_t)m->W);
+  put(m->base, m->base_h.data(), 4 * (size_t)m->Wmax);
+  put(m->laneM, m->M_h.data(), 4 * (size_t)m->Wmax);
   put(m->bitmap, m->bitmap_h.data(), 4 * m->bitmap_h.size());
   put(m->tlist, tl.data(), 4 * tl.size());
   cudaError_t e;
@@ -548,7 +621,7 @@ MultiModel describe(const tbtkkpm_server *s, const Model *m) {
   d.vec[1] = m->vec[1].as<float2>();
   d.bitmap = m->bitmap.as<uint32_t>();
   d.trow = m->tlist.as<uint32_t>();
-  d.tcol = m->tlist.as<uint32_t>() + 2 * m->W;
+  d.tcol = m->tlist.as<uint32_t>() + 2 * m->Wmax;
   d.tcount = m->tcount;
   d.base = m->base.as<int32_t>();
   d.lane_M = m->laneM.as<uint32_t>();
@@ -597,7 +670,7 @@ int plan_tick(tbtkkpm_server *s, std::vector<ClassPlan> &plans) {
       bool ok = true;
       for (size_t i = 0; i < members[c].size() && ok; i++) {
         int rc;
-        tp[i] = model_plan(members[c][i], cp.entry, &rc);
+        tp[i] = model_plan(members[c][i], cp.W, cp.entry, &rc);
         if (rc) return rc;
         ok = tp[i] != nullptr;
         if (ok) {
@@ -1154,7 +1227,14 @@ void worker(tbtkkpm_server *s) {
     s->working = true;
     std::vector<MultiJoin> joins;
     std::vector<JoinRef> refs;
-    rc = admit(s, joins, refs);
+    std::vector<Relayout> moves;
+    rc = admit(s, joins, refs, moves);
+    if (!rc && !moves.empty()) {
+      lk.unlock();
+      rc = run_relayouts(s, moves);
+      lk.lock();
+      s->relayouts += (double)moves.size();
+    }
     if (!rc && !joins.empty()) {
       // FP64 heads: a lane with head q starts at local step q + 1, and a
       // request ends with its last lane
@@ -1193,7 +1273,7 @@ void worker(tbtkkpm_server *s) {
     for (auto &p : s->models) {
       Model *m = p.get();
       if (!m->resident || !m->busy) continue;
-      for (uint32_t c = 0; c < m->W; c++) {
+      for (uint32_t c = 0; c < m->Wmax; c++) {
         if (!m->lane_req[c]) continue;
         const Request *r = s->requests.at(m->lane_req[c]).get();
         if (r->lanes.empty() || r->lanes[0] != c) continue;  // one entry per request
@@ -1239,7 +1319,7 @@ void worker(tbtkkpm_server *s) {
     for (auto &p : s->models) {
       Model *m = p.get();
       if (!m->resident || !m->busy) continue;
-      for (uint32_t c = 0; c < m->W; c++) {
+      for (uint32_t c = 0; c < m->Wmax; c++) {
         const uint64_t id = m->lane_req[c];
         if (!id) continue;
         Request *r = s->requests.at(id).get();
@@ -1377,7 +1457,7 @@ extern "C" int tbtkkpm_server_add_model(tbtkkpm_server *s, const uint32_t *rowpt
     return rc;
   }
   m->N = N;
-  m->W = width;
+  m->W = m->Wmax = width;
   m->scale = scale;
   m->real = use_real && m->mat->values_real;
   m->head_steps = head_steps;
@@ -1469,9 +1549,9 @@ extern "C" int tbtkkpm_server_submit(tbtkkpm_server *s, uint32_t model, const ui
   std::lock_guard<std::mutex> lk(s->mu);
   if (model < s->models.size()) {
     const Model *m = s->models[model].get();
-    if (n_sites == 0 || n_sites > m->W)
+    if (n_sites == 0 || n_sites > m->Wmax)
       return fail(TBTKKPM_ERR_ARGUMENT, "server_submit: %u sites for a model of %u lanes", n_sites,
-                  m->W);
+                  m->Wmax);
   }
   auto r = std::make_unique<Request>();
   r->model = model;
@@ -1508,9 +1588,9 @@ extern "C" int tbtkkpm_server_submit_greens(tbtkkpm_server *s, uint32_t model, c
   }
   if (model < s->models.size()) {
     const Model *m = s->models[model].get();
-    if (n_pairs == 0 || n_pairs > m->W)
+    if (n_pairs == 0 || n_pairs > m->Wmax)
       return fail(TBTKKPM_ERR_ARGUMENT, "server_submit_greens: %u pairs for a model of %u lanes",
-                  n_pairs, m->W);
+                  n_pairs, m->Wmax);
   }
   return queue_request(s, std::move(r), request, "server_submit_greens");
 }
@@ -1585,6 +1665,7 @@ extern "C" int tbtkkpm_server_stats(tbtkkpm_server *s, double *out, uint32_t n) 
   v[TBTKKPM_STAT_PLAN_S] = s->plan_s;
   v[TBTKKPM_STAT_TICK_S] = s->tick_s;
   v[TBTKKPM_STAT_GRAPH_TICKS] = s->graph_ticks;
+  v[TBTKKPM_STAT_RELAYOUTS] = s->relayouts;
   for (uint32_t i = 0; i < n && i < TBTKKPM_STAT_COUNT; i++) out[i] = v[i];
   return TBTKKPM_OK;
 }
@@ -1638,6 +1719,13 @@ extern "C" int tbtkkpm_server_set_graphs(tbtkkpm_server *s, int enable) {
   if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_set_graphs: NULL server");
   std::lock_guard<std::mutex> lk(s->mu);
   s->use_graphs = enable != 0;
+  return TBTKKPM_OK;
+}
+
+extern "C" int tbtkkpm_server_set_adaptive_width(tbtkkpm_server *s, int enable) {
+  if (!s) return fail(TBTKKPM_ERR_ARGUMENT, "server_set_adaptive_width: NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->adaptive_width = enable != 0;
   return TBTKKPM_OK;
 }
 
@@ -1719,7 +1807,7 @@ int tune_class(tbtkkpm_server *s, Model *probe, uint32_t width, uint32_t probe_s
     const MultiEntry &en = *ep;
     if ((uint32_t)(en.tpr * en.vpt) != W) continue;
     // a tile-staged entry needs the probe's plan and a ring that fits
-    const TilePlan *plan = model_plan(probe, &en, &rc);
+    const TilePlan *plan = model_plan(probe, W, &en, &rc);
     if (rc) break;
     TiledLayout ly{};
     if (is_multi_tiled(en.minb)) {
@@ -1820,11 +1908,12 @@ int tune_class(tbtkkpm_server *s, Model *probe, uint32_t width, uint32_t probe_s
   if (rc) return rc;
   if (!best) return fail(TBTKKPM_ERR_UNSUPPORTED, "server_autotune: no kernel for width %u", W);
   s->config[W | (real ? 1u << 16 : 0u)] = {best->tpr, best->vpt, best->minb};
+  s->tuned.insert(W | (real ? 1u << 16 : 0u));
   // a tile-staged pick: the plans of every model of the class now, not in
   // the first tick that needs them
   for (auto &p : s->models) {
-    if (p->W != W || p->real != real) continue;
-    model_plan(p.get(), best, &rc);
+    if (p->Wmax < W || (!s->adaptive_width && p->Wmax != W) || p->real != real) continue;
+    model_plan(p.get(), W, best, &rc);
     if (rc) return rc;
   }
   *best_out = best;
@@ -1850,7 +1939,7 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
   Model *probe[2] = {nullptr, nullptr};
   for (auto &p : s->models) {
     Model *&q = probe[p->real ? 1 : 0];
-    if (p->W == width && (!q || p->N > q->N)) q = p.get();
+    if (p->Wmax == width && (!q || p->N > q->N)) q = p.get();
   }
   if (!probe[0] && !probe[1]) return fail(TBTKKPM_ERR_STATE, "server_autotune: no model of width %u", width);
   const int main = !probe[0] || (probe[1] && probe[1]->N > probe[0]->N) ? 1 : 0;
@@ -1860,6 +1949,15 @@ extern "C" int tbtkkpm_server_autotune(tbtkkpm_server *s, uint32_t width, uint32
     if (!probe[c]) continue;
     const int rc = tune_class(s, probe[c], width, probe_steps, &best[c], &best_ms[c]);
     if (rc) return rc;
+    // the narrower widths these models step at when few lanes are busy
+    // (once: another width's autotune may have measured them)
+    for (uint32_t w = width / 2; s->adaptive_width && w >= std::min(kMinStepWidth, width); w /= 2) {
+      if (s->tuned.count(w | (probe[c]->real ? 1u << 16 : 0u))) continue;
+      const MultiEntry *b = nullptr;
+      double ms = 0;
+      const int rn = tune_class(s, probe[c], w, probe_steps, &b, &ms);
+      if (rn) return rn;
+    }
   }
   if (tpr) *tpr = best[main]->tpr;
   if (vpt) *vpt = best[main]->vpt;

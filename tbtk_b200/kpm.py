@@ -82,6 +82,7 @@ SIGNATURES = [
     ("tbtkkpm_table_create", _i, [_u32, _p, _u32, _d, _p]),
     ("tbtkkpm_table_upload", _i, [_u32, _u32, _p, _p]),
     ("tbtkkpm_table_create_clenshaw", _i, [_u32, _p, _u32, _d, _p]),
+    ("tbtkkpm_table_create_chebyshev", _i, [_u32, _u32, _d, _p, _p]),
     ("tbtkkpm_table_destroy", _i, [_p]),
     ("tbtkkpm_greens", _i, [_p, _p, _u32, _i, _p]),
     ("tbtkkpm_ldos", _i, [_p, _p, _u32, _p]),
@@ -114,6 +115,7 @@ SIGNATURES = [
     ("tbtkkpm_server_step_configs", _i, [_i, _u32, _p, _i]),
     ("tbtkkpm_server_set_wait_limit", _i, [_p, _u32]),
     ("tbtkkpm_server_set_graphs", _i, [_p, _i]),
+    ("tbtkkpm_server_set_adaptive_width", _i, [_p, _i]),
     ("tbtkkpm_server_set_real", _i, [_p, _i]),
     ("tbtkkpm_server_set_fp64_head", _i, [_p, _u32]),
     ("tbtkkpm_server_set_table_free", _i, [_p, _i]),
@@ -123,7 +125,8 @@ SIGNATURES = [
 PENDING = 1
 STAT_NAMES = ["completed", "p50_ms", "p99_ms", "mean_ms", "reruns", "ticks", "steps",
               "lane_steps", "resident_bytes", "evictions", "waited", "busy_s", "step_s",
-              "step_bytes", "finish_s", "rerun_s", "join_s", "plan_s", "tick_s", "graph_ticks"]
+              "step_bytes", "finish_s", "rerun_s", "join_s", "plan_s", "tick_s", "graph_ticks",
+              "relayouts"]
 
 
 def step_configs(precision, ldos=True):
@@ -284,10 +287,6 @@ class Matrix:
         vr, use = ctypes.c_int(), ctypes.c_int()
         _check(load_library().tbtkkpm_matrix_real(self._h, ctypes.byref(vr), ctypes.byref(use)))
         return bool(vr.value), bool(use.value)
-
-    def set_graphs(self, enable=True):
-        """Replay a captured CUDA graph per tick (default) or launch directly."""
-        _check(load_library().tbtkkpm_server_set_graphs(self._h, int(bool(enable))))
 
     def set_wait_limit(self, polls=0xFFFFFFFF):
         """Polls per staged-row wait of the tile-staged steps
@@ -469,6 +468,20 @@ class Table:
         return cls(h, M, energies.size)
 
     @classmethod
+    def create_chebyshev(cls, M, E, scale):
+        """A table handle on the grid of E Chebyshev nodes (E a power of two,
+        at most 4096): energy sums by one FFT per vector
+        (tbtkkpm_table_create_chebyshev).  The ascending grid is in
+        ``.energies``."""
+        energies = np.zeros(int(E), dtype=np.float64)
+        h = ctypes.c_void_p()
+        _check(load_library().tbtkkpm_table_create_chebyshev(int(M), int(E), float(scale),
+                                                             _ptr(energies), ctypes.byref(h)))
+        t = cls(h, M, int(E))
+        t.energies = energies
+        return t
+
+    @classmethod
     def upload(cls, table):
         table = _cxa(table)
         M, E = table.shape
@@ -596,6 +609,11 @@ class Server:
     def set_graphs(self, enable=True):
         """Replay a captured CUDA graph per tick (default) or launch directly."""
         _check(load_library().tbtkkpm_server_set_graphs(self._h, int(bool(enable))))
+
+    def set_adaptive_width(self, enable=True):
+        """Step each model at the narrowest width that covers its busy lanes
+        (default) or always at its full lane count."""
+        _check(load_library().tbtkkpm_server_set_adaptive_width(self._h, int(bool(enable))))
 
     def set_wait_limit(self, polls=0xFFFFFFFF):
         """Polls per staged-row wait of the tile-staged steps (default: the

@@ -127,6 +127,7 @@ def serve(a):
     srv = kpm.Server(4096, energies, hbm_budget=int(a.budget_gb * 2**30), tick_steps=a.tick,
                      tolerance=a.tolerance)
     srv.set_fp64_head(a.fp64_head)
+    srv.set_adaptive_width(not a.full_width)
     sizes, csrs = [], []
     t0 = time.perf_counter()
     for kind, L, J, W, alpha, seed in pool:
@@ -162,7 +163,7 @@ def serve(a):
     srv.close()
     return {
         "workload": f"serving: {a.models} models (N log-uniform 1e3-4e6, square/honeycomb/"
-                    f"Rashba, {a.width} lanes), Poisson {a.rate}/s for {a.duration}s, 1-16 sites, "
+                    f"Rashba, {a.width} lanes{', full-width steps' if a.full_width else ''}), Poisson {a.rate}/s for {a.duration}s, 1-16 sites, "
                     f"M in [512,4096], s=12, E=1000",
         "metric": "LDOS solves/s", "value": solves / wall, "unit": "LDOS solves/s",
         "requests": len(reqs), "requests_per_s": len(reqs) / wall, "wall_s": wall,
@@ -189,6 +190,8 @@ def main():
                     help="seed of the sampled solves checked against the FP64 path")
     ap.add_argument("--width", type=int, default=16,
                     help="lanes of every pool model (serve)")
+    ap.add_argument("--full-width", action="store_true",
+                    help="serve: step every model at its full lane count (no adaptive width)")
     ap.add_argument("--fp64-head", type=int, default=32,
                     help="FP64 head steps of every lane (0: none)")
     a = ap.parse_args()

@@ -60,6 +60,14 @@ def test_argument_errors_return_status(kpm):
             kpm.Matrix.from_triplets(np.array([0, 1]), np.array([1, 0]),
                                      np.array([bad, 1.0], dtype=np.complex128), 2, 10.0)
         assert e.value.status == kpm.ERR_ARGUMENT and "not finite" in str(e.value)
+    for M, E, s in ((0, 64, 10.0), (10, 0, 10.0), (10, 48, 10.0), (10, 8192, 10.0),
+                    (10, 64, 0.0), (10, 64, -1.0)):
+        with pytest.raises(kpm.TBTKError) as e:
+            kpm.Table.create_chebyshev(M, E, s)
+        assert e.value.status == kpm.ERR_ARGUMENT, (M, E, s)
+    with pytest.raises(kpm.TBTKError) as e:
+        kpm.Table.create_chebyshev(10, 6, 10.0)
+    assert "power of two" in str(e.value)
     lib = kpm.load_library()
     assert lib.tbtkkpm_matrix_set_batch_width(None, kpm.MIXED, 64) == kpm.ERR_ARGUMENT
     assert lib.tbtkkpm_matrix_set_batch_width(None, 7, 64) == kpm.ERR_ARGUMENT

@@ -69,3 +69,73 @@ def test_server_table_free(gpu):
         out.append(ldos)
         srv.close()
     assert rel_err(out[1], out[0]) <= 1e-12
+
+
+def _random_coefficients(K, M, seed):
+    rng = np.random.default_rng(seed)
+    decay = np.exp(-np.arange(M) / max(M / 4, 1))
+    return (rng.standard_normal((K, M)) + 1j * rng.standard_normal((K, M))) * decay
+
+
+def _node_sums(mu, E, s, ty):
+    """The five sums on the Chebyshev nodes with exactly reduced phases:
+    n theta_k = pi m / (2E), m = n (2k + 1) mod 4E (numpy, FP64)."""
+    K, M = mu.shape
+    k = np.arange(E)
+    ph = np.exp(1j * np.pi * ((np.arange(M)[:, None] * (2 * k + 1)) % (4 * E)) / (2 * E))
+    a = mu.copy()
+    a[:, 0] *= 0.5
+    C = (a @ ph + a @ np.conj(ph)) / 2
+    S = (a @ ph - a @ np.conj(ph)) / 2j
+    A = 2 / (s * np.sin(np.pi * (2 * k + 1) / (2 * E)))
+    g = {0: -A * (S - 1j * C), 1: -A * (S + 1j * C), 2: A * S, 3: 1j * A * C,
+         4: A * C.real / np.pi}[ty]
+    return g[:, ::-1]
+
+
+@pytest.mark.parametrize("M,E", [(1, 1), (7, 2), (300, 64), (1000, 1024), (3000, 512),
+                                 (2048, 2048), (4096, 4096)])
+def test_chebyshev_grid_matches_table_sums(gpu, M, E):
+    """Energy sums on the Chebyshev-node grid by one FFT per vector
+    (tbtkkpm_table_create_chebyshev), every type: against the same sums with
+    exactly reduced phases at 1e-13, and against the lookup-table sums on the
+    same energies at 1e-11 (the table's e^{-i n acos x} carries a phase
+    rounding that grows with n).  M > 2E folds terms onto the transform."""
+    s = 12.0
+    cheb = gpu.Table.create_chebyshev(M, E, s)
+    e = np.arange(E)
+    assert np.allclose(cheb.energies, -s * np.cos(np.pi * (2 * e + 1) / (2 * E)), rtol=0,
+                       atol=1e-14 * s)
+    assert np.all(np.diff(cheb.energies) > 0) and np.all(np.abs(cheb.energies) < s)
+    tab = gpu.Table.create(M, cheb.energies, s)
+    mu = _random_coefficients(5, M, M + E)
+    for ty in range(4):
+        G = cheb.greens(mu, ty)
+        assert rel_err(G, _node_sums(mu, E, s, ty)) <= 1e-13, ty
+        assert rel_err(G, tab.greens(mu, ty)) <= 1e-11, ty
+    rho = cheb.ldos(mu)
+    assert rel_err(rho, _node_sums(mu, E, s, 4)) <= 1e-13
+    assert rel_err(rho, tab.ldos(mu)) <= 1e-11
+    one = cheb.greens(mu[2:3], 1)
+    assert np.array_equal(one[0], cheb.greens(mu, 1)[2])  # one block per vector
+
+
+def test_chebyshev_grid_ldos_sites(gpu):
+    """ldos_sites through a Chebyshev-grid handle on the 30x30 spin lattice
+    (M = 1000) equals the table-handle result on the same energies."""
+    g = golden("cfg1")
+    s, M, bro = float(g["scale"]), int(g["M"]), float(g["broadening"])
+    m = gpu.Matrix.from_csr(g["rowptr"], g["col"], g["val"], s)
+    cheb = gpu.Table.create_chebyshev(M, 1024, s)
+    tab = gpu.Table.create(M, cheb.energies, s)
+    sites = g["ldos_sites"]
+    ref, _ = m.ldos_sites(tab, sites, bro, gpu.FP64)
+    got, _ = m.ldos_sites(cheb, sites, bro, gpu.FP64)
+    assert rel_err(got, ref) <= 1e-12
+    mixed, err = m.ldos_sites(cheb, sites, bro, gpu.MIXED)
+    assert rel_err(mixed, ref) <= 1e-6
+    # Gauss-Chebyshev quadrature: the integral of the LDOS (mu_0 = 1) is
+    # sum_e rho(E_e) (pi s / E) q_e
+    q = np.sqrt(1 - (cheb.energies / s) ** 2)
+    total = got @ (np.pi * s / 1024 * q)
+    assert np.allclose(total, 1.0, rtol=0, atol=1e-10)  # exact for degree < 2E

@@ -70,6 +70,9 @@ def _solo(kpm, csr, sites, M, broadening, width, config=None):
     srv = kpm.Server(512, grid(), hbm_budget=1 << 30, tick_steps=16, tolerance=0)
     mid = srv.add_model(*csr, S, width)
     if config:
+        # the model steps at `width` (not at the narrower width its busy
+        # lanes would take), so the configuration applies
+        srv.set_adaptive_width(False)
         srv.set_config(width, *config)
     out = srv.wait(srv.submit(mid, sites, M, broadening))
     srv.close()
@@ -147,6 +150,7 @@ def test_server_tiled_steps_equal_register_steps(gpu, width):
             srv = kpm.Server(256, grid(), hbm_budget=1 << 30, tick_steps=6, tolerance=0)
             ids = [srv.add_model(*c, S, width) for _, c in ms]
             if cfg is not None:
+                srv.set_adaptive_width(False)  # every step at `width`, in this configuration
                 srv.set_config(width, *cfg)
             outs[(real, cfg)] = _mixed_traffic(kpm, srv, ids, ms, 11)
             srv.close()
@@ -158,6 +162,47 @@ def test_server_tiled_steps_equal_register_steps(gpu, width):
             for x, y in zip(a, b):
                 assert np.array_equal(x, y), key
     assert tiled >= 1 or width < 4
+
+
+@pytest.mark.gpu
+def test_server_adaptive_width_equals_full_width(gpu):
+    """Models that step at the narrowest width covering their busy lanes,
+    restrided in place while requests are in flight (narrowed when short
+    requests leave, widened when new ones join), give the results of models
+    that always step at their full lane count bit for bit: real and complex
+    lanes, LDOS and directly gathered Green's-function lanes.  They move
+    fewer bytes."""
+    kpm = gpu
+    ms = models()[:2]
+    outs, stats = [], []
+    for adaptive in (True, False):
+        srv = kpm.Server(2048, grid(), hbm_budget=1 << 30, tick_steps=8, tolerance=0)
+        srv.set_adaptive_width(adaptive)
+        ids = [srv.add_model(*c, S, 32) for _, c in ms]
+
+        def sites(i, k, off):
+            N = ms[i][1][0].size - 1
+            return (np.arange(off, off + k, dtype=np.uint32) * 7) % N
+
+        first, late = [], []
+        for i in range(len(ms)):
+            first.append(srv.submit(ids[i], sites(i, 2, 1), 1600, 1e-3))
+            first.append(srv.submit_greens(ids[i], sites(i, 3, 5) + 1, sites(i, 3, 5), 900, 1e-3,
+                                           "Retarded"))
+        short = [srv.submit(ids[i], sites(i, k, 20 + k), M, 1e-3)
+                 for i in range(len(ms)) for k, M in ((10, 40), (16, 48))]
+        res = [srv.wait(q) for q in short]
+        for i in range(len(ms)):
+            late.append(srv.submit(ids[i], sites(i, 12, 60), 64, 1e-3))
+        res += [srv.wait(q) for q in first + late]
+        outs.append(res)
+        stats.append(srv.stats())
+        srv.close()
+    for a, b in zip(*outs):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    assert stats[0]["relayouts"] >= 2 and stats[1]["relayouts"] == 0
+    assert stats[0]["step_bytes"] < stats[1]["step_bytes"]
 
 
 @pytest.mark.gpu
