@@ -147,9 +147,11 @@ def kernel_name(real_vectors, tuned):
     tpr, vpt, variant = tuned[:3]
     if variant >= 100000:
         v = variant - 100000
+        cv = v // 1000000
         return (f"kpm_step_tiled<{'real' if real_vectors else 'complex64'}, tpr={tpr}, "
                 f"vpt={vpt}, rows/tile={(v % 1000000) // 1000}, consumer warps={(v % 1000) // 10}, "
-                f"blocks/SM={v % 10}, widening split={v // 1000000}>")
+                f"blocks/SM={v % 10}, widening split={cv % 100}"
+                f"{', row pairs' if cv >= 100 else ''}>")
     return f"{'kpm_step_real' if real_vectors else 'kpm_step<float2'}, tpr={tpr}, vpt={vpt}, minb={variant}"
 
 
@@ -436,7 +438,8 @@ def serving_sub():
     [512, 4096]): served throughput and the latency percentiles."""
     from tbtk_b200 import serve_bench
     a = argparse.Namespace(models=64, budget_gb=120.0, tick=64, tolerance=1e-6, samples=8,
-                           sample_seed=44, fp64_head=32, rate=100.0, duration=3.0, width=16)
+                           sample_seed=44, fp64_head=32, rate=100.0, duration=3.0, width=16,
+                           full_width=False)
     r = serve_bench.serve(a)
     st = r["server"]
     return {"workload": r["workload"], "value": r["value"], "unit": "LDOS solves/s",

@@ -221,8 +221,11 @@ TBTKKPM_API int tbtkkpm_table_create_clenshaw(
  * arithmetic per vector instead of the table's O(M E) multiply-adds and
  * 16 M E table bytes; 32 E bytes of device memory).  M is the most
  * coefficients a call may pass; any M works (terms beyond 2E fold onto the
- * transform).  Results equal the table sums on the same energies up to
- * rounding (~1e-13 relative).  The grid is not uniform: the properties
+ * transform).  Results are the sums at the exact node angles (~1e-13
+ * relative); the lookup-table sums on the same energies agree to ~1e-11
+ * away from the band edges, less at the outermost nodes, where the
+ * table's acos of the stored energy is ill-conditioned (a phase error of
+ * about n eps / sqrt(1 - x^2)).  The grid is not uniform: the properties
  * that integrate over energy with a spacing dE (density, magnetization,
  * expectation values) assume a uniform grid and are not meant for it.
  * (The discrete-cosine-transform energy-sum variant; no reference

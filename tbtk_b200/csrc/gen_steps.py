@@ -179,14 +179,19 @@ TILED_REAL = {
     (32, 4): _variants([(32, 8, 2), (64, 16, 1), (16, 8, 2)], [0, 51]),
     (32, 8): _variants([(16, 8, 2), (32, 16, 1), (16, 16, 1)], [0, 51]),
 }
+# CV >= 100: the row-pair form (two adjacent rows per thread group, each
+# gathered row widened once for both; 16-row tiles and up).
 TILED_CPLX = {
-    (32, 4): _variants([(16, 16, 1), (16, 8, 1), (8, 8, 1), (8, 8, 2)], [0, 40, 60, 90, 61]),
-    (16, 8): _variants([(16, 16, 1), (16, 8, 1), (8, 8, 1), (8, 8, 2)], [0, 60, 61]),
-    (64, 4): _variants([(8, 8, 1), (8, 16, 1)], [0, 60]),
-    (32, 8): _variants([(8, 8, 1), (8, 16, 1)], [0, 60]),
-    (16, 4): _variants([(16, 8, 1), (32, 8, 1), (16, 8, 2), (16, 4, 3)], [0, 60]),
-    (32, 2): _variants([(16, 8, 1), (16, 8, 2)], [0, 60]),
-    (8, 4): _variants([(16, 8, 2), (32, 8, 1), (32, 8, 2)], [0, 60]),
+    (32, 4): _variants([(16, 16, 1), (16, 8, 1), (8, 8, 1), (8, 8, 2)], [0, 40, 60, 90, 61])
+    + _variants([(16, 16, 1), (16, 8, 1), (32, 8, 1)], [100, 150, 151]),
+    (16, 8): _variants([(16, 16, 1), (16, 8, 1), (8, 8, 1), (8, 8, 2)], [0, 60, 61])
+    + _variants([(16, 16, 1), (16, 8, 1)], [100, 150]),
+    (64, 4): _variants([(8, 8, 1), (8, 16, 1)], [0, 60]) + _variants([(16, 8, 1), (16, 16, 1)], [100, 150]),
+    (32, 8): _variants([(8, 8, 1), (8, 16, 1)], [0, 60]) + _variants([(16, 8, 1)], [100, 150]),
+    (16, 4): _variants([(16, 8, 1), (32, 8, 1), (16, 8, 2), (16, 4, 3)], [0, 60])
+    + _variants([(16, 8, 1), (32, 8, 1)], [100, 150]),
+    (32, 2): _variants([(16, 8, 1), (16, 8, 2)], [0, 60]) + _variants([(16, 8, 1)], [100]),
+    (8, 4): _variants([(16, 8, 2), (32, 8, 1), (32, 8, 2)], [0, 60]) + _variants([(16, 4, 2)], [100]),
     (8, 2): _variants([(32, 8, 2), (16, 8, 2)], [0, 60]),
 }
 

@@ -84,6 +84,7 @@ struct TilePlan {
   uint32_t N, ntiles, R;
   uint32_t umax, wmax;     // most distinct outside columns / entries per row of a tile
   uint32_t nruns;          // runs of all tiles
+  uint32_t pairs;          // row-pair plan: entries of [w][R/2] row pairs, two values each
 };
 
 // Byte layout of one shared-memory ring stage of a tile-staged step
@@ -141,7 +142,8 @@ struct tbtkkpm_matrix {
   // autotuned step configuration per (kernel class, padded batch width):
   // {threads per row, values per thread, min blocks per SM}
   std::map<uint64_t, std::array<int, 3>> tuned;
-  // tile plans by (rows per tile, complex values): key 2*R + complex
+  // tile plans by (rows per tile, complex values, row pairs): key
+  // 1024*pairs + 2*R + complex
   std::map<int, tbtkkpm::TilePlanStore> plans;
   std::mutex lock;
   void release_all() {
@@ -171,9 +173,10 @@ struct tbtkkpm_table {
   // [2E] complex e^{i pi m / (2E)}
   bool chebyshev_grid = false;
   double scale = 0;
-  // largest weight of the energy sum on this grid, max_e |T[1][e]| / pi =
-  // max_e 2 / (pi s sqrt(1 - (E_e/s)^2)): the scale that turns a moment
-  // error into an LDOS error (ldos_error_estimate)
+  // error weight of this grid: the largest weight of the energy sum,
+  // max_e |T[1][e]| / pi = max_e 2 / (pi s sqrt(1 - (E_e/s)^2)), times the
+  // grid's edge coherence (edge_coherence, recursion.cu): the scale that
+  // turns a moment error into an LDOS error (ldos_error_estimate)
   double wmax = 0;
   tbtkkpm::DevBuf energies;  // [E]
   tbtkkpm::DevBuf twiddle;   // [2E] complex128 (Chebyshev-node grid)
@@ -201,8 +204,10 @@ int ldos_sites_terms(tbtkkpm_matrix *m, tbtkkpm_table *t, uint32_t M, const uint
 // Lorentz damping numerators a[n] and denominator b (host libm).
 void damping_factors(uint32_t M, double broadening, std::vector<double> &a, double &b);
 // Error estimate of doubled moments against the directly gathered ones.
-// Largest energy-sum weight of a grid (tbtkkpm_table::wmax).
+// Error weight of a grid (tbtkkpm_table::wmax): its largest energy-sum
+// weight times edge_coherence of its smallest node angle acos|E/s|.
 double grid_weight_max(const double *energies, uint32_t E, double scale);
+double edge_coherence(double theta_min);
 // LDOS-space error estimate of a doubling run from its moment estimate
 // (doubling_error): moment_err * wmax / max_e |v_e| over the result row, v
 // the LDOS (complex false), or G / pi for a Green's function row (complex
@@ -210,8 +215,9 @@ double grid_weight_max(const double *energies, uint32_t E, double scale);
 double ldos_error_estimate(double moment_err, double wmax, const double *row, uint32_t E, bool complex);
 void doubling_error(const std::vector<double2> &mu, const std::vector<double2> &direct,
                     uint32_t K, uint32_t M, uint32_t ld, double *err);
-// The matrix's gather plan for R-row tiles (real or complex values), built
-// on first use; *out is null when some tile is too large for the builder.
-int tile_plan(tbtkkpm_matrix *m, int R, bool cplx, const TilePlan **out);
+// The matrix's gather plan for R-row tiles (real or complex values; pairs:
+// the row-pair plan of complex values, R >= 16), built on first use; *out is
+// null when some tile is too large for the builder.
+int tile_plan(tbtkkpm_matrix *m, int R, bool cplx, const TilePlan **out, bool pairs = false);
 
 }  // namespace tbtkkpm

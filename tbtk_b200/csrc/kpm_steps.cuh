@@ -180,11 +180,12 @@ void launch_async(cudaStream_t st, int device, unsigned max_grid, const StepArgs
    &launch_async<P, true, D, S, WMAX, WPB>, &launch_async<P, false, D, S, WMAX, WPB>}
 
 // Tile-staged step variants: 100000 + 1000000*CV + 1000*R + 10*CW + BPS
-// (CV the widening split of kpm_step_tiled, R rows per tile, CW consumer
-// warps, BPS blocks per SM).
+// (CV the widening split of kpm_step_tiled, plus 100 for the row-pair
+// form, R rows per tile, CW consumer warps, BPS blocks per SM).
 constexpr int kTiledVariant = 100000;
 inline bool is_tiled_variant(int v) { return v >= kTiledVariant; }
 inline int tiled_rows(int v) { return ((v - kTiledVariant) % 1000000) / 1000; }
+inline bool tiled_pairs(int v) { return (v - kTiledVariant) / 1000000 >= 100; }
 inline int tiled_bps(int v) { return v % 10; }
 
 template <bool CPLX, int TPR, int VPT, int R, int CW, int BPS, bool FIRST, bool DOTS, int CV>
@@ -194,7 +195,7 @@ void launch_tiled(cudaStream_t st, int device, unsigned max_grid, const StepArgs
   using Val = typename TiledTypes<CPLX>::Val;
   auto kern = kpm_step_tiled<CPLX, TPR, VPT, R, CW, BPS, FIRST, DOTS, CV>;
   *grid = 0;
-  if (!a.plan || a.plan->R != (uint32_t)R) return;
+  if (!a.plan || a.plan->R != (uint32_t)R || a.plan->pairs != (CV >= 100 ? 1u : 0u)) return;
   const TilePlan &p = *a.plan;
   const TiledLayout ly =
       tiled_layout(p, a.Bp * (uint32_t)sizeof(E), (uint32_t)sizeof(Val), tiled_budget(BPS));

@@ -40,6 +40,9 @@
 namespace tbtkkpm {
 
 constexpr uint16_t kSlotPad = 0xffff;
+// a row-pair plan entry: bits 0-13 the slot, bit 14 the pair's first row
+// has the column, bit 15 its second row (kSlotPad: padding)
+constexpr uint32_t kPairSlotBits = 0x3fffu;
 constexpr uint32_t kPlanCap = 4096;  // entries of one tile the plan builder sorts
 constexpr int kPlanBlock = 256;
 constexpr uint32_t kTiledMaxStages = 8;
@@ -112,10 +115,16 @@ template <> struct TiledTypes<true> {
 // producer; warps 1..CW consume.  Consumer thread `sub` of a TPR-thread
 // group owns VPT elements of its row (interleaved 16-byte chunks, as
 // RPack / Pack), and the CW*32/TPR groups take the tile's rows in passes.
-// CV = 10*GA + PA splits the float -> FP64 widenings between the pipes:
-// the gathers of a row's first GA entries and, with PA, j_{n-1} and the
-// dot-product terms widen on the integer pipe (f2d_scaled), the rest by
-// conversion instructions.  Every choice gives the same stored vectors.
+// CV = 100*PAIR + 10*GA + PA.  GA and PA split the float -> FP64 widenings
+// between the pipes: the gathers of a row's first GA entries and, with PA,
+// j_{n-1} and the dot-product terms widen on the integer pipe
+// (f2d_scaled), the rest by conversion instructions.  PAIR (complex
+// vectors, R >= 16) reads a row-pair plan (tile_plan with pairs): a group
+// takes two adjacent rows, walks the merge of their column lists and
+// widens each gathered row once for both (a spin lattice site's two rows
+// share most columns), adding it into each row that has the column; each
+// row still sees its own entries in CSR order.  Every choice gives the same
+// stored vectors.
 template <bool CPLX, int TPR, int VPT, int R, int CW, int BPS, bool FIRST, bool DOTS, int CV = 0>
 __global__ void __launch_bounds__(32 * (CW + 1), BPS)
 kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
@@ -127,11 +136,14 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
   using Pk = typename std::conditional<CPLX, Pack<float2, TPR, VPT>, RPack<TPR, VPT>>::type;
   using L = typename Pk::L;
   constexpr int NL = Pk::NL;
-  constexpr int GA = CV / 10;
+  constexpr bool PAIR = CV >= 100;
+  constexpr int GA = (CV % 100) / 10;
   constexpr bool PA = CV % 10 != 0;
-  constexpr int RPP = CW * 32 / TPR;  // rows per pass
-  constexpr int PASSES = (R + RPP - 1) / RPP;
+  constexpr int RPP = CW * 32 / TPR;  // row units (rows, or row pairs) per pass
+  constexpr uint32_t EW = PAIR ? R / 2 : R;  // plan entries of one chunk row: a row or a pair
+  constexpr int PASSES = ((int)EW + RPP - 1) / RPP;
   static_assert(CW * 32 % TPR == 0, "a row group must divide the consumer threads");
+  static_assert(!PAIR || (CPLX && R >= 16), "row pairs: complex vectors, 16-byte slot chunks");
   extern __shared__ __align__(128) unsigned char tsm[];
   uint64_t *full = reinterpret_cast<uint64_t *>(tsm);
   uint64_t *empty = full + kTiledMaxStages;
@@ -180,15 +192,16 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
       unsigned char *st = ring + (size_t)s * LY.stage_bytes;
       const uint32_t w = h0.w & 0xffffu, nruns = h0.w >> 16, nuniq = h0.z;
       const uint32_t r0 = t * R, Rt = min((uint32_t)R, P.N - r0);
-      const uint32_t ebytes = w * R * (uint32_t)sizeof(Val), sbytes = w * R * 2u;
+      // pair entries carry two values each: w * R values either way
+      const uint32_t ebytes = w * R * (uint32_t)sizeof(Val), sbytes = w * EW * 2u;
       const uint32_t bytes =
           ebytes + sbytes + (Rt + nuniq + (FIRST ? 0u : Rt)) * rowbytes;
       if (lane == 0) mbar_expect_tx(&full[s], bytes);
       __syncwarp();
-      const uint64_t e0 = (uint64_t)h0.x * R;
+      const uint64_t e0 = (uint64_t)h0.x * EW;
       if (w) {
         if (lane == 0)
-          bulk_load(st, static_cast<const Val *>(P.eval) + e0, ebytes, &full[s]);
+          bulk_load(st, static_cast<const Val *>(P.eval) + e0 * (PAIR ? 2 : 1), ebytes, &full[s]);
         if (lane == 1) bulk_load(st + LY.off_slots, P.eslot + e0, sbytes, &full[s]);
       }
       if (lane == 2) bulk_load(st + LY.off_xs, x + (uint64_t)r0 * Bp, Rt * rowbytes, &full[s]);
@@ -228,7 +241,7 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
       uint32_t bw[PASSES];
 #pragma unroll
       for (int p = 0; p < PASSES; p++) {
-        const uint32_t lr = grp + p * RPP;
+        const uint32_t lr = (grp + p * RPP) * (PAIR ? 2 : 1);  // a pair's rows share a word
         bw[p] = lr < Rt ? __ldg(tg.bitmap + ((r0 + lr) >> 5)) : 0u;
       }
       if (!mbar_wait_limit(&full[s], (i / S) & 1u, wait_limit)) {
@@ -242,6 +255,95 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
       const E *prev = reinterpret_cast<const E *>(st + LY.off_prev);
 #pragma unroll
       for (int p = 0; p < PASSES; p++) {
+        if constexpr (PAIR) {
+          const uint32_t u = grp + p * RPP, la = 2 * u;
+          if (la >= Rt) continue;
+          const bool hb = la + 1 < Rt;
+          double2 acc[2][VPT];
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            if (FIRST || (h == 1 && !hb)) {
+#pragma unroll
+              for (int j = 0; j < VPT; j++) acc[h][j] = make_double2(0.0, 0.0);
+            } else {
+              L yv[NL];
+              Pk::load_rw(reinterpret_cast<const float2 *>(prev) + (size_t)(la + h) * Bp, sub, yv);
+#pragma unroll
+              for (int j = 0; j < VPT; j++) {
+                const float2 f = Pk::getf(yv, j);
+                if constexpr (PA)
+                  acc[h][j] = make_double2(f2d_scaled(f.x) * -kWideUp, f2d_scaled(f.y) * -kWideUp);
+                else
+                  acc[h][j] = make_double2(-(double)f.x, -(double)f.y);
+              }
+            }
+          }
+          for (uint32_t k = 0; k < w; k++) {
+            const uint16_t sl = slots[k * EW + u];
+            if (sl == kSlotPad) break;
+            const uint32_t mask = sl >> 14, slot = sl & kPairSlotBits;
+            double2 va = vals[2 * (k * EW + u)], vb = vals[2 * (k * EW + u) + 1];
+            if constexpr (FIRST) {
+              va = make_double2(va.x * 0.5, va.y * 0.5);
+              vb = make_double2(vb.x * 0.5, vb.y * 0.5);
+            }
+            L xr[NL];
+            Pk::load_rw(reinterpret_cast<const float2 *>(xs) + (size_t)slot * Bp, sub, xr);
+            const bool scaled = GA > 0 && k < (uint32_t)GA;
+            if (scaled) {
+              va = make_double2(va.x * kWideUp, va.y * kWideUp);
+              vb = make_double2(vb.x * kWideUp, vb.y * kWideUp);
+            }
+            double2 xd[VPT];
+#pragma unroll
+            for (int j = 0; j < VPT; j++) {
+              const float2 f = Pk::getf(xr, j);
+              xd[j] = scaled ? make_double2(f2d_scaled(f.x), f2d_scaled(f.y))
+                             : make_double2((double)f.x, (double)f.y);
+            }
+            if (mask & 1u) {
+#pragma unroll
+              for (int j = 0; j < VPT; j++) acc[0][j] = cmac<false>(acc[0][j], va, xd[j]);
+            }
+            if (mask & 2u) {
+#pragma unroll
+              for (int j = 0; j < VPT; j++) acc[1][j] = cmac<false>(acc[1][j], vb, xd[j]);
+            }
+          }
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            if (h == 1 && !hb) break;
+            const uint32_t lr = la + h, row = r0 + lr;
+            if ((bw[p] >> (row & 31)) & 1u) {
+              for (uint32_t q = target_first(tg, row); q < tg.count && __ldg(tg.row + q) == row; q++) {
+                const int jt = Pk::slot_of(sub, __ldg(tg.col + q));
+                if (jt >= 0) {
+#pragma unroll
+                  for (int j = 0; j < VPT; j++)
+                    if (j == jt) tg.mu[(uint64_t)__ldg(tg.out + q) * tg.ld + n_out] = acc[h][j];
+                }
+              }
+            }
+            float2 af[VPT];
+#pragma unroll
+            for (int j = 0; j < VPT; j++)
+              af[j] = make_float2(__double2float_rn(acc[h][j].x), __double2float_rn(acc[h][j].y));
+            Pk::storef(reinterpret_cast<float2 *>(y) + (uint64_t)row * Bp, sub, af);
+            if constexpr (DOTS) {
+              L self[NL];
+              Pk::load_rw(reinterpret_cast<const float2 *>(xs) + (size_t)lr * Bp, sub, self);
+#pragma unroll
+              for (int j = 0; j < VPT; j++) {
+                const float2 b = Pk::getf(self, j);
+                const float nn = fmaf(af[j].x, af[j].x, af[j].y * af[j].y);
+                const float np = fmaf(af[j].x, b.x, af[j].y * b.y);
+                d_nn[j] += PA ? f2d_scaled(nn) : (double)nn;
+                d_np[j] += PA ? f2d_scaled(np) : (double)np;
+              }
+            }
+          }
+          continue;
+        }
         const uint32_t lr = grp + p * RPP;
         if (lr >= Rt) continue;
         const uint32_t row = r0 + lr;
@@ -515,7 +617,41 @@ k_plan_count(uint32_t N, uint32_t ntiles, const uint32_t *__restrict__ rowptr,
   }
 }
 
-template <int R, bool CPLX>
+// Row-pair plans: the entries of a pair of rows (2u, 2u + 1 of a tile) are
+// the merge of their ascending column lists, one entry per distinct column.
+// tw[t] becomes the tile's most merged entries of a pair, maxes[3] the
+// most of any tile (one thread per pair).
+template <int R>
+__global__ void __launch_bounds__(kPlanBlock)
+k_plan_pair_width(uint32_t N, uint32_t ntiles, const uint32_t *__restrict__ rowptr,
+                  const uint32_t *__restrict__ col, uint32_t *tw, unsigned *maxes) {
+  const uint64_t pairs = (uint64_t)ntiles * (R / 2);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < pairs;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t t = (uint32_t)(i / (R / 2)), u = (uint32_t)(i % (R / 2));
+    const uint32_t a = t * R + 2 * u, b = a + 1;
+    uint32_t n = 0;
+    if (a < N) {
+      uint32_t ia = rowptr[a], ea = rowptr[a + 1], ib = 0, eb = 0;
+      if (b < N) {
+        ib = rowptr[b];
+        eb = rowptr[b + 1];
+      }
+      while (ia < ea || ib < eb) {
+        const uint32_t ca = ia < ea ? col[ia] : 0xffffffffu, cb = ib < eb ? col[ib] : 0xffffffffu;
+        if (ca <= cb) ia++;
+        if (cb <= ca) ib++;
+        n++;
+      }
+    }
+    if (n) {
+      atomicMax(tw + t, n);
+      atomicMax(maxes + 3, n);
+    }
+  }
+}
+
+template <int R, bool CPLX, bool PAIRS = false>
 __global__ void __launch_bounds__(kPlanBlock)
 k_plan_fill(uint32_t N, uint32_t ntiles, const uint32_t *__restrict__ rowptr,
             const uint32_t *__restrict__ col, const double2 *__restrict__ val,
@@ -554,6 +690,56 @@ k_plan_fill(uint32_t N, uint32_t ntiles, const uint32_t *__restrict__ rowptr,
       const uint32_t len = (q + 1 < nruns ? rstart[q + 1] : nuniq) - u;
       runs[run_begin[t] + q] = make_uint2(uniq[u], (u << 16) | len);
     }
+    // the shared-memory slot of column c (own rows first, then the runs)
+    auto slot_of = [&](uint32_t c) -> uint32_t {
+      if (c >= r0 && c < r1) return c - r0;
+      uint32_t lo = 0, hi = nuniq;
+      while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (uniq[mid] < c) lo = mid + 1; else hi = mid;
+      }
+      return R + lo;
+    };
+    if constexpr (PAIRS) {
+      // entries: [w][R/2] of {slot | rows << 14} and two values (zero for
+      // a row without the column), padding past each pair's merge
+      const uint64_t base = (uint64_t)ent_begin[t] * (R / 2);
+      for (uint32_t u = threadIdx.x; u < R / 2; u += blockDim.x) {
+        const uint32_t a = r0 + 2 * u, b = a + 1;
+        uint32_t ia = 0, ea = 0, ib = 0, eb = 0;
+        if (a < r1) {
+          ia = rowptr[a];
+          ea = rowptr[a + 1];
+        }
+        if (b < r1) {
+          ib = rowptr[b];
+          eb = rowptr[b + 1];
+        }
+        for (uint32_t k = 0; k < w; k++) {
+          uint16_t slot = kSlotPad;
+          Val va{}, vb{};
+          if (ia < ea || ib < eb) {
+            const uint32_t ca = ia < ea ? col[ia] : 0xffffffffu, cb = ib < eb ? col[ib] : 0xffffffffu;
+            const uint32_t c = ca < cb ? ca : cb;
+            uint32_t mask = 0;
+            if (ca == c) {
+              va = val[ia++];
+              mask |= 1u;
+            }
+            if (cb == c) {
+              vb = val[ib++];
+              mask |= 2u;
+            }
+            slot = (uint16_t)(slot_of(c) | (mask << 14));
+          }
+          eslot[base + (uint64_t)k * (R / 2) + u] = slot;
+          ev[2 * (base + (uint64_t)k * (R / 2) + u)] = va;
+          ev[2 * (base + (uint64_t)k * (R / 2) + u) + 1] = vb;
+        }
+      }
+      __syncthreads();
+      continue;
+    }
     // entries: [w][R] slots and values, padding past each row's length
     const uint64_t base = (uint64_t)ent_begin[t] * R;
     for (uint32_t it = threadIdx.x; it < w * R; it += blockDim.x) {
@@ -564,17 +750,7 @@ k_plan_fill(uint32_t N, uint32_t ntiles, const uint32_t *__restrict__ rowptr,
       if (r < r1) {
         const uint32_t rb = rowptr[r], re = rowptr[r + 1];
         if (rb + k < re) {
-          const uint32_t c = col[rb + k];
-          if (c >= r0 && c < r1) {
-            slot = (uint16_t)(c - r0);
-          } else {
-            uint32_t lo = 0, hi = nuniq;
-            while (lo < hi) {
-              const uint32_t mid = (lo + hi) >> 1;
-              if (uniq[mid] < c) lo = mid + 1; else hi = mid;
-            }
-            slot = (uint16_t)(R + lo);
-          }
+          slot = (uint16_t)slot_of(col[rb + k]);
           const double2 a = val[rb + k];
           if constexpr (CPLX) v = a;
           else v = a.x;

@@ -210,7 +210,7 @@ int resolve_tiled(tbtkkpm_matrix *m, int precision, bool dots, uint32_t B, bool 
   if (!fn || !is_tiled_variant(fn->minb)) return TBTKKPM_OK;
   const bool cplx = !(fn->cls == kClassMixedReal || fn->cls == kClassMixedRealDots);
   const TilePlan *p = nullptr;
-  int rc = tile_plan(m, tiled_rows(fn->minb), cplx, &p);
+  int rc = tile_plan(m, tiled_rows(fn->minb), cplx, &p, tiled_pairs(fn->minb));
   if (rc) return rc;
   const uint32_t esz = cplx ? sizeof(float2) : sizeof(float);
   const uint32_t vsz = cplx ? sizeof(double2) : sizeof(double);
@@ -449,13 +449,27 @@ int check_precision(int precision) {
 // difference between the directly gathered moments (n <= M/2) and the
 // doubling moments of the same n, relative to max |mu|, scaled by sqrt(2)
 // for the moments past M/2 and by a safety factor of 4.
+// Near the band edge (theta = acos|x| small) cos(n theta) stays close to 1
+// for n < 1/theta, so the rounding errors of that many moments add up with
+// little cancellation; their random sum grows as the square root of that
+// count.  The estimate's constant was measured on 1000-point open grids,
+// whose outermost node sits at theta_ref = acos(1 - 2/1001) = 0.063; a grid
+// reaching closer to the edge (the Chebyshev nodes: theta = pi/(2E)) scales
+// the weight by sqrt(theta_ref / theta_min), a grid that stays farther out
+// keeps it.
+double edge_coherence(double theta_min) {
+  const double ref = std::acos(1.0 - 2.0 / 1001.0);
+  return theta_min > 0 && theta_min < ref ? std::sqrt(ref / theta_min) : 1.0;
+}
+
 double grid_weight_max(const double *energies, uint32_t E, double scale) {
-  double w = 0;
+  double w = 0, th = M_PI;
   for (uint32_t e = 0; e < E; e++) {
     const double x = energies[e] / scale;
     w = std::max(w, 2.0 / (M_PI * scale * std::sqrt(1.0 - x * x)));
+    th = std::min(th, std::acos(std::fabs(x)));
   }
-  return w;
+  return w * edge_coherence(th);
 }
 
 // The moment estimate is an error scale of the moments the run returns; the
@@ -780,11 +794,19 @@ extern "C" int tbtkkpm_table_upload(uint32_t M, uint32_t E, const double *table,
   tbtkkpm_table *t = nullptr;
   int rc = table_alloc(M, E, &t);
   if (rc) return rc;
-  // |T[1][e]| = 2 / (s sqrt(1 - x^2)); T[0][e] carries half of it
+  // |T[1][e]| = 2 / (s sqrt(1 - x^2)); T[0][e] carries half of it.
+  // T[1][e] = (2/(s q)) e^{-i(theta + pi/2)} gives the node's angle theta
+  double th = M_PI;
   for (uint32_t e = 0; e < E; e++) {
     const double *v = table + 2 * ((size_t)(M > 1 ? E : 0) + e);
     t->wmax = std::max(t->wmax, (M > 1 ? 1.0 : 2.0) * std::hypot(v[0], v[1]) / M_PI);
+    if (M > 1) {
+      double a = std::remainder(-std::atan2(v[1], v[0]) - M_PI / 2, 2 * M_PI);  // theta in [0, pi]
+      a = std::fabs(a);
+      th = std::min(th, std::min(a, M_PI - a));
+    }
   }
+  t->wmax *= edge_coherence(th);
   DeviceGuard g(t->device);
   cudaError_t e = cudaMemcpyAsync(t->table.ptr, table, sizeof(double2) * (size_t)M * E,
                                   cudaMemcpyHostToDevice, t->stream);

@@ -21,11 +21,20 @@ int count_tiles(cudaStream_t st, const tbtkkpm_matrix *m, uint32_t ntiles, unsig
   return TBTKKPM_OK;
 }
 
-template <int R, bool CPLX>
+template <int R>
+int pair_width(cudaStream_t st, const tbtkkpm_matrix *m, uint32_t ntiles, unsigned grid, DevBuf &tw,
+               DevBuf &flags) {
+  k_plan_pair_width<R><<<grid, kPlanBlock, 0, st>>>(m->N, ntiles, m->rowptr.as<uint32_t>(),
+                                                     m->col.as<uint32_t>(), tw.as<uint32_t>(),
+                                                     flags.as<unsigned>());
+  return TBTKKPM_OK;
+}
+
+template <int R, bool CPLX, bool PAIRS = false>
 int fill_tiles(cudaStream_t st, const tbtkkpm_matrix *m, uint32_t ntiles, unsigned grid,
                const DevBuf &ent, const DevBuf &run, const DevBuf &tw, const DevBuf &truns,
                const DevBuf &tuniq, TilePlanStore &p) {
-  auto kern = k_plan_fill<R, CPLX>;
+  auto kern = k_plan_fill<R, CPLX, PAIRS>;
   constexpr int smem = 3 * kPlanCap * 4;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return cuda_fail(e, "tile plan: shared memory");
@@ -37,7 +46,10 @@ int fill_tiles(cudaStream_t st, const tbtkkpm_matrix *m, uint32_t ntiles, unsign
   return TBTKKPM_OK;
 }
 
-int build_plan(tbtkkpm_matrix *m, int R, bool cplx, TilePlanStore &p) {
+// pairs: the row-pair plan of complex values (R >= 16; k_plan_pair_width)
+int build_plan(tbtkkpm_matrix *m, int R, bool cplx, bool pairs, TilePlanStore &p) {
+  if (pairs && (!cplx || R < 16))
+    return fail(TBTKKPM_ERR_UNSUPPORTED, "tile plan: row pairs need complex values and R >= 16");
   cudaStream_t st = m->stream;
   const uint32_t ntiles = (m->N + R - 1) / R;
   const unsigned grid = (unsigned)std::min<uint64_t>(ntiles, (uint64_t)sm_count(m->device) * 8);
@@ -59,10 +71,21 @@ int build_plan(tbtkkpm_matrix *m, int R, bool cplx, TilePlanStore &p) {
   else return fail(TBTKKPM_ERR_UNSUPPORTED, "tile plan: no builder for %d rows per tile", R);
   count_launches(1);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "tile plan: count");
-  unsigned hf[3] = {0, 0, 0};  // most distinct outside columns, widest row, a tile too large
-  if ((e = cudaMemcpyAsync(hf, flags.ptr, 12, cudaMemcpyDeviceToHost, st)) ||
+  if (pairs) {
+    // entries per tile: the widest merge of a row pair instead of the widest row
+    if ((e = cudaMemsetAsync(tw.ptr, 0, 4 * (size_t)ntiles, st))) return cuda_fail(e, "tile plan: pairs");
+    if (R == 16) rc = pair_width<16>(st, m, ntiles, grid, tw, flags);
+    else if (R == 32) rc = pair_width<32>(st, m, ntiles, grid, tw, flags);
+    else rc = pair_width<64>(st, m, ntiles, grid, tw, flags);
+    count_launches(1);
+    if ((e = cudaGetLastError()) != cudaSuccess) return cuda_fail(e, "tile plan: pairs");
+  }
+  // most distinct outside columns, widest row, a tile too large, widest pair merge
+  unsigned hf[4] = {0, 0, 0, 0};
+  if ((e = cudaMemcpyAsync(hf, flags.ptr, 16, cudaMemcpyDeviceToHost, st)) ||
       (e = cudaStreamSynchronize(st)))
     return cuda_fail(e, "tile plan: count");
+  if (pairs) hf[1] = hf[3];
   p.ok = false;
   if (hf[2]) return TBTKKPM_OK;  // a tile past kPlanCap entries: no plan, other kernels run
   size_t tb = 0, tb2 = 0;
@@ -88,7 +111,11 @@ int build_plan(tbtkkpm_matrix *m, int R, bool cplx, TilePlanStore &p) {
 #define TBTKKPM_FILL(RR)                                                                      \
   (cplx ? fill_tiles<RR, true>(st, m, ntiles, grid, ent, run, tw, truns, tuniq, p)            \
         : fill_tiles<RR, false>(st, m, ntiles, grid, ent, run, tw, truns, tuniq, p))
-  if (R == 8) rc = TBTKKPM_FILL(8);
+  if (pairs) {
+    if (R == 16) rc = fill_tiles<16, true, true>(st, m, ntiles, grid, ent, run, tw, truns, tuniq, p);
+    else if (R == 32) rc = fill_tiles<32, true, true>(st, m, ntiles, grid, ent, run, tw, truns, tuniq, p);
+    else rc = fill_tiles<64, true, true>(st, m, ntiles, grid, ent, run, tw, truns, tuniq, p);
+  } else if (R == 8) rc = TBTKKPM_FILL(8);
   else if (R == 16) rc = TBTKKPM_FILL(16);
   else if (R == 32) rc = TBTKKPM_FILL(32);
   else rc = TBTKKPM_FILL(64);
@@ -107,6 +134,7 @@ int build_plan(tbtkkpm_matrix *m, int R, bool cplx, TilePlanStore &p) {
   p.plan.umax = hf[0];
   p.plan.wmax = hf[1];
   p.plan.nruns = nruns;
+  p.plan.pairs = pairs ? 1u : 0u;
   p.ok = true;
   return TBTKKPM_OK;
 }
@@ -114,15 +142,15 @@ int build_plan(tbtkkpm_matrix *m, int R, bool cplx, TilePlanStore &p) {
 }  // namespace
 
 // The handle's plan for R-row tiles with real (cplx false) or complex
-// values, built on first use; *out is null when the matrix has a tile the
-// builder cannot take.
-int tile_plan(tbtkkpm_matrix *m, int R, bool cplx, const TilePlan **out) {
+// values (pairs: the row-pair plan of complex values), built on first use;
+// *out is null when the matrix has a tile the builder cannot take.
+int tile_plan(tbtkkpm_matrix *m, int R, bool cplx, const TilePlan **out, bool pairs) {
   *out = nullptr;
-  const int key = 2 * R + (cplx ? 1 : 0);
+  const int key = (pairs ? 1024 : 0) + 2 * R + (cplx ? 1 : 0);
   auto it = m->plans.find(key);
   if (it == m->plans.end()) {
     TilePlanStore &p = m->plans[key];
-    int rc = build_plan(m, R, cplx, p);
+    int rc = build_plan(m, R, cplx, pairs, p);
     if (rc) {
       p.release();
       m->plans.erase(key);

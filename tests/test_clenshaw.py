@@ -99,8 +99,11 @@ def test_chebyshev_grid_matches_table_sums(gpu, M, E):
     """Energy sums on the Chebyshev-node grid by one FFT per vector
     (tbtkkpm_table_create_chebyshev), every type: against the same sums with
     exactly reduced phases at 1e-13, and against the lookup-table sums on the
-    same energies at 1e-11 (the table's e^{-i n acos x} carries a phase
-    rounding that grows with n).  M > 2E folds terms onto the transform."""
+    same energies.  The table evaluates e^{-i n acos x} at the energies as
+    stored; near the band edge acos turns their last-bit rounding into a
+    phase error of about eps / q (q = sqrt(1 - x^2)), times n.  So the table
+    agrees at 1e-11 on the nodes with q >= 1/2, and within 16 M eps / q_min
+    on all of them.  M > 2E folds terms onto the transform."""
     s = 12.0
     cheb = gpu.Table.create_chebyshev(M, E, s)
     e = np.arange(E)
@@ -109,13 +112,30 @@ def test_chebyshev_grid_matches_table_sums(gpu, M, E):
     assert np.all(np.diff(cheb.energies) > 0) and np.all(np.abs(cheb.energies) < s)
     tab = gpu.Table.create(M, cheb.energies, s)
     mu = _random_coefficients(5, M, M + E)
+    # errors against the largest Retarded value (it holds both the cosine
+    # and the sine sums; a single type can vanish, e.g. Principal at M = 1)
+    scale = np.abs(_node_sums(mu, E, s, 1)).max()
+
+    q = np.sqrt(1 - (cheb.energies / s) ** 2)
+    inner = q >= 0.5
+    edge_tol = 1e-11 + 16 * M * np.finfo(np.float64).eps / q.min()
+
+    def err(x, ref, where=slice(None)):
+        return float(np.abs(x[:, where] - ref[:, where]).max() / scale)
+
     for ty in range(4):
         G = cheb.greens(mu, ty)
-        assert rel_err(G, _node_sums(mu, E, s, ty)) <= 1e-13, ty
-        assert rel_err(G, tab.greens(mu, ty)) <= 1e-11, ty
+        assert err(G, _node_sums(mu, E, s, ty)) <= 1e-13, ty
+        T = tab.greens(mu, ty)
+        if inner.any():
+            assert err(G, T, inner) <= 1e-11, ty
+        assert err(G, T) <= edge_tol, ty
     rho = cheb.ldos(mu)
-    assert rel_err(rho, _node_sums(mu, E, s, 4)) <= 1e-13
-    assert rel_err(rho, tab.ldos(mu)) <= 1e-11
+    assert err(rho, _node_sums(mu, E, s, 4)) <= 1e-13
+    T = tab.ldos(mu)
+    if inner.any():
+        assert err(rho, T, inner) <= 1e-11
+    assert err(rho, T) <= edge_tol
     one = cheb.greens(mu[2:3], 1)
     assert np.array_equal(one[0], cheb.greens(mu, 1)[2])  # one block per vector
 
@@ -131,11 +151,21 @@ def test_chebyshev_grid_ldos_sites(gpu):
     sites = g["ldos_sites"]
     ref, _ = m.ldos_sites(tab, sites, bro, gpu.FP64)
     got, _ = m.ldos_sites(cheb, sites, bro, gpu.FP64)
-    assert rel_err(got, ref) <= 1e-12
-    mixed, err = m.ldos_sites(cheb, sites, bro, gpu.MIXED)
-    assert rel_err(mixed, ref) <= 1e-6
+    # the table's acos of the stored energies is ill-conditioned at the edge
+    # nodes (see test_chebyshev_grid_matches_table_sums)
+    q = np.sqrt(1 - (cheb.energies / s) ** 2)
+    inner = q >= 0.5
+    assert np.abs(got - ref)[:, inner].max() <= 1e-12 * np.abs(ref).max()
+    assert rel_err(got, ref) <= 1e-9
+    # the grid's outer nodes lie within q = 1.5e-3 of the band edge, where
+    # the 2/(s q) weight of the sum scales a mixed-precision moment error up
+    # ~650x: the inner nodes meet the mixed bar, and the per-site estimate
+    # (whose weight is the grid's largest) covers the error on all of them
+    mixed, est = m.ldos_sites(cheb, sites, bro, gpu.MIXED)
+    assert np.abs(mixed - ref)[:, inner].max() <= 1e-6 * np.abs(ref).max()
+    for k in range(len(sites)):
+        assert rel_err(mixed[k], ref[k]) <= est[k], k
     # Gauss-Chebyshev quadrature: the integral of the LDOS (mu_0 = 1) is
     # sum_e rho(E_e) (pi s / E) q_e
-    q = np.sqrt(1 - (cheb.energies / s) ** 2)
     total = got @ (np.pi * s / 1024 * q)
     assert np.allclose(total, 1.0, rtol=0, atol=1e-10)  # exact for degree < 2E

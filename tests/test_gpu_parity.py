@@ -290,6 +290,65 @@ def test_every_mixed_config_same_result(gpu, B):
         assert rel_err(out, fp64) <= 1e-6, (t, v, mb)
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("B", [32, 64, 128])
+def test_row_pair_steps_on_ragged_rows(gpu, B):
+    """The row-pair form of the tile-staged complex step (two adjacent rows
+    per thread group over the merge of their column lists) on a random
+    complex Hermitian matrix with an odd row count (the last pair has one
+    row), empty rows, rows of up to 13 entries and columns shared by some
+    pairs only:
+    directly gathered moments bit for bit against the library's default
+    step, and the same doubling LDOS up to the grouping of the dot-product
+    sums."""
+    rng = np.random.default_rng(B)
+    N = 301
+    A = {}
+    for i in range(N):
+        for j in rng.choice(N, size=int(rng.integers(0, 6)), replace=False):
+            v = complex(rng.standard_normal(), rng.standard_normal())
+            A[(i, int(j))] = A.get((i, int(j)), 0) + v
+            A[(int(j), i)] = A.get((int(j), i), 0) + v.conjugate()
+    for i in range(0, N, 3):
+        A[(i, i)] = A.get((i, i), 0) + rng.standard_normal()
+    rows = sorted(A)
+    rowptr = np.zeros(N + 1, dtype=np.uint32)
+    for (i, _) in rows:
+        rowptr[i + 1] += 1
+    rowptr = np.cumsum(rowptr).astype(np.uint32)
+    col = np.array([j for (_, j) in rows], dtype=np.uint32)
+    val = np.array([A[k] for k in rows], dtype=np.complex128)
+    s = 2.0 * np.abs(np.linalg.eigvalsh(_dense(rowptr, col, val, N))).max() + 1.0
+    M = 48
+    frm = rng.choice(N, size=B, replace=False).astype(np.uint32)
+    ref, _ = gpu.Matrix.from_csr(rowptr, col, val, s).moments_batched(
+        frm, frm, np.arange(B), M, 1e-3, gpu.MIXED)
+    pair = [c for c in gpu.configs_for(B, gpu.MIXED, ldos=False)
+            if c[2] >= 100000 and (c[2] - 100000) // 1000000 >= 100]
+    assert pair
+    for (t, v, mb) in pair:
+        m = gpu.Matrix.from_csr(rowptr, col, val, s)
+        m.set_config(B, gpu.MIXED, t, v, mb, ldos=False)
+        mu, _ = m.moments_batched(frm, frm, np.arange(B), M, 1e-3, gpu.MIXED)
+        assert np.array_equal(mu, ref), (t, v, mb)
+    tab = gpu.Table.create(M, gpu.tbtk_range(-s, s, 64, False, False), s)
+    dref, _ = gpu.Matrix.from_csr(rowptr, col, val, s).ldos_sites(tab, frm, 1e-3, gpu.MIXED)
+    for (t, v, mb) in [c for c in gpu.configs_for(B, gpu.MIXED, ldos=True)
+                       if c[2] >= 100000 and (c[2] - 100000) // 1000000 >= 100]:
+        m = gpu.Matrix.from_csr(rowptr, col, val, s)
+        m.set_config(B, gpu.MIXED, t, v, mb, ldos=True)
+        out, _ = m.ldos_sites(tab, frm, 1e-3, gpu.MIXED)
+        assert rel_err(out, dref) <= 1e-7, (t, v, mb)
+
+
+def _dense(rowptr, col, val, N):
+    d = np.zeros((N, N), dtype=np.complex128)
+    for i in range(N):
+        for k in range(int(rowptr[i]), int(rowptr[i + 1])):
+            d[i, int(col[k])] += val[k]
+    return d
+
+
 def test_real_matrix_detected(gpu):
     """A real Hamiltonian runs the mixed precisions on real vectors; a
     complex one (Rashba spin-orbit) and a forbidding caller keep complex64."""
