@@ -438,7 +438,7 @@ def serving_sub():
     [512, 4096]): served throughput and the latency percentiles."""
     from tbtk_b200 import serve_bench
     a = argparse.Namespace(models=64, budget_gb=120.0, tick=64, tolerance=1e-6, samples=8,
-                           sample_seed=44, fp64_head=32, rate=100.0, duration=3.0, width=16,
+                           sample_seed=44, fp64_head=32, rate=100.0, duration=3.0, width=32,
                            full_width=False)
     r = serve_bench.serve(a)
     st = r["server"]

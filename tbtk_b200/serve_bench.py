@@ -12,8 +12,9 @@ until the last one is done.  Each model gets the lane width of its site
 count rounded up to a power of two, and each width is autotuned first.
 
 serve: a pool of 64 seeded models (square, honeycomb, Rashba; N
-log-uniform in [1e3, 4e6]; 16 lanes each) answering Poisson arrivals at
---rate requests per second for --duration seconds, each request 1-16 sites
+log-uniform in [1e3, 4e6]; 32 lanes each, stepped at the width their busy
+lanes need) answering Poisson arrivals at --rate requests per second for
+--duration seconds, each request 1-16 sites
 with M uniform in [512, 4096].  Reports throughput and the latency
 percentiles of the server's own clock (submit to result).
 
@@ -188,7 +189,7 @@ def main():
     ap.add_argument("--samples", type=int, default=16)
     ap.add_argument("--sample-seed", type=int, default=44,
                     help="seed of the sampled solves checked against the FP64 path")
-    ap.add_argument("--width", type=int, default=16,
+    ap.add_argument("--width", type=int, default=32,
                     help="lanes of every pool model (serve)")
     ap.add_argument("--full-width", action="store_true",
                     help="serve: step every model at its full lane count (no adaptive width)")
