@@ -511,21 +511,30 @@ def ours(args, world, rank, local):
 
         # plain FP64 single-vector path (complex128, one site per recursion):
         # timing on the first sites
-        plain = []
+        plain, plain_out = [], []
         step(kpm.FP64, p.sites[:1])  # warm
         mat.profile()
         for i in range(args.plain_sites):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            step(kpm.FP64, p.sites[i:i + 1])
+            out1, _ = step(kpm.FP64, p.sites[i:i + 1])
             e1.record(stream)
             torch.cuda.synchronize()
             plain.append(e0.elapsed_time(e1))
+            plain_out.append(out1[0])
         plain_rec, _, plain_launches = mat.profile()
-        # FP64 LDOS of every site: the batched FP64 recursion gives each
-        # site's single-vector moments bit for bit
+        # FP64 LDOS of every site in one batched FP64 recursion (the
+        # reference's arithmetic, what TBTK's own API gets by default): it
+        # gives each site's single-vector result bit for bit
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
         ref_all, _ = step(kpm.FP64, p.sites)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        fp64_ms = f0.elapsed_time(f1)
+        fp64_rec, _, fp64_launches = mat.profile()
     errs = [float(np.abs(results[i] - ref_all[i]).max() / np.abs(ref_all[i]).max())
             for i in range(B)]
 
@@ -600,6 +609,20 @@ def ours(args, world, rank, local):
                                        "second (doubling runs step to M/2)"},
         "plain_fp64": {"value": plain_rate, "unit": "LDOS solves/s", "ms_per_solve": plain_ms,
                        "sites": args.plain_sites},
+        "fp64_batched": {
+            "value": B / (fp64_ms / 1e3), "unit": "LDOS solves/s", "ms_per_call": fp64_ms,
+            "sites": B,
+            "step_ms": fp64_rec / max(fp64_launches, 1),
+            "roofline": {"achieved_GBps": step_bytes(p, B, 16) / (fp64_rec / max(fp64_launches, 1)
+                                                                  / 1e3) / 1e9,
+                         "frac": step_bytes(p, B, 16) / (fp64_rec / max(fp64_launches, 1) / 1e3)
+                                 / 1e9 / peak,
+                         "bytes_per_launch": step_bytes(p, B, 16)},
+            "bit_identical_to_single_vector": all(np.array_equal(ref_all[i], plain_out[i])
+                                                  for i in range(len(plain_out))),
+            "note": ("the same sites in one batched FP64 recursion on complex128 vectors, M-1 "
+                     "steps in the reference's operation order (TBTK's default precision through "
+                     "the seam); its LDOS is the reference for ldos_rel_err_vs_fp64")},
         "speedup_vs_plain_fp64": (value / world) / plain_rate if plain_rate else None,
         "speedup_mechanisms": {
             "doubling": (p.M - 1) / (p.M // 2),

@@ -201,6 +201,27 @@ TILED_CPLX = {
 }
 
 
+# Tile-staged FP64 steps on complex128 vectors (kpm_step_tiled with F64):
+# (threads per row, complex values per thread) -> (rows per tile, consumer
+# warps, blocks per SM).  Rows of 16-byte values: B = 16 / 32 / 64 / 128
+# take 256 B / 512 B / 1 KB / 2 KB per row.
+TILED_FP64 = {
+    (16, 1): [(32, 8, 2), (64, 16, 1)],
+    (32, 1): [(32, 8, 2), (16, 8, 2), (64, 16, 1)],
+    (16, 2): [(32, 8, 2), (16, 8, 2)],
+    (32, 2): [(16, 16, 1), (16, 8, 1), (8, 8, 2), (8, 8, 1)],
+    (16, 4): [(16, 8, 1), (8, 8, 2)],
+    (32, 4): [(8, 8, 1), (8, 16, 1)],
+    (16, 8): [(8, 8, 1)],
+}
+
+
+def tiled_fp64_lines(cls):
+    return [f"    TBTKKPM_TILED_ENTRY_F64({cls}, {t}, {p}, {r}, {cw}, {bps}),"
+            for (t, p), variants in TILED_FP64.items() for (r, cw, bps) in variants
+            if (cw * 32) % t == 0]
+
+
 def tiled_lines(cls, cplx, dots):
     shapes = TILED_CPLX if cplx else TILED_REAL
     out = []
@@ -257,6 +278,8 @@ def main():
             for (s, wpb) in BULK_VARIANTS:
                 if bulk_smem(V, p, s, wpb, dots) <= SMEM_LIMIT:
                     lines.append(f"    TBTKKPM_BULK_ENTRY({cls}, {V}, {AR}, {p}, {dots}, {s}, {wpb}),")
+        if V == "double2":
+            lines += tiled_fp64_lines(cls)
         if V == "float2":
             lines += tiled_lines(cls, True, dots)
             for p in ASYNC_VPT:

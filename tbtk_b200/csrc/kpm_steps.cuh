@@ -188,12 +188,13 @@ inline int tiled_rows(int v) { return ((v - kTiledVariant) % 1000000) / 1000; }
 inline bool tiled_pairs(int v) { return (v - kTiledVariant) / 1000000 >= 100; }
 inline int tiled_bps(int v) { return v % 10; }
 
-template <bool CPLX, int TPR, int VPT, int R, int CW, int BPS, bool FIRST, bool DOTS, int CV>
+template <bool CPLX, int TPR, int VPT, int R, int CW, int BPS, bool FIRST, bool DOTS, int CV,
+          bool F64 = false>
 void launch_tiled(cudaStream_t st, int device, unsigned max_grid, const StepArgs &a,
                   unsigned *grid) {
-  using E = typename TiledTypes<CPLX>::E;
-  using Val = typename TiledTypes<CPLX>::Val;
-  auto kern = kpm_step_tiled<CPLX, TPR, VPT, R, CW, BPS, FIRST, DOTS, CV>;
+  using E = typename TiledTypes<CPLX, F64>::E;
+  using Val = typename TiledTypes<CPLX, F64>::Val;
+  auto kern = kpm_step_tiled<CPLX, TPR, VPT, R, CW, BPS, FIRST, DOTS, CV, F64>;
   *grid = 0;
   if (!a.plan || a.plan->R != (uint32_t)R || a.plan->pairs != (CV >= 100 ? 1u : 0u)) return;
   const TilePlan &p = *a.plan;
@@ -222,6 +223,11 @@ void launch_tiled(cudaStream_t st, int device, unsigned max_grid, const StepArgs
   {CLS, T, P, kTiledVariant + 1000000 * CV + 1000 * R + 10 * CW + BPS,               \
    &launch_tiled<CPLX, T, P, R, CW, BPS, true, D, CV>,                               \
    &launch_tiled<CPLX, T, P, R, CW, BPS, false, D, CV>}
+// the FP64 recursion on complex128 vectors (kClassFP64)
+#define TBTKKPM_TILED_ENTRY_F64(CLS, T, P, R, CW, BPS)                              \
+  {CLS, T, P, kTiledVariant + 1000 * R + 10 * CW + BPS,                              \
+   &launch_tiled<true, T, P, R, CW, BPS, true, false, 0, true>,                      \
+   &launch_tiled<true, T, P, R, CW, BPS, false, false, 0, true>}
 
 extern const StepEntry kStepsFP64[];
 extern const int kNumStepsFP64;

@@ -25,7 +25,8 @@
 // 2H/s.  Entries keep the CSR order of their row (ascending columns), so each
 // element sees the same FMAs in the same order as kpm_step_real /
 // kpm_step<float2, Wide64>: stored vectors and directly gathered moments are
-// bit-identical to theirs.
+// bit-identical to theirs.  The FP64 form stages complex128 rows and keeps
+// the reference's rounded products and sums (as kpm_step<double2, Exact64>).
 //
 // Only non-multicast bulk copies are issued.  Every mbarrier wait is
 // bounded (`wait_limit` polls; 0 gives up at once); a wait that runs out
@@ -99,14 +100,19 @@ __device__ __forceinline__ double f2d_scaled(float x) {
 }
 constexpr double kWideUp = 0x1p896;
 
-// Element type of a vector row and value type of an entry.
-template <bool CPLX> struct TiledTypes;
-template <> struct TiledTypes<false> {
+// Element type of a vector row and value type of an entry (F64: the
+// complex128 vectors of the FP64 recursion).
+template <bool CPLX, bool F64 = false> struct TiledTypes;
+template <> struct TiledTypes<false, false> {
   using E = float;
   using Val = double;
 };
-template <> struct TiledTypes<true> {
+template <> struct TiledTypes<true, false> {
   using E = float2;
+  using Val = double2;
+};
+template <> struct TiledTypes<true, true> {
+  using E = double2;
   using Val = double2;
 };
 
@@ -125,15 +131,24 @@ template <> struct TiledTypes<true> {
 // share most columns), adding it into each row that has the column; each
 // row still sees its own entries in CSR order.  Every choice gives the same
 // stored vectors.
-template <bool CPLX, int TPR, int VPT, int R, int CW, int BPS, bool FIRST, bool DOTS, int CV = 0>
+//
+// F64 (complex, CV 0, no dot products): the FP64 recursion on complex128
+// vectors in the reference's operation order (Exact64: each row's sum starts
+// at -j_{n-1} and adds every complex product, each rounded once, in CSR
+// order, Lib/src/Solver/ChebyshevExpander.cpp:171-186), the same as
+// kpm_step<double2, Exact64>: moments bit-identical to the reference's.
+template <bool CPLX, int TPR, int VPT, int R, int CW, int BPS, bool FIRST, bool DOTS, int CV = 0,
+          bool F64 = false>
 __global__ void __launch_bounds__(32 * (CW + 1), BPS)
 kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
-               const typename TiledTypes<CPLX>::E *__restrict__ x,
-               typename TiledTypes<CPLX>::E *__restrict__ y, Targets tg, uint32_t n_out,
+               const typename TiledTypes<CPLX, F64>::E *__restrict__ x,
+               typename TiledTypes<CPLX, F64>::E *__restrict__ y, Targets tg, uint32_t n_out,
                double2 *__restrict__ dots, int *err, uint32_t wait_limit) {
-  using E = typename TiledTypes<CPLX>::E;
-  using Val = typename TiledTypes<CPLX>::Val;
-  using Pk = typename std::conditional<CPLX, Pack<float2, TPR, VPT>, RPack<TPR, VPT>>::type;
+  using E = typename TiledTypes<CPLX, F64>::E;
+  using Val = typename TiledTypes<CPLX, F64>::Val;
+  using Pk = typename std::conditional<
+      CPLX, typename std::conditional<F64, Pack<double2, TPR, VPT>, Pack<float2, TPR, VPT>>::type,
+      RPack<TPR, VPT>>::type;
   using L = typename Pk::L;
   constexpr int NL = Pk::NL;
   constexpr bool PAIR = CV >= 100;
@@ -144,6 +159,7 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
   constexpr int PASSES = ((int)EW + RPP - 1) / RPP;
   static_assert(CW * 32 % TPR == 0, "a row group must divide the consumer threads");
   static_assert(!PAIR || (CPLX && R >= 16), "row pairs: complex vectors, 16-byte slot chunks");
+  static_assert(!F64 || (CPLX && CV == 0 && !DOTS), "FP64 steps: complex values, every moment direct");
   extern __shared__ __align__(128) unsigned char tsm[];
   uint64_t *full = reinterpret_cast<uint64_t *>(tsm);
   uint64_t *empty = full + kTiledMaxStages;
@@ -255,6 +271,46 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
       const E *prev = reinterpret_cast<const E *>(st + LY.off_prev);
 #pragma unroll
       for (int p = 0; p < PASSES; p++) {
+        if constexpr (F64) {
+          const uint32_t lr = grp + p * RPP;
+          if (lr >= Rt) continue;
+          const uint32_t row = r0 + lr;
+          double2 acc[VPT];
+          if constexpr (FIRST) {
+#pragma unroll
+            for (int j = 0; j < VPT; j++) acc[j] = make_double2(0.0, 0.0);
+          } else {
+            L yv[NL];
+            Pk::load_rw(reinterpret_cast<const double2 *>(prev) + (size_t)lr * Bp, sub, yv);
+#pragma unroll
+            for (int j = 0; j < VPT; j++) {
+              const double2 f = Pk::get(yv, j);
+              acc[j] = make_double2(-f.x, -f.y);
+            }
+          }
+          for (uint32_t k = 0; k < w; k++) {
+            const uint16_t sl = slots[k * R + lr];
+            if (sl == kSlotPad) break;
+            double2 v = vals[k * R + lr];
+            if constexpr (FIRST) v = make_double2(v.x * 0.5, v.y * 0.5);
+            L xr[NL];
+            Pk::load_rw(reinterpret_cast<const double2 *>(xs) + (size_t)sl * Bp, sub, xr);
+#pragma unroll
+            for (int j = 0; j < VPT; j++) acc[j] = cmac<true>(acc[j], v, Pk::get(xr, j));
+          }
+          if ((bw[p] >> (row & 31)) & 1u) {
+            for (uint32_t q = target_first(tg, row); q < tg.count && __ldg(tg.row + q) == row; q++) {
+              const int jt = Pk::slot_of(sub, __ldg(tg.col + q));
+              if (jt >= 0) {
+#pragma unroll
+                for (int j = 0; j < VPT; j++)
+                  if (j == jt) tg.mu[(uint64_t)__ldg(tg.out + q) * tg.ld + n_out] = acc[j];
+              }
+            }
+          }
+          Pk::store(reinterpret_cast<double2 *>(y) + (uint64_t)row * Bp, sub, acc);
+          continue;
+        }
         if constexpr (PAIR) {
           const uint32_t u = grp + p * RPP, la = 2 * u;
           if (la >= Rt) continue;
@@ -347,7 +403,7 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
         const uint32_t lr = grp + p * RPP;
         if (lr >= Rt) continue;
         const uint32_t row = r0 + lr;
-        if constexpr (CPLX) {
+        if constexpr (CPLX && !F64) {
           double2 acc[VPT];
           if constexpr (FIRST) {
 #pragma unroll
@@ -410,7 +466,7 @@ kpm_step_tiled(TilePlan P, TiledLayout LY, uint32_t Bp,
               d_np[j] += PA ? f2d_scaled(np) : (double)np;
             }
           }
-        } else {
+        } else if constexpr (!CPLX) {
           double acc[VPT];
           if constexpr (FIRST) {
 #pragma unroll
