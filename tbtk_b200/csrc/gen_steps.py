@@ -206,6 +206,10 @@ TILED_CPLX = {
 # warps, blocks per SM).  Rows of 16-byte values: B = 16 / 32 / 64 / 128
 # take 256 B / 512 B / 1 KB / 2 KB per row.
 TILED_FP64 = {
+    (1, 1): [(64, 2, 8), (64, 2, 6), (32, 1, 8), (64, 2, 4)],
+    (2, 1): [(64, 4, 6), (64, 4, 4), (32, 2, 8)],
+    (4, 1): [(64, 8, 4), (64, 8, 2), (32, 4, 6)],
+    (8, 1): [(64, 16, 2), (32, 8, 4), (64, 8, 3)],
     (16, 1): [(32, 8, 2), (64, 16, 1)],
     (32, 1): [(32, 8, 2), (16, 8, 2), (64, 16, 1)],
     (16, 2): [(32, 8, 2), (16, 8, 2)],

@@ -110,11 +110,23 @@ constexpr int tiled(int cv, int rows, int cw, int bps) {
 // (directly gathered moments) the real B = 64 step takes 1.29 ms (0.84 of
 // the measured copy bandwidth).  A matrix whose tiles do not fit the ring
 // falls back to register_shape_for.
-Shape shape_for(int precision, uint32_t B, bool real = false, bool dots = false) {
+// N: the matrix's rows (0: large).
+Shape shape_for(int precision, uint32_t B, bool real = false, bool dots = false, uint32_t N = 0) {
   if (!is_mixed(precision)) {
     // FP64 (complex128 vectors) on the 2048^2 lattice, ms per step for
-    // B = 32 / 64 / 128: 2.12 / 4.12 / 8.32 tile-staged (0.96-0.99 of the
-    // measured copy bandwidth) against 5.28 / 6.79 / 18.9 register-staged
+    // B = 1 / 2 / 4 / 8 / 16: 0.171 / 0.224 / 0.346 / 0.669 / 1.38
+    // tile-staged against 0.278 / 0.504 / 0.924 / 2.49 / 4.50
+    // register-staged, and for B = 32 / 64 / 128: 2.12 / 4.12 / 8.32
+    // (0.96-0.99 of the measured copy bandwidth) against 5.28 / 6.79 / 18.9.
+    // Below 2^17 rows a single source is faster register-staged (4.4 against
+    // 5.2 us per step at 32k rows); at 32 sources tile staging is as fast or
+    // faster from 2k rows on.
+    const bool big = N == 0 || N > (1u << 17);
+    if (B <= 1 && big) return {1, 1, tiled(0, 64, 2, 8)};
+    if (B == 2 && big) return {2, 1, tiled(0, 64, 4, 6)};
+    if (B > 2 && B <= 4 && big) return {4, 1, tiled(0, 64, 8, 4)};
+    if (B > 4 && B <= 8 && big) return {8, 1, tiled(0, 64, 16, 2)};
+    if (B > 8 && B <= 16 && big) return {16, 1, tiled(0, 32, 8, 2)};
     if (B > 16 && B <= 32) return {16, 2, tiled(0, 16, 8, 2)};
     if (B > 32 && B <= 64) return {16, 4, tiled(0, 8, 8, 2)};
     if (B > 64) return {32, 4, tiled(0, 8, 16, 1)};
@@ -191,7 +203,7 @@ const StepEntry *pick_step(const tbtkkpm_matrix *m, int precision, bool dots, ui
   if (force) return force;
   const bool real = real_mode(m, precision);
   const int cls = step_class(precision, dots, real);
-  const Shape s = shape_for(precision, B, real, dots);
+  const Shape s = shape_for(precision, B, real, dots, m->N);
   auto it = m->tuned.find(tune_key(cls, s.bp()));
   if (it != m->tuned.end()) {
     const StepEntry *e = find_step(cls, it->second[0], it->second[1], it->second[2]);

@@ -255,6 +255,26 @@ def test_every_config_same_result(gpu, oracle):
         m.set_config(40, gpu.MIXED, 32, 1, 2)
 
 
+@pytest.mark.parametrize("B", [1, 2, 4, 8, 16, 32])
+def test_every_fp64_config_small_batches(gpu, oracle, B):
+    """Every compiled FP64 configuration of small batches (register-staged,
+    per-warp rings, tile-staged) gives the reference's moments bit for bit,
+    on a lattice whose row count is not a multiple of any tile height."""
+    lat = L.square(13, 7, t=1.0, J=0.5, W=2.0, alpha=0.25, periodic=True, seed=B)
+    rowptr, col, val = lat.csr()
+    s, M = 12.0, 32
+    frm = L.random_sites(lat, B, seed=5)
+    refs = [oracle.moments(rowptr, col, val, s, M, int(f), [int(f)])[0] for f in frm]
+    configs = gpu.configs_for(B, gpu.FP64)
+    assert any(mb >= 100000 for (_, _, mb) in configs)
+    for (t, v, mb) in configs:
+        m = gpu.Matrix.from_csr(rowptr, col, val, s)
+        m.set_config(B, gpu.FP64, t, v, mb, ldos=False)
+        mu, _ = m.moments_batched(frm, frm, np.arange(B), M, 0.0, gpu.FP64)
+        for b in range(B):
+            assert np.array_equal(mu[b], refs[b]), (t, v, mb, b)
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("B", [20, 40, 100])
 def test_every_mixed_config_same_result(gpu, B):
