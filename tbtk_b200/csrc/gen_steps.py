@@ -178,6 +178,10 @@ TILED_REAL = {
     (16, 8): _variants([(32, 8, 2), (64, 16, 1), (16, 8, 2)], [0, 51]),
     (32, 4): _variants([(32, 8, 2), (64, 16, 1), (16, 8, 2)], [0, 51]),
     (32, 8): _variants([(16, 8, 2), (32, 16, 1), (16, 16, 1)], [0, 51]),
+    # 4-8 sources: small blocks, several per SM
+    (1, 4): _variants([(64, 2, 8), (64, 2, 6)], [0, 51]),
+    (1, 8): _variants([(64, 2, 8), (64, 2, 6)], [0, 51]),
+    (2, 4): _variants([(64, 4, 6), (64, 4, 4)], [0, 51]),
 }
 # CV >= 100: the row-pair form (two adjacent rows per thread group, each
 # gathered row widened once for both; 16-row tiles and up).  On the 1024^2
@@ -198,6 +202,12 @@ TILED_CPLX = {
     # (the unpaired 64 x 2 shape takes 2.72 ms)
     (64, 2): _variants([(16, 16, 1)], [100, 151]),
     (8, 2): _variants([(32, 8, 2), (16, 8, 2)], [0, 60]),
+    # 2-8 sources: small blocks, several per SM
+    (1, 2): _variants([(64, 2, 8), (64, 2, 6)], [0, 60]),
+    (1, 4): _variants([(64, 2, 8)], [0, 60]),
+    (2, 2): _variants([(64, 4, 6)], [0, 60]),
+    (2, 4): _variants([(64, 4, 4), (64, 4, 6)], [0, 60]),
+    (4, 2): _variants([(64, 8, 4)], [0, 60]),
 }
 
 

@@ -276,7 +276,7 @@ def test_every_fp64_config_small_batches(gpu, oracle, B):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("B", [20, 40, 100])
+@pytest.mark.parametrize("B", [4, 8, 20, 40, 100])
 def test_every_mixed_config_same_result(gpu, B):
     """Every compiled complex64 step configuration (register-staged, bulk
     ring, cp.async ring) takes the same per-element arithmetic in the same
@@ -381,7 +381,7 @@ def test_real_matrix_detected(gpu):
     assert gpu.Matrix.from_csr(*cplx.csr(), 12.0).real() == (False, False)
 
 
-@pytest.mark.parametrize("B", [1, 20, 64, 200])
+@pytest.mark.parametrize("B", [1, 4, 8, 20, 64, 200])
 def test_real_vectors_match_complex_vectors(gpu, B):
     """Real float vectors give the complex64 path's values: directly gathered
     moments bit for bit for every compiled real configuration; doubling LDOS
