@@ -132,6 +132,20 @@ Shape shape_for(int precision, uint32_t B, bool real = false, bool dots = false,
     if (B > 64) return {32, 4, tiled(0, 8, 16, 1)};
   }
   if (is_mixed(precision)) {
+    // 2-8 sources (rows of 16-64 bytes): small tile-staged blocks, several
+    // per SM; doubling LDOS, ms per step for real B = 4 / 8 on the 2048^2
+    // lattice 0.167 / 0.237 against 0.347 / 0.505 register-staged (0.0146 /
+    // 0.0165 against 0.0186 / 0.0234 at 131k rows), complex B = 2 / 4 / 8 on
+    // the 1024^2 Rashba lattice 0.079 / 0.099 / 0.156 against 0.138 / 0.170
+    // / 0.383
+    if (real) {
+      if (B > 2 && B <= 4) return {1, 4, tiled(0, 64, 2, 8)};
+      if (B > 4 && B <= 8) return {1, 8, tiled(0, 64, 2, 8)};
+    } else {
+      if (B == 2) return {1, 2, tiled(0, 64, 2, 6)};
+      if (B > 2 && B <= 4) return {2, 2, tiled(0, 64, 4, 6)};
+      if (B > 4 && B <= 8) return {2, 4, tiled(0, 64, 4, 4)};
+    }
     if (real) {
       if (B > 16 && B <= 32) return {8, 4, tiled(0, 64, 16, 1)};
       if (B > 32 && B <= 64) return {8, 8, tiled(51, 64, 16, 1)};
