@@ -173,7 +173,7 @@ def _variants(bases, cvs):
 TILED_REAL = {
     (8, 8): _variants([(32, 8, 2), (64, 16, 1), (32, 4, 3), (16, 4, 4)], [0, 30, 50, 51]),
     (16, 4): _variants([(32, 8, 2), (64, 16, 1)], [0, 51]),
-    (4, 4): _variants([(32, 8, 2), (64, 16, 1), (32, 4, 2)], [0, 51]),
+    (4, 4): _variants([(32, 8, 2), (64, 16, 1), (32, 4, 2), (64, 8, 3)], [0, 51]),
     (8, 4): _variants([(32, 8, 2), (64, 16, 1), (32, 4, 2)], [0, 51]),
     (16, 8): _variants([(32, 8, 2), (64, 16, 1), (16, 8, 2)], [0, 51]),
     (32, 4): _variants([(32, 8, 2), (64, 16, 1), (16, 8, 2)], [0, 51]),
@@ -182,6 +182,7 @@ TILED_REAL = {
     (1, 4): _variants([(64, 2, 8), (64, 2, 6)], [0, 51]),
     (1, 8): _variants([(64, 2, 8), (64, 2, 6)], [0, 51]),
     (2, 4): _variants([(64, 4, 6), (64, 4, 4)], [0, 51]),
+    (2, 8): _variants([(64, 4, 4), (64, 4, 6)], [0, 51]),
 }
 # CV >= 100: the row-pair form (two adjacent rows per thread group, each
 # gathered row widened once for both; 16-row tiles and up).  On the 1024^2

@@ -381,7 +381,7 @@ def test_real_matrix_detected(gpu):
     assert gpu.Matrix.from_csr(*cplx.csr(), 12.0).real() == (False, False)
 
 
-@pytest.mark.parametrize("B", [1, 4, 8, 20, 64, 200])
+@pytest.mark.parametrize("B", [1, 4, 8, 16, 20, 64, 200])
 def test_real_vectors_match_complex_vectors(gpu, B):
     """Real float vectors give the complex64 path's values: directly gathered
     moments bit for bit for every compiled real configuration; doubling LDOS
