@@ -200,7 +200,8 @@ TILED_CPLX = {
     (8, 4): _variants([(16, 8, 2), (32, 8, 1), (32, 8, 2)], [0, 60]) + _variants([(16, 4, 2)], [100]),
     # 64 threads per row pair, 2 values each: the pair form at the 16-warp
     # occupancy of the unpaired (32, 4) step; 2.19 ms against 2.14 ms there
-    # (the unpaired 64 x 2 shape takes 2.72 ms)
+    # (the unpaired 64 x 2 shape takes 2.72 ms; every merged gather widened
+    # on the integer pipe, CV 190 / 191, 2.23 / 2.24 ms)
     (64, 2): _variants([(16, 16, 1)], [100, 151]),
     (8, 2): _variants([(32, 8, 2), (16, 8, 2)], [0, 60]),
     # 2-8 sources: small blocks, several per SM
