@@ -15,11 +15,13 @@ max over ranks of the device time).  Beside it the line carries the plain
 FP64 single-vector path (one site per recursion, complex128, bit-exact with
 the reference) on the same matrix, the LDOS error of the mixed result of
 every site against the FP64 recursion (batched FP64, bit-identical per site
-to the single-vector path), the speed-up split into its mechanisms, the
-roofline of the recursion step, the CPU baseline, and three sub-results:
+to the single-vector path, timed as ``fp64_batched``), the speed-up split
+into its mechanisms, the roofline of the recursion step, the CPU baseline,
+and three sub-results:
 the 1024x1024 Rashba lattice (complex Hamiltonian, 256 sites, M = 2048),
 the LDOS server on the 1000-model uneven batch at tolerance 1e-6, and the
-server under Poisson arrivals (100 requests/s offered for 3 s).
+server under Poisson arrivals (100 requests/s offered for 3 s, 32 lanes
+per model).
 
 Inputs are larger than L2 (13.8 GB of matrix and vectors per recursion step
 against 126 MB of L2), so no flush is needed between steps.
