@@ -138,11 +138,14 @@ Shape shape_for(int precision, uint32_t B, bool real = false, bool dots = false,
     // 0.0165 against 0.0186 / 0.0234 at 131k rows), complex B = 2 / 4 / 8 on
     // the 1024^2 Rashba lattice 0.079 / 0.099 / 0.156 against 0.138 / 0.170
     // / 0.383; real B = 16: 0.408 against 0.836 (0.0207 against 0.0267 at
-    // 131k rows)
+    // 131k rows).  At 2k rows real B = 8 / 16 steps are faster with a
+    // register-staged thread per row (10.3 against 12.4 / 13.4 us; about
+    // even at 32k rows).
+    const bool tiny = N != 0 && N <= (1u << 14);
     if (real) {
       if (B > 2 && B <= 4) return {1, 4, tiled(0, 64, 2, 8)};
-      if (B > 4 && B <= 8) return {1, 8, tiled(0, 64, 2, 8)};
-      if (B > 8 && B <= 16) return {2, 8, tiled(51, 64, 4, 4)};
+      if (B > 4 && B <= 8 && !tiny) return {1, 8, tiled(0, 64, 2, 8)};
+      if (B > 8 && B <= 16 && !tiny) return {2, 8, tiled(51, 64, 4, 4)};
     } else {
       if (B == 2) return {1, 2, tiled(0, 64, 2, 6)};
       if (B > 2 && B <= 4) return {2, 2, tiled(0, 64, 4, 6)};
