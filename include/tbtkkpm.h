@@ -568,7 +568,9 @@ TBTKKPM_API int tbtkkpm_server_set_graphs(tbtkkpm_server *s, int enable);
  * so a step moves the vectors of those lanes only, not of all `width`
  * lanes; a request takes the lowest free lanes, and at a step boundary
  * where the width changes the model's two vector buffers are restrided in
- * place (TBTKKPM_STAT_RELAYOUTS counts these).  enable = 0: every model
+ * place (TBTKKPM_STAT_RELAYOUTS counts these).  A step runs the
+ * configuration of the width it steps at (tbtkkpm_server_set_config and
+ * tbtkkpm_server_autotune set one per width).  enable = 0: every model
  * steps at its full lane count.  Results do not depend on it.  (No
  * reference counterpart.) */
 TBTKKPM_API int tbtkkpm_server_set_adaptive_width(tbtkkpm_server *s, int enable);
